@@ -1,0 +1,437 @@
+"""Benchmark: the two-site effective-Hamiltonian matvec of the SU(2) Heisenberg chain.
+
+Workload (the configuration the headline metric is quoted on): the Heff matvec that
+Lanczos applies at a mid-chain bond of the spin-1/2 SU(2) Heisenberg chain (L = 64) with
+a maximum multiplet bond dimension of 256 -- 256 multiplets per bond over half-integer
+bond spins 2j = 1..17 -- and the S.S MPO bond of three multiplets (2j = 0, 0, 2).  The
+inputs are seeded synthetic tensors of exactly those structures (random FP64 blocks;
+the cost of a matvec depends on the structure only).  A step is one ``heff2``
+application: four pairwise contractions, each a pack gather, a grouped FP64 GEMM and an
+unpack gather, plus the three named-wire bends.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tenet|reference]
+
+``value`` is matvec TFLOP/s (algorithmic GEMM flops of the lowering, sum of 2 M K N over
+every coupled-sector product, divided by device time), inputs resident in HBM, L2
+flushed between timed steps.  ``e2e`` is the same metric through the public API with the
+two-site tensor copied from pinned host memory and the result copied back inside the
+timed region.  ``--impl reference`` times the oracle port of the reference's NumPy path
+on the host cores instead.  With ``--gpus N`` under torchrun every rank runs an
+independent replica (the path does not shard), and the job value is the sum of all
+ranks' matvecs over the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "tenet-py_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+METRIC = "Heff matvec TFLOP/s (SU(2) Heisenberg two-site, FP64)"
+# multiplets per bond sector, half-integer bond spins 2j = 1, 3, ..., 17 (sum 256)
+BOND = {1: 60, 3: 56, 5: 46, 7: 36, 9: 25, 11: 16, 13: 10, 15: 5, 17: 2}
+MPO = {0: 2, 2: 1}
+PHYS = {1: 1}
+
+
+def build_workload(seed: int = 0):
+    """(fl, w1, w2, fr, aa) as tenet tensors with the golden-vector leg conventions of the
+    reference's ``Env`` (``network/env.py``): F[(n-1,n)] = (ket IN, mpo OUT*, bra OUT),
+    F[(n+2,n+1)] = (ket OUT, mpo IN*, bra IN), W = (x IN*, P OUT, p IN, m OUT*)."""
+    import tenet
+    from tenet.structure import IN, OUT, GradedSpace, Leg
+    from tenet.symmetry import SU2
+
+    def sp(d):
+        return GradedSpace.new(SU2, {SU2.sector(a): m for a, m in d.items()})
+
+    B, M, P = sp(BOND), sp(MPO), sp(PHYS)
+    rnd = tenet.SymmetricTensor.random
+    fl = rnd((Leg(B, IN), Leg(M, OUT, True), Leg(B, OUT)), seed=seed)
+    fr = rnd((Leg(B, OUT), Leg(M, IN, True), Leg(B, IN)), seed=seed + 1)
+    w = (Leg(M, IN, True), Leg(P, OUT), Leg(P, IN), Leg(M, OUT, True))
+    w1, w2 = rnd(w, seed=seed + 2), rnd(w, seed=seed + 3)
+    aa = rnd((Leg(B, OUT), Leg(P, OUT), Leg(P, OUT), Leg(B, IN)), seed=seed + 4)
+    return fl, w1, w2, fr, aa
+
+
+def workload_structures():
+    """The five structures of ``build_workload`` (host only, no device needed)."""
+    from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure
+    from tenet.symmetry import SU2
+
+    def sp(d):
+        return GradedSpace.new(SU2, {SU2.sector(a): m for a, m in d.items()})
+
+    B, M, P = sp(BOND), sp(MPO), sp(PHYS)
+    w = TensorStructure((Leg(M, IN, True), Leg(P, OUT), Leg(P, IN), Leg(M, OUT, True)))
+    return (TensorStructure((Leg(B, IN), Leg(M, OUT, True), Leg(B, OUT))), w, w,
+            TensorStructure((Leg(B, OUT), Leg(M, IN, True), Leg(B, IN))),
+            TensorStructure((Leg(B, OUT), Leg(P, OUT), Leg(P, OUT), Leg(B, IN))))
+
+
+def oracle_workload(seed: int = 0):
+    """The same tensors for the oracle: same structures, same seeded draws."""
+    import oracle.tenet_oracle as O
+
+    out = []
+    for k, s in enumerate(workload_structures()):
+        legs = tuple(O.Leg(tuple((a.two_j, m) for a, m in leg.space.sectors),
+                           O.OUT if leg.side.value == "out" else O.IN, bool(leg.dual))
+                     for leg in s.legs)
+        out.append(O.random(O.Structure(O.SU2, legs), seed + (0, 2, 3, 1, 4)[k]))
+    return out
+
+
+def heff2_flops() -> int:
+    """Algorithmic flops of one heff2 from the plans alone (host, no device): the sum of
+    2 M K N over every coupled-sector product of the four contractions."""
+    from tenet import ops
+    from tenet.plan import repartition_plan, transpose_plan
+    from tenet.structure import OUT
+
+    def einsum_s(eq, sa, sb):
+        lhs, out = eq.split("->")
+        ta, tb = lhs.split(",")
+        shared = [x for x in ta if x in tb]
+        axes = (tuple(ta.index(x) for x in shared), tuple(tb.index(x) for x in shared))
+        ex = ops.contraction_exec(sa, sb, axes)
+        free = [x for x in ta if x not in shared] + [x for x in tb if x not in shared]
+        return transpose_plan(ex.out, tuple(free.index(x) for x in out))[0], ex.flops
+
+    def composed_s(eq, sa, sb, bend):
+        lhs, out = eq.split("->")
+        ta, tb = lhs.split(",")
+
+        def bent(s, term):
+            outs = tuple(i for i, ch in enumerate(term) if (s.legs[i].side is OUT) != (ch in bend))
+            ins = tuple(i for i in range(len(term)) if i not in outs)
+            return repartition_plan(s, outs, ins)[0], "".join(term[i] for i in (*outs, *ins))
+
+        sa, ta = bent(sa, ta)
+        sb, tb = bent(sb, tb)
+        return einsum_s(f"{ta},{tb}->{out}", sa, sb)
+
+    fl, w1, w2, fr, aa = workload_structures()
+    t, f0 = einsum_s("apqr,rys->apqys", aa, fr)
+    t, f1 = composed_s("apqys,mQqy->apQms", t, w2, "q")
+    t, f2 = composed_s("apQms,xPpm->aPQxs", t, w1, "p")
+    _, f3 = composed_s("aPQxs,axB->BPQs", t, fl, "a")
+    return f0 + f1 + f2 + f3
+
+
+def launches_per_matvec(tensors) -> int:
+    from tenet import _exec, network
+
+    log = _exec.LaunchLog(timed=False)
+    with log:
+        network.heff2(*tensors)
+    return log.count
+
+
+class Clocks:
+    """Samples nvidia-smi during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [x for x in out.splitlines() if x.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            f = [x.strip() for x in line.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, f[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs"), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def measure_dgemm_peak(torch) -> float:
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s), the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(flops: int, budget_s: float = 20.0) -> dict:
+    """The oracle's NumPy path (the reference's algorithm) on this host's cores."""
+    import oracle.tenet_oracle as O
+
+    fl, w1, w2, fr, aa = oracle_workload()
+    O.heff2(fl, w1, w2, fr, aa)  # warm the plan caches, as the reference's own bench does
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while time.perf_counter() < t_end and len(times) < 5:
+        t0 = time.perf_counter()
+        O.heff2(fl, w1, w2, fr, aa)
+        times.append(time.perf_counter() - t0)
+    med = float(np.median(times))
+    try:
+        from threadpoolctl import threadpool_info
+
+        cores = max((i.get("num_threads", 1) for i in threadpool_info()), default=1)
+    except Exception:
+        cores = os.cpu_count() or 1
+    return {"value": flops / med / 1e12, "unit": "TFLOP/s", "cores": int(cores), "kind": "port",
+            "sample": f"{len(times)} oracle heff2 matvecs on the same structures (median "
+                      f"{med * 1e3:.1f} ms each), plan caches warm",
+            "ms_per_matvec": med * 1e3}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    flops = heff2_flops()
+    import oracle.tenet_oracle as O
+
+    ot = oracle_workload()
+    for _ in range(max(1, min(args.warmup, 1))):
+        O.heff2(*ot)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.heff2(*ot)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = flops * len(times) / total / 1e12
+    try:
+        from threadpoolctl import threadpool_info
+
+        cores = max((i.get("num_threads", 1) for i in threadpool_info()), default=1)
+    except Exception:
+        cores = os.cpu_count() or 1
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / len(times) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "su2-heisenberg-heff2-L64-mid-bond-256-multiplets",
+                   "bond_multiplets": BOND, "mpo_multiplets": MPO},
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": int(cores), "kind": "port",
+                         "sample": f"{len(times)} oracle heff2 matvecs, one per step"},
+        "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_tenet(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    from tenet import _exec, _lib, network
+
+    tensors = build_workload(seed=rank)
+    fl, w1, w2, fr, aa = tensors
+    flops = heff2_flops()
+    launches_per_step = launches_per_matvec(tensors)
+
+    def step(x):
+        return network.heff2(fl, w1, w2, fr, x)
+
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        step(aa)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    # timed region: device time of each step, L2 flushed between steps (not timed)
+    log = _exec.LaunchLog(timed=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        with log:
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                ev[k][0].record()
+                step(aa)
+                ev[k][1].record()
+        torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = flops * args.steps * world / (ms * 1e-3) / 1e12
+    kernels = log.summary()
+
+    # end to end through the public API with host buffers
+    host_in = aa.arena.detach().cpu().pin_memory()
+    out_size = aa.arena.numel()
+    host_out = torch.empty(out_size, dtype=torch.float64).pin_memory()
+    from tenet.tensor import SymmetricTensor
+
+    def e2e_step():
+        dev_in = torch.empty_like(aa.arena)
+        dev_in.copy_(host_in, non_blocking=True)
+        y = step(SymmetricTensor(aa.structure, arena=dev_in))
+        host_out.copy_(y.arena, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e_ev[k][0].record()
+        e2e_step()
+        e_ev[k][1].record()
+    torch.cuda.synchronize()
+    e_ms = sum(a.elapsed_time(b) for a, b in e_ev)
+    if world > 1:
+        t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = flops * args.steps * world / (e_ms * 1e-3) / 1e12
+    assert _lib.device_error(0) == 0, "a kernel raised the device error word during the bench"
+
+    if rank == 0:
+        pk = peaks()
+        dgemm = measure_dgemm_peak(torch)
+        g = kernels.get("grouped_gemm_f64", {"launches": 0, "ms": 0.0, "work": 0})
+        gt = kernels.get("block_gather", {"launches": 0, "ms": 0.0, "work": 0})
+        total_kernel_ms = g["ms"] + gt["ms"]
+        gemm_tflops = g["work"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] else 0.0
+        gather_gbs = gt["work"] / (gt["ms"] * 1e-3) / 1e9 if gt["ms"] else 0.0
+        dominant_is_gemm = g["ms"] >= gt["ms"]
+        roofline = {
+            "bound": "tensor" if dominant_is_gemm else "hbm",
+            "kernel": "grouped_gemm_f64" if dominant_is_gemm else "block_gather",
+            "achieved": gemm_tflops if dominant_is_gemm else gather_gbs,
+            "peak": dgemm if dominant_is_gemm else pk["hbm_gbs"],
+            "unit": "TFLOP/s" if dominant_is_gemm else "GB/s",
+            "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in "
+                            "MEASURED_PEAKS.json)") if dominant_is_gemm
+            else f"MEASURED_PEAKS.json hbm_gbs ({pk['src']})",
+            "traffic": None,
+            "kernels": {
+                "grouped_gemm_f64": {"launches": g["launches"], "ms": g["ms"],
+                                     "share": g["ms"] / total_kernel_ms if total_kernel_ms else 0,
+                                     "tflops": gemm_tflops, "dgemm_peak_tflops": dgemm},
+                "block_gather": {"launches": gt["launches"], "ms": gt["ms"],
+                                 "share": gt["ms"] / total_kernel_ms if total_kernel_ms else 0,
+                                 "gbs": gather_gbs, "hbm_peak_gbs": pk["hbm_gbs"]},
+            },
+        }
+        roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
+        base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "su2-heisenberg-heff2-L64-mid-bond-256-multiplets",
+                       "bond_multiplets": BOND, "mpo_multiplets": MPO,
+                       "flops_per_matvec": flops, "elements_aa": int(aa.arena.numel()),
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "parallelism": f"replicas{world}"},
+            "e2e": {"value": e2e_value, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": int(aa.arena.numel() * 8),
+                    "d2h_bytes_per_step": int(out_size * 8)},
+            "gpu_launches": int(log.count),
+            "launches_per_step": launches_per_step,
+            "roofline": roofline,
+            "cpu_baseline": base,
+            "clocks": clk.summary(),
+        }))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tenet", choices=["tenet", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_tenet(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,158 @@
+/*
+ * tenet_b200.h -- C ABI of the B200 block-sparse symmetric-tensor engine.
+ *
+ * The reference (TeNeT-py) is pure Python: every block operation is an autoray
+ * dispatch `ar.do(name, block, ...)` inside a per-block loop.  This library replaces
+ * those loops with sm_100a kernels driven by flat descriptor tables that the Python
+ * host planner builds once per tensor structure.  A maintainer binds it from Python
+ * with ctypes; no torch type crosses this boundary.
+ *
+ * Conventions for every entry point
+ *   - All pointers are DEVICE pointers to caller-owned memory unless stated; the
+ *     library borrows them for the duration of the stream-ordered call only.
+ *   - `stream` is a cudaStream_t passed as void*; 0 is the legacy default stream.
+ *   - Return value: 0 on success, a nonzero TNB_E* code otherwise.  The message of
+ *     the last failure on the calling host thread is tnb_last_error().  Nothing is
+ *     launched when argument validation fails, so a refusal moves no data -- the
+ *     reference's "refuse before any block moves" rule (ops/contraction.py:35-39).
+ *   - Kernels bounds-check every table-driven access against the buffer lengths
+ *     they are given.  A violation skips the access and raises a sticky device
+ *     error word (never a trap); tnb_device_error() reads and clears it.
+ *   - FP64 throughout the plain form.  Calls are thread-compatible: one stream per
+ *     caller.  The only global state is the sticky device error word.
+ */
+#ifndef TENET_B200_H
+#define TENET_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TNB_OK 0
+#define TNB_EINVAL 1   /* bad argument (null pointer, negative size, bad table)   */
+#define TNB_ECUDA 2    /* a CUDA runtime call failed                               */
+#define TNB_EBOUNDS 3  /* a kernel saw an out-of-range table entry                 */
+
+/* Maximum tensor rank a gather segment may carry. */
+#define TNB_MAX_RANK 8
+
+/*
+ * Gather segment descriptor: one row of 40 int64 per destination block region.
+ *
+ *   [0]  dst_off       element offset of the region in its destination buffer
+ *   [1]  size          number of elements (product of dims), < 2^31
+ *   [2]  rank          number of dims used, 1..TNB_MAX_RANK
+ *   [3]  t_begin       first term index (into term_src / term_coeff / term_ld)
+ *   [4]  t_end         one past the last term index (t_end == t_begin: write zeros)
+ *   [5]  buf           0 or 1: which (src, dst) buffer pair the segment uses
+ *   [6]  chunk_begin   prefix sum of ceil(size / TNB_GATHER_CHUNK) over earlier rows
+ *   [7]  reserved, 0
+ *   [8..15]  dims        iteration extents, outermost first
+ *   [16..23] dst_stride  element stride of each dim in the destination
+ *   [24..31] src_rstride source stride of each dim, in units of the term's ld
+ *   [32..39] src_cstride source stride of each dim, in elements
+ *
+ * A source that is a plain block in an arena has src_rstride = 0; a source that is a
+ * window of a coupled-sector matrix splits its strides into a row part (multiplied by
+ * that matrix's leading dimension, which differs per term when the terms of one
+ * destination come from different coupled sectors) and a column part.  For an element
+ * with multi-index J, with R = sum_k J_k src_rstride_k and C = sum_k J_k src_cstride_k:
+ *   dst[buf][dst_off + sum_k J_k dst_stride_k] =
+ *       sum_{t in [t_begin, t_end)} term_coeff[t] * src[buf][term_src[t] + term_ld[t] * R + C]
+ */
+#define TNB_SEG_WIDTH 40
+#define TNB_GATHER_CHUNK 1024
+
+/*
+ * Block gather-permute-scale-accumulate.  Replaces the per-term execution loops of
+ *   transpose    ops/permutation.py:254-272   (blocks[dst] += c * transpose(blocks[src]))
+ *   bend         ops/repartition.py:224-248
+ *   repartition  ops/repartition.py:458-476
+ * and, because a destination may be a strided window of a coupled-sector matrix, the
+ * block <-> matrix lowering of
+ *   to_matrices   map_view.py:238-279  (transpose + reshape + concatenate)
+ *   from_matrices map_view.py:282-335  (slice + reshape + transpose)
+ * Rows must be sorted by chunk_begin; total_chunks is the sum of all rows' chunks.
+ * Every destination element must belong to exactly one row (rows never overlap).
+ */
+int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, int64_t total_chunks,
+                     const int64_t* term_src, const double* term_coeff,
+                     const int64_t* term_ld, int64_t n_term,
+                     const double* src0, int64_t n_src0, double* dst0, int64_t n_dst0,
+                     const double* src1, int64_t n_src1, double* dst1, int64_t n_dst1,
+                     void* stream);
+
+/*
+ * Grouped GEMM descriptor: one row of 16 int64 per product C = A * B (row-major).
+ *
+ *   [0] M  [1] N  [2] K  [3] a_off  [4] lda  [5] b_off  [6] ldb  [7] c_off  [8] ldc
+ *   [9] tile_begin   prefix sum of tiles over earlier rows
+ *   [10] tiles_n     number of tile columns, ceil(N / tile_n)
+ *   [11] tiles       number of tiles, ceil(M / tile_m) * tiles_n
+ *   [12..15] reserved, 0
+ *
+ * K == 0 writes zeros (a coupled sector carried by one operand only).
+ */
+#define TNB_GEMM_WIDTH 16
+#define TNB_GEMM_TILE_M 64
+#define TNB_GEMM_TILE_N 64
+
+/*
+ * Grouped FP64 GEMM over uneven coupled sectors, one launch for every sector.
+ * Replaces compose's per-sector loop ops/map.py:155-172 (`ar.do("matmul", ...)` per
+ * coupled sector, zeros for a sector one operand lacks).  Rows sorted by tile_begin.
+ */
+int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm, int64_t total_tiles,
+                         const double* a, int64_t n_a, const double* b, int64_t n_b,
+                         double* c, int64_t n_c, void* stream);
+
+/*
+ * Weighted inner product  out[0] = sum_r run_w[r] * sum_{i in run r} x[i] * y[i].
+ * Runs are contiguous element ranges [run_start[r], run_start[r+1]) of equal weight
+ * (consecutive blocks with the same qdim of their coupled sector merged).  Replaces
+ *   inner  ops/contraction.py:517-589  (sum_tau qdim(c_tau) <A_tau, B_tau>)
+ *   norm   ops/basic.py:309            (sqrt of inner(t, t))
+ * `work` is caller-provided scratch of tnb_dot_work_bytes(n) bytes whose leading
+ * counter word must be zero before the first call (a fresh cudaMemset); every call
+ * leaves it zero again.  The reduction order is fixed, so results are deterministic.
+ */
+int64_t tnb_dot_work_bytes(int64_t n);
+int tnb_weighted_dot(const double* x, const double* y, int64_t n,
+                     const int64_t* run_start, const double* run_w, int64_t n_runs,
+                     void* work, double* out, void* stream);
+
+/*
+ * out[i] = alpha * x[i] + beta * y[i], i < n.  `out` may alias `x` or `y`.
+ * Replaces add / subtract / multiply / divide over aligned blocks
+ * (ops/basic.py:81-236) and Lanczos' vector updates (network/dmrg.py:207-227).
+ */
+int tnb_axpby(int64_t n, double alpha, const double* x, double beta, const double* y,
+              double* out, void* stream);
+
+/*
+ * out[i] = sum_j coeffs[j] * vecs[j][i] for j < k, i < n.  `vecs` is a DEVICE array of
+ * k device pointers; `coeffs` a DEVICE array of k doubles.  The Lanczos Ritz-vector
+ * recombination (network/dmrg.py:224-227) in one pass.
+ */
+int tnb_lincomb(int64_t n, int64_t k, const double* coeffs, const double* const* vecs,
+                double* out, void* stream);
+
+/* Library version (major*10000 + minor*100 + patch). */
+int tnb_version(void);
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char* tnb_last_error(void);
+
+/*
+ * Read and clear the sticky device error word (0 = clean, else the TNB_E* code a
+ * kernel raised).  Synchronises `stream`.
+ */
+int tnb_device_error(int* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TENET_B200_H */

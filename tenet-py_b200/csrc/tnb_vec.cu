@@ -1,0 +1,165 @@
+// K3: the Lanczos vector space on a tensor arena -- qdim-weighted dot, axpby, lincomb.
+//
+// The reference's `inner`/`norm` are Python sums over blocks of
+// `qdim(c_tau) * ar.do("sum", conj(x) * y)` (ops/contraction.py:584-589, ops/basic.py:309)
+// and every Lanczos update is a per-block add (network/dmrg.py:207-227).  A tensor's
+// blocks live in one contiguous arena here, so each of these is one pass over it.  The
+// qdim weight is constant on runs of consecutive blocks; the host merges equal-weight
+// neighbours into runs and the dot walks runs, never a per-element lookup.
+#include "tnb_common.cuh"
+
+namespace tnb {
+
+constexpr int kDotThreads = 256;
+constexpr int64_t kDotMaxCtas = 4 * 148;
+constexpr int64_t kDotMinChunk = 2048;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum in a fixed order (deterministic); the result is valid in thread 0.
+__device__ double block_sum(double v) {
+  __shared__ double part[kDotThreads / 32];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = threadIdx.x < kDotThreads / 32 ? part[threadIdx.x] : 0.0;
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kDotThreads)
+wdot_kernel(const double* __restrict__ x, const double* __restrict__ y, int64_t n,
+            const int64_t* __restrict__ run_start, const double* __restrict__ run_w,
+            int64_t n_runs, int64_t chunk, unsigned int* counter, double* partial,
+            double* out) {
+  const int64_t lo = static_cast<int64_t>(blockIdx.x) * chunk;
+  const int64_t hi = min(n, lo + chunk);
+  // first run containing lo
+  __shared__ int64_t s_r0;
+  if (threadIdx.x == 0) {
+    int64_t a = 0, b = n_runs - 1;
+    while (a < b) {
+      const int64_t mid = (a + b + 1) >> 1;
+      if (run_start[mid] <= lo) a = mid; else b = mid - 1;
+    }
+    s_r0 = a;
+  }
+  __syncthreads();
+  double acc = 0.0;
+  for (int64_t r = s_r0; r < n_runs && run_start[r] < hi; ++r) {
+    const int64_t a = max(lo, run_start[r]);
+    const int64_t b = min(hi, run_start[r + 1]);
+    double s = 0.0;
+    for (int64_t i = a + threadIdx.x; i < b; i += kDotThreads) s = fma(x[i], y[i], s);
+    acc = fma(run_w[r], s, acc);
+  }
+  const double total = block_sum(acc);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = total;
+    __threadfence();
+    const unsigned int done = atomicAdd(counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int64_t i = threadIdx.x; i < gridDim.x; i += kDotThreads) v += ((volatile double*)partial)[i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) {
+    *out = v;
+    *counter = 0u;  // leave the workspace reusable
+  }
+}
+
+__global__ void axpby_kernel(int64_t n, double alpha, const double* x, double beta,
+                             const double* y, double* out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = fma(alpha, x[i], beta * y[i]);
+}
+
+__global__ void lincomb_kernel(int64_t n, int64_t k, const double* __restrict__ coeffs,
+                               const double* const* __restrict__ vecs, double* out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int64_t j = 0; j < k; ++j) s = fma(coeffs[j], vecs[j][i], s);
+    out[i] = s;
+  }
+}
+
+inline int64_t dot_grid(int64_t n) {
+  int64_t g = (n + kDotMinChunk - 1) / kDotMinChunk;
+  if (g < 1) g = 1;
+  if (g > kDotMaxCtas) g = kDotMaxCtas;
+  return g;
+}
+
+inline unsigned elementwise_grid(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 8 * 148) g = 8 * 148;
+  return static_cast<unsigned>(g);
+}
+
+}  // namespace tnb
+
+extern "C" int64_t tnb_dot_work_bytes(int64_t n) {
+  return 256 + 8 * tnb::dot_grid(n < 0 ? 0 : n);
+}
+
+extern "C" int tnb_weighted_dot(const double* x, const double* y, int64_t n,
+                                const int64_t* run_start, const double* run_w, int64_t n_runs,
+                                void* work, double* out, void* stream) {
+  TNB_REQUIRE(out != nullptr && work != nullptr, "tnb_weighted_dot: null out or work");
+  TNB_REQUIRE(n >= 0 && n_runs >= 0, "tnb_weighted_dot: negative size");
+  cudaStream_t s = tnb::as_stream(stream);
+  if (n == 0 || n_runs == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
+    if (e != cudaSuccess) {
+      tnb::set_error(std::string("tnb_weighted_dot: ") + cudaGetErrorString(e));
+      return TNB_ECUDA;
+    }
+    return TNB_OK;
+  }
+  TNB_REQUIRE(x != nullptr && y != nullptr && run_start != nullptr && run_w != nullptr,
+              "tnb_weighted_dot: null input");
+  const int64_t grid = tnb::dot_grid(n);
+  const int64_t chunk = (n + grid - 1) / grid;
+  auto* counter = static_cast<unsigned int*>(work);
+  auto* partial = reinterpret_cast<double*>(static_cast<char*>(work) + 256);
+  tnb::wdot_kernel<<<static_cast<unsigned>(grid), tnb::kDotThreads, 0, s>>>(
+      x, y, n, run_start, run_w, n_runs, chunk, counter, partial, out);
+  return tnb::check_launch("tnb_weighted_dot");
+}
+
+extern "C" int tnb_axpby(int64_t n, double alpha, const double* x, double beta, const double* y,
+                         double* out, void* stream) {
+  TNB_REQUIRE(n >= 0, "tnb_axpby: negative size");
+  if (n == 0) return TNB_OK;
+  TNB_REQUIRE(x != nullptr && y != nullptr && out != nullptr, "tnb_axpby: null pointer");
+  tnb::axpby_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(n, alpha, x,
+                                                                                  beta, y, out);
+  return tnb::check_launch("tnb_axpby");
+}
+
+extern "C" int tnb_lincomb(int64_t n, int64_t k, const double* coeffs,
+                           const double* const* vecs, double* out, void* stream) {
+  TNB_REQUIRE(n >= 0 && k >= 0, "tnb_lincomb: negative size");
+  if (n == 0) return TNB_OK;
+  TNB_REQUIRE(out != nullptr && (k == 0 || (coeffs != nullptr && vecs != nullptr)),
+              "tnb_lincomb: null pointer");
+  tnb::lincomb_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(n, k, coeffs,
+                                                                                    vecs, out);
+  return tnb::check_launch("tnb_lincomb");
+}

@@ -1,0 +1,41 @@
+"""NumPy emulation of the CUDA library's table-driven kernels, for CPU-only tests.
+
+Each function executes a descriptor table exactly as ``include/tenet_b200.h`` documents
+the kernel semantics, so the host planner's tables can be verified on a machine without
+a GPU.  This is test infrastructure; the shipped package never runs it.
+"""
+
+import numpy as np
+
+
+def gather(table, src0, dst0, src1=None, dst1=None):
+    srcs, dsts = (src0, src1), (dst0, dst1)
+    for row in table.seg:
+        dst_off, size, rank, t0, t1, buf = (int(x) for x in row[:6])
+        dims = [int(x) for x in row[8:8 + rank]]
+        dstr, rstr, cstr = (np.array(row[o:o + rank], dtype=np.int64) for o in (16, 24, 32))
+        J = np.indices(dims).reshape(rank, -1)
+        doff = dst_off + (J * dstr[:, None]).sum(0)
+        R = (J * rstr[:, None]).sum(0)
+        C = (J * cstr[:, None]).sum(0)
+        acc = np.zeros(J.shape[1])
+        for t in range(t0, t1):
+            o = table.tsrc[t] + table.tld[t] * R + C
+            assert o.min() >= 0 and o.max() < srcs[buf].size, "source out of bounds"
+            acc = acc + table.tcf[t] * srcs[buf][o]
+        assert doff.min() >= 0 and doff.max() < dsts[buf].size, "destination out of bounds"
+        dsts[buf][doff] = acc
+
+
+def gemm(table, a, b, c):
+    for row in table.table:
+        M, N, K, ao, lda, bo, ldb, co, ldc = (int(x) for x in row[:9])
+        if K == 0:
+            for m in range(M):
+                c[co + m * ldc: co + m * ldc + N] = 0.0
+            continue
+        A = np.lib.stride_tricks.as_strided(a[ao:], (M, K), (lda * 8, 8))
+        B = np.lib.stride_tricks.as_strided(b[bo:], (K, N), (ldb * 8, 8))
+        out = A @ B
+        for m in range(M):
+            c[co + m * ldc: co + m * ldc + N] = out[m]

@@ -1,0 +1,265 @@
+"""Parity of the CUDA path with the reference's golden vectors and with the oracle.
+
+Every test calls the library through the package's public API (which drives the C ABI)
+and compares against (a) outputs of the reference itself (``tests/golden``), at 1e-12
+relative per block -- the tolerance the north star states for the FP64 plain form -- and
+(b) the oracle on seeded random inputs at sizes the oracle finishes in seconds.  Block
+keys must be identical.  After each test the sticky device error word must be clear.
+"""
+
+import json
+
+import numpy as np
+import pytest
+import torch
+
+import oracle.tenet_oracle as O
+import tenet
+from tenet import _lib, linalg, network
+from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure
+from tenet.symmetry import SU2, U1, Z2, fZ2
+
+pytestmark = pytest.mark.gpu
+PROV = {"U1": U1, "Z2": Z2, "fZ2": fZ2, "SU2": SU2}
+RTOL = 1e-12
+
+
+def struct(legs_json):
+    p = PROV[legs_json[0]["provider"]]
+    return TensorStructure(tuple(
+        Leg(GradedSpace.new(p, {p.sector(a): m for a, m in leg["sectors"]}),
+            OUT if leg["side"] == "out" else IN, bool(leg["dual"])) for leg in legs_json))
+
+
+def keys(d):
+    t = lambda x: (tuple(x[0]), tuple(x[1]), x[2])  # noqa: E731
+    return tuple((t(o), t(i)) for o, i in d["keys"])
+
+
+def load(arrays, d):
+    s = struct(d["legs"])
+    assert s.keys == keys(d)
+    return tenet.SymmetricTensor.from_numpy_arena(s, arrays[d["arena"]])
+
+
+def close(got, want, rtol=RTOL):
+    got, want = np.asarray(got), np.asarray(want)
+    assert got.shape == want.shape
+    scale = max(np.abs(want).max(), 1e-300) if want.size else 1.0
+    err = np.abs(got - want).max() / scale if want.size else 0.0
+    assert err <= rtol, f"relative error {err:.3e} > {rtol:.1e}"
+
+
+@pytest.fixture(autouse=True)
+def _device_error_clear():
+    yield
+    torch.cuda.synchronize()
+    assert _lib.device_error(0) == 0, "a kernel raised the device error word"
+
+
+@pytest.fixture(scope="module")
+def cases(golden_dir):
+    return json.loads((golden_dir / "cases.json").read_text()), np.load(golden_dir / "cases.npz")
+
+
+def test_golden_cases(cases):
+    meta, arrays = cases
+    done = 0
+    for c in meta["cases"]:
+        op, a = c["op"], c["args"]
+        ins = [load(arrays, d) for d in c["operands"]]
+        if op == "einsum":
+            out = tenet.einsum(a["equation"], *ins)
+        elif op == "transpose":
+            out = tenet.transpose(ins[0], a["axes"])
+        elif op == "repartition":
+            out = tenet.repartition(ins[0], a["outputs"], a["inputs"])
+        elif op == "tensordot":
+            out = tenet.tensordot(ins[0], ins[1], a["axes"])
+        elif op == "inner":
+            assert tenet.inner(*ins) == pytest.approx(a["value"], rel=RTOL)
+            continue
+        elif op == "norm":
+            assert tenet.norm(*ins) == pytest.approx(a["value"], rel=RTOL)
+            continue
+        elif op == "svd_truncated":
+            u, s, vh = linalg.svd_truncated(ins[0], a["axes"], max_bond=a["max_bond"],
+                                            cutoff=a["cutoff"])
+            want = struct(c["output"]["legs"])
+            assert s.structure == want, "kept bond sectors differ from the reference"
+            close(s.numpy_arena(), arrays[c["output"]["arena"]])
+            # U S Vh reconstructs the truncated tensor (vectors carry a sign gauge)
+            rec = tenet.einsum("abx,xy->aby", u, s)
+            rec = tenet.compose(tenet.repartition(rec, (0, 1), (2,)), vh)
+            ref = O.svd_truncated(O.from_arena(O.structure_from_json(c["operands"][0]["legs"]),
+                                               arrays[c["operands"][0]["arena"]]),
+                                  a["axes"], max_bond=a["max_bond"], cutoff=a["cutoff"])
+            want_rec = O.compose(O.repartition(O.einsum("abx,xy->aby", ref[0], ref[1]), (0, 1),
+                                               (2,)), ref[2]).arena()
+            close(rec.numpy_arena(), want_rec, 1e-11)
+            continue
+        else:
+            continue
+        assert out.structure == struct(c["output"]["legs"]), c["name"]
+        close(out.numpy_arena(), arrays[c["output"]["arena"]])
+        done += 1
+    assert done >= 15
+
+
+def test_heff2_lanczos_svd_golden(golden_dir):
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    out = network.heff2(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"])
+    assert out.structure == struct(m["heff_aa"]["legs"])
+    close(out.numpy_arena(), h[m["heff_aa"]["arena"]])
+    e, v = network.lanczos(lambda x: network.heff2(T["fl"], T["w1"], T["w2"], T["fr"], x),
+                           T["aa"], ncv=20)
+    assert e == pytest.approx(m["lanczos_ncv20_energy"], rel=1e-12)
+    _, s, _ = linalg.svd_truncated(v, ((0, 1), (2, 3)), max_bond=16, cutoff=1e-10)
+    assert [[SU2.label(a), k] for a, k in s.legs[0].space.sectors] == m["svd_bond"]
+    close(s.numpy_arena(), h[m["svd_s"]["arena"]], 1e-9)
+
+
+def test_env_folds_match_oracle(golden_dir):
+    """Both environment folds on a seeded site tensor (``network/env.py:620-629``)."""
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    fl, fr, w1 = (load(h, m[k]) for k in ("fl", "fr", "w1"))
+    ofl, ofr, ow1 = (O.from_arena(O.structure_from_json(m[k]["legs"]), h[m[k]["arena"]])
+                     for k in ("fl", "fr", "w1"))
+    bond, phys = m["aa"]["legs"][0], m["aa"]["legs"][1]
+    site = [dict(bond, side="out"), dict(phys, side="out"), dict(bond, side="in")]
+    a = tenet.SymmetricTensor.random(struct(site).legs, seed=5)
+    oa = O.random(O.structure_from_json(site), 5)
+    got, want = network.env_update_last(fl, a, w1), O.env_update_last(ofl, oa, ow1)
+    assert got.structure.keys == O.block_order(want.structure)
+    close(got.numpy_arena(), want.arena())
+    got, want = network.env_update_first(fr, a, w1), O.env_update_first(ofr, oa, ow1)
+    assert got.structure.keys == O.block_order(want.structure)
+    close(got.numpy_arena(), want.arena())
+
+
+def test_config1_full_size_against_reference_checksums(golden_dir):
+    g = json.loads((golden_dir / "config1.json").read_text())
+    V = GradedSpace.new(U1, {U1.sector(q): d for q, d in g["degeneracies"]})
+    A = tenet.SymmetricTensor.random((Leg(V, OUT),) * 4, seed=0)
+    B = tenet.SymmetricTensor.random((Leg(V, IN), Leg(V, IN), Leg(V, OUT), Leg(V, OUT)), seed=1)
+    C = tenet.einsum(g["equation"], A, B)
+    assert C.structure.keys == keys(g)
+    probe = np.random.default_rng(g["checksum_seed"])
+    for blk, (s, ss, pr) in zip(C.blocks, g["blocks_sum_sumsq_probe"]):
+        x = blk.cpu().numpy().ravel()
+        w = probe.standard_normal(x.size)
+        assert float((x * x).sum()) == pytest.approx(ss, rel=1e-12)
+        assert float(w @ x) == pytest.approx(pr, rel=1e-10, abs=1e-9)
+    close(C.blocks[0].cpu().numpy().ravel(), np.array(g["first_block"]))
+
+
+SU2_SPACES = [
+    {0: 2, 2: 3, 4: 1},
+    {1: 2, 3: 1},
+    {0: 1, 2: 2, 4: 2, 6: 1},
+]
+
+
+def _o_leg(p, sec, side, dual=False):
+    return O.Leg(tuple(sorted(sec.items())), side, dual)
+
+
+def _leg(p, sec, side, dual=False):
+    return Leg(GradedSpace.new(p, {p.sector(a): m for a, m in sec.items()}), side, dual)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_su2_contractions_against_oracle(seed):
+    rng = np.random.default_rng(100 + seed)
+    bond = SU2_SPACES[seed % 3]
+    half = {1: 1}
+    sides = [OUT if x else IN for x in rng.integers(0, 2, 4)]
+    duals = [bool(x) for x in rng.integers(0, 2, 4)]
+    spaces = [bond, half, half, bond]
+    legs = [_leg(SU2, sp, sd, du) for sp, sd, du in zip(spaces, sides, duals)]
+    olegs = [_o_leg(SU2, sp, O.OUT if sd is OUT else O.IN, du)
+             for sp, sd, du in zip(spaces, sides, duals)]
+    a = tenet.SymmetricTensor.random(legs, seed=seed)
+    oa = O.random(O.Structure(O.SU2, tuple(olegs)), seed)
+    if oa.arena().size == 0:
+        pytest.skip("no allowed block for this random leg pattern")
+    perm = tuple(int(x) for x in rng.permutation(4))
+    close(tenet.transpose(a, perm).numpy_arena(), O.transpose(oa, perm).arena())
+    outs = tuple(int(x) for x in rng.permutation(4)[:2])
+    ins = tuple(i for i in range(4) if i not in outs)
+    close(tenet.repartition(a, outs, ins).numpy_arena(), O.repartition(oa, outs, ins).arena())
+    # contract legs 2,3 against a partner built to be contractible
+    plegs = [Leg(legs[2].space, legs[2].side, not legs[2].dual),
+             Leg(legs[3].space, legs[3].side, not legs[3].dual), _leg(SU2, bond, OUT)]
+    oplegs = [O.Leg(olegs[2].sectors, olegs[2].side, not olegs[2].dual),
+              O.Leg(olegs[3].sectors, olegs[3].side, not olegs[3].dual),
+              _o_leg(SU2, bond, O.OUT)]
+    b = tenet.SymmetricTensor.random(plegs, seed=seed + 50)
+    ob = O.random(O.Structure(O.SU2, tuple(oplegs)), seed + 50)
+    got = tenet.einsum("abcd,cde->eab", a, b)
+    want = O.einsum("abcd,cde->eab", oa, ob)
+    assert got.structure.keys == O.block_order(want.structure)
+    close(got.numpy_arena(), want.arena())
+
+
+@pytest.mark.parametrize("prov", ["U1", "fZ2", "Z2"])
+def test_random_abelian_contractions_against_oracle(prov):
+    p, op = PROV[prov], {"U1": O.U1, "fZ2": O.FZ2, "Z2": O.Z2}[prov]
+    sec = {-1: 2, 0: 3, 1: 2} if prov == "U1" else {0: 3, 1: 2}
+    A = [(sec, OUT, False), (sec, IN, False), (sec, OUT, True), (sec, IN, False)]
+    a = tenet.SymmetricTensor.random([_leg(p, *x) for x in A], seed=7)
+    oa = O.random(O.Structure(op, tuple(_o_leg(op, s, O.OUT if sd is OUT else O.IN, d)
+                                        for s, sd, d in A)), 7)
+    B = [(sec, OUT, False), (sec, OUT, False), (sec, IN, False)]
+    b = tenet.SymmetricTensor.random([_leg(p, *x) for x in B], seed=8)
+    ob = O.random(O.Structure(op, tuple(_o_leg(op, s, O.OUT if sd is OUT else O.IN, d)
+                                        for s, sd, d in B)), 8)
+    for eq in ("abcd,dbe->ace", "abcd,bef->acdfe"):
+        got = tenet.einsum(eq, a, b)
+        want = O.einsum(eq, oa, ob)
+        assert got.structure.keys == O.block_order(want.structure)
+        close(got.numpy_arena(), want.arena())
+    close(tenet.transpose(a, (3, 1, 0, 2)).numpy_arena(), O.transpose(oa, (3, 1, 0, 2)).arena())
+
+
+def test_vector_ops_and_cabi_direct():
+    """The C ABI called with raw device pointers: axpby and the weighted dot."""
+    import ctypes
+
+    n = 100_003
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y = torch.randn(n, dtype=torch.float64, device="cuda")
+    out = torch.empty_like(x)
+    lib = _lib.load()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.tnb_axpby(n, 2.0, x.data_ptr(), -0.5, y.data_ptr(), out.data_ptr(), s) == 0
+    close(out.cpu().numpy(), 2.0 * x.cpu().numpy() - 0.5 * y.cpu().numpy(), 1e-15)
+    starts = torch.tensor([0, 10, 50_000, n], dtype=torch.int64, device="cuda")
+    w = torch.tensor([1.0, 3.0, 2.0], dtype=torch.float64, device="cuda")
+    work = torch.zeros(lib.tnb_dot_work_bytes(n), dtype=torch.uint8, device="cuda")
+    res = torch.empty(1, dtype=torch.float64, device="cuda")
+    for _ in range(2):  # the workspace is reusable
+        assert lib.tnb_weighted_dot(x.data_ptr(), y.data_ptr(), n, starts.data_ptr(),
+                                    w.data_ptr(), 3, work.data_ptr(), res.data_ptr(), s) == 0
+        xh, yh = x.cpu().numpy(), y.cpu().numpy()
+        want = (xh[:10] @ yh[:10]) + 3 * (xh[10:50000] @ yh[10:50000]) + 2 * (xh[50000:] @ yh[50000:])
+        assert res.item() == pytest.approx(want, rel=1e-12)
+
+
+def test_empty_and_degenerate_inputs():
+    # a U(1) leg pattern with no charge-conserving block: empty arena end to end
+    V = GradedSpace.new(U1, {U1.sector(1): 2})
+    t = tenet.SymmetricTensor.random((Leg(V, OUT), Leg(V, OUT)), seed=0)
+    assert t.arena.numel() == 0
+    assert tenet.transpose(t, (1, 0)).arena.numel() == 0
+    assert tenet.norm(t) == 0.0
+    # outer product: no contracted axis
+    W = GradedSpace.new(U1, {U1.sector(0): 2, U1.sector(1): 1})
+    a = tenet.SymmetricTensor.random((Leg(W, OUT), Leg(W, IN)), seed=1)
+    b = tenet.SymmetricTensor.random((Leg(W, OUT), Leg(W, IN)), seed=2)
+    oa = O.random(O.Structure(O.U1, (O.Leg(((0, 2), (1, 1)), O.OUT), O.Leg(((0, 2), (1, 1)), O.IN))), 1)
+    ob = O.random(O.Structure(O.U1, (O.Leg(((0, 2), (1, 1)), O.OUT), O.Leg(((0, 2), (1, 1)), O.IN))), 2)
+    close(tenet.tensordot(a, b, ((), ())).numpy_arena(), O.tensordot(oa, ob, ((), ())).arena())

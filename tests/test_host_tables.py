@@ -1,0 +1,148 @@
+"""Host planner and descriptor tables against the reference's golden vectors, on CPU.
+
+The planner must reproduce the reference's block keys exactly; its gather and grouped-
+GEMM tables, executed by a NumPy emulation of the kernels' documented semantics
+(``tests/_emulate.py``), must reproduce the reference's results.  No GPU is needed.
+"""
+
+import json
+
+import numpy as np
+import pytest
+
+import _emulate
+from tenet import ops
+from tenet.plan import repartition_plan, transpose_plan
+from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure, layout
+from tenet._exec import gather_rows, make_gather
+from tenet.symmetry import SU2, U1, Z2, fZ2
+
+PROV = {"U1": U1, "Z2": Z2, "fZ2": fZ2, "SU2": SU2}
+
+
+def structure_from_json(legs):
+    p = PROV[legs[0]["provider"]]
+    return TensorStructure(tuple(
+        Leg(GradedSpace.new(p, {p.sector(a): m for a, m in leg["sectors"]}),
+            OUT if leg["side"] == "out" else IN, bool(leg["dual"])) for leg in legs))
+
+
+def keys_from_json(keys):
+    t = lambda x: (tuple(x[0]), tuple(x[1]), x[2])  # noqa: E731
+    return tuple((t(o), t(i)) for o, i in keys)
+
+
+def _load(arrays, d):
+    s = structure_from_json(d["legs"])
+    assert s.keys == keys_from_json(d["keys"]), "block keys differ from the reference"
+    return s, np.array(arrays[d["arena"]], dtype=np.float64)
+
+
+def run_map(src_s, arena, plan):
+    dst, perm, terms = plan
+    table = make_gather(gather_rows(src_s, "arena", dst, "arena", perm, terms))
+    out = np.full(layout(dst).size, np.nan)
+    _emulate.gather(table, arena, out)
+    return dst, out
+
+
+def run_tensordot(sa, a, sb, b, axes):
+    ex = ops.contraction_exec(sa, sb, ops._validated_axes(sa, sb, axes))
+    ap, bp, cp = np.full(ex.a_mat, np.nan), np.full(ex.b_mat, np.nan), np.full(ex.c_mat, np.nan)
+    _emulate.gather(ex.pack, a, ap, b, bp)
+    _emulate.gemm(ex.gemm, ap, bp, cp)
+    out = np.full(layout(ex.out).size, np.nan)
+    _emulate.gather(ex.unpack, cp, out)
+    return ex.out, out
+
+
+def run_einsum(eq, ops_):
+    lhs, outl = eq.split("->")
+    ta, tb = lhs.split(",")
+    (sa, a), (sb, b) = ops_
+    shared = [x for x in ta if x in tb]
+    axes = (tuple(ta.index(x) for x in shared), tuple(tb.index(x) for x in shared))
+    free = [x for x in ta if x not in shared] + [x for x in tb if x not in shared]
+    s, c = run_tensordot(sa, a, sb, b, axes)
+    return run_map(s, c, transpose_plan(s, tuple(free.index(x) for x in outl)))
+
+
+@pytest.fixture(scope="module")
+def cases(golden_dir):
+    return json.loads((golden_dir / "cases.json").read_text()), np.load(golden_dir / "cases.npz")
+
+
+def test_block_keys_match_reference(cases):
+    meta, arrays = cases
+    n = 0
+    for c in meta["cases"]:
+        for d in c["operands"] + ([c["output"]] if "output" in c else []):
+            _load(arrays, d)
+            n += 1
+    assert n > 40
+
+
+def test_tables_reproduce_reference(cases):
+    meta, arrays = cases
+    done = 0
+    for c in meta["cases"]:
+        op, a = c["op"], c["args"]
+        if op not in ("einsum", "transpose", "repartition", "tensordot"):
+            continue
+        ins = [_load(arrays, d) for d in c["operands"]]
+        es, ex = _load(arrays, c["output"])
+        if op == "einsum":
+            s, out = run_einsum(a["equation"], ins)
+        elif op == "transpose":
+            s, out = run_map(ins[0][0], ins[0][1], transpose_plan(ins[0][0], tuple(a["axes"])))
+        elif op == "repartition":
+            s, out = run_map(ins[0][0], ins[0][1],
+                             repartition_plan(ins[0][0], tuple(a["outputs"]), tuple(a["inputs"])))
+        else:
+            s, out = run_tensordot(ins[0][0], ins[0][1], ins[1][0], ins[1][1], a["axes"])
+        assert s == es, c["name"]
+        assert not np.isnan(out).any(), c["name"]
+        np.testing.assert_allclose(out, ex, rtol=1e-12, atol=1e-12 * np.abs(ex).max(),
+                                   err_msg=c["name"])
+        done += 1
+    assert done >= 15
+
+
+def test_heff2_tables_reproduce_reference(golden_dir):
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: _load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2", "heff_aa")}
+
+    def composed(eq, A, B, bend):
+        lhs, out = eq.split("->")
+        ta, tb = lhs.split(",")
+
+        def bent(t, term):
+            s, arr = t
+            flip = set(bend)
+            outs = tuple(i for i, ch in enumerate(term) if (s.legs[i].side is OUT) != (ch in flip))
+            ins = tuple(i for i in range(len(term)) if i not in outs)
+            return run_map(s, arr, repartition_plan(s, outs, ins)), "".join(term[i] for i in (*outs, *ins))
+
+        A, ta = bent(A, ta)
+        B, tb = bent(B, tb)
+        return run_einsum(f"{ta},{tb}->{out}", [A, B])
+
+    t = run_einsum("apqr,rys->apqys", [T["aa"], T["fr"]])
+    t = composed("apqys,mQqy->apQms", t, T["w2"], "q")
+    t = composed("apQms,xPpm->aPQxs", t, T["w1"], "p")
+    s, out = composed("aPQxs,axB->BPQs", t, T["fl"], "a")
+    es, ex = T["heff_aa"]
+    assert s == es
+    np.testing.assert_allclose(out, ex, rtol=1e-12, atol=1e-12 * np.abs(ex).max())
+
+
+def test_config1_plan_sizes(golden_dir):
+    g = json.loads((golden_dir / "config1.json").read_text())
+    V = GradedSpace.new(U1, {U1.sector(q): d for q, d in g["degeneracies"]})
+    sa = TensorStructure((Leg(V, OUT),) * 4)
+    sb = TensorStructure((Leg(V, IN), Leg(V, IN), Leg(V, OUT), Leg(V, OUT)))
+    ex = ops.contraction_exec(sa, sb, ((2, 3), (0, 1)))
+    assert ex.out.keys == keys_from_json(g["keys"])
+    assert layout(sa).size == 387756 and ex.gemm.n_gemm == 13
+    assert ex.flops == 215_736_784 or abs(ex.flops - 2.157e8) / 2.157e8 < 1e-3
