@@ -293,68 +293,77 @@ def run_tenet(args) -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     from tenet import _exec, _lib, network
+    from tenet.program import GraphMatvec, heff2_program
 
     tensors = build_workload(seed=rank)
     fl, w1, w2, fr, aa = tensors
     flops = heff2_flops()
-    launches_per_step = launches_per_matvec(tensors)
-
-    def step(x):
-        return network.heff2(fl, w1, w2, fr, x)
-
+    launches_eager = launches_per_matvec(tensors)
+    prog = heff2_program(fl, w1, w2, fr, aa.structure)
+    assert prog.flops == flops
+    gm = GraphMatvec(prog)
+    gm.x.copy_(aa.arena)
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+
+    def timed(fn, steps):
+        """Device time of ``steps`` calls, L2 flushed (untimed) between them."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        torch.cuda.synchronize()
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            fn()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev)
+
+    # the two eager forms, for comparison (the plain FP64 form is the eager op-by-op path)
+    eager_ms = {}
+    for name, fn in (("eager_ops", lambda: network.heff2(fl, w1, w2, fr, aa)),
+                     ("eager_chain", lambda: prog.run(gm.x, gm.y))):
+        for _ in range(args.warmup):
+            fn()
+        eager_ms[name] = timed(fn, args.steps) / args.steps
+
     for _ in range(args.warmup):
-        step(aa)
+        gm.replay()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-
-    # timed region: device time of each step, L2 flushed between steps (not timed)
-    log = _exec.LaunchLog(timed=True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
     with Clocks(local) as clk:
-        torch.cuda.synchronize()
-        with log:
-            for k in range(args.steps):
-                flush.fill_(float(k))
-                ev[k][0].record()
-                step(aa)
-                ev[k][1].record()
-        torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
+        ms = timed(gm.replay, args.steps)
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
     value = flops * args.steps * world / (ms * 1e-3) / 1e12
+    launches_per_step = prog.launches
+
+    # kernel timing pass: the same steps, each enqueued behind a GPU-side head start so
+    # the per-launch events bracket device execution only (no host gaps)
+    log = _exec.LaunchLog(timed=True)
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda._sleep(2_000_000)
+        with log:
+            prog.run(gm.x, gm.y)
     kernels = log.summary()
+    log.count = args.steps * launches_per_step
 
     # end to end through the public API with host buffers
     host_in = aa.arena.detach().cpu().pin_memory()
     out_size = aa.arena.numel()
     host_out = torch.empty(out_size, dtype=torch.float64).pin_memory()
-    from tenet.tensor import SymmetricTensor
-
     def e2e_step():
-        dev_in = torch.empty_like(aa.arena)
-        dev_in.copy_(host_in, non_blocking=True)
-        y = step(SymmetricTensor(aa.structure, arena=dev_in))
-        host_out.copy_(y.arena, non_blocking=True)
+        gm.x.copy_(host_in, non_blocking=True)
+        gm.replay()
+        host_out.copy_(gm.y, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
-    torch.cuda.synchronize()
-    e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        e_ev[k][0].record()
-        e2e_step()
-        e_ev[k][1].record()
-    torch.cuda.synchronize()
-    e_ms = sum(a.elapsed_time(b) for a, b in e_ev)
+    e_ms = timed(e2e_step, args.steps)
     if world > 1:
         t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -405,8 +414,12 @@ def run_tenet(args) -> None:
             "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(aa.arena.numel() * 8),
                     "d2h_bytes_per_step": int(out_size * 8)},
-            "gpu_launches": int(log.count),
+            "gpu_launches": int(args.steps * launches_per_step),
             "launches_per_step": launches_per_step,
+            "forms_ms_per_matvec": {"graph_chain": ms / args.steps, **eager_ms},
+            "forms_tflops": {"graph_chain": flops / (ms / args.steps * 1e-3) / 1e12,
+                             **{k: flops / (v * 1e-3) / 1e12 for k, v in eager_ms.items()}},
+            "launches_per_matvec_eager_ops": launches_eager,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),

@@ -1,0 +1,226 @@
+"""Compiled contraction chains: a matvec as a fixed sequence of kernel launches.
+
+The two-site matvec (``network/env.py:416-432``) is a chain: each pairwise contraction's
+left operand is the previous result, its right operand a tensor that does not change
+during a Lanczos solve (an environment or an MPO site).  In the reference every link is
+``repartition -> to_matrices -> matmul -> from_matrices -> repartition -> transpose``
+(``ops/contraction.py:368-376``), plus the explicit bends of ``_composed``
+(``network/env.py:60-90``).  Here the chain is planned once:
+
+* each fixed operand is packed into its coupled-sector matrices once per program;
+* everything between two GEMMs -- the previous product's ``from_matrices``, its
+  restoring repartition, the einsum's final transpose, the next bend and the next
+  operand's repartition and ``to_matrices`` -- composes into one block map, executed by
+  one gather straight from the previous product's packed matrices into the next
+  operand's packed matrices;
+* every buffer is allocated once, so ``run`` is a fixed launch sequence that a CUDA
+  graph captures and replays.
+
+For ``heff2`` that is 5 gathers and 4 grouped GEMMs per matvec.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from tenet import _exec
+from tenet.plan import chain, repartition_plan, transpose_plan
+from tenet.structure import IN, OUT, TensorStructure, layout, matrix_layout
+from tenet.tensor import SymmetricTensor
+
+__all__ = ["ChainProgram", "heff2_program"]
+
+
+def _identity_plan(s: TensorStructure):
+    return s, tuple(range(s.ndim)), tuple((i, i, 1.0) for i in range(s.num_blocks))
+
+
+class _Link:
+    """One contraction of the chain, with its gathers and GEMM table."""
+
+    def __init__(self, src_struct, src_kind, a_plan, b_tensor, b_plan, axes):
+        ca, cb = axes
+        sa_logical = a_plan[0]
+        sb_logical = b_plan[0]
+        fa = tuple(i for i in range(sa_logical.ndim) if i not in ca)
+        fb = tuple(j for j in range(sb_logical.ndim) if j not in cb)
+        for i, j in zip(ca, cb):
+            x, y = sa_logical.legs[i], sb_logical.legs[j]
+            if x.space != y.space or (x.dual != (x.side is IN)) == (y.dual != (y.side is IN)):
+                raise ValueError(f"chain: axis {i} and axis {j} do not contract")
+        sa2, pa, ta = chain(a_plan, repartition_plan(sa_logical, fa, ca))
+        sb2, pb, tb = chain(b_plan, repartition_plan(sb_logical, cb, fb))
+        sc = TensorStructure((*sa2.codomain, *sb2.domain))
+        free = (*(sa_logical.legs[i] for i in fa), *(sb_logical.legs[j] for j in fb))
+        ro = tuple(k for k, leg in enumerate(free) if leg.side is OUT)
+        ri = tuple(k for k, leg in enumerate(free) if leg.side is IN)
+        pos = {k: q for q, k in enumerate((*ro, *ri))}
+        ft = tuple(pos[k] for k in range(len(free)))
+        rp = repartition_plan(sc, ro, ri)
+        self.after = chain(rp, transpose_plan(rp[0], ft))  # C' -> tensordot output
+        assert self.after[0].legs == free
+        ma, mb, mc = matrix_layout(sa2), matrix_layout(sb2), matrix_layout(sc)
+        products, used = [], set()
+        for c in mc.sectors:
+            M, N = mc.shape[c]
+            if c in ma.shape and c in mb.shape:
+                K = ma.shape[c][1]
+                products.append((M, N, K, ma.base[c], K, mb.base[c], N, mc.base[c], N))
+                used.add(c)
+            else:
+                products.append((M, N, 0, 0, 0, 0, N, mc.base[c], N))
+        keep_a = [int(x) in used for x in ma.block_sector]
+        keep_b = [int(x) in used for x in mb.block_sector]
+        self.a_gather = _exec.make_gather(
+            _exec.gather_rows(src_struct, src_kind, sa2, "matrix", pa, ta, 0, keep_a))
+        self.b_gather = _exec.make_gather(
+            _exec.gather_rows(b_tensor.structure, "arena", sb2, "matrix", pb, tb, 0, keep_b))
+        self.gemm = _exec.make_gemm(products)
+        self.c_struct = sc
+        self.a_size, self.b_size, self.c_size = ma.size, mb.size, mc.size
+        self.b_tensor = b_tensor
+
+
+class ChainProgram:
+    """``y = chain(x)`` for a fixed input structure; see the module docstring."""
+
+    def __init__(self, in_struct: TensorStructure) -> None:
+        self.in_struct = in_struct
+        self.src = (in_struct, "arena")
+        self.pending = _identity_plan(in_struct)
+        self.links: list[_Link] = []
+        self._built = False
+
+    # --- building -----------------------------------------------------------------------
+    @property
+    def structure(self) -> TensorStructure:
+        return self.pending[0]
+
+    def transpose(self, axes) -> ChainProgram:
+        self.pending = chain(self.pending, transpose_plan(self.structure, tuple(axes)))
+        return self
+
+    def repartition(self, outputs, inputs) -> ChainProgram:
+        self.pending = chain(self.pending, repartition_plan(self.structure, tuple(outputs),
+                                                           tuple(inputs)))
+        return self
+
+    def contract(self, b: SymmetricTensor, axes, b_plan=None) -> ChainProgram:
+        b_plan = b_plan or _identity_plan(b.structure)
+        link = _Link(self.src[0], self.src[1], self.pending, b, b_plan, axes)
+        self.links.append(link)
+        self.src = (link.c_struct, "matrix")
+        self.pending = link.after
+        return self
+
+    def einsum(self, equation: str, b: SymmetricTensor, bend: str = "") -> ChainProgram:
+        """``einsum(equation, <chain>, b)`` with the wires in ``bend`` bent first on both
+        operands (the reference's ``_composed``)."""
+        lhs, out = equation.split("->")
+        ta, tb = lhs.split(",")
+        b_plan = _identity_plan(b.structure)
+        if bend:
+            flip = set(bend)
+            s = self.structure
+            outs = tuple(i for i, ch in enumerate(ta) if (s.legs[i].side is OUT) != (ch in flip))
+            ins = tuple(i for i in range(len(ta)) if i not in outs)
+            self.repartition(outs, ins)
+            ta = "".join(ta[i] for i in (*outs, *ins))
+            sb = b.structure
+            bo = tuple(i for i, ch in enumerate(tb) if (sb.legs[i].side is OUT) != (ch in flip))
+            bi = tuple(i for i in range(len(tb)) if i not in bo)
+            b_plan = repartition_plan(sb, bo, bi)
+            tb = "".join(tb[i] for i in (*bo, *bi))
+        shared = [x for x in ta if x in tb]
+        axes = (tuple(ta.index(x) for x in shared), tuple(tb.index(x) for x in shared))
+        self.contract(b, axes, b_plan)
+        free = [x for x in ta if x not in shared] + [x for x in tb if x not in shared]
+        return self.transpose(tuple(free.index(x) for x in out))
+
+    def finish(self, allocate: bool = True) -> ChainProgram:
+        dst, perm, terms = self.pending
+        self.out_struct = dst
+        self.out_gather = _exec.make_gather(
+            _exec.gather_rows(self.src[0], self.src[1], dst, "arena", perm, terms))
+        if allocate:
+            self.allocate()
+        return self
+
+    def allocate(self) -> None:
+        """Allocate every buffer once and pack the fixed operands (needs the device)."""
+        dev = _exec.device()
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.a_bufs = [torch.empty(max(1, lk.a_size), **f64) for lk in self.links]
+        self.c_bufs = [torch.empty(max(1, lk.c_size), **f64) for lk in self.links]
+        self.b_bufs = [torch.empty(max(1, lk.b_size), **f64) for lk in self.links]
+        self.refresh()
+        self._built = True
+
+    def refresh(self) -> None:
+        """Re-pack the fixed operands (after their values changed, same structures)."""
+        for lk, buf in zip(self.links, self.b_bufs):
+            lk.b_gather.run(lk.b_tensor.arena, buf)
+
+    # --- running ------------------------------------------------------------------------
+    @property
+    def flops(self) -> int:
+        return sum(lk.gemm.flops for lk in self.links)
+
+    @property
+    def launches(self) -> int:
+        return 2 * len(self.links) + 1
+
+    def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        src = x
+        for lk, ab, bb, cb in zip(self.links, self.a_bufs, self.b_bufs, self.c_bufs):
+            lk.a_gather.run(src, ab)
+            lk.gemm.run(ab, bb, cb)
+            src = cb
+        self.out_gather.run(src, out)
+        return out
+
+    def __call__(self, x: SymmetricTensor) -> SymmetricTensor:
+        if x.structure != self.in_struct:
+            raise ValueError("ChainProgram: input structure differs from the compiled one")
+        out = SymmetricTensor.empty(self.out_struct)
+        self.run(x.arena, out.arena)
+        return out
+
+
+class GraphMatvec:
+    """A ``ChainProgram`` captured in a CUDA graph: copy in, replay, copy out."""
+
+    def __init__(self, program: ChainProgram, warmup: int = 2) -> None:
+        self.program = program
+        dev = _exec.device()
+        self.x = torch.zeros(layout(program.in_struct).size, dtype=torch.float64, device=dev)
+        self.y = torch.empty(layout(program.out_struct).size, dtype=torch.float64, device=dev)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                program.run(self.x, self.y)
+        torch.cuda.current_stream().wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            program.run(self.x, self.y)
+
+    def __call__(self, x: SymmetricTensor) -> SymmetricTensor:
+        self.x.copy_(x.arena)
+        self.graph.replay()
+        return SymmetricTensor(self.program.out_struct, arena=self.y.clone())
+
+    def replay(self) -> None:
+        self.graph.replay()
+
+
+def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = True
+                  ) -> ChainProgram:
+    """The site-tensor two-site matvec (``network/env.py:416-432``) as a chain program.
+    ``fl``, ``w1``, ``w2``, ``fr`` need only ``.structure`` when ``allocate`` is False."""
+    p = ChainProgram(in_struct)
+    p.einsum("apqr,rys->apqys", fr)
+    p.einsum("apqys,mQqy->apQms", w2, bend="q")
+    p.einsum("apQms,xPpm->aPQxs", w1, bend="p")
+    p.einsum("aPQxs,axB->BPQs", fl, bend="a")
+    return p.finish(allocate)

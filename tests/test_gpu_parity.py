@@ -263,3 +263,34 @@ def test_empty_and_degenerate_inputs():
     oa = O.random(O.Structure(O.U1, (O.Leg(((0, 2), (1, 1)), O.OUT), O.Leg(((0, 2), (1, 1)), O.IN))), 1)
     ob = O.random(O.Structure(O.U1, (O.Leg(((0, 2), (1, 1)), O.OUT), O.Leg(((0, 2), (1, 1)), O.IN))), 2)
     close(tenet.tensordot(a, b, ((), ())).numpy_arena(), O.tensordot(oa, ob, ((), ())).arena())
+
+
+def test_compiled_chain_and_graph_match_golden(golden_dir):
+    """The compiled heff2 program (eager and CUDA-graph replay) against the reference."""
+    from tenet.program import GraphMatvec, heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
+    want = h[m["heff_aa"]["arena"]]
+    close(prog(T["aa"]).numpy_arena(), want)
+    gm = GraphMatvec(prog)
+    for _ in range(3):  # replays are repeatable
+        close(gm(T["aa"]).numpy_arena(), want)
+    e, _ = network.lanczos(gm, T["aa"], ncv=20)
+    assert e == pytest.approx(m["lanczos_ncv20_energy"], rel=1e-12)
+
+
+def test_bench_workload_program_matches_oracle():
+    """The bench's 256-multiplet workload: compiled chain against the oracle, per block."""
+    import bench
+
+    tensors = bench.build_workload()
+    from tenet.program import heff2_program
+
+    prog = heff2_program(*tensors[:4], tensors[4].structure)
+    assert prog.flops == bench.heff2_flops()
+    got = prog(tensors[4]).numpy_arena()
+    want = O.heff2(*bench.oracle_workload()).arena()
+    close(got, want)

@@ -146,3 +146,32 @@ def test_config1_plan_sizes(golden_dir):
     assert ex.out.keys == keys_from_json(g["keys"])
     assert layout(sa).size == 387756 and ex.gemm.n_gemm == 13
     assert ex.flops == 215_736_784 or abs(ex.flops - 2.157e8) / 2.157e8 < 1e-3
+
+
+def test_heff2_chain_program_reproduces_reference(golden_dir):
+    """The compiled chain (5 gathers + 4 GEMMs, fixed operands pre-packed) on CPU."""
+    from types import SimpleNamespace
+
+    from tenet.program import heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: _load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2", "heff_aa")}
+    ops_ = {k: SimpleNamespace(structure=T[k][0]) for k in ("fl", "w1", "w2", "fr")}
+    prog = heff2_program(ops_["fl"], ops_["w1"], ops_["w2"], ops_["fr"], T["aa"][0],
+                         allocate=False)
+    assert prog.launches == 9
+    src = T["aa"][1]
+    for lk in prog.links:
+        name = next(k for k in ("fl", "w1", "w2", "fr") if ops_[k] is lk.b_tensor)
+        bbuf = np.full(lk.b_size, np.nan)
+        _emulate.gather(lk.b_gather, T[name][1], bbuf)
+        abuf, cbuf = np.full(lk.a_size, np.nan), np.full(lk.c_size, np.nan)
+        _emulate.gather(lk.a_gather, src, abuf)
+        _emulate.gemm(lk.gemm, abuf, bbuf, cbuf)
+        src = cbuf
+    out = np.full(layout(prog.out_struct).size, np.nan)
+    _emulate.gather(prog.out_gather, src, out)
+    es, ex = T["heff_aa"]
+    assert prog.out_struct == es
+    np.testing.assert_allclose(out, ex, rtol=1e-12, atol=1e-12 * np.abs(ex).max())
