@@ -124,6 +124,29 @@ int tnb_weighted_dot(const double* x, const double* y, int64_t n,
                      void* work, double* out, void* stream);
 
 /*
+ * Allocation-free weighted dot: the same result as tnb_weighted_dot (up to the order of
+ * the partial sums), with no caller scratch.  No counterpart in the reference: it exists
+ * for callers that cannot allocate device memory -- code being captured into a CUDA
+ * graph under the global capture mode, where cudaMalloc is an error; a serving loop that
+ * admits work against a fixed HBM budget and must not grow its footprint once a request
+ * runs; a foreign-language host that holds only borrowed buffers and no allocator.
+ *
+ * Its scratch is a file-scope device array of 8448 bytes (a counter plus 1024 FP64
+ * partials) that every GPU loading the library holds until exit, so n is limited to
+ * TNB_DOT_NOALLOC_MAX_N = 2,097,152 elements; a larger n is refused with
+ * TNB_EINVAL before anything runs.  The first call on a device looks up the array's
+ * device address (set-up, once per device, with that device current): make that first
+ * call before any stream capture.  Each call zeroes the counter and overwrites the
+ * partials; every call shares the one array, so calls that overlap on the GPU (two
+ * streams at once) race -- serialise them.  No cudaMalloc, cudaFree or allocating
+ * library routine is called.
+ */
+#define TNB_DOT_NOALLOC_MAX_N 2097152
+int tnb_weighted_dot_noalloc(const double* x, const double* y, int64_t n,
+                             const int64_t* run_start, const double* run_w, int64_t n_runs,
+                             double* out, void* stream);
+
+/*
  * out[i] = alpha * x[i] + beta * y[i], i < n.  `out` may alias `x` or `y`.
  * Replaces add / subtract / multiply / divide over aligned blocks
  * (ops/basic.py:81-236) and Lanczos' vector updates (network/dmrg.py:207-227).

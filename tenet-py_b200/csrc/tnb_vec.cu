@@ -6,6 +6,9 @@
 // blocks live in one contiguous arena here, so each of these is one pass over it.  The
 // qdim weight is constant on runs of consecutive blocks; the host merges equal-weight
 // neighbours into runs and the dot walks runs, never a per-element lookup.
+#include <mutex>
+#include <string>
+
 #include "tnb_common.cuh"
 
 namespace tnb {
@@ -141,6 +144,85 @@ extern "C" int tnb_weighted_dot(const double* x, const double* y, int64_t n,
   tnb::wdot_kernel<<<static_cast<unsigned>(grid), tnb::kDotThreads, 0, s>>>(
       x, y, n, run_start, run_w, n_runs, chunk, counter, partial, out);
   return tnb::check_launch("tnb_weighted_dot");
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free variant of the weighted dot.  Its scratch (a counter word padded to
+// 256 bytes, then one FP64 partial per CTA) is this file-scope array instead of a
+// caller buffer.  Every device that loads the library holds it until the process exits.
+// Each CTA reduces a fixed kNoAllocChunk elements, so the array bounds n.
+namespace tnb {
+constexpr int64_t kNoAllocMaxCtas = 1024;
+constexpr int64_t kNoAllocChunk = 2048;
+constexpr int64_t kNoAllocMaxN = kNoAllocMaxCtas * kNoAllocChunk;
+static_assert(kNoAllocMaxN == TNB_DOT_NOALLOC_MAX_N, "header and kernel disagree on the limit");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[256 + 8 * kNoAllocMaxCtas];
+
+// Device address of g_noalloc_scratch, looked up once per device with that device
+// current.  In host code the symbol itself is only a host-side stand-in.
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[128] = {};
+
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 128) {
+    set_error(std::string("tnb_weighted_dot_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error(std::string("tnb_weighted_dot_noalloc: cudaGetSymbolAddress: ") +
+                cudaGetErrorString(e));
+      return TNB_ECUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return TNB_OK;
+}
+}  // namespace tnb
+
+extern "C" int tnb_weighted_dot_noalloc(const double* x, const double* y, int64_t n,
+                                        const int64_t* run_start, const double* run_w,
+                                        int64_t n_runs, double* out, void* stream) {
+  TNB_REQUIRE(out != nullptr, "tnb_weighted_dot_noalloc: null out");
+  TNB_REQUIRE(n >= 0 && n_runs >= 0, "tnb_weighted_dot_noalloc: negative size");
+  if (n > tnb::kNoAllocMaxN) {
+    tnb::set_error("tnb_weighted_dot_noalloc: n = " + std::to_string(n) +
+                   " exceeds the allocation-free maximum of " +
+                   std::to_string(tnb::kNoAllocMaxN) +
+                   " elements; use tnb_weighted_dot with caller-provided scratch");
+    return TNB_EINVAL;
+  }
+  cudaStream_t s = tnb::as_stream(stream);
+  if (n == 0 || n_runs == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double), s);
+    if (e != cudaSuccess) {
+      tnb::set_error(std::string("tnb_weighted_dot_noalloc: ") + cudaGetErrorString(e));
+      return TNB_ECUDA;
+    }
+    return TNB_OK;
+  }
+  TNB_REQUIRE(x != nullptr && y != nullptr && run_start != nullptr && run_w != nullptr,
+              "tnb_weighted_dot_noalloc: null input");
+  void* base = nullptr;
+  if (int st = tnb::noalloc_scratch(&base)) return st;
+  auto* counter = static_cast<unsigned int*>(base);
+  auto* partial = reinterpret_cast<double*>(static_cast<char*>(base) + 256);
+  // the counter must start at zero whatever an earlier (possibly failed) call left
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_weighted_dot_noalloc: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  const int64_t grid = (n + tnb::kNoAllocChunk - 1) / tnb::kNoAllocChunk;
+  tnb::wdot_kernel<<<static_cast<unsigned>(grid), tnb::kDotThreads, 0, s>>>(
+      x, y, n, run_start, run_w, n_runs, tnb::kNoAllocChunk, counter, partial, out);
+  return tnb::check_launch("tnb_weighted_dot_noalloc");
 }
 
 extern "C" int tnb_axpby(int64_t n, double alpha, const double* x, double beta, const double* y,

@@ -24,6 +24,7 @@ SIGNATURES = {
     "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
     "tnb_dot_work_bytes": (_i64, [_i64]),
     "tnb_weighted_dot": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp]),
+    "tnb_weighted_dot_noalloc": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp]),
     "tnb_axpby": (_i32, [_i64, _f64, _vp, _f64, _vp, _vp, _vp]),
     "tnb_lincomb": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp]),
     "tnb_version": (_i32, []),
