@@ -186,7 +186,8 @@ class Clocks:
                 if val.lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "reasons": sorted(reasons),
+                "window": "timed steps plus 1 s of the same graph replay loop"}
 
 
 def peaks() -> dict:
@@ -333,6 +334,13 @@ def run_tenet(args) -> None:
         dist.barrier()
     with Clocks(local) as clk:
         ms = timed(gm.replay, args.steps)
+        # the timed steps take milliseconds, shorter than the 200 ms sampling period:
+        # keep the same replay loop running for a second so the sampler sees it under load
+        t_end = time.perf_counter() + 1.0
+        while time.perf_counter() < t_end:
+            for _ in range(50):
+                gm.replay()
+            torch.cuda.synchronize()
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -74,10 +74,12 @@ extern "C" {
  * block <-> matrix lowering of
  *   to_matrices   map_view.py:238-279  (transpose + reshape + concatenate)
  *   from_matrices map_view.py:282-335  (slice + reshape + transpose)
- * Rows must be sorted by chunk_begin; total_chunks is the sum of all rows' chunks.
+ * Rows must be sorted by chunk_begin; total_chunks is the sum of all rows' chunks and
+ * chunk_map[k] (int32, length total_chunks) is the row that chunk k belongs to.
  * Every destination element must belong to exactly one row (rows never overlap).
  */
-int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, int64_t total_chunks,
+int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chunk_map,
+                     int64_t total_chunks,
                      const int64_t* term_src, const double* term_coeff,
                      const int64_t* term_ld, int64_t n_term,
                      const double* src0, int64_t n_src0, double* dst0, int64_t n_dst0,
@@ -89,24 +91,40 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, int64_t total_chun
  *
  *   [0] M  [1] N  [2] K  [3] a_off  [4] lda  [5] b_off  [6] ldb  [7] c_off  [8] ldc
  *   [9] tile_begin   prefix sum of tiles over earlier rows
- *   [10] tiles_n     number of tile columns, ceil(N / tile_n)
- *   [11] tiles       number of tiles, ceil(M / tile_m) * tiles_n
- *   [12..15] reserved, 0
+ *   [10] tiles_n     number of tile columns (ceil(N / tile width); 1 for TNB_TILE_SKINNY)
+ *   [11] tiles       number of tiles of this row (output tiles x splits)
+ *   [12] splits      K splits per output tile (0 or 1: none); tiled kinds only
+ *   [13] ksplit      K extent of one split, a multiple of 16
+ *   [14] part_off    offset (in doubles) of this row's partial tiles in the work buffer
+ *   [15] cnt_off     index of this row's first tile counter in the work buffer
  *
- * K == 0 writes zeros (a coupled sector carried by one operand only).
+ * Split-K is deterministic: each split parks its partial tile, and the last of a tile's
+ * splits to finish sums all of them in split order.  The work buffer holds n_counters
+ * uint32 counters (padded to 256 bytes), then the partial tiles; its counters must be
+ * zero before the first call (a fresh cudaMemset) and every call leaves them zero.
+ * A table without splits may pass work = NULL, work_bytes = 0, n_counters = 0.
+ *
+ * K == 0 writes zeros (a coupled sector carried by one operand only).  All rows of one
+ * launch use one tile kind:
+ *   TNB_TILE_64      64 x 64 output tiles (tiles = ceil(M/64) * ceil(N/64))
+ *   TNB_TILE_32      32 x 32 output tiles, for compositions too small to fill the GPU
+ *   TNB_TILE_SKINNY  256 output rows per tile (tiles = ceil(M/256)); needs N, K <= 16
  */
 #define TNB_GEMM_WIDTH 16
-#define TNB_GEMM_TILE_M 64
-#define TNB_GEMM_TILE_N 64
+#define TNB_TILE_64 0
+#define TNB_TILE_32 1
+#define TNB_TILE_SKINNY 2
 
 /*
  * Grouped FP64 GEMM over uneven coupled sectors, one launch for every sector.
  * Replaces compose's per-sector loop ops/map.py:155-172 (`ar.do("matmul", ...)` per
- * coupled sector, zeros for a sector one operand lacks).  Rows sorted by tile_begin.
+ * coupled sector, zeros for a sector one operand lacks).  Rows sorted by tile_begin;
+ * tile_map[k] (int32, length total_tiles) is the row that tile k belongs to.
  */
-int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm, int64_t total_tiles,
-                         const double* a, int64_t n_a, const double* b, int64_t n_b,
-                         double* c, int64_t n_c, void* stream);
+int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm, const int32_t* tile_map,
+                         int64_t total_tiles, int32_t tile_kind, const double* a, int64_t n_a,
+                         const double* b, int64_t n_b, double* c, int64_t n_c, void* work,
+                         int64_t work_bytes, int64_t n_counters, void* stream);
 
 /*
  * Weighted inner product  out[0] = sum_r run_w[r] * sum_{i in run r} x[i] * y[i].

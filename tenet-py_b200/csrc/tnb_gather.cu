@@ -9,8 +9,9 @@
 // one row, so the sum over terms happens in registers: no atomics, no pre-zeroing, and a
 // fixed summation order (the order of the terms in the plan), hence deterministic.
 //
-// Work is cut into TNB_GATHER_CHUNK-element chunks; CTA b finds its row by binary search
-// over the rows' chunk prefix.  The kernel is HBM-bound: algorithmic bytes per element
+// Work is cut into TNB_GATHER_CHUNK-element chunks; CTA b reads its row index from a
+// chunk -> row map (one load, no search), stages the row and up to kStagedTerms terms in
+// shared memory, then streams its elements.  The kernel is HBM-bound: algorithmic bytes per element
 // are 8 * (terms + 1).  A source term may be a strided window of a coupled-sector matrix
 // with its own leading dimension (see the row layout in tenet_b200.h).
 #include "tnb_common.cuh"
@@ -19,28 +20,26 @@ namespace tnb {
 
 constexpr int kGatherThreads = 256;
 constexpr int kGatherEpt = TNB_GATHER_CHUNK / kGatherThreads;
+constexpr int kStagedTerms = 64;
 
 __global__ void __launch_bounds__(kGatherThreads)
 gather_kernel(const int64_t* __restrict__ segs, int64_t n_seg,
-              const int64_t* __restrict__ term_src, const double* __restrict__ term_coeff,
+              const int32_t* __restrict__ chunk_map, const int64_t* __restrict__ term_src, const double* __restrict__ term_coeff,
               const int64_t* __restrict__ term_ld, int64_t n_term,
               const double* __restrict__ src0, int64_t n_src0, double* __restrict__ dst0,
               int64_t n_dst0,
               const double* __restrict__ src1, int64_t n_src1, double* __restrict__ dst1,
               int64_t n_dst1) {
   __shared__ int64_t row[TNB_SEG_WIDTH];
-  __shared__ int64_t s_seg;
+  __shared__ int64_t t_src[kStagedTerms], t_ld[kStagedTerms];
+  __shared__ double t_cf[kStagedTerms];
   const int64_t chunk = blockIdx.x;
-  if (threadIdx.x == 0) {
-    int64_t lo = 0, hi = n_seg - 1;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi + 1) >> 1;
-      if (segs[mid * TNB_SEG_WIDTH + 6] <= chunk) lo = mid; else hi = mid - 1;
-    }
-    s_seg = lo;
+  const int64_t seg = chunk_map[chunk];
+  if (seg < 0 || seg >= n_seg) {
+    if (threadIdx.x == 0) raise_bounds();
+    return;
   }
-  __syncthreads();
-  if (threadIdx.x < TNB_SEG_WIDTH) row[threadIdx.x] = segs[s_seg * TNB_SEG_WIDTH + threadIdx.x];
+  if (threadIdx.x < TNB_SEG_WIDTH) row[threadIdx.x] = segs[seg * TNB_SEG_WIDTH + threadIdx.x];
   __syncthreads();
 
   const int64_t dst_off = row[0];
@@ -56,6 +55,14 @@ gather_kernel(const int64_t* __restrict__ segs, int64_t n_seg,
     if (threadIdx.x == 0) raise_bounds();
     return;
   }
+  const int nt = static_cast<int>(t1 - t0);
+  const bool staged = nt <= kStagedTerms;
+  if (staged && threadIdx.x < nt) {
+    t_src[threadIdx.x] = term_src[t0 + threadIdx.x];
+    t_ld[threadIdx.x] = term_ld[t0 + threadIdx.x];
+    t_cf[threadIdx.x] = term_coeff[t0 + threadIdx.x];
+  }
+  __syncthreads();
 
   // per-row dims and strides into registers (uniform across the CTA)
   uint32_t dims[TNB_MAX_RANK];
@@ -86,10 +93,18 @@ gather_kernel(const int64_t* __restrict__ segs, int64_t n_seg,
       }
     }
     double acc = 0.0;
-    for (int64_t t = t0; t < t1; ++t) {
-      const int64_t o = __ldg(term_src + t) + __ldg(term_ld + t) * roff + coff;
-      if (o < 0 || o >= n_src) { raise_bounds(); continue; }
-      acc = fma(__ldg(term_coeff + t), __ldg(src + o), acc);
+    if (staged) {
+      for (int t = 0; t < nt; ++t) {
+        const int64_t o = t_src[t] + t_ld[t] * roff + coff;
+        if (o < 0 || o >= n_src) { raise_bounds(); continue; }
+        acc = fma(t_cf[t], __ldg(src + o), acc);
+      }
+    } else {
+      for (int64_t t = t0; t < t1; ++t) {
+        const int64_t o = __ldg(term_src + t) + __ldg(term_ld + t) * roff + coff;
+        if (o < 0 || o >= n_src) { raise_bounds(); continue; }
+        acc = fma(__ldg(term_coeff + t), __ldg(src + o), acc);
+      }
     }
     const int64_t w = dst_off + doff;
     if (w < 0 || w >= n_dst) { raise_bounds(); continue; }
@@ -99,20 +114,22 @@ gather_kernel(const int64_t* __restrict__ segs, int64_t n_seg,
 
 }  // namespace tnb
 
-extern "C" int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, int64_t total_chunks,
+extern "C" int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chunk_map,
+                                int64_t total_chunks,
                                 const int64_t* term_src, const double* term_coeff,
                                 const int64_t* term_ld, int64_t n_term, const double* src0, int64_t n_src0, double* dst0, int64_t n_dst0,
                                 const double* src1, int64_t n_src1, double* dst1, int64_t n_dst1,
                                 void* stream) {
   TNB_REQUIRE(n_seg >= 0 && total_chunks >= 0 && n_term >= 0, "tnb_block_gather: negative size");
   if (n_seg == 0 || total_chunks == 0) return TNB_OK;
-  TNB_REQUIRE(seg_table != nullptr, "tnb_block_gather: seg_table is null");
+  TNB_REQUIRE(seg_table != nullptr && chunk_map != nullptr,
+              "tnb_block_gather: seg_table or chunk_map is null");
   TNB_REQUIRE(n_term == 0 || (term_src != nullptr && term_coeff != nullptr && term_ld != nullptr),
               "tnb_block_gather: term arrays are null");
   TNB_REQUIRE(dst0 != nullptr || dst1 != nullptr, "tnb_block_gather: no destination buffer");
   TNB_REQUIRE(total_chunks < (int64_t(1) << 31), "tnb_block_gather: too many chunks for one launch");
   tnb::gather_kernel<<<static_cast<unsigned>(total_chunks), tnb::kGatherThreads, 0,
-                       tnb::as_stream(stream)>>>(seg_table, n_seg, term_src, term_coeff, term_ld, n_term,
+                       tnb::as_stream(stream)>>>(seg_table, n_seg, chunk_map, term_src, term_coeff, term_ld, n_term,
                                                  src0, n_src0, dst0, n_dst0, src1, n_src1,
                                                  dst1, n_dst1);
   return tnb::check_launch("tnb_block_gather");

@@ -27,8 +27,10 @@ from tenet.structure import TensorStructure, layout, matrix_layout
 SEG_W = 40
 GEMM_W = 16
 CHUNK = 1024
-TILE_M = TILE_N = 64
 MAX_RANK = 8
+TILE_64, TILE_32, TILE_SKINNY = 0, 1, 2
+SKINNY_ROWS, SKINNY_MAX = 256, 16
+N_SM = 148
 
 
 def device() -> torch.device:
@@ -199,6 +201,8 @@ class GatherTable:
         self.chunks = int(((seg[:, 1] + CHUNK - 1) // CHUNK).sum()) if len(seg) else 0
         self.elems = int(seg[:, 1].sum()) if len(seg) else 0
         self.term_elems = int((seg[:, 1] * (seg[:, 4] - seg[:, 3])).sum()) if len(seg) else 0
+        per = (seg[:, 1] + CHUNK - 1) // CHUNK if len(seg) else np.zeros(0, np.int64)
+        self.chunk_map = np.repeat(np.arange(len(seg), dtype=np.int32), per)
         self._dev = None
 
     @property
@@ -211,15 +215,15 @@ class GatherTable:
         if self._dev is None:
             dev = device()
             self._dev = tuple(torch.from_numpy(x).to(dev) for x in
-                              (self.seg, self.tsrc, self.tcf, self.tld))
+                              (self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map))
         return self._dev
 
     def run(self, src0, dst0, src1=None, dst1=None) -> None:
         if self.n_seg == 0:
             return
-        seg, tsrc, tcf, tld = self.device_arrays()
+        seg, tsrc, tcf, tld, cmap = self.device_arrays()
         mark = _LOG.begin() if _LOG is not None else None
-        _lib.call("tnb_block_gather", ptr(seg), self.n_seg, self.chunks, ptr(tsrc),
+        _lib.call("tnb_block_gather", ptr(seg), self.n_seg, ptr(cmap), self.chunks, ptr(tsrc),
                   ptr(tcf), ptr(tld), self.n_term,
                   ptr(src0), src0.numel(), ptr(dst0), dst0.numel(),
                   ptr(src1), 0 if src1 is None else src1.numel(),
@@ -254,42 +258,126 @@ def make_gather(*parts) -> GatherTable:
 
 
 class GemmTable:
-    """A grouped-GEMM program; host table uploaded on first use."""
+    """A grouped-GEMM program (one tile kind); host table uploaded on first use."""
 
-    def __init__(self, table: np.ndarray, tiles: int, flops: int) -> None:
+    def __init__(self, table: np.ndarray, tiles: int, flops: int, kind: int,
+                 n_counters: int = 0, n_parts: int = 0) -> None:
         self.table = table
         self.n_gemm = len(table)
         self.tiles = tiles
         self.flops = flops
+        self.kind = kind
+        self.n_counters = n_counters
+        self.work_bytes = (((4 * n_counters + 255) // 256) * 256 + 8 * n_parts) if n_counters else 0
+        per = table[:, 11] if len(table) else np.zeros(0, np.int64)
+        self.tile_map = np.repeat(np.arange(len(table), dtype=np.int32), per)
         self._dev = None
 
     def run(self, a, b, c) -> None:
+        """Launch on the current stream.  The split-K work buffer belongs to this table, so
+        one table must not run on two streams at once."""
         if self.n_gemm == 0:
             return
         if self._dev is None:
-            self._dev = torch.from_numpy(self.table).to(device())
+            dev = device()
+            work = torch.zeros(max(self.work_bytes, 1), dtype=torch.uint8, device=dev)
+            self._dev = (torch.from_numpy(self.table).to(dev),
+                         torch.from_numpy(self.tile_map).to(dev), work)
         mark = _LOG.begin() if _LOG is not None else None
-        _lib.call("tnb_grouped_gemm_f64", ptr(self._dev), self.n_gemm, self.tiles,
-                  ptr(a), a.numel(), ptr(b), b.numel(), ptr(c), c.numel(), stream_ptr())
+        _lib.call("tnb_grouped_gemm_f64", ptr(self._dev[0]), self.n_gemm, ptr(self._dev[1]),
+                  self.tiles, self.kind, ptr(a), a.numel(), ptr(b), b.numel(), ptr(c),
+                  c.numel(), ptr(self._dev[2]) if self.work_bytes else None, self.work_bytes,
+                  self.n_counters, stream_ptr())
         if _LOG is not None:
             _LOG.end("grouped_gemm_f64", mark, self.flops)
 
 
-def make_gemm(products) -> GemmTable:
+def _tiles(M, N, kind):
+    if kind == TILE_SKINNY:
+        return (M + SKINNY_ROWS - 1) // SKINNY_ROWS, 1
+    t = 64 if kind == TILE_64 else 32
+    tn = (N + t - 1) // t
+    return ((M + t - 1) // t) * tn, tn
+
+
+def choose_kind(products) -> int:
+    """Skinny when every product is tall and thin; else 64x64 tiles unless they would
+    not fill two waves of the GPU, then 32x32."""
+    live = [p for p in products if p[0] and p[1]]
+    if live and all(_is_skinny(p) for p in live):
+        return TILE_SKINNY
+    big = sum(_tiles(p[0], p[1], TILE_64)[0] for p in live)
+    return TILE_64 if big >= 2 * N_SM else TILE_32
+
+
+def _is_skinny(p) -> bool:
+    """A tall product (many rows, at most 16 columns and 16 contracted) goes to the
+    one-thread-per-row kernel; a small one stays in the tiled launch."""
+    return p[0] >= SKINNY_ROWS and p[1] <= SKINNY_MAX and p[2] <= SKINNY_MAX
+
+
+class GemmGroup:
+    """One composition's products, split into at most two launches: the tall skinny ones
+    and the rest (so an MPO-like product never occupies a 64-wide tile)."""
+
+    def __init__(self, products) -> None:
+        skinny = [p for p in products if _is_skinny(p)]
+        rest = [p for p in products if not _is_skinny(p)]
+        self.parts = []
+        if rest:
+            self.parts.append(make_gemm(rest, choose_kind(rest)))
+        if skinny:
+            self.parts.append(make_gemm(skinny, TILE_SKINNY))
+        self.flops = sum(p.flops for p in self.parts)
+        self.tiles = sum(p.tiles for p in self.parts)
+        self.n_gemm = sum(p.n_gemm for p in self.parts)
+        self.launches = len(self.parts)
+
+    @property
+    def table(self):
+        return np.concatenate([p.table for p in self.parts]) if self.parts else \
+            np.zeros((0, GEMM_W), np.int64)
+
+    def run(self, a, b, c) -> None:
+        for p in self.parts:
+            p.run(a, b, c)
+
+
+def _splits(K: int, out_tiles_total: int) -> tuple[int, int]:
+    """K splits for a long-K product when the composition's output tiles cannot fill two
+    waves: (splits, ksplit) with ksplit a multiple of 16 and at least 32."""
+    if K <= 64 or out_tiles_total >= 2 * N_SM:
+        return 1, 0
+    want = max(1, -(-2 * N_SM // max(out_tiles_total, 1)))
+    ks = max(32, -(-K // want))
+    ks = -(-ks // 16) * 16
+    return -(-K // ks), ks
+
+
+def make_gemm(products, kind: int | None = None, split_k: bool = True) -> GemmTable:
     """``products``: iterable of (M, N, K, a_off, lda, b_off, ldb, c_off, ldc)."""
+    products = [p for p in products if p[0] and p[1]]
+    if kind is None:
+        kind = choose_kind(products)
+    tw = 64 if kind == TILE_64 else 32
+    out_total = sum(_tiles(p[0], p[1], kind)[0] for p in products)
     rows = []
-    tile = 0
-    flops = 0
+    tile = flops = n_cnt = n_parts = 0
     for M, N, K, ao, lda, bo, ldb, co, ldc in products:
-        if M == 0 or N == 0:
-            continue
-        tn = (N + TILE_N - 1) // TILE_N
-        tiles = ((M + TILE_M - 1) // TILE_M) * tn
-        rows.append([M, N, K, ao, lda, bo, ldb, co, ldc, tile, tn, tiles, 0, 0, 0, 0])
-        tile += tiles
+        out_tiles, tn = _tiles(M, N, kind)
+        S, ks = (1, 0)
+        if split_k and kind != TILE_SKINNY:
+            S, ks = _splits(K, out_total)
+        row = [M, N, K, ao, lda, bo, ldb, co, ldc, tile, tn, out_tiles * S, 0, 0, 0, 0]
+        if S > 1:
+            row[12:16] = [S, ks, n_parts, n_cnt]
+            n_parts += out_tiles * S * tw * tw
+            n_cnt += out_tiles
+        rows.append(row)
+        tile += out_tiles * S
         flops += 2 * M * N * K
     arr = np.array(rows, dtype=np.int64).reshape(-1, GEMM_W)
-    return GemmTable(arr, tile, flops)
+    return GemmTable(arr, tile, flops, kind, n_cnt, n_parts)
 
 
 # ---------------------------------------------------------------------------------------

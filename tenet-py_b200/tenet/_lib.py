@@ -19,9 +19,10 @@ _i64, _i32, _f64, _vp = ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_
 
 #: every exported entry point and its (restype, argtypes)
 SIGNATURES = {
-    "tnb_block_gather": (_i32, [_vp, _i64, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp, _i64,
-                                _vp, _i64, _vp, _i64, _vp]),
-    "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
+    "tnb_block_gather": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
+                                _i64, _vp, _i64, _vp, _i64, _vp]),
+    "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
+                                    _i64, _vp, _i64, _i64, _vp]),
     "tnb_dot_work_bytes": (_i64, [_i64]),
     "tnb_weighted_dot": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp]),
     "tnb_weighted_dot_noalloc": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp]),

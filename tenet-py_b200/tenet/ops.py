@@ -181,7 +181,7 @@ def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes) -> Contract
         _exec.gather_rows(sa, "arena", sa2, "matrix", perm_a, terms_a, 0, keep_a),
         _exec.gather_rows(sb, "arena", sb2, "matrix", perm_b, terms_b, 1, keep_b))
     unpack = _exec.make_gather(_exec.gather_rows(sc, "matrix", so, "arena", perm_u, terms_u))
-    return ContractionExec(so, ma.size, mb.size, mc.size, pack, _exec.make_gemm(products), unpack)
+    return ContractionExec(so, ma.size, mb.size, mc.size, pack, _exec.GemmGroup(products), unpack)
 
 
 def tensordot(a: SymmetricTensor, b: SymmetricTensor, axes) -> SymmetricTensor:

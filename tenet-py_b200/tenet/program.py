@@ -75,7 +75,7 @@ class _Link:
             _exec.gather_rows(src_struct, src_kind, sa2, "matrix", pa, ta, 0, keep_a))
         self.b_gather = _exec.make_gather(
             _exec.gather_rows(b_tensor.structure, "arena", sb2, "matrix", pb, tb, 0, keep_b))
-        self.gemm = _exec.make_gemm(products)
+        self.gemm = _exec.GemmGroup(products)
         self.c_struct = sc
         self.a_size, self.b_size, self.c_size = ma.size, mb.size, mc.size
         self.b_tensor = b_tensor

@@ -28,6 +28,11 @@ def gather(table, src0, dst0, src1=None, dst1=None):
 
 
 def gemm(table, a, b, c):
+    parts = getattr(table, "parts", None)
+    if parts is not None:
+        for p in parts:
+            gemm(p, a, b, c)
+        return
     for row in table.table:
         M, N, K, ao, lda, bo, ldb, co, ldc = (int(x) for x in row[:9])
         if K == 0:

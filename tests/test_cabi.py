@@ -34,5 +34,7 @@ def test_refusals_move_nothing_and_set_a_message():
     assert lib.tnb_axpby(-1, 1.0, None, 1.0, None, None, None) == 1
     assert b"negative" in lib.tnb_last_error()
     assert lib.tnb_weighted_dot(None, None, 5, None, None, 1, None, None, None) == 1
-    assert lib.tnb_block_gather(None, 1, 1, None, None, None, 0, None, 0, None, 0, None, 0,
-                                None, 0, None) == 1
+    assert lib.tnb_block_gather(None, 1, None, 1, None, None, None, 0, None, 0, None, 0, None,
+                                0, None, 0, None) == 1
+    assert lib.tnb_grouped_gemm_f64(None, 1, None, 1, 7, None, 0, None, 0, None, 0, None, 0, 0,
+                                    None) == 1

@@ -294,3 +294,37 @@ def test_bench_workload_program_matches_oracle():
     got = prog(tensors[4]).numpy_arena()
     want = O.heff2(*bench.oracle_workload()).arena()
     close(got, want)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_grouped_gemm_kinds_against_numpy(kind):
+    """Every tile kind on uneven products, K = 0 included, through the C ABI."""
+    from tenet import _exec
+
+    rng = np.random.default_rng(kind)
+    if kind == 2:
+        shapes = [(1000, 3, 3), (777, 1, 1), (5, 16, 16), (300, 2, 0)]
+    else:
+        shapes = [(176, 236, 60), (9, 11, 2), (64, 64, 64), (65, 33, 17), (40, 7, 0), (1, 1, 1),
+                  (176, 60, 236), (41, 10, 511), (3, 2, 1000)]
+    a_off = b_off = c_off = 0
+    prods, mats = [], []
+    for M, N, K in shapes:
+        prods.append((M, N, K, a_off, K, b_off, N, c_off, N))
+        mats.append((a_off, b_off, c_off))
+        a_off += M * K
+        b_off += K * N
+        c_off += M * N
+    A = rng.standard_normal(a_off)
+    B = rng.standard_normal(b_off)
+    table = _exec.make_gemm(prods, kind)
+    if kind != 2:
+        assert table.n_counters > 0, "the long-K products must take the split-K path"
+    ta, tb = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    for _ in range(2):  # the split-K counters must be left zero for the next run
+        tc = torch.full((c_off,), float("nan"), dtype=torch.float64, device="cuda")
+        table.run(ta, tb, tc)
+        C = tc.cpu().numpy()
+        for (M, N, K), (ao, bo, co) in zip(shapes, mats):
+            want = A[ao:ao + M * K].reshape(M, K) @ B[bo:bo + K * N].reshape(K, N)
+            close(C[co:co + M * N].reshape(M, N), want, 1e-13)
