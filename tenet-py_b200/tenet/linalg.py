@@ -22,7 +22,7 @@ from tenet.plan import repartition_plan, validate_partition
 from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure, layout, matrix_layout
 from tenet.tensor import SymmetricTensor
 
-__all__ = ["BondSelection", "svd_truncated"]
+__all__ = ["BondSelection", "lq", "svd_truncated"]
 
 _CUTOFF_MODES = ("abs", "rel", "sum2", "rsum2", "sum1", "rsum1")
 
@@ -165,3 +165,38 @@ def singular_values(s: SymmetricTensor) -> dict:
         blk = host[int(lay.offsets[b]):int(lay.offsets[b]) + n * n].reshape(n, n)
         out[ot[2]] = np.diag(blk).copy()
     return out
+
+
+def lq(t: SymmetricTensor, axes=None):
+    """``T = L o Q``, the reduced LQ per coupled sector (``ops/linalg.py:549-620``): per
+    sector ``B^T = q r`` on the device, ``L = r^T`` with legs ``(*left, bond IN)`` and
+    ``Q = q^T`` with legs ``(bond OUT, *right)``, bond degeneracy ``min(rows, cols)``."""
+    if axes is None:
+        axes = (t.structure.out_axes, t.structure.in_axes)
+    outputs, inputs = validate_partition(t.ndim, axes[0], axes[1])
+    m, lower = _lower_exec(t.structure, outputs, inputs)
+    ml = matrix_layout(m)
+    buf = torch.empty(ml.size, dtype=torch.float64, device=t.arena.device)
+    lower.run(t.arena, buf)
+    p = t.provider
+    parts = {}
+    for c in ml.sectors:
+        r, q = ml.shape[c]
+        qq, rr = torch.linalg.qr(buf[ml.base[c]:ml.base[c] + r * q].view(r, q).T)
+        parts[c] = (rr.T, qq.T)
+    bond = GradedSpace.new(p, {p.sector(c): min(ml.shape[c]) for c in ml.sectors})
+    sl = TensorStructure((*m.codomain, Leg(bond, IN)))
+    sq = TensorStructure((Leg(bond, OUT), *m.domain))
+    dev = t.arena.device
+
+    def assemble(structure, piece):
+        lay = matrix_layout(structure)
+        mbuf = torch.empty(lay.size, dtype=torch.float64, device=dev)
+        for c in lay.sectors:
+            r, q = lay.shape[c]
+            mbuf[lay.base[c]:lay.base[c] + r * q].view(r, q).copy_(piece(c))
+        out = SymmetricTensor.empty(structure)
+        _raise_exec(structure).run(mbuf, out.arena)
+        return out
+
+    return assemble(sl, lambda c: parts[c][0]), assemble(sq, lambda c: parts[c][1])

@@ -98,3 +98,261 @@ def lanczos(matvec: Callable[[SymmetricTensor], SymmetricTensor], v: SymmetricTe
     _lib.call("tnb_lincomb", v.arena.numel(), len(vecs), _exec.ptr(coeffs), _exec.ptr(ptrs),
               _exec.ptr(out.arena), _exec.stream_ptr())
     return float(values[0]), out / ops.norm(out)
+
+
+# ---------------------------------------------------------------------------------------
+# MPS / MPO / environments / sweeps  (network/mps.py, network/env.py, network/dmrg.py)
+
+
+def ones(legs) -> SymmetricTensor:
+    """A tensor with every structurally allowed entry 1 (``network/common.py:323-346``)."""
+    t = SymmetricTensor.zeros(legs)
+    t.arena.fill_(1.0)
+    return t
+
+
+class MPS:
+    """Site tensors on the partition ``(bond OUT, phys OUT | bond IN)`` (``network/mps.py``)."""
+
+    def __init__(self, sites, center=None) -> None:
+        from tenet import ops
+
+        self.sites = [ops.repartition(t, (0, 1), (2,)) for t in sites]
+        self.center = center
+
+    def __len__(self) -> int:
+        return len(self.sites)
+
+    def __getitem__(self, n: int) -> SymmetricTensor:
+        return self.sites[n]
+
+    def __setitem__(self, n: int, t: SymmetricTensor) -> None:
+        """The write barrier: every factor is put back on ``(l, p | r)``
+        (``network/mps.py:126-143``)."""
+        from tenet import ops
+
+        if t.ndim != 3:
+            raise ValueError(f"an MPS site tensor is rank 3, got rank {t.ndim}")
+        self.sites[n] = ops.repartition(t, (0, 1), (2,))
+
+    @classmethod
+    def random(cls, phys, bonds, *, seed: int = 0) -> "MPS":
+        """Site ``i`` draws with ``seed + i`` (``network/mps.py:161-191``), so a seeded state
+        here holds the reference's numbers."""
+        from tenet.structure import IN, Leg
+
+        return cls(SymmetricTensor.random((Leg(bonds[i], OUT), Leg(phys, OUT),
+                                           Leg(bonds[i + 1], IN)), seed=seed + i)
+                   for i in range(len(bonds) - 1))
+
+    def canonize_(self, to: int = 0) -> "MPS":
+        """Right-canonicalise by one LQ per site from the right (``network/mps.py:312-352``)."""
+        from tenet import linalg, ops
+
+        if to != 0:
+            raise NotImplementedError("only to=0 (right-canonical) is implemented")
+        for n in range(len(self) - 1, 0, -1):
+            left, q = linalg.lq(self[n], ((0,), (1, 2)))
+            self[n] = q
+            self[n - 1] = ops.einsum("apx,xy->apy", self[n - 1], left)
+        self[0] = self[0] / ops.norm(self[0])
+        self.center = to
+        return self
+
+
+class MPO:
+    """Site operators ``W = (x IN, P OUT, p IN, m OUT)`` (the materialised site-tensor form
+    of ``network/mps.py:2551-2729``)."""
+
+    def __init__(self, sites) -> None:
+        self.sites = list(sites)
+
+    def __len__(self) -> int:
+        return len(self.sites)
+
+    def __getitem__(self, n: int) -> SymmetricTensor:
+        return self.sites[n]
+
+
+def heisenberg_mpo_su2(n_sites: int, j: float = 1.0) -> MPO:
+    """``H = J sum_i S_i . S_{i+1}`` on spin-1/2 SU(2) sites, as site tensors.
+
+    The MPO bond carries the finite-state machine of a nearest-neighbour invariant term:
+    a spin-0 "not started" channel, a spin-1 channel carrying the first ``S``, and a spin-0
+    "finished" channel -- multiplets ``{0: 2, 2: 1}`` in the bulk, as the reference's
+    ``MPO.from_terms(...).materialize()`` builds for ``spin_half(SU2).ops["S.S"]``.  In the
+    fusion-tree basis of the blocks ``(P, m | x, p)`` the reduced coefficients are 1 for
+    the identity channels, ``sqrt(3/2)`` for opening the spin-1 channel and
+    ``-sqrt(3/8) J`` for closing it (their product is ``-3/4 J``, the reduced S.S).
+    """
+    import math
+
+    from tenet.structure import IN, GradedSpace, Leg, TensorStructure, layout
+    from tenet.symmetry import SU2
+
+    if n_sites < 2:
+        raise ValueError("a Heisenberg chain needs at least two sites")
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    # states per bond: list of (label, sector two_j) in degeneracy order within a sector
+    def states(b):
+        if b == 0:
+            return [("start", 0)]
+        if b == n_sites:
+            return [("done", 0)]
+        if b == 1:
+            return [("start", 0), ("open", 2)]
+        if b == n_sites - 1:
+            return [("done", 0), ("open", 2)]
+        return [("start", 0), ("done", 0), ("open", 2)]
+
+    def space(st):
+        count: dict = {}
+        for _, s in st:
+            count[s] = count.get(s, 0) + 1
+        return GradedSpace.new(SU2, {SU2.sector(s): m for s, m in count.items()})
+
+    def index(st, label):
+        sec = dict(st)[label]
+        return sec, [lab for lab, s in st if s == sec].index(label)
+
+    opn, cls = math.sqrt(1.5), -math.sqrt(3.0 / 8.0) * j
+    rules = [("start", "start", 1.0), ("done", "done", 1.0), ("start", "open", opn),
+             ("open", "done", cls)]
+    sites = []
+    for n in range(n_sites):
+        sl, sr = states(n), states(n + 1)
+        legs = (Leg(space(sl), IN, True), Leg(phys, OUT), Leg(phys, IN), Leg(space(sr), OUT, True))
+        s = TensorStructure(legs)
+        lay = layout(s)
+        host = np.zeros(lay.size)
+        for b, (ot, it) in enumerate(s.keys):
+            (ps, ms), _, c = ot
+            (xs, pps), _, _ = it
+            if c != 1:
+                continue  # only the spin-1/2 coupled channel carries these operators
+            shape = tuple(int(x) for x in lay.shapes[b])
+            blk = np.zeros(shape)
+            for a, bb, v in rules:
+                if a not in dict(sl) or bb not in dict(sr):
+                    continue
+                xsec, xi = index(sl, a)
+                msec, mi = index(sr, bb)
+                if xsec == xs and msec == ms:
+                    blk[xi, 0, 0, mi] = v
+            o = int(lay.offsets[b])
+            host[o:o + blk.size] = blk.ravel()
+        sites.append(SymmetricTensor.from_numpy_arena(s, host))
+    return MPO(sites)
+
+
+class Env:
+    """``<psi|H|psi>`` environments keyed by directed bond (``network/env.py:435-645``):
+    ``F[(n, n+1)] = (ket IN, mpo OUT, bra OUT)`` from sites ``<= n``, ``F[(n, n-1)] =
+    (ket OUT, mpo IN, bra IN)`` from sites ``>= n``.  ``compiled=True`` runs ``heff2`` as a
+    CUDA-graph-captured chain program, rebuilt whenever the bond's tensors change."""
+
+    def __init__(self, psi: MPS, h: MPO, *, compiled: bool = True) -> None:
+        from tenet.structure import IN, Leg
+
+        self.psi, self.h, self.compiled = psi, h, compiled
+        n = len(psi)
+        kl, kr = psi[0].legs[0], psi[n - 1].legs[2]
+        wl, wr = h[0].legs[0], h[n - 1].legs[3]
+        self.F = {
+            (-1, 0): ones((Leg(kl.space, IN, kl.dual), Leg(wl.space, OUT, wl.dual),
+                           Leg(kl.space, OUT, kl.dual))),
+            (n, n - 1): ones((Leg(kr.space, OUT, kr.dual), Leg(wr.space, IN, wr.dual),
+                              Leg(kr.space, IN, kr.dual))),
+        }
+        self._prog: dict = {}
+
+    def setup_(self, to: int = 0) -> "Env":
+        for n in range(len(self.psi) - 1, 0, -1):
+            self.update_(n, to="first")
+        return self
+
+    def update_(self, n: int, *, to: str) -> None:
+        if to == "last":
+            self.F[n, n + 1] = env_update_last(self.F[n - 1, n], self.psi[n], self.h[n])
+        else:
+            self.F[n, n - 1] = env_update_first(self.F[n + 1, n], self.psi[n], self.h[n])
+
+    def clear_(self, *sites: int) -> None:
+        for n in sites:
+            self.F.pop((n, n - 1), None)
+            self.F.pop((n, n + 1), None)
+
+    def heff2(self, n: int, aa: SymmetricTensor) -> SymmetricTensor:
+        fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
+        if not self.compiled:
+            return heff2(fl, self.h[n], self.h[n + 1], fr, aa)
+        return self.matvec(n, aa.structure)(aa)
+
+    def matvec(self, n: int, structure):
+        """The graph-captured matvec of bond n for the current environments."""
+        from tenet.program import GraphMatvec, heff2_program
+
+        fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
+        key = (n, id(fl), id(fr), structure)
+        hit = self._prog.get(n)
+        if hit is None or hit[0] != key:
+            prog = heff2_program(fl, self.h[n], self.h[n + 1], fr, structure)
+            hit = (key, GraphMatvec(prog), (fl, fr))  # keep fl, fr alive with the key
+            self._prog[n] = hit
+        return hit[1]
+
+
+def _pair(left: SymmetricTensor, right: SymmetricTensor) -> SymmetricTensor:
+    from tenet import ops
+
+    return ops.einsum("apx,xqr->apqr", left, right)
+
+
+def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3):
+    """One left-to-right then right-to-left two-site sweep (``network/dmrg.py:321-542``,
+    noiseless branch).  Returns ``(energy, max discarded weight)``."""
+    from tenet import linalg, ops
+
+    n_sites = len(psi)
+    energy, max_dw = 0.0, 0.0
+    for direction in ("right", "left"):
+        forward = direction == "right"
+        bonds = range(n_sites - 1) if forward else range(n_sites - 2, -1, -1)
+        for n in bonds:
+            aa = _pair(psi[n], psi[n + 1])
+            matvec = (lambda v, n=n: env.heff2(n, v))
+            energy, aa = lanczos(matvec, aa, ncv=ncv)
+            u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff)
+            norm_s = ops.norm(s)
+            max_dw = max(max_dw, 1.0 - float(norm_s / ops.norm(aa)) ** 2)
+            s = s / norm_s
+            psi[n + 1] = vh
+            if forward:
+                psi[n] = u
+                psi[n + 1] = ops.einsum("xy,yqr->xqr", s, psi[n + 1])
+            else:
+                psi[n] = ops.einsum("apx,xy->apy", u, s)
+            psi.center = n + 1 if forward else n
+            env.clear_(n, n + 1)
+            if forward:
+                env.update_(n, to="last")
+            else:
+                env.update_(n + 1, to="first")
+    return energy, max_dw
+
+
+def dmrg_(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
+          max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True):
+    """Two-site DMRG to convergence (``network/dmrg.py:620-843``, flat ``chi``/``cutoff``,
+    no noise): returns ``(energy, history, psi)`` with ``history`` the per-sweep energies.
+    Stops on ``|dE| < energy_tol`` or after ``max_sweeps``."""
+    psi.canonize_(0)
+    env = Env(psi, h, compiled=compiled).setup_(0)
+    energy, history = float("inf"), []
+    for _ in range(max_sweeps):
+        old = energy
+        energy, _ = sweep_(psi, h, env, chi=chi, cutoff=cutoff, ncv=ncv)
+        history.append(energy)
+        if abs(old - energy) < energy_tol:
+            break
+    return energy, history, psi

@@ -328,3 +328,37 @@ def test_grouped_gemm_kinds_against_numpy(kind):
         for (M, N, K), (ao, bo, co) in zip(shapes, mats):
             want = A[ao:ao + M * K].reshape(M, K) @ B[bo:bo + K * N].reshape(K, N)
             close(C[co:co + M * N].reshape(M, N), want, 1e-13)
+
+
+def test_heisenberg_mpo_matches_reference_site_tensors(golden_dir):
+    """The SU(2) Heisenberg MPO builder against the reference's materialised W (L = 12)."""
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    mpo = network.heisenberg_mpo_su2(12)
+    for site, key in ((5, "w1"), (6, "w2")):
+        assert mpo[site].structure == struct(m[key]["legs"])
+        close(mpo[site].numpy_arena(), h[m[key]["arena"]], 1e-14)  # the reference splits S.S by an SVD
+    # boundary sites: same spaces as the reference's, up to the dual flag of a spin-0 leg
+    for site, key in ((0, "w_first"), (11, "w_last")):
+        got = [leg.space for leg in mpo[site].legs]
+        want = [leg.space for leg in struct(m[key]["legs"]).legs]
+        assert got == want
+
+
+@pytest.mark.parametrize("run", ["L12_chi32", "L16_chi24"])
+def test_dmrg_su2_matches_reference(golden_dir, run):
+    """Full two-site DMRG on the GPU: per-sweep energies and every kept bond space equal to
+    the reference's own run (``dmrg_`` at ncv = 20, cutoff 1e-10, same seeded start)."""
+    g = json.loads((golden_dir / "dmrg.json").read_text())[run]
+    L, chi = g["L"], g["chi"]
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
+             for i in range(L + 1)]
+    psi = network.MPS.random(phys, bonds, seed=0)
+    e, hist, psi = network.dmrg_(psi, network.heisenberg_mpo_su2(L), chi=chi, cutoff=1e-10,
+                                 ncv=20, max_sweeps=g["sweeps"], energy_tol=0.0)
+    assert len(hist) == g["sweeps"]
+    for got, want in zip(hist, g["history"]):
+        assert got == pytest.approx(want, rel=1e-10, abs=1e-10)
+    kept = [[[SU2.label(a), k] for a, k in psi[i].legs[0].space.sectors] for i in range(L)]
+    assert kept == g["bonds"], "kept bond sectors differ from the reference's"
