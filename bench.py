@@ -327,6 +327,15 @@ def run_tenet(args) -> None:
             fn()
         eager_ms[name] = timed(fn, args.steps) / args.steps
 
+    # the same graph-captured chain without programmatic dependent launch, for comparison
+    lib = _lib.load()
+    lib.tnb_set_pdl(0)
+    gm_plain = GraphMatvec(prog)
+    lib.tnb_set_pdl(1)
+    for _ in range(args.warmup):
+        gm_plain.replay()
+    eager_ms["graph_chain_without_pdl"] = timed(gm_plain.replay, args.steps) / args.steps
+
     for _ in range(args.warmup):
         gm.replay()
     torch.cuda.synchronize()

@@ -180,6 +180,15 @@ int tnb_axpby(int64_t n, double alpha, const double* x, double beta, const doubl
 int tnb_lincomb(int64_t n, int64_t k, const double* coeffs, const double* const* vecs,
                 double* out, void* stream);
 
+/*
+ * Enable (1) or disable (0) programmatic dependent launch for the table-driven kernels
+ * (tnb_block_gather, tnb_grouped_gemm_f64); returns the previous setting.  When enabled,
+ * each such kernel lets the next kernel of the stream begin loading its own static
+ * tables while it runs, and waits for the previous kernel's results before reading them;
+ * results are identical either way.  Default: enabled.
+ */
+int tnb_set_pdl(int enabled);
+
 /* Library version (major*10000 + minor*100 + patch). */
 int tnb_version(void);
 

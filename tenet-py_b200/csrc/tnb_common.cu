@@ -9,6 +9,9 @@ namespace tnb {
 __device__ int g_device_error = 0;
 
 static thread_local std::string g_last_error;
+static bool g_pdl = true;
+
+bool pdl_enabled() { return g_pdl; }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 
@@ -24,6 +27,12 @@ int check_launch(const char* what) {
 }  // namespace tnb
 
 extern "C" int tnb_version(void) { return 100; }
+
+extern "C" int tnb_set_pdl(int enabled) {
+  const int prev = tnb::g_pdl ? 1 : 0;
+  tnb::g_pdl = enabled != 0;
+  return prev;
+}
 
 extern "C" const char* tnb_last_error(void) { return tnb::g_last_error.c_str(); }
 

@@ -14,6 +14,8 @@
 // shared memory, then streams its elements.  The kernel is HBM-bound: algorithmic bytes per element
 // are 8 * (terms + 1).  A source term may be a strided window of a coupled-sector matrix
 // with its own leading dimension (see the row layout in tenet_b200.h).
+#include <string>
+
 #include "tnb_common.cuh"
 
 namespace tnb {
@@ -33,6 +35,7 @@ gather_kernel(const int64_t* __restrict__ segs, int64_t n_seg,
   __shared__ int64_t row[TNB_SEG_WIDTH];
   __shared__ int64_t t_src[kStagedTerms], t_ld[kStagedTerms];
   __shared__ double t_cf[kStagedTerms];
+  pdl_launch_dependents();
   const int64_t chunk = blockIdx.x;
   const int64_t seg = chunk_map[chunk];
   if (seg < 0 || seg >= n_seg) {
@@ -63,6 +66,7 @@ gather_kernel(const int64_t* __restrict__ segs, int64_t n_seg,
     t_cf[threadIdx.x] = term_coeff[t0 + threadIdx.x];
   }
   __syncthreads();
+  pdl_wait();  // the tables are static; the source may be the previous kernel's output
 
   // per-row dims and strides into registers (uniform across the CTA)
   uint32_t dims[TNB_MAX_RANK];
@@ -128,9 +132,13 @@ extern "C" int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const i
               "tnb_block_gather: term arrays are null");
   TNB_REQUIRE(dst0 != nullptr || dst1 != nullptr, "tnb_block_gather: no destination buffer");
   TNB_REQUIRE(total_chunks < (int64_t(1) << 31), "tnb_block_gather: too many chunks for one launch");
-  tnb::gather_kernel<<<static_cast<unsigned>(total_chunks), tnb::kGatherThreads, 0,
-                       tnb::as_stream(stream)>>>(seg_table, n_seg, chunk_map, term_src, term_coeff, term_ld, n_term,
-                                                 src0, n_src0, dst0, n_dst0, src1, n_src1,
-                                                 dst1, n_dst1);
+  cudaError_t e = tnb::launch(tnb::gather_kernel, static_cast<unsigned>(total_chunks),
+                              tnb::kGatherThreads, tnb::as_stream(stream), seg_table, n_seg,
+                              chunk_map, term_src, term_coeff, term_ld, n_term, src0, n_src0,
+                              dst0, n_dst0, src1, n_src1, dst1, n_dst1);
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_block_gather: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
   return tnb::check_launch("tnb_block_gather");
 }

@@ -16,6 +16,8 @@
 // The plain form computes in FP64 on the DFMA pipe; micro-tile rows/cols are strided so
 // shared-memory reads are conflict-free, and the next K slab is prefetched into
 // registers while the current one is consumed.
+#include <string>
+
 #include "tnb_common.cuh"
 
 namespace tnb {
@@ -70,6 +72,7 @@ gemm_f64_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   __shared__ GemmRow s_row;
   __shared__ int s_ok;
   __shared__ int s_last;
+  pdl_launch_dependents();
   const int64_t tile = blockIdx.x;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -95,6 +98,7 @@ gemm_f64_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   // this CTA's K range: the whole of K, or one split of it
   const int64_t kb = r.splits > 1 ? split * r.ksplit : 0;
   const int64_t ke = r.splits > 1 ? min(r.K, kb + r.ksplit) : r.K;
+  pdl_wait();  // A may be the previous kernel's output
 
   const int tx = tid % TX, ty = tid / TX;
   double acc[4][4];
@@ -209,6 +213,7 @@ gemm_f64_skinny_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   __shared__ double Bs[kSkinnyMax * kSkinnyMax];
   __shared__ GemmRow s_row;
   __shared__ int s_ok;
+  pdl_launch_dependents();
   const int64_t tile = blockIdx.x;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -223,6 +228,7 @@ gemm_f64_skinny_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   if (!s_ok) return;
   const GemmRow r = s_row;
   const int K = static_cast<int>(r.K), N = static_cast<int>(r.N);
+  pdl_wait();  // A may be the previous kernel's output
   if (tid < K * N) Bs[tid] = __ldg(b + r.boff + (tid / N) * r.ldb + (tid % N));
   __syncthreads();
   const int64_t m = (tile - r.tile_begin) * kSkinnyThreads + tid;
@@ -264,24 +270,27 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
   const int64_t n_parts = work_bytes > poff ? (work_bytes - poff) / 8 : 0;
   const unsigned grid = static_cast<unsigned>(total_tiles);
   cudaStream_t s = tnb::as_stream(stream);
+  cudaError_t e = cudaSuccess;
   switch (tile_kind) {
     case TNB_TILE_64:
-      tnb::gemm_f64_kernel<64, 64><<<grid, 256, 0, s>>>(gemm_table, n_gemm, tile_map, a, n_a,
-                                                        b, n_b, c, n_c, counters, n_counters,
-                                                        parts, n_parts);
+      e = tnb::launch(tnb::gemm_f64_kernel<64, 64>, grid, 256, s, gemm_table, n_gemm, tile_map,
+                      a, n_a, b, n_b, c, n_c, counters, n_counters, parts, n_parts);
       break;
     case TNB_TILE_32:
-      tnb::gemm_f64_kernel<32, 32><<<grid, 64, 0, s>>>(gemm_table, n_gemm, tile_map, a, n_a,
-                                                       b, n_b, c, n_c, counters, n_counters,
-                                                       parts, n_parts);
+      e = tnb::launch(tnb::gemm_f64_kernel<32, 32>, grid, 64, s, gemm_table, n_gemm, tile_map,
+                      a, n_a, b, n_b, c, n_c, counters, n_counters, parts, n_parts);
       break;
     case TNB_TILE_SKINNY:
-      tnb::gemm_f64_skinny_kernel<<<grid, tnb::kSkinnyThreads, 0, s>>>(
-          gemm_table, n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
+      e = tnb::launch(tnb::gemm_f64_skinny_kernel, grid, tnb::kSkinnyThreads, s, gemm_table,
+                      n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
       break;
     default:
       tnb::set_error("tnb_grouped_gemm_f64: unknown tile kind");
       return TNB_EINVAL;
+  }
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_grouped_gemm_f64: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
   }
   return tnb::check_launch("tnb_grouped_gemm_f64");
 }

@@ -28,6 +28,7 @@ SIGNATURES = {
     "tnb_weighted_dot_noalloc": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp]),
     "tnb_axpby": (_i32, [_i64, _f64, _vp, _f64, _vp, _vp, _vp]),
     "tnb_lincomb": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp]),
+    "tnb_set_pdl": (_i32, [_i32]),
     "tnb_version": (_i32, []),
     "tnb_last_error": (ctypes.c_char_p, []),
     "tnb_device_error": (_i32, [ctypes.POINTER(ctypes.c_int), _vp]),

@@ -362,3 +362,25 @@ def test_dmrg_su2_matches_reference(golden_dir, run):
         assert got == pytest.approx(want, rel=1e-10, abs=1e-10)
     kept = [[[SU2.label(a), k] for a, k in psi[i].legs[0].space.sectors] for i in range(L)]
     assert kept == g["bonds"], "kept bond sectors differ from the reference's"
+
+
+def test_programmatic_dependent_launch_changes_nothing(golden_dir):
+    """The chain with and without programmatic dependent launch: bit-identical results."""
+    from tenet.program import GraphMatvec, heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    lib = _lib.load()
+    outs = []
+    try:
+        for flag in (0, 1):
+            lib.tnb_set_pdl(flag)
+            prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
+            gm = GraphMatvec(prog)
+            outs.append([gm(T["aa"]).numpy_arena() for _ in range(3)])
+    finally:
+        lib.tnb_set_pdl(1)
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    close(outs[1][0], h[m["heff_aa"]["arena"]])
