@@ -534,6 +534,16 @@ def einsum(equation: str, *ops: Tensor) -> Tensor:
     terms = lhs.split(",")
     if len(ops) == 1:
         return transpose(ops[0], tuple(terms[0].index(x) for x in out))
+    if len(ops) > 2:
+        # three or more operands: pairwise, left to right (a valid contraction path; the
+        # reference's order comes from opt_einsum and differs only in rounding here)
+        acc, at = ops[0], terms[0]
+        for k in range(1, len(ops)):
+            later = set(out).union(*map(set, terms[k + 1:]))
+            mid = "".join([x for x in at if x in later] + [x for x in terms[k] if x in later])
+            acc = einsum(f"{at},{terms[k]}->{mid}", acc, ops[k])
+            at = mid
+        return transpose(acc, tuple(at.index(x) for x in out))
     shared = [x for x in terms[0] if x in terms[1]]
     axes = (tuple(terms[0].index(x) for x in shared), tuple(terms[1].index(x) for x in shared))
     free = [x for x in terms[0] if x not in shared] + [x for x in terms[1] if x not in shared]
@@ -705,3 +715,98 @@ def keys_from_json(keys_json) -> tuple:
     def tree(t):
         return (tuple(t[0]), tuple(t[1]), t[2])
     return tuple((tree(o), tree(i)) for o, i in keys_json)
+
+
+# ---------------------------------------------------------------------------------------
+# C4v CTMRG, single layer  (network/ctmrg.py:166-660, examples/toy_codes/ctmrg.py:547-592)
+
+
+def identity_tensor(p: Provider, leg: Leg) -> Tensor:
+    """``identity((leg,))``: legs ``(leg OUT, leg IN)``, eye per coupled sector
+    (``ops/map.py:175-234``)."""
+    s = Structure(p, (replace(leg, side=OUT), replace(leg, side=IN)))
+    return from_matrices(s, {c: np.eye(nr) for c, (_, _, nr, nc) in map_layout(s).items()})
+
+
+def ones(s: Structure) -> Tensor:
+    return Tensor(s, [np.ones(block_shape(s, k)) for k in block_order(s)])
+
+
+def ctm_seed(bulk: Tensor):
+    """``init_env(bulk, Leg(bulk.legs[0].space, IN))`` (``network/ctmrg.py:337-385``)."""
+    p = bulk.structure.provider
+    unit = Leg(((p.unit(), 1),), OUT)
+    c = identity_tensor(p, unit)
+    e = ones(Structure(p, (Leg(unit.sectors, IN), Leg(unit.sectors, OUT),
+                           Leg(bulk.legs[0].sectors, IN))))
+    return c, e
+
+
+def ctm_corner(c: Tensor, e: Tensor, bulk: Tensor) -> Tensor:
+    """``einsum("ab,ace,fbg,gehi->chfi", c, e, e, bulk)`` (``network/ctmrg.py:238-244``),
+    contracted left to right."""
+    t = einsum("ab,ace->bce", c, e)
+    t = einsum("bce,fbg->cefg", t, e)
+    return einsum("cefg,gehi->chfi", t, bulk)
+
+
+def ctm_edge(e: Tensor, p: Tensor, bulk: Tensor) -> Tensor:
+    """``network/ctmrg.py:246-253``."""
+    big = einsum("abe,gehi->abghi", e, bulk)
+    t = einsum("abghi,agx->bhix", big, p)
+    return einsum("bhix,bhy->xyi", t, adjoint(p))
+
+
+def ctm_move(c: Tensor, e: Tensor, bulk: Tensor, chi: int):
+    """One C4v move (``network/ctmrg.py:451-526``): new corner = the singular values."""
+    big = ctm_corner(c, e, bulk)
+    p, s, _ = svd_truncated(big, ((0, 1), (2, 3)), max_bond=chi)
+    new_e = ctm_edge(e, p, bulk)
+    return scale(s, 1.0 / norm(s)), scale(new_e, 1.0 / norm(new_e)), p.structure.legs[-1].sectors
+
+
+def corner_spectrum(s: Tensor) -> list:
+    """Diagonal values times sqrt(qdim), descending (``network/common.py:147-194``)."""
+    p = s.structure.provider
+    out = []
+    for c, m in to_matrices(s).items():
+        out.extend(float(v) * p.qdim(c) ** 0.5 for v in np.diag(m))
+    return sorted(out, reverse=True)
+
+
+def _spectrum_change(old, new) -> float:
+    n = max(len(old), len(new))
+    a = np.array(list(old) + [0.0] * (n - len(old)))
+    b = np.array(list(new) + [0.0] * (n - len(new)))
+    return float(np.abs(a - b).max()) if n else 0.0
+
+
+def ctmrg(bulk: Tensor, *, chi: int, tol: float, max_sweeps: int):
+    """The move loop to a corner-spectrum tolerance (``network/ctmrg.py:572-660``)."""
+    c, e = ctm_seed(bulk)
+    prev, history, bond = corner_spectrum(c), [], None
+    for _ in range(max_sweeps):
+        c, e, bond = ctm_move(c, e, bulk, chi)
+        cur = corner_spectrum(c)
+        history.append(_spectrum_change(prev, cur))
+        prev = cur
+        if history[-1] < tol:
+            break
+    return c, e, bond, history
+
+
+def full_trace(t: Tensor) -> float:
+    """``sum_c qdim(c) tr(M_c)`` (``ops/contraction.py:440-514``)."""
+    p = t.structure.provider
+    return float(sum(p.qdim(c) * np.trace(m) for c, m in to_matrices(t).items()))
+
+
+def beta_free_energy(c: Tensor, e: Tensor, bulk: Tensor) -> float:
+    """``beta f = -ln kappa``, Baxter's corner-transfer ratio on the converged environment
+    (``examples/toy_codes/ctmrg.py:547-592`` with no unrolled moves)."""
+    cc, ca, ec, ea = c, adjoint(c), e, adjoint(e)
+    z_c = full_trace(einsum("ab,ac,dc,eb->de", cc, ca, cc, ca))
+    z_h = full_trace(einsum("ab,ac,dcf,ed,eg,ghf->hb", cc, ca, ea, cc, ca, ec))
+    z_a = full_trace(einsum("ab,acp,cd,edq,fe,gfr,gh,hks,spqr->kb",
+                            cc, ec, ca, ea, cc, ea, ca, ec, bulk))
+    return -float(np.log(z_a * z_c / z_h ** 2))

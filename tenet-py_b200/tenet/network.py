@@ -356,3 +356,109 @@ def dmrg_(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 
         if abs(old - energy) < energy_tol:
             break
     return energy, history, psi
+
+
+# ---------------------------------------------------------------------------------------
+# C4v CTMRG, single layer  (network/ctmrg.py:166-660)
+
+
+def ising_bulk(beta: float) -> SymmetricTensor:
+    """Classical 2D Ising transfer tensor on Z2 legs ``(l OUT, u OUT, r IN, d IN)``: the
+    weights ``sum_s W[s,l] W[s,u] W[s,r] W[s,d]`` with ``W = [[sqrt cosh b, sqrt sinh b],
+    [sqrt cosh b, -sqrt sinh b]]`` (the splitting of ``examples/toy_codes/ctmrg.py:162-187``),
+    which is already the parity basis, so each Z2 block is one dense entry."""
+    import math
+
+    from tenet.structure import IN, GradedSpace, Leg, TensorStructure, layout
+    from tenet.symmetry import Z2
+
+    c, s = math.sqrt(math.cosh(beta)), math.sqrt(math.sinh(beta))
+    w = np.array([[c, s], [c, -s]])
+    dense = np.einsum("sl,su,sr,sd->lurd", w, w, w, w)
+    space = GradedSpace.new(Z2, {Z2.sector(0): 1, Z2.sector(1): 1})
+    st = TensorStructure((Leg(space, OUT), Leg(space, OUT), Leg(space, IN), Leg(space, IN)))
+    lay = layout(st)
+    host = np.zeros(lay.size)
+    for b, (ot, it) in enumerate(st.keys):
+        (lu, _, _), (rd, _, _) = ot, it
+        host[int(lay.offsets[b])] = dense[lu[0], lu[1], rd[0], rd[1]]
+    return SymmetricTensor.from_numpy_arena(st, host)
+
+
+class Absorb:
+    """The single-layer absorption pair over one bulk tensor (``network/ctmrg.py:217-253``)."""
+
+    def __init__(self, bulk: SymmetricTensor) -> None:
+        self.bulk = bulk
+
+    def corner(self, c: SymmetricTensor, e: SymmetricTensor) -> SymmetricTensor:
+        return ops.einsum("ab,ace,fbg,gehi->chfi", c, e, e, self.bulk)
+
+    def edge(self, e: SymmetricTensor, p: SymmetricTensor) -> SymmetricTensor:
+        big = ops.einsum("abe,gehi->abghi", e, self.bulk)
+        return ops.einsum("abghi,agx,bhy->xyi", big, p, ops.adjoint(p))
+
+
+def single_layer_ctm(bulk: SymmetricTensor):
+    """``(absorber, c, e)``: the seed corner is the identity on the unit sector and the seed
+    edge ones on ``(unit IN, unit OUT, bulk bond IN)`` (``network/ctmrg.py:337-410``)."""
+    from tenet.structure import IN, GradedSpace, Leg
+
+    p = bulk.provider
+    unit = GradedSpace.new(p, {p.unit: 1})
+    c = ops.identity((Leg(unit, OUT),))
+    e = ones((Leg(unit, IN), Leg(unit, OUT), Leg(bulk.legs[0].space, IN)))
+    return Absorb(bulk), c, e
+
+
+def spectrum(s: SymmetricTensor) -> list[float]:
+    """Diagonal of a singular-value tensor times sqrt(qdim), descending
+    (``network/common.py:147-194``)."""
+    from tenet.linalg import singular_values
+
+    p = s.provider
+    out = []
+    for c, vals in singular_values(s).items():
+        out.extend(float(v) * p._qdim(c) ** 0.5 for v in vals)
+    return sorted(out, reverse=True)
+
+
+def move(c: SymmetricTensor, e: SymmetricTensor, absorb: Absorb, *, chi: int):
+    """One C4v move (``network/ctmrg.py:451-526``): the enlarged corner's truncated SVD;
+    the new corner is the singular-value tensor, the new edge is projected with ``u``."""
+    from tenet import linalg
+
+    big = absorb.corner(c, e)
+    n = big.ndim // 2
+    p, s, _ = linalg.svd_truncated(big, (tuple(range(n)), tuple(range(n, 2 * n))), max_bond=chi)
+    e2 = absorb.edge(e, p)
+    return s / ops.norm(s), e2 / ops.norm(e2), p.legs[-1].space
+
+
+def ctmrg(absorb: Absorb, c: SymmetricTensor, e: SymmetricTensor, *, chi: int,
+          tol: float = 1e-10, max_sweeps: int = 100):
+    """Moves until the corner spectrum changes by less than ``tol`` (``network/ctmrg.py:572-660``).
+    Returns ``(c, e, bond, history)``."""
+    prev, history, bond = spectrum(c), [], None
+    for _ in range(max_sweeps):
+        c, e, bond = move(c, e, absorb, chi=chi)
+        cur = spectrum(c)
+        n = max(len(prev), len(cur))
+        a = np.array(prev + [0.0] * (n - len(prev)))
+        b = np.array(cur + [0.0] * (n - len(cur)))
+        history.append(float(np.abs(a - b).max()))
+        prev = cur
+        if history[-1] < tol:
+            break
+    return c, e, bond, history
+
+
+def beta_free_energy(c: SymmetricTensor, e: SymmetricTensor, bulk: SymmetricTensor) -> float:
+    """``beta f = -ln kappa`` from the environment, Baxter's corner-transfer ratio
+    (``examples/toy_codes/ctmrg.py:547-592`` with no unrolled moves)."""
+    cc, ca, ec, ea = c, ops.adjoint(c), e, ops.adjoint(e)
+    z_c = ops.full_trace(ops.einsum("ab,ac,dc,eb->de", cc, ca, cc, ca))
+    z_h = ops.full_trace(ops.einsum("ab,ac,dcf,ed,eg,ghf->hb", cc, ca, ea, cc, ca, ec))
+    z_a = ops.full_trace(ops.einsum("ab,acp,cd,edq,fe,gfr,gh,hks,spqr->kb",
+                                    cc, ec, ca, ea, cc, ea, ca, ec, bulk))
+    return -float(np.log(z_a * z_c / z_h ** 2))

@@ -30,8 +30,9 @@ from tenet.structure import IN, OUT, TensorStructure, layout, matrix_layout
 from tenet.symmetry import CapabilityError
 from tenet.tensor import SymmetricTensor
 
-__all__ = ["add", "adjoint", "compose", "contractible", "divide", "einsum", "inner", "multiply",
-           "norm", "outward_dual", "repartition", "subtract", "tensordot", "transpose"]
+__all__ = ["add", "adjoint", "compose", "contractible", "divide", "einsum", "full_trace",
+           "identity", "inner", "multiply", "norm", "outward_dual", "repartition", "subtract",
+           "tensordot", "transpose"]
 
 
 # ---------------------------------------------------------------------------------------
@@ -310,3 +311,47 @@ def multiply(t: SymmetricTensor, s) -> SymmetricTensor:
 
 def divide(t: SymmetricTensor, s) -> SymmetricTensor:
     return _axpby(1.0 / float(s), t, 0.0, t)
+
+
+# ---------------------------------------------------------------------------------------
+# identity and trace
+
+
+def identity(legs) -> SymmetricTensor:
+    """``id`` on the legs: ``(*legs OUT, *legs IN)``, one eye per coupled sector
+    (``ops/map.py:175-234``)."""
+    import numpy as np
+
+    from tenet.linalg import _raise_exec
+    from tenet.structure import Leg
+
+    legs = tuple(legs)
+    s = TensorStructure((*(Leg(l.space, OUT, l.dual, l.name) for l in legs),
+                         *(Leg(l.space, IN, l.dual, l.name) for l in legs)))
+    ml = matrix_layout(s)
+    host = np.zeros(ml.size)
+    for c in ml.sectors:
+        r, q = ml.shape[c]
+        host[ml.base[c]:ml.base[c] + r * q] = np.eye(r, q).ravel()
+    out = SymmetricTensor.empty(s)
+    _raise_exec(s).run(torch.from_numpy(host).to(out.arena.device), out.arena)
+    return out
+
+
+def full_trace(t: SymmetricTensor) -> float:
+    """``sum_c qdim(c) tr(M_c)`` of an endomorphism (``ops/contraction.py:440-514``)."""
+    from tenet.linalg import _lower_exec
+
+    s = t.structure
+    m, lower = _lower_exec(s, s.out_axes, s.in_axes)
+    ml = matrix_layout(m)
+    buf = torch.empty(ml.size, dtype=torch.float64, device=t.arena.device)
+    lower.run(t.arena, buf)
+    p = t.provider
+    total = 0.0
+    for c in ml.sectors:
+        r, q = ml.shape[c]
+        if r != q:
+            raise ValueError("full_trace: the tensor is not an endomorphism (non-square sector)")
+        total += p._qdim(c) * float(torch.diagonal(buf[ml.base[c]:ml.base[c] + r * q].view(r, q)).sum())
+    return total

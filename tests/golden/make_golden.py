@@ -18,6 +18,9 @@ here is the reference's own output on seeded inputs:
   mid-chain bond (site-tensor path), its Lanczos ground energy at ``ncv=20``, and the
   truncated SVD of the result;
 * ``dmrg.json``: reference DMRG energies and per-bond kept sectors;
+* ``ctmrg.json``: Z2 Ising CTMRG (beta = 0.44 at chi = 16 and 128 for a fixed number of
+  moves; beta = 0.40, chi = 16 to convergence): per-sweep corner-spectrum changes, final
+  corner spectrum and bond sectors, the reference's beta f estimate and Onsager's;
 * ``su2_f_sample.txt``: every 37th row of the reference's F-symbol fixture with the
   value the reference's F-symbol route returns.
 
@@ -275,6 +278,35 @@ def make_dmrg() -> dict:
     return runs
 
 
+def make_ctmrg(ref: Path) -> dict:
+    """Z2 CTMRG of the 2D Ising model (``network/ctmrg.py:451-660``): beta = 0.44 near the
+    critical point (a fixed number of moves, chi = 16 and 128) and beta = 0.40 run to its
+    1e-10 tolerance with the reference's free-energy estimator on the result."""
+    sys.path.insert(0, str(ref / "examples" / "toy_codes"))
+    import ctmrg as toy  # examples/toy_codes/ctmrg.py: ising_bulk, beta_free_energy, onsager
+
+    from tenet.network import ctmrg, single_layer_ctm
+    from tenet.network.common import spectrum
+
+    out = {}
+    for name, beta, chi, tol, sweeps in (("b044_chi16", 0.44, 16, 0.0, 60),
+                                         ("b044_chi128", 0.44, 128, 0.0, 20),
+                                         ("b040_chi16", 0.40, 16, 1e-10, 200)):
+        bulk = toy.ising_bulk(beta)
+        res = ctmrg(*single_layer_ctm(bulk), chi=chi, tol=tol, max_sweeps=sweeps)
+        c, e, bond = res.env
+        out[name] = {
+            "beta": beta, "chi": chi, "tol": tol, "max_sweeps": sweeps, "sweeps": res.sweeps,
+            "converged": bool(res.converged), "history": [float(x) for x in res.history],
+            "spectrum": spectrum(c), "bond": [[_sector_int(a), m] for a, m in bond.sectors],
+            "bulk": {"legs": _legs(bulk), "keys": _keys(bulk), "arena": _arena(bulk).tolist()},
+        }
+        if res.converged:
+            out[name]["beta_f"] = float(toy.beta_free_energy(beta, res.env, k=0))
+            out[name]["onsager_beta_f"] = float(toy.onsager(beta))
+    return out
+
+
 def make_f_sample(ref: Path) -> None:
     from tenet.symmetry import SU2, SU2Sector
 
@@ -301,6 +333,7 @@ def main() -> None:
     hs.meta = make_heff(hs)
     hs.dump("heff")
     (HERE / "dmrg.json").write_text(json.dumps(make_dmrg(), indent=1))
+    (HERE / "ctmrg.json").write_text(json.dumps(make_ctmrg(ref)))
     make_f_sample(ref)
 
 

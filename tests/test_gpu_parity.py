@@ -384,3 +384,24 @@ def test_programmatic_dependent_launch_changes_nothing(golden_dir):
     for a, b in zip(outs[0], outs[1]):
         assert np.array_equal(a, b)
     close(outs[1][0], h[m["heff_aa"]["arena"]])
+
+
+@pytest.mark.parametrize("name", ["b044_chi16", "b040_chi16", "b044_chi128"])
+def test_ctmrg_z2_ising_matches_reference(golden_dir, name):
+    """Z2 Ising CTMRG on the GPU against the reference's runs: the bulk tensor, the sweep
+    count, every per-sweep corner-spectrum change, the final spectrum, the even/odd bond
+    split, and (converged run) the free energy vs the reference and Onsager."""
+    r = json.loads((golden_dir / "ctmrg.json").read_text())[name]
+    bulk = network.ising_bulk(r["beta"])
+    assert bulk.structure == struct(r["bulk"]["legs"])
+    close(bulk.numpy_arena(), np.array(r["bulk"]["arena"]), 1e-14)
+    c, e, bond, hist = network.ctmrg(*network.single_layer_ctm(bulk), chi=r["chi"], tol=r["tol"],
+                                     max_sweeps=r["max_sweeps"])
+    assert len(hist) == r["sweeps"]
+    np.testing.assert_allclose(hist, r["history"], rtol=1e-5, atol=1e-10)
+    np.testing.assert_allclose(network.spectrum(c), r["spectrum"], rtol=1e-8, atol=1e-12)
+    assert [[Z2.label(a), m] for a, m in bond.sectors] == r["bond"]
+    if "beta_f" in r:
+        bf = network.beta_free_energy(c, e, bulk)
+        assert bf == pytest.approx(r["beta_f"], rel=1e-10)
+        assert bf == pytest.approx(r["onsager_beta_f"], rel=1e-6)

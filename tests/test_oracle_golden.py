@@ -122,3 +122,21 @@ def test_su2_r_and_frobenius_schur():
                     for c in range(abs(a - b), a + b + 1, 2)]
             m = np.concatenate(rows, axis=1)
             assert np.allclose(m.T @ m, np.eye(m.shape[1]), atol=1e-14)
+
+
+def test_ctmrg_matches_reference(golden_dir):
+    """Z2 Ising CTMRG: sweeps, per-sweep spectrum change, corner spectrum, bond split and
+    the free-energy estimate against the reference's own runs."""
+    g = json.loads((golden_dir / "ctmrg.json").read_text())
+    for name in ("b044_chi16", "b040_chi16"):
+        r = g[name]
+        bs = O.structure_from_json(r["bulk"]["legs"])
+        bulk = O.from_arena(bs, np.array(r["bulk"]["arena"]))
+        c, e, bond, hist = O.ctmrg(bulk, chi=r["chi"], tol=r["tol"], max_sweeps=r["max_sweeps"])
+        assert len(hist) == r["sweeps"]
+        np.testing.assert_allclose(hist, r["history"], rtol=1e-6, atol=1e-11)
+        np.testing.assert_allclose(O.corner_spectrum(c), r["spectrum"], rtol=1e-9, atol=1e-12)
+        assert [list(x) for x in bond] == r["bond"]
+        if "beta_f" in r:
+            assert O.beta_free_energy(c, e, bulk) == pytest.approx(r["beta_f"], rel=1e-10)
+            assert O.beta_free_energy(c, e, bulk) == pytest.approx(r["onsager_beta_f"], rel=1e-6)
