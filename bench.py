@@ -336,6 +336,21 @@ def run_tenet(args) -> None:
         gm_plain.replay()
     eager_ms["graph_chain_without_pdl"] = timed(gm_plain.replay, args.steps) / args.steps
 
+    # the precision form: every non-skinny sector product on the tcgen05 tensor cores
+    mixed = {}
+    ref_out = prog(aa).numpy_arena()
+    for precision in ("3xbf16", "tf32"):
+        mprog = heff2_program(fl, w1, w2, fr, aa.structure, precision=precision)
+        mg = GraphMatvec(mprog)
+        mg.x.copy_(aa.arena)
+        for _ in range(args.warmup):
+            mg.replay()
+        mms = timed(mg.replay, args.steps) / args.steps
+        got = mg(aa).numpy_arena()
+        mixed[precision] = {
+            "ms_per_matvec": mms, "tflops": flops / (mms * 1e-3) / 1e12,
+            "rel_error_vs_f64": float(np.linalg.norm(got - ref_out) / np.linalg.norm(ref_out))}
+
     for _ in range(args.warmup):
         gm.replay()
     torch.cuda.synchronize()
@@ -437,6 +452,7 @@ def run_tenet(args) -> None:
             "forms_tflops": {"graph_chain": flops / (ms / args.steps * 1e-3) / 1e12,
                              **{k: flops / (v * 1e-3) / 1e12 for k, v in eager_ms.items()}},
             "launches_per_matvec_eager_ops": launches_eager,
+            "mixed_precision_forms": mixed,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),

@@ -34,6 +34,7 @@ extern "C" {
 #define TNB_EINVAL 1   /* bad argument (null pointer, negative size, bad table)   */
 #define TNB_ECUDA 2    /* a CUDA runtime call failed                               */
 #define TNB_EBOUNDS 3  /* a kernel saw an out-of-range table entry                 */
+#define TNB_ETIMEOUT 4 /* a kernel gave up a bounded wait (tensor-core completion)  */
 
 /* Maximum tensor rank a gather segment may carry. */
 #define TNB_MAX_RANK 8
@@ -109,11 +110,19 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
  *   TNB_TILE_64      64 x 64 output tiles (tiles = ceil(M/64) * ceil(N/64))
  *   TNB_TILE_32      32 x 32 output tiles, for compositions too small to fill the GPU
  *   TNB_TILE_SKINNY  256 output rows per tile (tiles = ceil(M/256)); needs N, K <= 16
+ *   TNB_TILE_TC_TF32    128 x 64 tiles on the tcgen05 tensor cores, operands rounded to
+ *                       TF32, FP32 accumulation (tiles = ceil(M/128) * ceil(N/64))
+ *   TNB_TILE_TC_3XBF16  same tiles, operands split into BF16 hi + lo pairs and the product
+ *                       taken as hi.hi + hi.lo + lo.hi, FP32 accumulation
+ * The tensor-core kinds read and write FP64 like the others; only the arithmetic inside
+ * is reduced, and they take no split-K.
  */
 #define TNB_GEMM_WIDTH 16
 #define TNB_TILE_64 0
 #define TNB_TILE_32 1
 #define TNB_TILE_SKINNY 2
+#define TNB_TILE_TC_TF32 3
+#define TNB_TILE_TC_3XBF16 4
 
 /*
  * Grouped FP64 GEMM over uneven coupled sectors, one launch for every sector.

@@ -284,6 +284,11 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
       e = tnb::launch(tnb::gemm_f64_skinny_kernel, grid, tnb::kSkinnyThreads, s, gemm_table,
                       n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
       break;
+    case TNB_TILE_TC_TF32:
+    case TNB_TILE_TC_3XBF16:
+      e = tnb::launch_gemm_tc(tile_kind, grid, s, gemm_table, n_gemm, tile_map, a, n_a, b, n_b,
+                              c, n_c);
+      break;
     default:
       tnb::set_error("tnb_grouped_gemm_f64: unknown tile kind");
       return TNB_EINVAL;

@@ -28,7 +28,8 @@ SEG_W = 40
 GEMM_W = 16
 CHUNK = 1024
 MAX_RANK = 8
-TILE_64, TILE_32, TILE_SKINNY = 0, 1, 2
+TILE_64, TILE_32, TILE_SKINNY, TILE_TC_TF32, TILE_TC_3XBF16 = 0, 1, 2, 3, 4
+TC_KINDS = {"tf32": TILE_TC_TF32, "3xbf16": TILE_TC_3XBF16}
 SKINNY_ROWS, SKINNY_MAX = 256, 16
 N_SM = 148
 
@@ -289,12 +290,16 @@ class GemmTable:
                   c.numel(), ptr(self._dev[2]) if self.work_bytes else None, self.work_bytes,
                   self.n_counters, stream_ptr())
         if _LOG is not None:
-            _LOG.end("grouped_gemm_f64", mark, self.flops)
+            _LOG.end("grouped_gemm_tc" if self.kind in (TILE_TC_TF32, TILE_TC_3XBF16)
+                     else "grouped_gemm_f64", mark, self.flops)
 
 
 def _tiles(M, N, kind):
     if kind == TILE_SKINNY:
         return (M + SKINNY_ROWS - 1) // SKINNY_ROWS, 1
+    if kind in (TILE_TC_TF32, TILE_TC_3XBF16):
+        tn = (N + 63) // 64
+        return ((M + 127) // 128) * tn, tn
     t = 64 if kind == TILE_64 else 32
     tn = (N + t - 1) // t
     return ((M + t - 1) // t) * tn, tn
@@ -320,12 +325,13 @@ class GemmGroup:
     """One composition's products, split into at most two launches: the tall skinny ones
     and the rest (so an MPO-like product never occupies a 64-wide tile)."""
 
-    def __init__(self, products) -> None:
+    def __init__(self, products, precision: str = "f64") -> None:
         skinny = [p for p in products if _is_skinny(p)]
         rest = [p for p in products if not _is_skinny(p)]
         self.parts = []
         if rest:
-            self.parts.append(make_gemm(rest, choose_kind(rest)))
+            kind = TC_KINDS[precision] if precision in TC_KINDS else choose_kind(rest)
+            self.parts.append(make_gemm(rest, kind))
         if skinny:
             self.parts.append(make_gemm(skinny, TILE_SKINNY))
         self.flops = sum(p.flops for p in self.parts)
@@ -359,14 +365,14 @@ def make_gemm(products, kind: int | None = None, split_k: bool = True) -> GemmTa
     products = [p for p in products if p[0] and p[1]]
     if kind is None:
         kind = choose_kind(products)
-    tw = 64 if kind == TILE_64 else 32
+    tw = 64 if kind == TILE_64 else 32  # split-K partial tile width (tiled FP64 kinds only)
     out_total = sum(_tiles(p[0], p[1], kind)[0] for p in products)
     rows = []
     tile = flops = n_cnt = n_parts = 0
     for M, N, K, ao, lda, bo, ldb, co, ldc in products:
         out_tiles, tn = _tiles(M, N, kind)
         S, ks = (1, 0)
-        if split_k and kind != TILE_SKINNY:
+        if split_k and kind in (TILE_64, TILE_32):
             S, ks = _splits(K, out_total)
         row = [M, N, K, ao, lda, bo, ldb, co, ldc, tile, tn, out_tiles * S, 0, 0, 0, 0]
         if S > 1:

@@ -38,7 +38,7 @@ def _identity_plan(s: TensorStructure):
 class _Link:
     """One contraction of the chain, with its gathers and GEMM table."""
 
-    def __init__(self, src_struct, src_kind, a_plan, b_tensor, b_plan, axes):
+    def __init__(self, src_struct, src_kind, a_plan, b_tensor, b_plan, axes, precision="f64"):
         ca, cb = axes
         sa_logical = a_plan[0]
         sb_logical = b_plan[0]
@@ -75,7 +75,7 @@ class _Link:
             _exec.gather_rows(src_struct, src_kind, sa2, "matrix", pa, ta, 0, keep_a))
         self.b_gather = _exec.make_gather(
             _exec.gather_rows(b_tensor.structure, "arena", sb2, "matrix", pb, tb, 0, keep_b))
-        self.gemm = _exec.GemmGroup(products)
+        self.gemm = _exec.GemmGroup(products, precision)
         self.c_struct = sc
         self.a_size, self.b_size, self.c_size = ma.size, mb.size, mc.size
         self.b_tensor = b_tensor
@@ -84,7 +84,10 @@ class _Link:
 class ChainProgram:
     """``y = chain(x)`` for a fixed input structure; see the module docstring."""
 
-    def __init__(self, in_struct: TensorStructure) -> None:
+    def __init__(self, in_struct: TensorStructure, precision: str = "f64") -> None:
+        """``precision``: "f64" (the plain FP64 form), or "tf32" / "3xbf16" to run every
+        coupled-sector product that is not tall-and-thin on the tcgen05 tensor cores."""
+        self.precision = precision
         self.in_struct = in_struct
         self.src = (in_struct, "arena")
         self.pending = _identity_plan(in_struct)
@@ -107,7 +110,7 @@ class ChainProgram:
 
     def contract(self, b: SymmetricTensor, axes, b_plan=None) -> ChainProgram:
         b_plan = b_plan or _identity_plan(b.structure)
-        link = _Link(self.src[0], self.src[1], self.pending, b, b_plan, axes)
+        link = _Link(self.src[0], self.src[1], self.pending, b, b_plan, axes, self.precision)
         self.links.append(link)
         self.src = (link.c_struct, "matrix")
         self.pending = link.after
@@ -214,11 +217,11 @@ class GraphMatvec:
         self.graph.replay()
 
 
-def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = True
-                  ) -> ChainProgram:
+def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = True,
+                  precision: str = "f64") -> ChainProgram:
     """The site-tensor two-site matvec (``network/env.py:416-432``) as a chain program.
     ``fl``, ``w1``, ``w2``, ``fr`` need only ``.structure`` when ``allocate`` is False."""
-    p = ChainProgram(in_struct)
+    p = ChainProgram(in_struct, precision)
     p.einsum("apqr,rys->apqys", fr)
     p.einsum("apqys,mQqy->apQms", w2, bend="q")
     p.einsum("apQms,xPpm->aPQxs", w1, bend="p")

@@ -1,0 +1,70 @@
+"""The tcgen05 tensor-core GEMM kinds (TF32 and 3xBF16) against FP64.
+
+The precision form of the block GEMMs: FP64 in and out, reduced arithmetic inside.  The
+bounds are written as relative Frobenius errors: TF32 keeps 11 significand bits of each
+operand (error ~ 2^-11), the 3xBF16 split keeps ~16 (error ~ 2^-16), both with FP32
+accumulation.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle.tenet_oracle as O
+from tenet import _exec, _lib
+
+pytestmark = pytest.mark.gpu
+
+TOL = {3: 5e-3, 4: 5e-5}
+
+
+@pytest.fixture(autouse=True)
+def _device_error_clear():
+    yield
+    torch.cuda.synchronize()
+    assert _lib.device_error(0) == 0, "a kernel raised the device error word"
+
+
+@pytest.mark.parametrize("kind", [3, 4])
+def test_tensorcore_gemm_kinds(kind):
+    rng = np.random.default_rng(kind)
+    shapes = [(176, 236, 60), (9, 11, 2), (300, 200, 500), (40, 7, 0), (128, 64, 32),
+              (129, 65, 33), (1, 1, 1)]
+    a_off = b_off = c_off = 0
+    prods, offs = [], []
+    for M, N, K in shapes:
+        prods.append((M, N, K, a_off, K, b_off, N, c_off, N))
+        offs.append((a_off, b_off, c_off))
+        a_off += M * K
+        b_off += K * N
+        c_off += M * N
+    A, B = rng.standard_normal(a_off), rng.standard_normal(b_off)
+    table = _exec.make_gemm(prods, kind)
+    ta, tb = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    for _ in range(2):
+        tc = torch.full((c_off,), float("nan"), dtype=torch.float64, device="cuda")
+        table.run(ta, tb, tc)
+        C = tc.cpu().numpy()
+        for (M, N, K), (ao, bo, co) in zip(shapes, offs):
+            want = A[ao:ao + M * K].reshape(M, K) @ B[bo:bo + K * N].reshape(K, N)
+            got = C[co:co + M * N].reshape(M, N)
+            assert not np.isnan(got).any()
+            if K == 0:
+                assert (got == 0).all()
+                continue
+            err = np.linalg.norm(got - want) / np.linalg.norm(want)
+            assert err < TOL[kind], f"{(M, N, K)}: relative error {err:.2e}"
+
+
+@pytest.mark.parametrize("precision,tol", [("3xbf16", 1e-4), ("tf32", 1e-2)])
+def test_mixed_precision_heff2_chain(precision, tol):
+    """The bench's SU(2) matvec with its sector products on the tensor cores."""
+    import bench
+    from tenet.program import heff2_program
+
+    tensors = bench.build_workload()
+    exact = heff2_program(*tensors[:4], tensors[4].structure)(tensors[4]).numpy_arena()
+    prog = heff2_program(*tensors[:4], tensors[4].structure, precision=precision)
+    got = prog(tensors[4]).numpy_arena()
+    err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
+    assert err < tol, f"{precision}: relative error {err:.2e}"
