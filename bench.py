@@ -243,6 +243,39 @@ def cpu_baseline(flops: int, budget_s: float = 20.0) -> dict:
             "ms_per_matvec": med * 1e3}
 
 
+def dmrg_solves(args) -> dict:
+    """Time-to-solution of full DMRG solves on the device, plain FP64 form against the
+    precision form: SU(2) Heisenberg, ``L`` sites, dense ``chi``, ncv = 20, a fixed number
+    of sweeps, the reference's seeded start."""
+    import torch
+
+    from tenet import network
+    from tenet.structure import GradedSpace
+    from tenet.symmetry import SU2
+
+    L, chi, sweeps = args.solve_L, args.solve_chi, args.solve_sweeps
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
+             for i in range(L + 1)]
+    h = network.heisenberg_mpo_su2(L)
+    out = {"workload": f"su2-heisenberg-L{L}-chi{chi}-{sweeps}sweeps-ncv20"}
+    for precision in ("f64", "3xbf16"):
+        times, energy = [], None
+        for _ in range(args.solves):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            energy, _, _ = network.dmrg_(network.MPS.random(phys, bonds, seed=0), h, chi=chi,
+                                         cutoff=1e-10, ncv=20, max_sweeps=sweeps,
+                                         energy_tol=0.0, precision=precision)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        out[precision] = {"s_per_solve": float(np.median(times)),
+                          "solves_per_s": 1.0 / float(np.median(times)), "energy": energy,
+                          "runs": len(times)}
+    out["abs_dE_per_site"] = abs(out["3xbf16"]["energy"] - out["f64"]["energy"]) / L
+    return out
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -433,6 +466,7 @@ def run_tenet(args) -> None:
         }
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
+        solves = dmrg_solves(args) if args.solves > 0 else None
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -453,6 +487,7 @@ def run_tenet(args) -> None:
                              **{k: flops / (v * 1e-3) / 1e12 for k, v in eager_ms.items()}},
             "launches_per_matvec_eager_ops": launches_eager,
             "mixed_precision_forms": mixed,
+            "dmrg_solves": solves,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),
@@ -470,6 +505,10 @@ def main() -> None:
     ap.add_argument("--impl", default="tenet", choices=["tenet", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--solves", type=int, default=1, help="DMRG solves per precision form")
+    ap.add_argument("--solve-L", type=int, default=32)
+    ap.add_argument("--solve-chi", type=int, default=64)
+    ap.add_argument("--solve-sweeps", type=int, default=4)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -69,8 +69,15 @@ def env_update_first(f: SymmetricTensor, a: SymmetricTensor, w: SymmetricTensor)
 
 
 def lanczos(matvec: Callable[[SymmetricTensor], SymmetricTensor], v: SymmetricTensor, *,
-            ncv: int = 3, tol: float = 1e-13) -> tuple[float, SymmetricTensor]:
-    """Ground Ritz pair of a Hermitian ``matvec`` (``network/dmrg.py:106-227``)."""
+            ncv: int = 3, tol: float = 1e-13,
+            correct: Callable[[SymmetricTensor], SymmetricTensor] | None = None
+            ) -> tuple[float, SymmetricTensor]:
+    """Ground Ritz pair of a Hermitian ``matvec`` (``network/dmrg.py:106-227``).
+
+    ``correct`` is the FP64 correction of the precision form: when ``matvec`` runs its
+    products in reduced precision, the returned energy is the Rayleigh quotient
+    ``<v|H v>`` of the Ritz vector under the FP64 operator ``correct`` -- one FP64 matvec
+    per solve -- whose error is quadratic in the Ritz vector's."""
     vecs = [v / ops.norm(v)]
     alphas: list[float] = []
     betas: list[float] = []
@@ -97,7 +104,10 @@ def lanczos(matvec: Callable[[SymmetricTensor], SymmetricTensor], v: SymmetricTe
 
     _lib.call("tnb_lincomb", v.arena.numel(), len(vecs), _exec.ptr(coeffs), _exec.ptr(ptrs),
               _exec.ptr(out.arena), _exec.stream_ptr())
-    return float(values[0]), out / ops.norm(out)
+    out = out / ops.norm(out)
+    if correct is not None:
+        return ops.inner(out, correct(out)), out
+    return float(values[0]), out
 
 
 # ---------------------------------------------------------------------------------------
@@ -251,10 +261,11 @@ class Env:
     (ket OUT, mpo IN, bra IN)`` from sites ``>= n``.  ``compiled=True`` runs ``heff2`` as a
     CUDA-graph-captured chain program, rebuilt whenever the bond's tensors change."""
 
-    def __init__(self, psi: MPS, h: MPO, *, compiled: bool = True) -> None:
+    def __init__(self, psi: MPS, h: MPO, *, compiled: bool = True,
+                 precision: str = "f64") -> None:
         from tenet.structure import IN, Leg
 
-        self.psi, self.h, self.compiled = psi, h, compiled
+        self.psi, self.h, self.compiled, self.precision = psi, h, compiled, precision
         n = len(psi)
         kl, kr = psi[0].legs[0], psi[n - 1].legs[2]
         wl, wr = h[0].legs[0], h[n - 1].legs[3]
@@ -288,18 +299,27 @@ class Env:
             return heff2(fl, self.h[n], self.h[n + 1], fr, aa)
         return self.matvec(n, aa.structure)(aa)
 
-    def matvec(self, n: int, structure):
-        """The graph-captured matvec of bond n for the current environments."""
+    def matvec(self, n: int, structure, precision: str | None = None):
+        """The graph-captured matvec of bond n for the current environments, in the
+        env's precision (or ``precision``)."""
         from tenet.program import GraphMatvec, heff2_program
 
+        precision = precision or self.precision
         fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
-        key = (n, id(fl), id(fr), structure)
-        hit = self._prog.get(n)
+        key = (n, precision, id(fl), id(fr), structure)
+        hit = self._prog.get((n, precision))
         if hit is None or hit[0] != key:
-            prog = heff2_program(fl, self.h[n], self.h[n + 1], fr, structure)
+            prog = heff2_program(fl, self.h[n], self.h[n + 1], fr, structure,
+                                 precision=precision)
             hit = (key, GraphMatvec(prog), (fl, fr))  # keep fl, fr alive with the key
-            self._prog[n] = hit
+            self._prog[(n, precision)] = hit
         return hit[1]
+
+    def correction(self, n: int):
+        """The FP64 matvec that corrects a reduced-precision solve at bond n (None in FP64)."""
+        if self.precision == "f64" or not self.compiled:
+            return None
+        return lambda v, n=n: self.matvec(n, v.structure, "f64")(v)
 
 
 def _pair(left: SymmetricTensor, right: SymmetricTensor) -> SymmetricTensor:
@@ -321,7 +341,7 @@ def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3)
         for n in bonds:
             aa = _pair(psi[n], psi[n + 1])
             matvec = (lambda v, n=n: env.heff2(n, v))
-            energy, aa = lanczos(matvec, aa, ncv=ncv)
+            energy, aa = lanczos(matvec, aa, ncv=ncv, correct=env.correction(n))
             u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff)
             norm_s = ops.norm(s)
             max_dw = max(max_dw, 1.0 - float(norm_s / ops.norm(aa)) ** 2)
@@ -342,12 +362,15 @@ def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3)
 
 
 def dmrg_(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
-          max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True):
+          max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True,
+          precision: str = "f64"):
     """Two-site DMRG to convergence (``network/dmrg.py:620-843``, flat ``chi``/``cutoff``,
     no noise): returns ``(energy, history, psi)`` with ``history`` the per-sweep energies.
-    Stops on ``|dE| < energy_tol`` or after ``max_sweeps``."""
+    Stops on ``|dE| < energy_tol`` or after ``max_sweeps``.  ``precision`` "tf32" or
+    "3xbf16" runs the matvec products on the tensor cores with the FP64 Rayleigh-quotient
+    correction of every solve; Lanczos, the SVD and the truncation stay FP64."""
     psi.canonize_(0)
-    env = Env(psi, h, compiled=compiled).setup_(0)
+    env = Env(psi, h, compiled=compiled, precision=precision).setup_(0)
     energy, history = float("inf"), []
     for _ in range(max_sweeps):
         old = energy

@@ -68,3 +68,24 @@ def test_mixed_precision_heff2_chain(precision, tol):
     got = prog(tensors[4]).numpy_arena()
     err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
     assert err < tol, f"{precision}: relative error {err:.2e}"
+
+
+@pytest.mark.parametrize("precision", ["3xbf16"])
+def test_mixed_precision_dmrg_energy(golden_dir, precision):
+    """DMRG with tensor-core matvecs and the FP64 correction: |dE/L| <= 1e-8 against the
+    reference's FP64 run (SU(2) Heisenberg L = 16, chi = 24, ncv = 20)."""
+    import json
+
+    from tenet import network
+    from tenet.structure import GradedSpace
+    from tenet.symmetry import SU2
+
+    g = json.loads((golden_dir / "dmrg.json").read_text())["L16_chi24"]
+    L, chi = g["L"], g["chi"]
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
+             for i in range(L + 1)]
+    e, hist, _ = network.dmrg_(network.MPS.random(phys, bonds, seed=0),
+                               network.heisenberg_mpo_su2(L), chi=chi, cutoff=1e-10, ncv=20,
+                               max_sweeps=g["sweeps"], energy_tol=0.0, precision=precision)
+    assert abs(e - g["energy"]) / L <= 1e-8, f"|dE/L| = {abs(e - g['energy']) / L:.2e}"
