@@ -258,9 +258,13 @@ def dmrg_solves(args) -> dict:
     bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
              for i in range(L + 1)]
     h = network.heisenberg_mpo_su2(L)
-    out = {"workload": f"su2-heisenberg-L{L}-chi{chi}-{sweeps}sweeps-ncv20"}
+    out = {"workload": f"su2-heisenberg-L{L}-chi{chi}-{sweeps}sweeps-ncv20",
+           "timing": "median of the timed solves after one untimed warm-up solve per form "
+                     "(host plan caches warm, as a served stream of repeated shapes sees them)"}
     for precision in ("f64", "3xbf16"):
         times, energy = [], None
+        network.dmrg_(network.MPS.random(phys, bonds, seed=0), h, chi=chi, cutoff=1e-10, ncv=20,
+                      max_sweeps=sweeps, energy_tol=0.0, precision=precision)
         for _ in range(args.solves):
             torch.cuda.synchronize()
             t0 = time.perf_counter()

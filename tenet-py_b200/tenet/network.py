@@ -306,14 +306,24 @@ class Env:
 
         precision = precision or self.precision
         fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
-        key = (n, precision, id(fl), id(fr), structure)
+        w1, w2 = self.h[n], self.h[n + 1]
+        skey = (fl.structure, fr.structure, structure)
         hit = self._prog.get((n, precision))
-        if hit is None or hit[0] != key:
-            prog = heff2_program(fl, self.h[n], self.h[n + 1], fr, structure,
-                                 precision=precision)
-            hit = (key, GraphMatvec(prog), (fl, fr))  # keep fl, fr alive with the key
+        if hit is None or hit[2] != skey:
+            # one captured program per bond and precision; a new structure replaces it
+            prog = heff2_program(fl, w1, w2, fr, structure, precision=precision)
+            hit = [GraphMatvec(prog), (fl, fr), skey]
             self._prog[(n, precision)] = hit
-        return hit[1]
+        elif hit[1][0] is not fl or hit[1][1] is not fr:
+            # same structures, new environment values: re-pack the fixed operands into the
+            # captured program's buffers; the graph itself stays valid
+            gm = hit[0]
+            bound = dict(zip(("fr", "w2", "w1", "fl"), (fr, w2, w1, fl)))
+            for lk, name in zip(gm.program.links, gm.program.operand_names):
+                lk.b_tensor = bound[name]
+            gm.program.refresh()
+            hit[1] = (fl, fr)
+        return hit[0]
 
     def correction(self, n: int):
         """The FP64 matvec that corrects a reduced-precision solve at bond n (None in FP64)."""

@@ -31,6 +31,15 @@ from tenet.tensor import SymmetricTensor
 __all__ = ["ChainProgram", "heff2_program"]
 
 
+class _StructureOnly:
+    """Stand-in for a fixed operand in a shared program template: its structure only."""
+
+    __slots__ = ("structure",)
+
+    def __init__(self, structure) -> None:
+        self.structure = structure
+
+
 def _identity_plan(s: TensorStructure):
     return s, tuple(range(s.ndim)), tuple((i, i, 1.0) for i in range(s.num_blocks))
 
@@ -149,6 +158,28 @@ class ChainProgram:
             self.allocate()
         return self
 
+    def rebind(self, operands: dict) -> ChainProgram:
+        """A new program sharing this one's tables, with the fixed operands replaced by
+        tensors of the same structures (``operands`` maps the names given at planning)."""
+        import copy
+
+        q = copy.copy(self)
+        q.links = []
+        for lk, name in zip(self.links, self.operand_names):
+            t = operands[name]
+            if t.structure != lk.b_tensor.structure:
+                raise ValueError("ChainProgram.rebind: operand structure differs")
+            nl = copy.copy(lk)
+            nl.b_tensor = t
+            q.links.append(nl)
+        q._built = False
+        return q
+
+    def finish_alloc(self, allocate: bool) -> ChainProgram:
+        if allocate:
+            self.allocate()
+        return self
+
     def allocate(self) -> None:
         """Allocate every buffer once and pack the fixed operands (needs the device)."""
         dev = _exec.device()
@@ -217,13 +248,34 @@ class GraphMatvec:
         self.graph.replay()
 
 
+_HEFF_TABLES: dict = {}
+_HEFF_TABLES_MAX = 512
+
+
 def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = True,
                   precision: str = "f64") -> ChainProgram:
     """The site-tensor two-site matvec (``network/env.py:416-432``) as a chain program.
-    ``fl``, ``w1``, ``w2``, ``fr`` need only ``.structure`` when ``allocate`` is False."""
+    ``fl``, ``w1``, ``w2``, ``fr`` need only ``.structure`` when ``allocate`` is False.
+
+    The program's tables depend on the five structures and the precision only, so they
+    are planned once per such key and shared: a later call with the same structures
+    builds a fresh program (own buffers, bound to the given tensors) around them."""
+    key = (fl.structure, w1.structure, w2.structure, fr.structure, in_struct, precision)
+    cached = _HEFF_TABLES.get(key)
+    if cached is not None:
+        return cached.rebind(dict(zip(cached.operand_names, (fr, w2, w1, fl)))) \
+            .finish_alloc(allocate)
     p = ChainProgram(in_struct, precision)
     p.einsum("apqr,rys->apqys", fr)
     p.einsum("apqys,mQqy->apQms", w2, bend="q")
     p.einsum("apQms,xPpm->aPQxs", w1, bend="p")
     p.einsum("aPQxs,axB->BPQs", fl, bend="a")
-    return p.finish(allocate)
+    p.operand_names = ("fr", "w2", "w1", "fl")
+    p.finish(False)
+    bound = dict(zip(p.operand_names, (fr, w2, w1, fl)))
+    for lk in p.links:  # the shared template keeps structures, never device tensors
+        lk.b_tensor = _StructureOnly(lk.b_tensor.structure)
+    if len(_HEFF_TABLES) >= _HEFF_TABLES_MAX:
+        _HEFF_TABLES.pop(next(iter(_HEFF_TABLES)))
+    _HEFF_TABLES[key] = p
+    return p.rebind(bound).finish_alloc(allocate)
