@@ -182,6 +182,41 @@ int tnb_axpby(int64_t n, double alpha, const double* x, double beta, const doubl
               double* out, void* stream);
 
 /*
+ * Device-resident Lanczos (network/dmrg.py:106-227 without host round trips).  `state`
+ * holds 3 ncv + 2 doubles: alpha[0, ncv), beta[ncv, 2 ncv), squared norms [2 ncv, 3 ncv),
+ * the Krylov size m at [3 ncv] and a stopped flag at [3 ncv + 1], zeroed before step 0.
+ * Step j of the three-term recurrence, with w = H v_j and alpha[j] = <v_j, w> already
+ * written (tnb_weighted_dot into state + j):
+ *   tnb_lanczos_update  w <- w - alpha_j v_j - beta_{j-1} v_{j-1}   (no-op once stopped)
+ *   (tnb_weighted_dot of w with itself into state + 2 ncv + j)
+ *   tnb_lanczos_next    beta_j = ||w||; stop when j + 1 == ncv or beta_j < tol (the
+ *                       reference's happy breakdown); else v_{j+1} = w / beta_j, beta[j]
+ *                       and m = j + 2 recorded; once stopped v_{j+1} = 0.
+ * tnb_scale_rsqrt: out = x / sqrt(s2[0]) with s2 a device scalar (normalisation by a
+ * device-side squared norm).
+ */
+int tnb_lanczos_update(int64_t n, double* w, const double* v, const double* vprev,
+                       const double* state, int32_t j, int32_t ncv, void* stream);
+int tnb_lanczos_next(int64_t n, const double* w, double* vnext, double* state, int32_t j,
+                     int32_t ncv, double tol, void* stream);
+int tnb_scale_rsqrt(int64_t n, const double* s2, const double* x, double* out, void* stream);
+
+/*
+ * FP64 reorthogonalisation for the precision form (no counterpart in the reference,
+ * whose Lanczos is not reorthogonalised): tnb_multi_dot writes out[j] = <vecs[j], x>
+ * (qdim-weighted, runs as tnb_weighted_dot) for j < k in one pass with caller scratch of
+ * tnb_multi_dot_work_bytes(n, k) bytes (counter zero before first use, left zero);
+ * tnb_lanczos_reorth does w -= sum_j coeffs[j] vecs[j] (a no-op once `state` says the
+ * recurrence stopped; state may be NULL).  vecs and coeffs are device arrays.
+ */
+int64_t tnb_multi_dot_work_bytes(int64_t n, int64_t k);
+int tnb_multi_dot(int64_t n, int64_t k, const double* const* vecs, const double* x,
+                  const int64_t* run_start, const double* run_w, int64_t n_runs, void* work,
+                  double* out, void* stream);
+int tnb_lanczos_reorth(int64_t n, int64_t k, const double* coeffs, const double* const* vecs,
+                       double* w, const double* state, int32_t ncv, void* stream);
+
+/*
  * out[i] = sum_j coeffs[j] * vecs[j][i] for j < k, i < n.  `vecs` is a DEVICE array of
  * k device pointers; `coeffs` a DEVICE array of k doubles.  The Lanczos Ritz-vector
  * recombination (network/dmrg.py:224-227) in one pass.

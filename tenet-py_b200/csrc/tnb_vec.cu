@@ -101,6 +101,128 @@ __global__ void lincomb_kernel(int64_t n, int64_t k, const double* __restrict__ 
   }
 }
 
+// Lanczos state on the device (doubles): [0, ncv) alpha, [ncv, 2 ncv) beta, [2 ncv, 3 ncv)
+// squared norms, [3 ncv] Krylov size m, [3 ncv + 1] stopped flag.
+__global__ void lanczos_update_kernel(int64_t n, double* w, const double* __restrict__ v,
+                                      const double* __restrict__ vprev,
+                                      const double* __restrict__ state, int j, int ncv) {
+  if (state[3 * ncv + 1] != 0.0) return;  // the recurrence already stopped
+  const double a = state[j];
+  const double b = j > 0 ? state[ncv + j - 1] : 0.0;
+  // the reference's rounding exactly: w - (v * alpha), then - (vprev * beta), each
+  // product and each difference rounded on its own (no fused multiply-add)
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double x = __dsub_rn(w[i], __dmul_rn(v[i], a));
+    if (j > 0) x = __dsub_rn(x, __dmul_rn(vprev[i], b));
+    w[i] = x;
+  }
+}
+
+__device__ __forceinline__ void lanczos_decide(const double* state, int j, int ncv, double tol,
+                                               bool& live, bool& stop_now, double& beta) {
+  const bool stopped = state[3 * ncv + 1] != 0.0;
+  beta = sqrt(fmax(state[2 * ncv + j], 0.0));
+  stop_now = !stopped && (j + 1 == ncv || beta < tol);
+  live = !stopped && !stop_now;
+}
+
+// v_{j+1} = w / beta_j while the recurrence lives, zero once it stopped.  Reads the state
+// only; lanczos_record_kernel (launched right after) writes the step's outcome.
+__global__ void lanczos_next_kernel(int64_t n, const double* __restrict__ w, double* vnext,
+                                    const double* __restrict__ state, int j, int ncv, double tol) {
+  bool live, stop_now;
+  double beta;
+  lanczos_decide(state, j, ncv, tol, live, stop_now, beta);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    vnext[i] = live ? __ddiv_rn(w[i], beta) : 0.0;  // w / beta, as the reference divides
+}
+
+__global__ void lanczos_record_kernel(double* state, int j, int ncv, double tol) {
+  bool live, stop_now;
+  double beta;
+  lanczos_decide(state, j, ncv, tol, live, stop_now, beta);
+  if (live) {
+    state[ncv + j] = beta;
+    state[3 * ncv] = static_cast<double>(j + 2);
+  } else if (stop_now) {
+    state[3 * ncv] = static_cast<double>(j + 1);
+    state[3 * ncv + 1] = 1.0;
+  }
+}
+
+__global__ void scale_rsqrt_kernel(int64_t n, const double* __restrict__ s2, const double* x,
+                                   double* out) {
+  const double nrm = sqrt(s2[0]);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = __ddiv_rn(x[i], nrm);  // x / ||x||, as the reference divides
+}
+
+// out[j] = <vecs[j], x>_qdim for j < k: one pass per j over this CTA's chunk, partials
+// [j][cta] in the workspace, the last CTA reduces each j in a fixed order.
+__global__ void __launch_bounds__(kDotThreads)
+multi_dot_kernel(int64_t n, int64_t k, const double* const* __restrict__ vecs,
+                 const double* __restrict__ x, const int64_t* __restrict__ run_start,
+                 const double* __restrict__ run_w, int64_t n_runs, int64_t chunk,
+                 unsigned int* counter, double* partial, double* out) {
+  const int64_t lo = static_cast<int64_t>(blockIdx.x) * chunk;
+  const int64_t hi = min(n, lo + chunk);
+  __shared__ int64_t s_r0;
+  if (threadIdx.x == 0) {
+    int64_t a = 0, b = n_runs - 1;
+    while (a < b) {
+      const int64_t mid = (a + b + 1) >> 1;
+      if (run_start[mid] <= lo) a = mid; else b = mid - 1;
+    }
+    s_r0 = a;
+  }
+  __syncthreads();
+  for (int64_t j = 0; j < k; ++j) {
+    const double* v = vecs[j];
+    double acc = 0.0;
+    for (int64_t r = s_r0; r < n_runs && run_start[r] < hi; ++r) {
+      const int64_t a = max(lo, run_start[r]);
+      const int64_t b = min(hi, run_start[r + 1]);
+      double sum = 0.0;
+      for (int64_t i = a + threadIdx.x; i < b; i += kDotThreads) sum = fma(v[i], x[i], sum);
+      acc = fma(run_w[r], sum, acc);
+    }
+    const double total = block_sum(acc);
+    if (threadIdx.x == 0) partial[j * gridDim.x + blockIdx.x] = total;
+  }
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int64_t j = 0; j < k; ++j) {
+    double v = 0.0;
+    for (int64_t i = threadIdx.x; i < gridDim.x; i += kDotThreads)
+      v += ((volatile double*)partial)[j * gridDim.x + i];
+    v = block_sum(v);
+    if (threadIdx.x == 0) out[j] = v;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
+// w[i] -= sum_j coeffs[j] vecs[j][i]   (no-op once the recurrence stopped)
+__global__ void reorth_kernel(int64_t n, int64_t k, const double* __restrict__ coeffs,
+                              const double* const* __restrict__ vecs, double* w,
+                              const double* __restrict__ state, int ncv) {
+  if (state != nullptr && state[3 * ncv + 1] != 0.0) return;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int64_t j = 0; j < k; ++j) s = fma(coeffs[j], vecs[j][i], s);
+    w[i] -= s;
+  }
+}
+
 inline int64_t dot_grid(int64_t n) {
   int64_t g = (n + kDotMinChunk - 1) / kDotMinChunk;
   if (g < 1) g = 1;
@@ -223,6 +345,79 @@ extern "C" int tnb_weighted_dot_noalloc(const double* x, const double* y, int64_
   tnb::wdot_kernel<<<static_cast<unsigned>(grid), tnb::kDotThreads, 0, s>>>(
       x, y, n, run_start, run_w, n_runs, tnb::kNoAllocChunk, counter, partial, out);
   return tnb::check_launch("tnb_weighted_dot_noalloc");
+}
+
+extern "C" int tnb_lanczos_update(int64_t n, double* w, const double* v, const double* vprev,
+                                  const double* state, int32_t j, int32_t ncv, void* stream) {
+  TNB_REQUIRE(n >= 0 && j >= 0 && ncv > 0 && j < ncv, "tnb_lanczos_update: bad size or step");
+  if (n == 0) return TNB_OK;
+  TNB_REQUIRE(w && v && state && (j == 0 || vprev), "tnb_lanczos_update: null pointer");
+  tnb::lanczos_update_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(
+      n, w, v, vprev, state, j, ncv);
+  return tnb::check_launch("tnb_lanczos_update");
+}
+
+extern "C" int tnb_lanczos_next(int64_t n, const double* w, double* vnext, double* state,
+                                int32_t j, int32_t ncv, double tol, void* stream) {
+  TNB_REQUIRE(n >= 0 && j >= 0 && ncv > 0 && j < ncv, "tnb_lanczos_next: bad size or step");
+  TNB_REQUIRE(w && vnext && state, "tnb_lanczos_next: null pointer");
+  cudaStream_t s = tnb::as_stream(stream);
+  if (n > 0)
+    tnb::lanczos_next_kernel<<<tnb::elementwise_grid(n), 256, 0, s>>>(n, w, vnext, state, j, ncv,
+                                                                      tol);
+  // stream order puts the record after every read of the state above
+  tnb::lanczos_record_kernel<<<1, 1, 0, s>>>(state, j, ncv, tol);
+  return tnb::check_launch("tnb_lanczos_next");
+}
+
+extern "C" int tnb_scale_rsqrt(int64_t n, const double* s2, const double* x, double* out,
+                               void* stream) {
+  TNB_REQUIRE(n >= 0, "tnb_scale_rsqrt: negative size");
+  if (n == 0) return TNB_OK;
+  TNB_REQUIRE(s2 && x && out, "tnb_scale_rsqrt: null pointer");
+  tnb::scale_rsqrt_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(n, s2, x,
+                                                                                       out);
+  return tnb::check_launch("tnb_scale_rsqrt");
+}
+
+extern "C" int64_t tnb_multi_dot_work_bytes(int64_t n, int64_t k) {
+  return 256 + 8 * tnb::dot_grid(n < 0 ? 0 : n) * (k < 1 ? 1 : k);
+}
+
+extern "C" int tnb_multi_dot(int64_t n, int64_t k, const double* const* vecs, const double* x,
+                             const int64_t* run_start, const double* run_w, int64_t n_runs,
+                             void* work, double* out, void* stream) {
+  TNB_REQUIRE(n >= 0 && k >= 0 && n_runs >= 0, "tnb_multi_dot: negative size");
+  cudaStream_t s = tnb::as_stream(stream);
+  if (k == 0) return TNB_OK;
+  TNB_REQUIRE(out && work, "tnb_multi_dot: null out or work");
+  if (n == 0 || n_runs == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(double) * k, s);
+    if (e != cudaSuccess) {
+      tnb::set_error(std::string("tnb_multi_dot: ") + cudaGetErrorString(e));
+      return TNB_ECUDA;
+    }
+    return TNB_OK;
+  }
+  TNB_REQUIRE(vecs && x && run_start && run_w, "tnb_multi_dot: null input");
+  const int64_t grid = tnb::dot_grid(n);
+  const int64_t chunk = (n + grid - 1) / grid;
+  auto* counter = static_cast<unsigned int*>(work);
+  auto* partial = reinterpret_cast<double*>(static_cast<char*>(work) + 256);
+  tnb::multi_dot_kernel<<<static_cast<unsigned>(grid), tnb::kDotThreads, 0, s>>>(
+      n, k, vecs, x, run_start, run_w, n_runs, chunk, counter, partial, out);
+  return tnb::check_launch("tnb_multi_dot");
+}
+
+extern "C" int tnb_lanczos_reorth(int64_t n, int64_t k, const double* coeffs,
+                                  const double* const* vecs, double* w, const double* state,
+                                  int32_t ncv, void* stream) {
+  TNB_REQUIRE(n >= 0 && k >= 0, "tnb_lanczos_reorth: negative size");
+  if (n == 0 || k == 0) return TNB_OK;
+  TNB_REQUIRE(coeffs && vecs && w, "tnb_lanczos_reorth: null pointer");
+  tnb::reorth_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(
+      n, k, coeffs, vecs, w, state, ncv);
+  return tnb::check_launch("tnb_lanczos_reorth");
 }
 
 extern "C" int tnb_axpby(int64_t n, double alpha, const double* x, double beta, const double* y,

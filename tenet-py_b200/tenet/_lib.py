@@ -28,6 +28,12 @@ SIGNATURES = {
     "tnb_weighted_dot_noalloc": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp]),
     "tnb_axpby": (_i32, [_i64, _f64, _vp, _f64, _vp, _vp, _vp]),
     "tnb_lincomb": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp]),
+    "tnb_lanczos_update": (_i32, [_i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp]),
+    "tnb_lanczos_next": (_i32, [_i64, _vp, _vp, _vp, _i32, _i32, _f64, _vp]),
+    "tnb_scale_rsqrt": (_i32, [_i64, _vp, _vp, _vp, _vp]),
+    "tnb_multi_dot_work_bytes": (_i64, [_i64, _i64]),
+    "tnb_multi_dot": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
+    "tnb_lanczos_reorth": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp, _i32, _vp]),
     "tnb_set_pdl": (_i32, [_i32]),
     "tnb_version": (_i32, []),
     "tnb_last_error": (ctypes.c_char_p, []),

@@ -110,6 +110,131 @@ def lanczos(matvec: Callable[[SymmetricTensor], SymmetricTensor], v: SymmetricTe
     return float(values[0]), out
 
 
+class LanczosGraph:
+    """The reference's Lanczos (``network/dmrg.py:106-227``) with the whole recurrence on
+    the device: the ``ncv`` matvecs, every ``alpha``/``beta``, the three-term update and the
+    happy-breakdown stop run inside one captured CUDA graph with device-resident scalars.
+    The host then makes one synchronising read of the tridiagonal, solves it with
+    ``np.linalg.eigh`` exactly as the reference does, and a second small graph forms and
+    normalises the Ritz vector (and, in the precision form, applies the FP64 correction
+    program for the Rayleigh-quotient energy)."""
+
+    def __init__(self, program, ncv: int, tol: float = 1e-13, correct=None,
+                 reorthogonalize: bool | None = None) -> None:
+        """``reorthogonalize`` (default: on exactly when ``correct`` is given, i.e. in the
+        precision form) adds classical Gram-Schmidt, applied twice, of every new Krylov
+        vector against all earlier ones in FP64.  A reduced-precision matvec never drives
+        ``beta`` below an absolute breakdown tolerance, so without it the recurrence runs
+        on past an exhausted Krylov space and produces spurious Ritz values; the FP64
+        form keeps the reference's unreorthogonalised recurrence."""
+        from tenet import _exec, _lib
+        from tenet.structure import layout
+
+        self.program, self.ncv, self.tol, self.correct = program, ncv, tol, correct
+        self.reorth = (correct is not None) if reorthogonalize is None else reorthogonalize
+        s = program.in_struct
+        n = layout(s).size
+        dev = _exec.device()
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.n = n
+        self.V = torch.zeros((ncv + 1, max(n, 1)), **f64)
+        self.W = torch.zeros(max(n, 1), **f64)
+        self.W2 = torch.zeros(max(n, 1), **f64)
+        self.x = torch.zeros(max(n, 1), **f64)
+        self.out = torch.zeros(max(n, 1), **f64)
+        self.state = torch.zeros(3 * ncv + 2, **f64)
+        self.scal = torch.zeros(2, **f64)  # [0] a squared norm, [1] the corrected energy
+        self.coef = torch.zeros(ncv, **f64)
+        self.ptrs = torch.tensor([self.V[k].data_ptr() for k in range(ncv)], dtype=torch.int64,
+                                 device=dev)
+        self.work = torch.zeros(int(_lib.load().tnb_dot_work_bytes(n)), dtype=torch.uint8,
+                                device=dev)
+        self.mwork = torch.zeros(int(_lib.load().tnb_multi_dot_work_bytes(n, ncv)),
+                                 dtype=torch.uint8, device=dev)
+        self.gs = torch.zeros(ncv, **f64)
+        self.runs = ops._runs(s)
+        self._host_state = torch.zeros(3 * ncv + 2, dtype=torch.float64).pin_memory()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self._solve_body()
+            self._finish_body()
+        torch.cuda.current_stream().wait_stream(side)
+        self.g1, self.g2 = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g1):
+            self._solve_body()
+        with torch.cuda.graph(self.g2):
+            self._finish_body()
+
+    def _dot(self, a, b, out) -> None:
+        from tenet import _exec, _lib
+
+        r = self.runs
+        _lib.call("tnb_weighted_dot", _exec.ptr(a), _exec.ptr(b), self.n, _exec.ptr(r.start),
+                  _exec.ptr(r.weight), r.n_runs, _exec.ptr(self.work), _exec.ptr(out),
+                  _exec.stream_ptr())
+
+    def _solve_body(self) -> None:
+        from tenet import _exec, _lib
+
+        n, ncv, V, W, st = self.n, self.ncv, self.V, self.W, self.state
+        P = _exec.ptr
+        sp = _exec.stream_ptr()
+        st.zero_()
+        self._dot(self.x, self.x, self.scal)
+        _lib.call("tnb_scale_rsqrt", n, P(self.scal), P(self.x), P(V[0]), sp)
+        for j in range(ncv):
+            self.program.run(V[j], W)
+            self._dot(V[j], W, st[j:j + 1])
+            _lib.call("tnb_lanczos_update", n, P(W), P(V[j]), P(V[j - 1]) if j else None, P(st),
+                      j, ncv, sp)
+            if self.reorth:
+                r = self.runs
+                for _ in range(2):  # classical Gram-Schmidt, twice
+                    _lib.call("tnb_multi_dot", n, j + 1, P(self.ptrs), P(W), P(r.start),
+                              P(r.weight), r.n_runs, P(self.mwork), P(self.gs), sp)
+                    _lib.call("tnb_lanczos_reorth", n, j + 1, P(self.gs), P(self.ptrs), P(W),
+                              P(st), ncv, sp)
+            self._dot(W, W, st[2 * ncv + j:2 * ncv + j + 1])
+            _lib.call("tnb_lanczos_next", n, P(W), P(V[j + 1]), P(st), j, ncv, float(self.tol),
+                      sp)
+
+    def _finish_body(self) -> None:
+        from tenet import _exec, _lib
+
+        P = _exec.ptr
+        sp = _exec.stream_ptr()
+        _lib.call("tnb_lincomb", self.n, self.ncv, P(self.coef), P(self.ptrs), P(self.out), sp)
+        self._dot(self.out, self.out, self.scal)
+        _lib.call("tnb_scale_rsqrt", self.n, P(self.scal), P(self.out), P(self.out), sp)
+        if self.correct is not None:
+            self.correct.run(self.out, self.W2)
+            self._dot(self.out, self.W2, self.scal[1:2])
+
+    def solve(self, v: SymmetricTensor) -> tuple[float, SymmetricTensor]:
+        if v.structure != self.program.in_struct:
+            raise ValueError("LanczosGraph: the start vector's structure differs")
+        if self.n == 0:
+            return 0.0, v
+        self.x.copy_(v.arena)
+        self.g1.replay()
+        self._host_state.copy_(self.state)  # the one synchronising read of the solve
+        st = self._host_state.numpy()
+        ncv = self.ncv
+        m = int(st[3 * ncv])
+        alphas, betas = st[:m], st[ncv:ncv + m - 1]
+        tri = np.diag(alphas) + np.diag(betas, 1) + np.diag(betas, -1)
+        values, states = np.linalg.eigh(tri)
+        coef = np.zeros(ncv)
+        coef[:m] = states[:, 0]
+        self.coef.copy_(torch.from_numpy(coef))
+        self.g2.replay()
+        out = SymmetricTensor(v.structure, arena=self.out[: self.n].clone())
+        if self.correct is not None:
+            return float(self.scal[1].item()), out
+        return float(values[0]), out
+
+
 # ---------------------------------------------------------------------------------------
 # MPS / MPO / environments / sweeps  (network/mps.py, network/env.py, network/dmrg.py)
 
@@ -299,31 +424,53 @@ class Env:
             return heff2(fl, self.h[n], self.h[n + 1], fr, aa)
         return self.matvec(n, aa.structure)(aa)
 
-    def matvec(self, n: int, structure, precision: str | None = None):
-        """The graph-captured matvec of bond n for the current environments, in the
-        env's precision (or ``precision``)."""
-        from tenet.program import GraphMatvec, heff2_program
+    def _bond(self, n: int, structure, precision: str) -> dict:
+        """The bond's cached programs: one allocated heff2 program per precision (plus what
+        was captured around it), re-packed when only the environment values changed."""
+        from tenet.program import heff2_program
 
-        precision = precision or self.precision
         fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
         w1, w2 = self.h[n], self.h[n + 1]
         skey = (fl.structure, fr.structure, structure)
         hit = self._prog.get((n, precision))
-        if hit is None or hit[2] != skey:
-            # one captured program per bond and precision; a new structure replaces it
-            prog = heff2_program(fl, w1, w2, fr, structure, precision=precision)
-            hit = [GraphMatvec(prog), (fl, fr), skey]
+        if hit is None or hit["skey"] != skey:
+            # one program per bond and precision; a new structure replaces it
+            hit = {"skey": skey, "bound": (fl, fr), "captured": {},
+                   "program": heff2_program(fl, w1, w2, fr, structure, precision=precision)}
             self._prog[(n, precision)] = hit
-        elif hit[1][0] is not fl or hit[1][1] is not fr:
+        elif hit["bound"][0] is not fl or hit["bound"][1] is not fr:
             # same structures, new environment values: re-pack the fixed operands into the
-            # captured program's buffers; the graph itself stays valid
-            gm = hit[0]
+            # program's buffers; everything captured around them stays valid
             bound = dict(zip(("fr", "w2", "w1", "fl"), (fr, w2, w1, fl)))
-            for lk, name in zip(gm.program.links, gm.program.operand_names):
+            prog = hit["program"]
+            for lk, name in zip(prog.links, prog.operand_names):
                 lk.b_tensor = bound[name]
-            gm.program.refresh()
-            hit[1] = (fl, fr)
-        return hit[0]
+            prog.refresh()
+            hit["bound"] = (fl, fr)
+        return hit
+
+    def matvec(self, n: int, structure, precision: str | None = None):
+        """The graph-captured matvec of bond n for the current environments, in the
+        env's precision (or ``precision``)."""
+        from tenet.program import GraphMatvec
+
+        hit = self._bond(n, structure, precision or self.precision)
+        if "matvec" not in hit["captured"]:
+            hit["captured"]["matvec"] = GraphMatvec(hit["program"])
+        return hit["captured"]["matvec"]
+
+    def solve(self, n: int, aa: SymmetricTensor, ncv: int) -> tuple[float, SymmetricTensor]:
+        """Ground Ritz pair at bond n by the device-resident Lanczos (``LanczosGraph``)."""
+        hit = self._bond(n, aa.structure, self.precision)
+        correct = None
+        if self.precision != "f64":
+            correct = self._bond(n, aa.structure, "f64")["program"]
+        key = ("lanczos", ncv)
+        lg = hit["captured"].get(key)
+        if lg is None or lg.correct is not correct:
+            lg = LanczosGraph(hit["program"], ncv, correct=correct)
+            hit["captured"][key] = lg
+        return lg.solve(aa)
 
     def correction(self, n: int):
         """The FP64 matvec that corrects a reduced-precision solve at bond n (None in FP64)."""
@@ -350,8 +497,10 @@ def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3)
         bonds = range(n_sites - 1) if forward else range(n_sites - 2, -1, -1)
         for n in bonds:
             aa = _pair(psi[n], psi[n + 1])
-            matvec = (lambda v, n=n: env.heff2(n, v))
-            energy, aa = lanczos(matvec, aa, ncv=ncv, correct=env.correction(n))
+            if env.compiled:
+                energy, aa = env.solve(n, aa, ncv)
+            else:
+                energy, aa = lanczos(lambda v, n=n: env.heff2(n, v), aa, ncv=ncv)
             u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff)
             norm_s = ops.norm(s)
             max_dw = max(max_dw, 1.0 - float(norm_s / ops.norm(aa)) ** 2)

@@ -405,3 +405,54 @@ def test_ctmrg_z2_ising_matches_reference(golden_dir, name):
         bf = network.beta_free_energy(c, e, bulk)
         assert bf == pytest.approx(r["beta_f"], rel=1e-10)
         assert bf == pytest.approx(r["onsager_beta_f"], rel=1e-6)
+
+
+def test_device_lanczos_graph_matches_reference(golden_dir):
+    """The whole recurrence in one captured graph: the reference's ncv=20 energy and the
+    same Ritz vector (up to sign) as the host-driven Lanczos; replays are repeatable."""
+    from tenet.program import heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
+    lg = network.LanczosGraph(prog, 20)
+    e_host, v_host = network.lanczos(prog, T["aa"], ncv=20)
+    for _ in range(2):
+        e, v = lg.solve(T["aa"])
+        assert e == pytest.approx(m["lanczos_ncv20_energy"], rel=1e-12)
+        assert e == pytest.approx(e_host, rel=1e-13)
+        a, b = v.numpy_arena(), v_host.numpy_arena()
+        sign = np.sign(a @ b)
+        close(sign * a, b, 1e-10)
+    # a Krylov space that breaks down early (ncv larger than the space allows)
+    small = network.LanczosGraph(prog, 60)
+    e60, _ = small.solve(T["aa"])
+    assert e60 == pytest.approx(network.lanczos(prog, T["aa"], ncv=60)[0], rel=1e-10)
+
+
+def test_multi_dot_and_reorth_kernels():
+    """The reorthogonalisation primitives through the C ABI against NumPy."""
+    import ctypes
+
+    lib = _lib.load()
+    n, k = 70_001, 7
+    g = torch.Generator(device="cuda").manual_seed(3)
+    V = torch.randn((k, n), dtype=torch.float64, device="cuda", generator=g)
+    x = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    ptrs = torch.tensor([V[i].data_ptr() for i in range(k)], dtype=torch.int64, device="cuda")
+    starts = torch.tensor([0, 100, n], dtype=torch.int64, device="cuda")
+    w = torch.tensor([2.0, 1.0], dtype=torch.float64, device="cuda")
+    work = torch.zeros(lib.tnb_multi_dot_work_bytes(n, k), dtype=torch.uint8, device="cuda")
+    out = torch.empty(k, dtype=torch.float64, device="cuda")
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        assert lib.tnb_multi_dot(n, k, ptrs.data_ptr(), x.data_ptr(), starts.data_ptr(),
+                                 w.data_ptr(), 2, work.data_ptr(), out.data_ptr(), s) == 0
+        Vh, xh = V.cpu().numpy(), x.cpu().numpy()
+        want = 2.0 * Vh[:, :100] @ xh[:100] + Vh[:, 100:] @ xh[100:]
+        close(out.cpu().numpy(), want, 1e-12)
+    y = x.clone()
+    assert lib.tnb_lanczos_reorth(n, k, out.data_ptr(), ptrs.data_ptr(), y.data_ptr(), None, 1,
+                                  s) == 0
+    close(y.cpu().numpy(), xh - out.cpu().numpy() @ Vh, 1e-12)
