@@ -233,6 +233,57 @@ int tnb_lincomb(int64_t n, int64_t k, const double* coeffs, const double* const*
  */
 int tnb_set_pdl(int enabled);
 
+/*
+ * Recorded launch sequences (no counterpart in the reference, whose per-block loops run
+ * in Python; this is the native replacement of the host loop around them).  A sequence
+ * records tnb_block_gather / tnb_grouped_gemm_f64 launches -- tables, buffers, sizes --
+ * and tnb_seq_run replays them in order on `stream`, first substituting every data
+ * buffer pointer equal to from[i] by to[i] (HOST arrays of n_patch pointers; 0 = none).
+ * A compiled matvec is recorded once on placeholder input/output buffers and replayed
+ * on any vectors of the same sizes.  The sequence borrows every recorded pointer: the
+ * caller keeps tables and buffers alive while it may run.  Replay returns the first
+ * failing launch's status.  A sequence is not thread-safe; replays only read it.
+ */
+typedef struct tnb_seq tnb_seq;
+int tnb_seq_create(tnb_seq** out);
+void tnb_seq_destroy(tnb_seq* s);
+int64_t tnb_seq_length(const tnb_seq* s);
+int tnb_seq_add_gather(tnb_seq* s, const int64_t* seg_table, int64_t n_seg,
+                       const int32_t* chunk_map, int64_t total_chunks, const int64_t* term_src,
+                       const double* term_coeff, const int64_t* term_ld, int64_t n_term,
+                       const double* src0, int64_t n_src0, double* dst0, int64_t n_dst0,
+                       const double* src1, int64_t n_src1, double* dst1, int64_t n_dst1);
+int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
+                     const int32_t* tile_map, int64_t total_tiles, int32_t tile_kind,
+                     const double* a, int64_t n_a, const double* b, int64_t n_b, double* c,
+                     int64_t n_c, void* work, int64_t work_bytes, int64_t n_counters);
+int tnb_seq_append(tnb_seq* dst, const tnb_seq* src);
+int tnb_seq_run(const tnb_seq* s, int32_t n_patch, const void* const* from, void* const* to,
+                void* stream);
+
+/*
+ * One whole Lanczos solve from one host call (replaces the loop of
+ * network/dmrg.py:106-227): zero `state`, v_0 = x0/||x0||, then for j < ncv the matvec
+ * sequence replayed with x_slot -> v_j and y_slot -> w, alpha_j, tnb_lanczos_update,
+ * optional classical Gram-Schmidt twice against v_0..v_j (reorth != 0; vptrs = DEVICE
+ * array of the ncv row pointers of v, gs = ncv doubles, multi_work of
+ * tnb_multi_dot_work_bytes(n, ncv) bytes), ||w||^2 and tnb_lanczos_next.  `v` holds
+ * ncv + 1 rows of stride ldv >= n; `scal` 2 doubles; dot_work tnb_dot_work_bytes(n).
+ * The caller reads `state` (one synchronising copy), solves the tridiagonal, and calls
+ * tnb_lanczos_ritz: out = normalised sum_j coef[j] v_j, and, when `correct` is given
+ * (the FP64 sequence of the precision form), scal[1] = <out, H out> with H out in w2.
+ */
+int tnb_lanczos_solve(const tnb_seq* matvec, const void* x_slot, const void* y_slot, int64_t n,
+                      int32_t ncv, double tol, int32_t reorth, const double* x0, double* v,
+                      int64_t ldv, double* w, double* state, double* scal,
+                      const double* const* vptrs, double* gs, const int64_t* run_start,
+                      const double* run_w, int64_t n_runs, void* dot_work, void* multi_work,
+                      void* stream);
+int tnb_lanczos_ritz(const tnb_seq* correct, const void* x_slot, const void* y_slot, int64_t n,
+                     int32_t ncv, const double* coef, const double* const* vptrs, double* out,
+                     double* w2, double* scal, const int64_t* run_start, const double* run_w,
+                     int64_t n_runs, void* dot_work, void* stream);
+
 /* Library version (major*10000 + minor*100 + patch). */
 int tnb_version(void);
 

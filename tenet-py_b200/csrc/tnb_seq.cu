@@ -1,0 +1,204 @@
+// Recorded launch sequences and the native Lanczos driver.
+//
+// A sequence is a list of table-driven launches (gathers and grouped GEMMs) recorded
+// once, with their tables, buffers and sizes, and replayed by one call.  Replay can
+// substitute buffer pointers (a compiled matvec is recorded on placeholder input and
+// output buffers and replayed on the Krylov vectors), so one recorded chain program
+// serves every matvec of a solve without host work per launch.  The Lanczos driver
+// launches a whole solve -- ncv matvecs, the recurrence, optional FP64
+// reorthogonalisation -- from one host call; nothing in it waits on the host.
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "tnb_common.cuh"
+
+struct tnb_seq {
+  struct Op {
+    int32_t code;
+    int64_t w[16];
+  };
+  std::vector<Op> ops;
+};
+
+namespace tnb {
+namespace {
+
+constexpr int32_t kOpGather = 1;
+constexpr int32_t kOpGemm = 2;
+
+// word positions of the data buffers a replay may substitute
+constexpr int kGatherBufs[] = {8, 10, 12, 14};  // src0, dst0, src1, dst1
+constexpr int kGemmBufs[] = {5, 7, 9};          // a, b, c
+
+inline void* as_ptr(int64_t w) { return reinterpret_cast<void*>(static_cast<intptr_t>(w)); }
+inline int64_t as_word(const void* p) { return static_cast<int64_t>(reinterpret_cast<intptr_t>(p)); }
+
+int64_t patched(int64_t w, int32_t n_patch, const void* const* from, void* const* to) {
+  for (int32_t i = 0; i < n_patch; ++i)
+    if (w == as_word(from[i])) return as_word(to[i]);
+  return w;
+}
+
+int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* const* to,
+           cudaStream_t stream) {
+  for (const auto& op : s->ops) {
+    int64_t w[16];
+    std::memcpy(w, op.w, sizeof(w));
+    int rc = TNB_EINVAL;
+    if (op.code == kOpGather) {
+      for (int k : kGatherBufs) w[k] = patched(w[k], n_patch, from, to);
+      rc = tnb_block_gather(
+          static_cast<const int64_t*>(as_ptr(w[0])), w[1], static_cast<const int32_t*>(as_ptr(w[2])),
+          w[3], static_cast<const int64_t*>(as_ptr(w[4])), static_cast<const double*>(as_ptr(w[5])),
+          static_cast<const int64_t*>(as_ptr(w[6])), w[7], static_cast<const double*>(as_ptr(w[8])),
+          w[9], static_cast<double*>(as_ptr(w[10])), w[11],
+          static_cast<const double*>(as_ptr(w[12])), w[13], static_cast<double*>(as_ptr(w[14])),
+          w[15], stream);
+    } else if (op.code == kOpGemm) {
+      for (int k : kGemmBufs) w[k] = patched(w[k], n_patch, from, to);
+      rc = tnb_grouped_gemm_f64(
+          static_cast<const int64_t*>(as_ptr(w[0])), w[1], static_cast<const int32_t*>(as_ptr(w[2])),
+          w[3], static_cast<int32_t>(w[4]), static_cast<const double*>(as_ptr(w[5])), w[6],
+          static_cast<const double*>(as_ptr(w[7])), w[8], static_cast<double*>(as_ptr(w[9])), w[10],
+          as_ptr(w[11]), w[12], w[13], stream);
+    } else {
+      set_error("tnb_seq_run: corrupt sequence");
+    }
+    if (rc != TNB_OK) return rc;
+  }
+  return TNB_OK;
+}
+
+}  // namespace
+}  // namespace tnb
+
+extern "C" int tnb_seq_create(tnb_seq** out) {
+  TNB_REQUIRE(out != nullptr, "tnb_seq_create: out is null");
+  *out = new (std::nothrow) tnb_seq();
+  TNB_REQUIRE(*out != nullptr, "tnb_seq_create: out of host memory");
+  return TNB_OK;
+}
+
+extern "C" void tnb_seq_destroy(tnb_seq* s) { delete s; }
+
+extern "C" int64_t tnb_seq_length(const tnb_seq* s) {
+  return s ? static_cast<int64_t>(s->ops.size()) : -1;
+}
+
+extern "C" int tnb_seq_add_gather(tnb_seq* s, const int64_t* seg_table, int64_t n_seg,
+                                  const int32_t* chunk_map, int64_t total_chunks,
+                                  const int64_t* term_src, const double* term_coeff,
+                                  const int64_t* term_ld, int64_t n_term, const double* src0,
+                                  int64_t n_src0, double* dst0, int64_t n_dst0,
+                                  const double* src1, int64_t n_src1, double* dst1,
+                                  int64_t n_dst1) {
+  TNB_REQUIRE(s != nullptr, "tnb_seq_add_gather: null sequence");
+  TNB_REQUIRE(n_seg >= 0 && total_chunks >= 0 && n_term >= 0, "tnb_seq_add_gather: negative size");
+  using tnb::as_word;
+  tnb_seq::Op op{tnb::kOpGather,
+                 {as_word(seg_table), n_seg, as_word(chunk_map), total_chunks, as_word(term_src),
+                  as_word(term_coeff), as_word(term_ld), n_term, as_word(src0), n_src0,
+                  as_word(dst0), n_dst0, as_word(src1), n_src1, as_word(dst1), n_dst1}};
+  s->ops.push_back(op);
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
+                                const int32_t* tile_map, int64_t total_tiles, int32_t tile_kind,
+                                const double* a, int64_t n_a, const double* b, int64_t n_b,
+                                double* c, int64_t n_c, void* work, int64_t work_bytes,
+                                int64_t n_counters) {
+  TNB_REQUIRE(s != nullptr, "tnb_seq_add_gemm: null sequence");
+  TNB_REQUIRE(n_gemm >= 0 && total_tiles >= 0, "tnb_seq_add_gemm: negative size");
+  using tnb::as_word;
+  tnb_seq::Op op{tnb::kOpGemm,
+                 {as_word(gemm_table), n_gemm, as_word(tile_map), total_tiles, tile_kind,
+                  as_word(a), n_a, as_word(b), n_b, as_word(c), n_c, as_word(work), work_bytes,
+                  n_counters, 0, 0}};
+  s->ops.push_back(op);
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_append(tnb_seq* dst, const tnb_seq* src) {
+  TNB_REQUIRE(dst != nullptr && src != nullptr, "tnb_seq_append: null sequence");
+  TNB_REQUIRE(dst != src, "tnb_seq_append: a sequence cannot append itself");
+  dst->ops.insert(dst->ops.end(), src->ops.begin(), src->ops.end());
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_run(const tnb_seq* s, int32_t n_patch, const void* const* from,
+                           void* const* to, void* stream) {
+  TNB_REQUIRE(s != nullptr, "tnb_seq_run: null sequence");
+  TNB_REQUIRE(n_patch >= 0 && (n_patch == 0 || (from && to)), "tnb_seq_run: bad patch list");
+  return tnb::replay(s, n_patch, from, to, tnb::as_stream(stream));
+}
+
+#define TNB_TRY(expr)            \
+  do {                           \
+    const int rc_ = (expr);      \
+    if (rc_ != TNB_OK) return rc_; \
+  } while (0)
+
+extern "C" int tnb_lanczos_solve(const tnb_seq* matvec, const void* x_slot, const void* y_slot,
+                                 int64_t n, int32_t ncv, double tol, int32_t reorth,
+                                 const double* x0, double* v, int64_t ldv, double* w,
+                                 double* state, double* scal, const double* const* vptrs,
+                                 double* gs, const int64_t* run_start, const double* run_w,
+                                 int64_t n_runs, void* dot_work, void* multi_work,
+                                 void* stream) {
+  TNB_REQUIRE(matvec != nullptr, "tnb_lanczos_solve: null matvec sequence");
+  TNB_REQUIRE(n > 0 && ncv > 0 && ldv >= n, "tnb_lanczos_solve: bad sizes");
+  TNB_REQUIRE(x0 && v && w && state && scal && run_start && run_w && dot_work,
+              "tnb_lanczos_solve: null buffer");
+  TNB_REQUIRE(!reorth || (vptrs && gs && multi_work), "tnb_lanczos_solve: reorth buffers");
+  cudaStream_t s = tnb::as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(state, 0, sizeof(double) * (3 * ncv + 2), s);
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_lanczos_solve: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  // v_0 = x0 / ||x0||
+  TNB_TRY(tnb_weighted_dot(x0, x0, n, run_start, run_w, n_runs, dot_work, scal, stream));
+  TNB_TRY(tnb_scale_rsqrt(n, scal, x0, v, stream));
+  const void* from[2] = {x_slot, y_slot};
+  for (int32_t j = 0; j < ncv; ++j) {
+    double* vj = v + static_cast<int64_t>(j) * ldv;
+    void* to[2] = {vj, w};
+    TNB_TRY(tnb::replay(matvec, 2, from, to, s));
+    TNB_TRY(tnb_weighted_dot(vj, w, n, run_start, run_w, n_runs, dot_work, state + j, stream));
+    TNB_TRY(tnb_lanczos_update(n, w, vj, j ? vj - ldv : nullptr, state, j, ncv, stream));
+    if (reorth) {
+      for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+        TNB_TRY(tnb_multi_dot(n, j + 1, vptrs, w, run_start, run_w, n_runs, multi_work, gs,
+                              stream));
+        TNB_TRY(tnb_lanczos_reorth(n, j + 1, gs, vptrs, w, state, ncv, stream));
+      }
+    }
+    TNB_TRY(tnb_weighted_dot(w, w, n, run_start, run_w, n_runs, dot_work,
+                             state + 2 * ncv + j, stream));
+    TNB_TRY(tnb_lanczos_next(n, w, vj + ldv, state, j, ncv, tol, stream));
+  }
+  return TNB_OK;
+}
+
+extern "C" int tnb_lanczos_ritz(const tnb_seq* correct, const void* x_slot, const void* y_slot,
+                                int64_t n, int32_t ncv, const double* coef,
+                                const double* const* vptrs, double* out, double* w2,
+                                double* scal, const int64_t* run_start, const double* run_w,
+                                int64_t n_runs, void* dot_work, void* stream) {
+  TNB_REQUIRE(n > 0 && ncv > 0, "tnb_lanczos_ritz: bad sizes");
+  TNB_REQUIRE(coef && vptrs && out && scal && run_start && run_w && dot_work,
+              "tnb_lanczos_ritz: null buffer");
+  TNB_REQUIRE(!correct || w2, "tnb_lanczos_ritz: the correction needs w2");
+  TNB_TRY(tnb_lincomb(n, ncv, coef, vptrs, out, stream));
+  TNB_TRY(tnb_weighted_dot(out, out, n, run_start, run_w, n_runs, dot_work, scal, stream));
+  TNB_TRY(tnb_scale_rsqrt(n, scal, out, out, stream));
+  if (correct) {
+    const void* from[2] = {x_slot, y_slot};
+    void* to[2] = {out, w2};
+    TNB_TRY(tnb::replay(correct, 2, from, to, tnb::as_stream(stream)));
+    TNB_TRY(tnb_weighted_dot(out, w2, n, run_start, run_w, n_runs, dot_work, scal + 1, stream));
+  }
+  return TNB_OK;
+}

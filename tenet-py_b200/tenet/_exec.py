@@ -40,12 +40,57 @@ def device() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
-def stream_ptr():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+def stream_ptr() -> int:
+    """The raw ``cudaStream_t`` of the current device's current stream."""
+    return torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice())
 
 
-def ptr(t: torch.Tensor | None):
-    return ctypes.c_void_p(0 if t is None or t.numel() == 0 else t.data_ptr())
+def ptr(t: torch.Tensor | None) -> int:
+    return 0 if t is None or t.numel() == 0 else t.data_ptr()
+
+
+class Seq:
+    """A recorded launch sequence (``tnb_seq`` in ``include/tenet_b200.h``): gathers and
+    grouped GEMMs recorded once and replayed by one library call, optionally with buffer
+    pointers substituted.  The owner keeps every recorded table and buffer alive."""
+
+    def __init__(self) -> None:
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.call("tnb_seq_create", ctypes.byref(h))
+        self.handle = h.value
+        self._destroy = lib.tnb_seq_destroy
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self._destroy(self.handle)
+            self.handle = None
+
+    def __len__(self) -> int:
+        return int(_lib.load().tnb_seq_length(self.handle))
+
+    def __enter__(self):
+        global _REC
+        self._prev, _REC = _REC, self
+        return self
+
+    def __exit__(self, *exc):
+        global _REC
+        _REC = self._prev
+
+    def run(self, patch: dict | None = None) -> None:
+        """Replay on the current stream; ``patch`` maps recorded buffer addresses to the
+        addresses to use instead."""
+        if patch:
+            n = len(patch)
+            src = (ctypes.c_void_p * n)(*patch.keys())
+            dst = (ctypes.c_void_p * n)(*patch.values())
+            _lib.call("tnb_seq_run", self.handle, n, src, dst, stream_ptr())
+        else:
+            _lib.call("tnb_seq_run", self.handle, 0, None, None, stream_ptr())
+
+
+_REC: Seq | None = None
 
 
 class LaunchLog:
@@ -223,6 +268,13 @@ class GatherTable:
         if self.n_seg == 0:
             return
         seg, tsrc, tcf, tld, cmap = self.device_arrays()
+        if _REC is not None:
+            _lib.call("tnb_seq_add_gather", _REC.handle, ptr(seg), self.n_seg, ptr(cmap),
+                      self.chunks, ptr(tsrc), ptr(tcf), ptr(tld), self.n_term,
+                      ptr(src0), src0.numel(), ptr(dst0), dst0.numel(),
+                      ptr(src1), 0 if src1 is None else src1.numel(),
+                      ptr(dst1), 0 if dst1 is None else dst1.numel())
+            return
         mark = _LOG.begin() if _LOG is not None else None
         _lib.call("tnb_block_gather", ptr(seg), self.n_seg, ptr(cmap), self.chunks, ptr(tsrc),
                   ptr(tcf), ptr(tld), self.n_term,
@@ -284,6 +336,13 @@ class GemmTable:
             work = torch.zeros(max(self.work_bytes, 1), dtype=torch.uint8, device=dev)
             self._dev = (torch.from_numpy(self.table).to(dev),
                          torch.from_numpy(self.tile_map).to(dev), work)
+        if _REC is not None:
+            _lib.call("tnb_seq_add_gemm", _REC.handle, ptr(self._dev[0]), self.n_gemm,
+                      ptr(self._dev[1]), self.tiles, self.kind, ptr(a), a.numel(), ptr(b),
+                      b.numel(), ptr(c), c.numel(),
+                      ptr(self._dev[2]) if self.work_bytes else None, self.work_bytes,
+                      self.n_counters)
+            return
         mark = _LOG.begin() if _LOG is not None else None
         _lib.call("tnb_grouped_gemm_f64", ptr(self._dev[0]), self.n_gemm, ptr(self._dev[1]),
                   self.tiles, self.kind, ptr(a), a.numel(), ptr(b), b.numel(), ptr(c),

@@ -34,6 +34,19 @@ SIGNATURES = {
     "tnb_multi_dot_work_bytes": (_i64, [_i64, _i64]),
     "tnb_multi_dot": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
     "tnb_lanczos_reorth": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "tnb_seq_create": (_i32, [ctypes.POINTER(_vp)]),
+    "tnb_seq_destroy": (None, [_vp]),
+    "tnb_seq_length": (_i64, [_vp]),
+    "tnb_seq_add_gather": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64,
+                                  _vp, _i64, _vp, _i64, _vp, _i64]),
+    "tnb_seq_add_gemm": (_i32, [_vp, _vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
+                                _i64, _vp, _i64, _i64]),
+    "tnb_seq_append": (_i32, [_vp, _vp]),
+    "tnb_seq_run": (_i32, [_vp, _i32, _vp, _vp, _vp]),
+    "tnb_lanczos_solve": (_i32, [_vp, _vp, _vp, _i64, _i32, _f64, _i32, _vp, _vp, _i64, _vp,
+                                 _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
+    "tnb_lanczos_ritz": (_i32, [_vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                _i64, _vp, _vp]),
     "tnb_set_pdl": (_i32, [_i32]),
     "tnb_version": (_i32, []),
     "tnb_last_error": (ctypes.c_char_p, []),

@@ -110,14 +110,16 @@ def lanczos(matvec: Callable[[SymmetricTensor], SymmetricTensor], v: SymmetricTe
     return float(values[0]), out
 
 
-class LanczosGraph:
+class DeviceLanczos:
     """The reference's Lanczos (``network/dmrg.py:106-227``) with the whole recurrence on
-    the device: the ``ncv`` matvecs, every ``alpha``/``beta``, the three-term update and the
-    happy-breakdown stop run inside one captured CUDA graph with device-resident scalars.
-    The host then makes one synchronising read of the tridiagonal, solves it with
-    ``np.linalg.eigh`` exactly as the reference does, and a second small graph forms and
-    normalises the Ritz vector (and, in the precision form, applies the FP64 correction
-    program for the Rayleigh-quotient energy)."""
+    the device: one library call (``tnb_lanczos_solve``) launches the ``ncv`` matvecs --
+    the program's recorded launch sequence replayed on each Krylov vector -- every
+    ``alpha``/``beta``, the three-term update and the happy-breakdown stop, with
+    device-resident scalars.  The host then makes one synchronising read of the
+    tridiagonal, solves it with ``np.linalg.eigh`` exactly as the reference does, and a
+    second call (``tnb_lanczos_ritz``) forms and normalises the Ritz vector (and, in the
+    precision form, applies the FP64 correction program for the Rayleigh-quotient
+    energy)."""
 
     def __init__(self, program, ncv: int, tol: float = 1e-13, correct=None,
                  reorthogonalize: bool | None = None) -> None:
@@ -140,85 +142,34 @@ class LanczosGraph:
         self.V = torch.zeros((ncv + 1, max(n, 1)), **f64)
         self.W = torch.zeros(max(n, 1), **f64)
         self.W2 = torch.zeros(max(n, 1), **f64)
-        self.x = torch.zeros(max(n, 1), **f64)
-        self.out = torch.zeros(max(n, 1), **f64)
         self.state = torch.zeros(3 * ncv + 2, **f64)
         self.scal = torch.zeros(2, **f64)  # [0] a squared norm, [1] the corrected energy
         self.coef = torch.zeros(ncv, **f64)
         self.ptrs = torch.tensor([self.V[k].data_ptr() for k in range(ncv)], dtype=torch.int64,
                                  device=dev)
-        self.work = torch.zeros(int(_lib.load().tnb_dot_work_bytes(n)), dtype=torch.uint8,
-                                device=dev)
-        self.mwork = torch.zeros(int(_lib.load().tnb_multi_dot_work_bytes(n, ncv)),
-                                 dtype=torch.uint8, device=dev)
+        lib = _lib.load()
+        self.work = torch.zeros(int(lib.tnb_dot_work_bytes(n)), dtype=torch.uint8, device=dev)
+        self.mwork = torch.zeros(int(lib.tnb_multi_dot_work_bytes(n, ncv)) if self.reorth
+                                 else 1, dtype=torch.uint8, device=dev)
         self.gs = torch.zeros(ncv, **f64)
         self.runs = ops._runs(s)
         self._host_state = torch.zeros(3 * ncv + 2, dtype=torch.float64).pin_memory()
-        side = torch.cuda.Stream()
-        side.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(side):
-            self._solve_body()
-            self._finish_body()
-        torch.cuda.current_stream().wait_stream(side)
-        self.g1, self.g2 = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.g1):
-            self._solve_body()
-        with torch.cuda.graph(self.g2):
-            self._finish_body()
+        self._host_coef = torch.zeros(ncv, dtype=torch.float64).pin_memory()
 
-    def _dot(self, a, b, out) -> None:
+    def launch(self, x: torch.Tensor) -> None:
+        """Enqueue the recurrence from start vector ``x`` (an arena of ``n`` doubles)."""
         from tenet import _exec, _lib
 
-        r = self.runs
-        _lib.call("tnb_weighted_dot", _exec.ptr(a), _exec.ptr(b), self.n, _exec.ptr(r.start),
-                  _exec.ptr(r.weight), r.n_runs, _exec.ptr(self.work), _exec.ptr(out),
-                  _exec.stream_ptr())
+        P, p, r = _exec.ptr, self.program, self.runs
+        _lib.call("tnb_lanczos_solve", p.seq.handle, P(p.x_slot), P(p.y_slot), self.n,
+                  self.ncv, float(self.tol), int(self.reorth), P(x), P(self.V),
+                  self.V.stride(0), P(self.W), P(self.state), P(self.scal),
+                  P(self.ptrs), P(self.gs), P(r.start), P(r.weight), r.n_runs, P(self.work),
+                  P(self.mwork), _exec.stream_ptr())
 
-    def _solve_body(self) -> None:
-        from tenet import _exec, _lib
-
-        n, ncv, V, W, st = self.n, self.ncv, self.V, self.W, self.state
-        P = _exec.ptr
-        sp = _exec.stream_ptr()
-        st.zero_()
-        self._dot(self.x, self.x, self.scal)
-        _lib.call("tnb_scale_rsqrt", n, P(self.scal), P(self.x), P(V[0]), sp)
-        for j in range(ncv):
-            self.program.run(V[j], W)
-            self._dot(V[j], W, st[j:j + 1])
-            _lib.call("tnb_lanczos_update", n, P(W), P(V[j]), P(V[j - 1]) if j else None, P(st),
-                      j, ncv, sp)
-            if self.reorth:
-                r = self.runs
-                for _ in range(2):  # classical Gram-Schmidt, twice
-                    _lib.call("tnb_multi_dot", n, j + 1, P(self.ptrs), P(W), P(r.start),
-                              P(r.weight), r.n_runs, P(self.mwork), P(self.gs), sp)
-                    _lib.call("tnb_lanczos_reorth", n, j + 1, P(self.gs), P(self.ptrs), P(W),
-                              P(st), ncv, sp)
-            self._dot(W, W, st[2 * ncv + j:2 * ncv + j + 1])
-            _lib.call("tnb_lanczos_next", n, P(W), P(V[j + 1]), P(st), j, ncv, float(self.tol),
-                      sp)
-
-    def _finish_body(self) -> None:
-        from tenet import _exec, _lib
-
-        P = _exec.ptr
-        sp = _exec.stream_ptr()
-        _lib.call("tnb_lincomb", self.n, self.ncv, P(self.coef), P(self.ptrs), P(self.out), sp)
-        self._dot(self.out, self.out, self.scal)
-        _lib.call("tnb_scale_rsqrt", self.n, P(self.scal), P(self.out), P(self.out), sp)
-        if self.correct is not None:
-            self.correct.run(self.out, self.W2)
-            self._dot(self.out, self.W2, self.scal[1:2])
-
-    def solve(self, v: SymmetricTensor) -> tuple[float, SymmetricTensor]:
-        if v.structure != self.program.in_struct:
-            raise ValueError("LanczosGraph: the start vector's structure differs")
-        if self.n == 0:
-            return 0.0, v
-        self.x.copy_(v.arena)
-        self.g1.replay()
-        self._host_state.copy_(self.state)  # the one synchronising read of the solve
+    def tridiagonal(self) -> tuple[np.ndarray, np.ndarray]:
+        """Ground eigenpair of the recorded tridiagonal (one synchronising read)."""
+        self._host_state.copy_(self.state)
         st = self._host_state.numpy()
         ncv = self.ncv
         m = int(st[3 * ncv])
@@ -227,9 +178,31 @@ class LanczosGraph:
         values, states = np.linalg.eigh(tri)
         coef = np.zeros(ncv)
         coef[:m] = states[:, 0]
-        self.coef.copy_(torch.from_numpy(coef))
-        self.g2.replay()
-        out = SymmetricTensor(v.structure, arena=self.out[: self.n].clone())
+        return values, coef
+
+    def ritz(self, coef: np.ndarray, out: torch.Tensor) -> None:
+        """Enqueue the normalised Ritz vector ``sum_j coef[j] v_j`` into ``out`` (and the
+        corrected energy into ``scal[1]`` in the precision form)."""
+        from tenet import _exec, _lib
+
+        P, c, r = _exec.ptr, self.correct, self.runs
+        self._host_coef.numpy()[:] = coef
+        self.coef.copy_(self._host_coef, non_blocking=True)
+        _lib.call("tnb_lanczos_ritz", c.seq.handle if c is not None else None,
+                  P(c.x_slot) if c is not None else None, P(c.y_slot) if c is not None else None,
+                  self.n, self.ncv, P(self.coef), P(self.ptrs), P(out), P(self.W2),
+                  P(self.scal), P(r.start), P(r.weight), r.n_runs, P(self.work),
+                  _exec.stream_ptr())
+
+    def solve(self, v: SymmetricTensor) -> tuple[float, SymmetricTensor]:
+        if v.structure != self.program.in_struct:
+            raise ValueError("DeviceLanczos: the start vector's structure differs")
+        if self.n == 0:
+            return 0.0, v
+        self.launch(v.arena)
+        values, coef = self.tridiagonal()
+        out = SymmetricTensor.empty(v.structure)
+        self.ritz(coef, out.arena)
         if self.correct is not None:
             return float(self.scal[1].item()), out
         return float(values[0]), out
@@ -460,7 +433,7 @@ class Env:
         return hit["captured"]["matvec"]
 
     def solve(self, n: int, aa: SymmetricTensor, ncv: int) -> tuple[float, SymmetricTensor]:
-        """Ground Ritz pair at bond n by the device-resident Lanczos (``LanczosGraph``)."""
+        """Ground Ritz pair at bond n by the device-resident Lanczos (``DeviceLanczos``)."""
         hit = self._bond(n, aa.structure, self.precision)
         correct = None
         if self.precision != "f64":
@@ -468,7 +441,7 @@ class Env:
         key = ("lanczos", ncv)
         lg = hit["captured"].get(key)
         if lg is None or lg.correct is not correct:
-            lg = LanczosGraph(hit["program"], ncv, correct=correct)
+            lg = DeviceLanczos(hit["program"], ncv, correct=correct)
             hit["captured"][key] = lg
         return lg.solve(aa)
 

@@ -187,7 +187,14 @@ class ChainProgram:
         self.a_bufs = [torch.empty(max(1, lk.a_size), **f64) for lk in self.links]
         self.c_bufs = [torch.empty(max(1, lk.c_size), **f64) for lk in self.links]
         self.b_bufs = [torch.empty(max(1, lk.b_size), **f64) for lk in self.links]
+        # placeholder input/output: the recorded sequence reads and writes these, and a
+        # replay substitutes the caller's vectors for them
+        self.x_slot = torch.zeros(max(1, layout(self.in_struct).size), **f64)
+        self.y_slot = torch.zeros(max(1, layout(self.out_struct).size), **f64)
         self.refresh()
+        self.seq = _exec.Seq()
+        with self.seq:
+            self._run_tables(self.x_slot, self.y_slot)
         self._built = True
 
     def refresh(self) -> None:
@@ -205,6 +212,15 @@ class ChainProgram:
         return 2 * len(self.links) + 1
 
     def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``out = chain(x)`` on the current stream: one replay of the recorded sequence
+        (or launch by launch while a ``LaunchLog`` times each kernel)."""
+        if _exec._LOG is None and _exec._REC is None:
+            self.seq.run({self.x_slot.data_ptr(): x.data_ptr(),
+                          self.y_slot.data_ptr(): out.data_ptr()})
+            return out
+        return self._run_tables(x, out)
+
+    def _run_tables(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         src = x
         for lk, ab, bb, cb in zip(self.links, self.a_bufs, self.b_bufs, self.c_bufs):
             lk.a_gather.run(src, ab)

@@ -38,3 +38,31 @@ def test_refusals_move_nothing_and_set_a_message():
                                 0, None, 0, None) == 1
     assert lib.tnb_grouped_gemm_f64(None, 1, None, 1, 7, None, 0, None, 0, None, 0, None, 0, 0,
                                     None) == 1
+
+
+def test_launch_sequence_bookkeeping_needs_no_gpu():
+    """Recording, appending and the refusals of the sequence API are host-only."""
+    import ctypes
+
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    assert lib.tnb_seq_create(ctypes.byref(h)) == 0
+    assert lib.tnb_seq_length(h) == 0
+    # recording borrows pointers; nothing is dereferenced until a replay
+    assert lib.tnb_seq_add_gather(h, 16, 1, 32, 1, 48, 64, 80, 1, 96, 4, 112, 4, None, 0, None,
+                                  0) == 0
+    assert lib.tnb_seq_add_gemm(h, 16, 1, 32, 1, 0, 48, 1, 64, 1, 80, 1, None, 0, 0) == 0
+    assert lib.tnb_seq_length(h) == 2
+    assert lib.tnb_seq_add_gemm(h, 16, -1, 32, 1, 0, 48, 1, 64, 1, 80, 1, None, 0, 0) == 1
+    assert lib.tnb_seq_append(h, h) == 1
+    h2 = ctypes.c_void_p()
+    assert lib.tnb_seq_create(ctypes.byref(h2)) == 0
+    assert lib.tnb_seq_append(h2, h) == 0 and lib.tnb_seq_append(h2, h) == 0
+    assert lib.tnb_seq_length(h2) == 4
+    assert lib.tnb_seq_run(h2, -1, None, None, None) == 1
+    assert lib.tnb_seq_run(None, 0, None, None, None) == 1
+    assert lib.tnb_lanczos_solve(None, None, None, 4, 2, 1e-13, 0, None, None, 4, None, None,
+                                 None, None, None, None, None, 1, None, None, None) == 1
+    assert lib.tnb_seq_length(None) == -1
+    lib.tnb_seq_destroy(h)
+    lib.tnb_seq_destroy(h2)

@@ -407,16 +407,16 @@ def test_ctmrg_z2_ising_matches_reference(golden_dir, name):
         assert bf == pytest.approx(r["onsager_beta_f"], rel=1e-6)
 
 
-def test_device_lanczos_graph_matches_reference(golden_dir):
-    """The whole recurrence in one captured graph: the reference's ncv=20 energy and the
-    same Ritz vector (up to sign) as the host-driven Lanczos; replays are repeatable."""
+def test_device_lanczos_matches_reference(golden_dir):
+    """The whole recurrence from one library call: the reference's ncv=20 energy and the
+    same Ritz vector (up to sign) as the host-driven Lanczos; repeated solves agree."""
     from tenet.program import heff2_program
 
     m = json.loads((golden_dir / "heff.json").read_text())
     h = np.load(golden_dir / "heff.npz")
     T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
     prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
-    lg = network.LanczosGraph(prog, 20)
+    lg = network.DeviceLanczos(prog, 20)
     e_host, v_host = network.lanczos(prog, T["aa"], ncv=20)
     for _ in range(2):
         e, v = lg.solve(T["aa"])
@@ -426,7 +426,7 @@ def test_device_lanczos_graph_matches_reference(golden_dir):
         sign = np.sign(a @ b)
         close(sign * a, b, 1e-10)
     # a Krylov space that breaks down early (ncv larger than the space allows)
-    small = network.LanczosGraph(prog, 60)
+    small = network.DeviceLanczos(prog, 60)
     e60, _ = small.solve(T["aa"])
     assert e60 == pytest.approx(network.lanczos(prog, T["aa"], ncv=60)[0], rel=1e-10)
 
@@ -456,3 +456,43 @@ def test_multi_dot_and_reorth_kernels():
     assert lib.tnb_lanczos_reorth(n, k, out.data_ptr(), ptrs.data_ptr(), y.data_ptr(), None, 1,
                                   s) == 0
     close(y.cpu().numpy(), xh - out.cpu().numpy() @ Vh, 1e-12)
+
+
+def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
+    """A chain program's recorded launch sequence, replayed with its placeholder buffers
+    patched to other vectors, gives bit-identical results to launching the same tables
+    one by one from the host, and can be captured in a CUDA graph."""
+    from tenet import _exec
+    from tenet.program import heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
+    assert len(prog.seq) == prog.launches + sum(lk.gemm.launches - 1 for lk in prog.links)
+    x = T["aa"].arena
+    y_seq = torch.full_like(prog.y_slot, float("nan"))
+    y_py = torch.full_like(prog.y_slot, float("nan"))
+    prog.run(x, y_seq)
+    prog._run_tables(x, y_py)
+    assert torch.equal(y_seq, y_py)
+    close(y_seq.cpu().numpy(), load(h, m["heff_aa"]).numpy_arena(), 1e-12)
+    # a sequence appended to itself twice replays both copies
+    s2 = _exec.Seq()
+    _lib.call("tnb_seq_append", s2.handle, prog.seq.handle)
+    _lib.call("tnb_seq_append", s2.handle, prog.seq.handle)
+    assert len(s2) == 2 * len(prog.seq)
+    # graph capture of a replay
+    g = torch.cuda.CUDAGraph()
+    y_g = torch.zeros_like(y_py)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        prog.run(x, y_g)
+    torch.cuda.current_stream().wait_stream(side)
+    y_g.zero_()
+    with torch.cuda.graph(g):
+        prog.run(x, y_g)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(y_g, y_py)
