@@ -284,6 +284,31 @@ int tnb_lanczos_ritz(const tnb_seq* correct, const void* x_slot, const void* y_s
                      double* w2, double* scal, const int64_t* run_start, const double* run_w,
                      int64_t n_runs, void* dot_work, void* stream);
 
+/*
+ * Host-side planner kernels (no device; plain loops over host arrays).  They replace the
+ * per-block loops of the table builder (the reference runs its block maps directly:
+ * ops/permutation.py:254-272, ops/repartition.py:298-316).
+ *
+ * tnb_plan_gather_rows: one TNB_SEG_WIDTH row per destination block r < n_rows from its
+ *   dims, destination strides, source row/column strides (n_rows x nd, row-major, the
+ *   source's permuted to destination axis order), offset, size and term range: dims
+ *   ordered by destination stride (descending; ties by source column, then row stride,
+ *   stable), extent-1 dims dropped, dims contiguous in destination and source merged,
+ *   a rank-1 unit row when nothing is left.  TNB_EINVAL when a row keeps more than
+ *   TNB_MAX_RANK dims.
+ * tnb_plan_compose: the sparse product of block maps a (n_a x 3: src, mid, coeff) and
+ *   b (n_b x 3: mid, dst, coeff): each (src, dst) pair once, in order of first occurrence
+ *   walking a in order and b's terms of each mid in their order, coefficients summed in
+ *   that order from zero.  Writes at most `cap` rows to `out`; returns the row count, -1
+ *   on a bad argument, -2 when `cap` is too small.
+ */
+int tnb_plan_gather_rows(int64_t n_rows, int32_t nd, const int64_t* dims, const int64_t* dstr,
+                         const int64_t* rstr, const int64_t* cstr, const int64_t* d_off,
+                         const int64_t* sizes, const int64_t* t_begin, const int64_t* t_end,
+                         int64_t buf, int64_t* rows);
+int64_t tnb_plan_compose(int64_t n_a, const double* a, int64_t n_b, const double* b, double* out,
+                         int64_t cap);
+
 /* Library version (major*10000 + minor*100 + patch). */
 int tnb_version(void);
 

@@ -14,7 +14,7 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = sorted((PKG / "csrc").glob("*.cu"))
+SOURCES = sorted([*(PKG / "csrc").glob("*.cu"), *(PKG / "csrc").glob("*.cpp")])
 OUT = PKG / "tenet" / "libtenet_b200.so"
 
 NVCC_FLAGS = [

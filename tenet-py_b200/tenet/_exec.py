@@ -93,6 +93,49 @@ class Seq:
 _REC: Seq | None = None
 
 
+_TORCH_DTYPE = {np.dtype(np.int64).str: torch.int64, np.dtype(np.int32).str: torch.int32,
+                np.dtype(np.float64).str: torch.float64}
+
+
+class Uploaded:
+    """Device copies of host arrays, made on the current stream.  A copy from pageable
+    host memory may still be in flight when the call returns, so a kernel on another
+    stream waits for the upload's event before first reading them (the serving loop runs
+    requests that share plan tables on different streams)."""
+
+    __slots__ = ("arrays", "stream", "event")
+
+    def __init__(self, host_arrays) -> None:
+        # one host->device copy: the arrays packed at 16-byte aligned offsets of one
+        # buffer, then typed views into its device copy
+        host_arrays = [np.ascontiguousarray(x) for x in host_arrays]
+        offs, total = [], 0
+        for x in host_arrays:
+            offs.append(total)
+            total += -(-x.nbytes // 16) * 16
+        packed = np.zeros(max(total, 16), dtype=np.uint8)
+        for x, o in zip(host_arrays, offs):
+            packed[o:o + x.nbytes] = x.reshape(-1).view(np.uint8)
+        dev_buf = torch.from_numpy(packed).to(device())
+        views = []
+        for x, o in zip(host_arrays, offs):
+            t = dev_buf[o:o + x.nbytes].view(_TORCH_DTYPE[x.dtype.str])
+            views.append(t.view(x.shape) if x.ndim > 1 else t)
+        self.arrays = tuple(views)
+        self.stream = stream_ptr()
+        self.event = torch.cuda.Event()
+        self.event.record()
+
+    def ready(self) -> tuple:
+        if self.event is not None and stream_ptr() != self.stream \
+                and not torch.cuda.is_current_stream_capturing():
+            if self.event.query():
+                self.event = None
+            else:
+                torch.cuda.current_stream().wait_event(self.event)
+        return self.arrays
+
+
 class LaunchLog:
     """Optional per-launch record: ``(kind, start event, end event, work)`` for every
     library kernel launched while installed, events on the launching stream.  ``work``
@@ -145,41 +188,28 @@ _LOG: LaunchLog | None = None
 # gather tables
 
 
-def _group(terms):
-    by_dst: dict = {}
-    for s, d, c in terms:
-        by_dst.setdefault(d, []).append((s, c))
-    return by_dst
-
-
-def _normalise(dims, dstr, rstr, cstr):
-    """Order dims by destination stride (descending), drop extent-1 dims, merge dims that
-    are contiguous in destination and source alike."""
-    order = sorted(range(len(dims)), key=lambda k: (-dstr[k], -cstr[k], -rstr[k]))
-    out = []
-    for k in order:
-        if dims[k] == 1:
-            continue
-        d, a, b, c = dims[k], dstr[k], rstr[k], cstr[k]
-        if out:
-            pd, pa, pb, pc = out[-1]
-            if pa == a * d and pb == b * d and pc == c * d:
-                out[-1] = (pd * d, a, b, c)
-                continue
-        out.append((d, a, b, c))
-    if not out:
-        out = [(1, 1, 0, 0)]
-    if len(out) > MAX_RANK:
-        raise ValueError(f"a block of rank {len(out)} exceeds the kernel's {MAX_RANK}")
-    return out
+def _plan_rows(D, DS, RS, CS, d_off, sizes, tb, te, buf):
+    """Descriptor rows by the library's host planner (``tnb_plan_gather_rows``)."""
+    R, nd = D.shape
+    rows = np.zeros((R, SEG_W), np.int64)
+    if not R:
+        return rows
+    arrs = [np.ascontiguousarray(x, dtype=np.int64) for x in (D, DS, RS, CS, d_off, sizes, tb, te)]
+    status = _lib.load().tnb_plan_gather_rows(R, nd, *(x.ctypes.data for x in arrs), buf,
+                                              rows.ctypes.data)
+    if status != 0:
+        raise ValueError(f"a block of rank above the kernel's {MAX_RANK} in a gather plan")
+    return rows
 
 
 def gather_rows(src_s: TensorStructure, src_kind: str, dst_s: TensorStructure, dst_kind: str,
                 perm, terms, buf: int = 0, dst_keep=None):
-    """Rows + term arrays executing ``dst[j] = sum c * transpose(src[i], perm)``.
-
-    ``dst_keep`` optionally restricts the emitted destination blocks (a boolean mask).
-    """
+    """Rows + term arrays executing ``dst[j] = sum c * transpose(src[i], perm)``: one row
+    per destination block that has terms (in block order, its terms in the order given),
+    then one zero-writing row per destination block without any.  ``dst_keep``
+    optionally restricts the emitted destination blocks (a boolean mask).  Returns
+    ``(rows (R, SEG_W), term sources, term coefficients, term leading dimensions)`` as
+    arrays, term ranges relative to this part."""
     sl, dl = layout(src_s), layout(dst_s)
     if src_kind == "matrix":
         sm = matrix_layout(src_s)
@@ -193,44 +223,36 @@ def gather_rows(src_s: TensorStructure, src_kind: str, dst_s: TensorStructure, d
         d_str = dm.rstride * dm.block_ld[:, None] + dm.cstride
     else:
         d_off, d_str = dl.offsets, dl.strides
-    perm = list(perm)
-    rows, tsrc, tcf, tld = [], [], [], []
-    for j, lst in sorted(_group(terms).items()):
-        if dst_keep is not None and not dst_keep[j]:
-            continue
-        i0 = lst[0][0]
-        dims = [int(x) for x in dl.shapes[j]]
-        segs = _normalise(dims, [int(x) for x in d_str[j]], [int(s_rs[i0][p]) for p in perm],
-                          [int(s_cs[i0][p]) for p in perm])
-        row = np.zeros(SEG_W, dtype=np.int64)
-        row[0] = d_off[j]
-        row[1] = dl.sizes[j]
-        row[2] = len(segs)
-        row[3] = len(tsrc)
-        row[4] = len(tsrc) + len(lst)
-        row[5] = buf
-        for k, (d, a, b, c) in enumerate(segs):
-            row[8 + k], row[16 + k], row[24 + k], row[32 + k] = d, a, b, c
-        rows.append(row)
-        for i, c in lst:
-            tsrc.append(int(s_off[i]))
-            tcf.append(float(c))
-            tld.append(int(s_ld[i]))
-    # destination blocks with no term at all are written as zeros
-    covered = set(_group(terms))
-    for j in range(len(dl.sizes)):
-        if j in covered or (dst_keep is not None and not dst_keep[j]):
-            continue
-        dims = [int(x) for x in dl.shapes[j]]
-        segs = _normalise(dims, [int(x) for x in d_str[j]], [0] * len(dims), [0] * len(dims))
-        row = np.zeros(SEG_W, dtype=np.int64)
-        row[0], row[1], row[2] = d_off[j], dl.sizes[j], len(segs)
-        row[3] = row[4] = len(tsrc)
-        row[5] = buf
-        for k, (d, a, b, c) in enumerate(segs):
-            row[8 + k], row[16 + k], row[24 + k], row[32 + k] = d, a, b, c
-        rows.append(row)
-    return rows, tsrc, tcf, tld
+    perm = np.asarray(perm, dtype=np.int64)
+    n_dst = len(dl.sizes)
+    keep = np.ones(n_dst, bool) if dst_keep is None else np.asarray(dst_keep, bool)
+    if len(terms):
+        tarr = np.asarray(terms, dtype=np.float64).reshape(-1, 3)
+        ts, td, tc = tarr[:, 0].astype(np.int64), tarr[:, 1].astype(np.int64), tarr[:, 2]
+    else:
+        ts = td = np.zeros(0, np.int64)
+        tc = np.zeros(0)
+    covered = np.zeros(n_dst, bool)
+    covered[td] = True
+    sel = keep[td]
+    ts, td, tc = ts[sel], td[sel], tc[sel]
+    o = np.argsort(td, kind="stable")
+    ts, td, tc = ts[o], td[o], tc[o]
+    js, first, counts = np.unique(td, return_index=True, return_counts=True)
+    i0 = ts[first]
+    if perm.size:
+        RS, CS = s_rs[i0][:, perm], s_cs[i0][:, perm]
+    else:
+        RS = CS = np.zeros((len(js), 0), np.int64)
+    parts = [(js, dl.shapes[js], d_str[js], RS, CS, first, first + counts)]
+    zj = np.nonzero(~covered & keep)[0]
+    nt = len(ts)
+    z = np.zeros((len(zj), dl.shapes.shape[1]), np.int64)
+    parts.append((zj, dl.shapes[zj], d_str[zj], z, z, np.full(len(zj), nt), np.full(len(zj), nt)))
+    rows = [_plan_rows(D, DS, RS_, CS_, d_off[j], dl.sizes[j], tb, te, buf)
+            for j, D, DS, RS_, CS_, tb, te in parts]
+    return (np.concatenate(rows), s_off[ts].astype(np.int64), tc.astype(np.float64),
+            s_ld[ts].astype(np.int64))
 
 
 class GatherTable:
@@ -259,10 +281,8 @@ class GatherTable:
 
     def device_arrays(self):
         if self._dev is None:
-            dev = device()
-            self._dev = tuple(torch.from_numpy(x).to(dev) for x in
-                              (self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map))
-        return self._dev
+            self._dev = Uploaded((self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map))
+        return self._dev.ready()
 
     def run(self, src0, dst0, src1=None, dst1=None) -> None:
         if self.n_seg == 0:
@@ -288,22 +308,21 @@ class GatherTable:
 def make_gather(*parts) -> GatherTable:
     """Concatenate one or more ``gather_rows`` results into a single table."""
     rows, tsrc, tcf, tld = [], [], [], []
-    for r, s, c, ld in parts:
-        base = len(tsrc)
-        for row in r:
-            row = row.copy()
-            row[3] += base
-            row[4] += base
-            rows.append(row)
-        tsrc += s
-        tcf += c
-        tld += ld
-    chunk = 0
-    for row in rows:
-        row[6] = chunk
-        chunk += (int(row[1]) + CHUNK - 1) // CHUNK
-    seg = np.stack(rows) if rows else np.zeros((0, SEG_W), np.int64)
-    return GatherTable(seg, tsrc, tcf, tld)
+    base = 0
+    for r, ts, tc, tl in parts:
+        r = np.array(r, dtype=np.int64).reshape(-1, SEG_W)
+        r[:, 3:5] += base
+        rows.append(r)
+        tsrc.append(np.asarray(ts, np.int64))
+        tcf.append(np.asarray(tc, np.float64))
+        tld.append(np.asarray(tl, np.int64))
+        base += len(ts)
+    seg = np.concatenate(rows) if rows else np.zeros((0, SEG_W), np.int64)
+    per = (seg[:, 1] + CHUNK - 1) // CHUNK
+    seg[:, 6] = np.cumsum(per) - per
+    return GatherTable(seg, np.concatenate(tsrc) if tsrc else np.zeros(0, np.int64),
+                       np.concatenate(tcf) if tcf else np.zeros(0),
+                       np.concatenate(tld) if tld else np.zeros(0, np.int64))
 
 
 # ---------------------------------------------------------------------------------------
@@ -325,29 +344,48 @@ class GemmTable:
         per = table[:, 11] if len(table) else np.zeros(0, np.int64)
         self.tile_map = np.repeat(np.arange(len(table), dtype=np.int32), per)
         self._dev = None
+        self._work: dict = {}
+        self._private = False
+
+    def private(self) -> GemmTable:
+        """The same table with a split-K work buffer of its own (a compiled program's
+        copy, so that programs sharing a cached table can run on different streams)."""
+        import copy
+
+        q = copy.copy(self)
+        q._work = {}
+        q._private = True
+        return q
+
+    def work(self):
+        """The split-K scratch: the table's own when private, else one per stream."""
+        if not self.work_bytes:
+            return None
+        key = 0 if self._private else stream_ptr()
+        buf = self._work.get(key)
+        if buf is None:
+            buf = torch.zeros(self.work_bytes, dtype=torch.uint8, device=device())
+            self._work[key] = buf
+        return buf
 
     def run(self, a, b, c) -> None:
-        """Launch on the current stream.  The split-K work buffer belongs to this table, so
-        one table must not run on two streams at once."""
+        """Launch on the current stream.  The split-K counters of a private table belong
+        to it, so one private table must not run on two streams at once."""
         if self.n_gemm == 0:
             return
         if self._dev is None:
-            dev = device()
-            work = torch.zeros(max(self.work_bytes, 1), dtype=torch.uint8, device=dev)
-            self._dev = (torch.from_numpy(self.table).to(dev),
-                         torch.from_numpy(self.tile_map).to(dev), work)
+            self._dev = Uploaded((self.table, self.tile_map))
+        table, tile_map = self._dev.ready()
+        work = self.work()
         if _REC is not None:
-            _lib.call("tnb_seq_add_gemm", _REC.handle, ptr(self._dev[0]), self.n_gemm,
-                      ptr(self._dev[1]), self.tiles, self.kind, ptr(a), a.numel(), ptr(b),
-                      b.numel(), ptr(c), c.numel(),
-                      ptr(self._dev[2]) if self.work_bytes else None, self.work_bytes,
-                      self.n_counters)
+            _lib.call("tnb_seq_add_gemm", _REC.handle, ptr(table), self.n_gemm, ptr(tile_map),
+                      self.tiles, self.kind, ptr(a), a.numel(), ptr(b), b.numel(), ptr(c),
+                      c.numel(), ptr(work), self.work_bytes, self.n_counters)
             return
         mark = _LOG.begin() if _LOG is not None else None
-        _lib.call("tnb_grouped_gemm_f64", ptr(self._dev[0]), self.n_gemm, ptr(self._dev[1]),
+        _lib.call("tnb_grouped_gemm_f64", ptr(table), self.n_gemm, ptr(tile_map),
                   self.tiles, self.kind, ptr(a), a.numel(), ptr(b), b.numel(), ptr(c),
-                  c.numel(), ptr(self._dev[2]) if self.work_bytes else None, self.work_bytes,
-                  self.n_counters, stream_ptr())
+                  c.numel(), ptr(work), self.work_bytes, self.n_counters, stream_ptr())
         if _LOG is not None:
             _LOG.end("grouped_gemm_tc" if self.kind in (TILE_TC_TF32, TILE_TC_3XBF16)
                      else "grouped_gemm_f64", mark, self.flops)
@@ -380,19 +418,38 @@ def _is_skinny(p) -> bool:
     return p[0] >= SKINNY_ROWS and p[1] <= SKINNY_MAX and p[2] <= SKINNY_MAX
 
 
-class GemmGroup:
-    """One composition's products, split into at most two launches: the tall skinny ones
-    and the rest (so an MPO-like product never occupies a 64-wide tile)."""
+#: A coupled-sector product goes to the tensor cores in the precision form only when it
+#: is at least one full 128 x 64 x 64 tile of work; smaller ones stay on the FP64 path.
+TC_MIN_FLOPS = 2 * 128 * 64 * 64
 
-    def __init__(self, products, precision: str = "f64") -> None:
+
+def tc_worthy(p, min_flops: int | None = None) -> bool:
+    M, N, K = p[0], p[1], p[2]
+    return K >= 16 and 2 * M * N * K >= (TC_MIN_FLOPS if min_flops is None else min_flops)
+
+
+class GemmGroup:
+    """One composition's products in at most three launches: the tall skinny ones, the
+    rest in FP64 tiles, and -- in the precision form -- the products big enough to be
+    dense contractions on the tcgen05 tensor cores (``tc_min_flops`` overrides the size
+    rule)."""
+
+    def __init__(self, products, precision: str = "f64", tc_min_flops: int | None = None):
         skinny = [p for p in products if _is_skinny(p)]
         rest = [p for p in products if not _is_skinny(p)]
+        tc = []
+        if precision in TC_KINDS:
+            tc = [p for p in rest if tc_worthy(p, tc_min_flops)]
+            rest = [p for p in rest if not tc_worthy(p, tc_min_flops)]
         self.parts = []
+        if tc:
+            self.parts.append(make_gemm(tc, TC_KINDS[precision]))
         if rest:
-            kind = TC_KINDS[precision] if precision in TC_KINDS else choose_kind(rest)
-            self.parts.append(make_gemm(rest, kind))
+            self.parts.append(make_gemm(rest, choose_kind(rest)))
         if skinny:
             self.parts.append(make_gemm(skinny, TILE_SKINNY))
+        self.tensor_core = bool(tc)
+        self.products = list(products)
         self.flops = sum(p.flops for p in self.parts)
         self.tiles = sum(p.tiles for p in self.parts)
         self.n_gemm = sum(p.n_gemm for p in self.parts)
@@ -406,6 +463,13 @@ class GemmGroup:
     def run(self, a, b, c) -> None:
         for p in self.parts:
             p.run(a, b, c)
+
+    def private(self) -> GemmGroup:
+        import copy
+
+        q = copy.copy(self)
+        q.parts = [p.private() for p in self.parts]
+        return q
 
 
 def _splits(K: int, out_tiles_total: int) -> tuple[int, int]:
@@ -449,11 +513,21 @@ def make_gemm(products, kind: int | None = None, split_k: bool = True) -> GemmTa
 # weighted runs for inner / norm
 
 
-@dataclass
 class DotRuns:
-    start: torch.Tensor
-    weight: torch.Tensor
-    n_runs: int
+    """Equal-weight element runs of a structure (device arrays, see ``Uploaded``)."""
+
+    def __init__(self, starts, weights) -> None:
+        self._up = Uploaded((np.asarray(starts, dtype=np.int64),
+                             np.asarray(weights, dtype=np.float64)))
+        self.n_runs = len(weights)
+
+    @property
+    def start(self) -> torch.Tensor:
+        return self._up.ready()[0]
+
+    @property
+    def weight(self) -> torch.Tensor:
+        return self._up.ready()[1]
 
 
 def make_runs(s: TensorStructure) -> DotRuns:
@@ -467,9 +541,7 @@ def make_runs(s: TensorStructure) -> DotRuns:
         starts.append(int(lay.offsets[b]))
         weights.append(w)
     starts.append(lay.size)
-    dev = device()
-    return DotRuns(torch.tensor(starts, dtype=torch.int64, device=dev),
-                   torch.tensor(weights, dtype=torch.float64, device=dev), len(weights))
+    return DotRuns(starts, weights)
 
 
 _WORK: dict = {}

@@ -47,6 +47,9 @@ SIGNATURES = {
                                  _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
     "tnb_lanczos_ritz": (_i32, [_vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                 _i64, _vp, _vp]),
+    "tnb_plan_gather_rows": (_i32, [_i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
+                                    _vp]),
+    "tnb_plan_compose": (_i64, [_i64, _vp, _i64, _vp, _vp, _i64]),
     "tnb_set_pdl": (_i32, [_i32]),
     "tnb_version": (_i32, []),
     "tnb_last_error": (ctypes.c_char_p, []),

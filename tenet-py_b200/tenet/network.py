@@ -194,18 +194,22 @@ class DeviceLanczos:
                   P(self.scal), P(r.start), P(r.weight), r.n_runs, P(self.work),
                   _exec.stream_ptr())
 
+    def finish(self) -> tuple[float, SymmetricTensor]:
+        """After ``launch``: read the tridiagonal, form the Ritz vector, return the pair."""
+        values, coef = self.tridiagonal()
+        out = SymmetricTensor.empty(self.program.in_struct)
+        self.ritz(coef, out.arena)
+        if self.correct is not None:
+            return float(self.scal[1].item()), out
+        return float(values[0]), out
+
     def solve(self, v: SymmetricTensor) -> tuple[float, SymmetricTensor]:
         if v.structure != self.program.in_struct:
             raise ValueError("DeviceLanczos: the start vector's structure differs")
         if self.n == 0:
             return 0.0, v
         self.launch(v.arena)
-        values, coef = self.tridiagonal()
-        out = SymmetricTensor.empty(v.structure)
-        self.ritz(coef, out.arena)
-        if self.correct is not None:
-            return float(self.scal[1].item()), out
-        return float(values[0]), out
+        return self.finish()
 
 
 # ---------------------------------------------------------------------------------------
@@ -282,16 +286,34 @@ class MPO:
         return self.sites[n]
 
 
-def heisenberg_mpo_su2(n_sites: int, j: float = 1.0) -> MPO:
-    """``H = J sum_i S_i . S_{i+1}`` on spin-1/2 SU(2) sites, as site tensors.
+def identity_w(aux, phys) -> SymmetricTensor:
+    """A spectator MPO site: ``id(aux) (x) id(phys)`` on ``(wl IN, p OUT, p IN, wr OUT)``
+    (``network/mps.py:1170-1182``), the identity that carries an open channel of a
+    non-adjacent term through a site it does not touch.  Built as the reference does:
+    the outer product of the two identities, then put on the MPO partition
+    (``_as_w``, ``network/mps.py:1044-1056``)."""
+    from tenet import ops
+    from tenet.structure import IN, Leg
 
-    The MPO bond carries the finite-state machine of a nearest-neighbour invariant term:
-    a spin-0 "not started" channel, a spin-1 channel carrying the first ``S``, and a spin-0
-    "finished" channel -- multiplets ``{0: 2, 2: 1}`` in the bulk, as the reference's
+    t = ops.einsum("ba,pq->apqb", ops.identity((aux,)), ops.identity((Leg(phys, IN),)))
+    return ops.transpose(ops.repartition(t, (1, 3), (0, 2)), (2, 0, 3, 1))
+
+
+def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
+    """``H = J sum_i S_i . S_{i+1} + J2 sum_i S_i . S_{i+2}`` on spin-1/2 SU(2) sites, as
+    site tensors.
+
+    The MPO bond carries the finite-state machine of the invariant terms: a spin-0 "not
+    started" channel, a spin-1 channel carrying the first ``S``, and a spin-0 "finished"
+    channel -- multiplets ``{0: 2, 2: 1}`` in the bulk, as the reference's
     ``MPO.from_terms(...).materialize()`` builds for ``spin_half(SU2).ops["S.S"]``.  In the
     fusion-tree basis of the blocks ``(P, m | x, p)`` the reduced coefficients are 1 for
     the identity channels, ``sqrt(3/2)`` for opening the spin-1 channel and
-    ``-sqrt(3/8) J`` for closing it (their product is ``-3/4 J``, the reduced S.S).
+    ``-sqrt(3/8) J`` for closing it (their product is ``-3/4 J``, the reduced S.S).  With
+    ``j2`` a second spin-1 channel carries the opened ``S`` one site further: the open
+    channel passes a site through the spectator identity (``identity_w``) and closes
+    with ``-sqrt(3/8) J2`` -- the reference's reading of a non-adjacent invariant S.S
+    term in ``from_terms`` (bulk multiplets ``{0: 2, 2: 2}``).
     """
     import math
 
@@ -301,17 +323,22 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0) -> MPO:
     if n_sites < 2:
         raise ValueError("a Heisenberg chain needs at least two sites")
     phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+
     # states per bond: list of (label, sector two_j) in degeneracy order within a sector
     def states(b):
         if b == 0:
-            return [("start", 0)]
-        if b == n_sites:
-            return [("done", 0)]
-        if b == 1:
-            return [("start", 0), ("open", 2)]
-        if b == n_sites - 1:
-            return [("done", 0), ("open", 2)]
-        return [("start", 0), ("done", 0), ("open", 2)]
+            st = [("start", 0)]
+        elif b == n_sites:
+            st = [("done", 0)]
+        elif b == 1:
+            st = [("start", 0), ("open", 2)]
+        elif b == n_sites - 1:
+            st = [("done", 0), ("open", 2)]
+        else:
+            st = [("start", 0), ("done", 0), ("open", 2)]
+        if j2 and 2 <= b <= n_sites - 1:
+            st.append(("open2", 2))
+        return st
 
     def space(st):
         count: dict = {}
@@ -323,9 +350,17 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0) -> MPO:
         sec = dict(st)[label]
         return sec, [lab for lab, s in st if s == sec].index(label)
 
-    opn, cls = math.sqrt(1.5), -math.sqrt(3.0 / 8.0) * j
+    opn, cls = math.sqrt(1.5), -math.sqrt(3.0 / 8.0)
     rules = [("start", "start", 1.0), ("done", "done", 1.0), ("start", "open", opn),
-             ("open", "done", cls)]
+             ("open", "done", cls * j), ("open2", "done", cls * j2)]
+    spec = None
+    if j2:
+        # the spectator's reduced blocks, keyed like the site tensor's own block keys
+        v1 = GradedSpace.new(SU2, {SU2.sector(2): 1})
+        t = identity_w(Leg(v1, IN, True), phys)
+        tl, th = layout(t.structure), t.numpy_arena()
+        spec = {key: th[int(tl.offsets[b]):int(tl.offsets[b]) + int(tl.sizes[b])]
+                for b, key in enumerate(t.structure.keys)}
     sites = []
     for n in range(n_sites):
         sl, sr = states(n), states(n + 1)
@@ -333,20 +368,25 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0) -> MPO:
         s = TensorStructure(legs)
         lay = layout(s)
         host = np.zeros(lay.size)
-        for b, (ot, it) in enumerate(s.keys):
+        for b, key in enumerate(s.keys):
+            ot, it = key
             (ps, ms), _, c = ot
             (xs, pps), _, _ = it
-            if c != 1:
-                continue  # only the spin-1/2 coupled channel carries these operators
             shape = tuple(int(x) for x in lay.shapes[b])
             blk = np.zeros(shape)
-            for a, bb, v in rules:
-                if a not in dict(sl) or bb not in dict(sr):
-                    continue
-                xsec, xi = index(sl, a)
-                msec, mi = index(sr, bb)
-                if xsec == xs and msec == ms:
-                    blk[xi, 0, 0, mi] = v
+            if c == 1:  # the spin-1/2 coupled channel carries the single-site operators
+                for a, bb, v in rules:
+                    if a not in dict(sl) or bb not in dict(sr):
+                        continue
+                    xsec, xi = index(sl, a)
+                    msec, mi = index(sr, bb)
+                    if xsec == xs and msec == ms:
+                        blk[xi, 0, 0, mi] = v
+            if spec is not None and key in spec and "open" in dict(sl) \
+                    and "open2" in dict(sr):
+                _, xi = index(sl, "open")
+                _, mi = index(sr, "open2")
+                blk[xi, 0, 0, mi] = spec[key][0]
             o = int(lay.offsets[b])
             host[o:o + blk.size] = blk.ravel()
         sites.append(SymmetricTensor.from_numpy_arena(s, host))
@@ -360,10 +400,11 @@ class Env:
     CUDA-graph-captured chain program, rebuilt whenever the bond's tensors change."""
 
     def __init__(self, psi: MPS, h: MPO, *, compiled: bool = True,
-                 precision: str = "f64") -> None:
+                 precision: str = "f64", tc_min_flops: int | None = None) -> None:
         from tenet.structure import IN, Leg
 
         self.psi, self.h, self.compiled, self.precision = psi, h, compiled, precision
+        self.tc_min_flops = tc_min_flops
         n = len(psi)
         kl, kr = psi[0].legs[0], psi[n - 1].legs[2]
         wl, wr = h[0].legs[0], h[n - 1].legs[3]
@@ -409,7 +450,8 @@ class Env:
         if hit is None or hit["skey"] != skey:
             # one program per bond and precision; a new structure replaces it
             hit = {"skey": skey, "bound": (fl, fr), "captured": {},
-                   "program": heff2_program(fl, w1, w2, fr, structure, precision=precision)}
+                   "program": heff2_program(fl, w1, w2, fr, structure, precision=precision,
+                                            tc_min_flops=self.tc_min_flops)}
             self._prog[(n, precision)] = hit
         elif hit["bound"][0] is not fl or hit["bound"][1] is not fr:
             # same structures, new environment values: re-pack the fixed operands into the
@@ -432,18 +474,27 @@ class Env:
             hit["captured"]["matvec"] = GraphMatvec(hit["program"])
         return hit["captured"]["matvec"]
 
-    def solve(self, n: int, aa: SymmetricTensor, ncv: int) -> tuple[float, SymmetricTensor]:
-        """Ground Ritz pair at bond n by the device-resident Lanczos (``DeviceLanczos``)."""
-        hit = self._bond(n, aa.structure, self.precision)
+    def lanczos(self, n: int, structure, ncv: int) -> DeviceLanczos:
+        """The bond's device Lanczos.  In the precision form its matvec is the tensor-core
+        program, corrected by the FP64 one; when no product of the bond is big enough for
+        the tensor cores, the precision program is all FP64 and the FP64 program serves
+        alone, uncorrected."""
         correct = None
-        if self.precision != "f64":
-            correct = self._bond(n, aa.structure, "f64")["program"]
+        hit = self._bond(n, structure, "f64")
+        if self.precision != "f64" and \
+                hit["program"].tensor_core_candidates(self.tc_min_flops):
+            correct = hit["program"]
+            hit = self._bond(n, structure, self.precision)
         key = ("lanczos", ncv)
         lg = hit["captured"].get(key)
         if lg is None or lg.correct is not correct:
             lg = DeviceLanczos(hit["program"], ncv, correct=correct)
             hit["captured"][key] = lg
-        return lg.solve(aa)
+        return lg
+
+    def solve(self, n: int, aa: SymmetricTensor, ncv: int) -> tuple[float, SymmetricTensor]:
+        """Ground Ritz pair at bond n by the device-resident Lanczos (``DeviceLanczos``)."""
+        return self.lanczos(n, aa.structure, ncv).solve(aa)
 
     def correction(self, n: int):
         """The FP64 matvec that corrects a reduced-precision solve at bond n (None in FP64)."""
@@ -458,9 +509,20 @@ def _pair(left: SymmetricTensor, right: SymmetricTensor) -> SymmetricTensor:
     return ops.einsum("apx,xqr->apqr", left, right)
 
 
-def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3):
+def drain(gen):
+    """Run a step generator (``sweep_steps``, ``dmrg_steps``) to its return value."""
+    while True:
+        try:
+            next(gen)
+        except StopIteration as stop:
+            return stop.value
+
+
+def sweep_steps(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3):
     """One left-to-right then right-to-left two-site sweep (``network/dmrg.py:321-542``,
-    noiseless branch).  Returns ``(energy, max discarded weight)``."""
+    noiseless branch) as a generator: it yields right after each bond's Lanczos solve is
+    enqueued on the current stream (so a scheduler can run other work while the device
+    computes) and returns ``(energy, max discarded weight)``."""
     from tenet import linalg, ops
 
     n_sites = len(psi)
@@ -471,7 +533,13 @@ def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3)
         for n in bonds:
             aa = _pair(psi[n], psi[n + 1])
             if env.compiled:
-                energy, aa = env.solve(n, aa, ncv)
+                lz = env.lanczos(n, aa.structure, ncv)
+                if lz.n:
+                    lz.launch(aa.arena)
+                    yield n
+                    energy, aa = lz.finish()
+                else:
+                    energy = 0.0
             else:
                 energy, aa = lanczos(lambda v, n=n: env.heff2(n, v), aa, ncv=ncv)
             u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff)
@@ -493,24 +561,40 @@ def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3)
     return energy, max_dw
 
 
-def dmrg_(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
-          max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True,
-          precision: str = "f64"):
-    """Two-site DMRG to convergence (``network/dmrg.py:620-843``, flat ``chi``/``cutoff``,
-    no noise): returns ``(energy, history, psi)`` with ``history`` the per-sweep energies.
-    Stops on ``|dE| < energy_tol`` or after ``max_sweeps``.  ``precision`` "tf32" or
-    "3xbf16" runs the matvec products on the tensor cores with the FP64 Rayleigh-quotient
-    correction of every solve; Lanczos, the SVD and the truncation stay FP64."""
+def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3):
+    """One two-site sweep; returns ``(energy, max discarded weight)``."""
+    return drain(sweep_steps(psi, h, env, chi=chi, cutoff=cutoff, ncv=ncv))
+
+
+def dmrg_steps(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
+               max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True,
+               precision: str = "f64", tc_min_flops: int | None = None):
+    """``dmrg_`` as a step generator (see ``sweep_steps``)."""
     psi.canonize_(0)
-    env = Env(psi, h, compiled=compiled, precision=precision).setup_(0)
+    env = Env(psi, h, compiled=compiled, precision=precision,
+              tc_min_flops=tc_min_flops).setup_(0)
     energy, history = float("inf"), []
     for _ in range(max_sweeps):
         old = energy
-        energy, _ = sweep_(psi, h, env, chi=chi, cutoff=cutoff, ncv=ncv)
+        energy, _ = yield from sweep_steps(psi, h, env, chi=chi, cutoff=cutoff, ncv=ncv)
         history.append(energy)
         if abs(old - energy) < energy_tol:
             break
     return energy, history, psi
+
+
+def dmrg_(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
+          max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True,
+          precision: str = "f64", tc_min_flops: int | None = None):
+    """Two-site DMRG to convergence (``network/dmrg.py:620-843``, flat ``chi``/``cutoff``,
+    no noise): returns ``(energy, history, psi)`` with ``history`` the per-sweep energies.
+    Stops on ``|dE| < energy_tol`` or after ``max_sweeps``.  ``precision`` "tf32" or
+    "3xbf16" runs the matvec products big enough for the tensor cores there (see
+    ``tc_min_flops``), with FP64 reorthogonalisation and the FP64 Rayleigh-quotient
+    correction of every such solve; Lanczos, the SVD and the truncation stay FP64."""
+    return drain(dmrg_steps(psi, h, chi=chi, cutoff=cutoff, ncv=ncv, max_sweeps=max_sweeps,
+                            energy_tol=energy_tol, compiled=compiled, precision=precision,
+                            tc_min_flops=tc_min_flops))
 
 
 # ---------------------------------------------------------------------------------------

@@ -21,6 +21,7 @@ from collections import Counter
 from dataclasses import dataclass
 from functools import cache
 
+import numpy as np
 import torch
 
 from tenet import _exec, _lib
@@ -40,36 +41,44 @@ __all__ = ["add", "adjoint", "compose", "contractible", "divide", "einsum", "ful
 
 
 @cache
-def _map_exec(src: TensorStructure, plan) -> _exec.GatherTable:
+def _map_exec(src: TensorStructure, kind: str, a=None, b=None):
+    """``(destination structure, gather or None)`` of a cached unary block map: a
+    transpose (``kind`` "t", axes ``a``), a repartition ("r", outputs ``a``, inputs ``b``)
+    or the adjoint ("a").  ``None`` marks an identity map, whose result shares the arena."""
+    plan = (transpose_plan(src, a) if kind == "t" else
+            repartition_plan(src, a, b) if kind == "r" else adjoint_plan(src))
     dst, perm, terms = plan
-    return _exec.make_gather(_exec.gather_rows(src, "arena", dst, "arena", perm, terms))
+    t = np.asarray(terms, dtype=np.float64).reshape(-1, 3)
+    if perm == tuple(range(src.ndim)) and len(t) == dst.num_blocks \
+            and (t[:, 0] == t[:, 1]).all() and (t[:, 2] == 1.0).all():
+        return dst, None
+    return dst, _exec.make_gather(_exec.gather_rows(src, "arena", dst, "arena", perm, terms))
 
 
-def _apply_map(t: SymmetricTensor, plan) -> SymmetricTensor:
-    dst, perm, terms = plan
-    if perm == tuple(range(t.ndim)) and all(s == d and c == 1.0 for s, d, c in terms) \
-            and len(terms) == dst.num_blocks:
+def _apply_map(t: SymmetricTensor, kind: str, a=None, b=None) -> SymmetricTensor:
+    dst, table = _map_exec(t.structure, kind, a, b)
+    if table is None:
         return SymmetricTensor(dst, arena=t.arena)  # identity block map: share the arena
     out = SymmetricTensor.empty(dst)
-    _map_exec(t.structure, plan).run(t.arena, out.arena)
+    table.run(t.arena, out.arena)
     return out
 
 
 def transpose(t: SymmetricTensor, axes=None) -> SymmetricTensor:
     """Public-axis permutation; within-side reorders are braids (``ops/permutation.py``)."""
     axes = tuple(reversed(range(t.ndim))) if axes is None else validate_axes(t.ndim, axes)
-    return _apply_map(t, transpose_plan(t.structure, axes))
+    return _apply_map(t, "t", axes)
 
 
 def repartition(t: SymmetricTensor, outputs, inputs) -> SymmetricTensor:
     """``outputs`` become OUT, ``inputs`` IN, in that public order (``ops/repartition.py``)."""
     outputs, inputs = validate_partition(t.ndim, outputs, inputs)
-    return _apply_map(t, repartition_plan(t.structure, outputs, inputs))
+    return _apply_map(t, "r", outputs, inputs)
 
 
 def adjoint(t: SymmetricTensor) -> SymmetricTensor:
     """Every leg flips side; block ``(ot, it)`` <- block ``(it, ot)`` (``ops/map.py:446-493``)."""
-    return _apply_map(t, adjoint_plan(t.structure))
+    return _apply_map(t, "a")
 
 
 # ---------------------------------------------------------------------------------------

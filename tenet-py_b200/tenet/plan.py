@@ -13,6 +13,8 @@ from __future__ import annotations
 from functools import cache
 from math import sqrt
 
+import numpy as np
+
 from tenet import _su2
 from tenet.structure import IN, OUT, Leg, Pattern, TensorStructure, all_trees, block_keys, \
     coupled_of, key_index, trees_to
@@ -166,17 +168,29 @@ def bend_map(pat: Pattern, axis: int):
     return new, tuple(terms)
 
 
-def compose_terms(terms, following) -> tuple:
-    """Sparse product of two block maps, duplicates summed (``ops/repartition.py:298-316``)."""
-    by_src: dict = {}
-    for s, d, c in following:
-        by_src.setdefault(s, []).append((d, c))
-    merged: dict = {}
-    for s, m, c in terms:
-        for d, o in by_src.get(m, ()):
-            k = (s, d)
-            merged[k] = merged.get(k, 0.0) + c * o
-    return tuple((s, d, c) for (s, d), c in merged.items())
+def compose_terms(terms, following) -> np.ndarray:
+    """Sparse product of two block maps, duplicates summed (``ops/repartition.py:298-316``).
+
+    Terms are ``(src, dst, coeff)`` rows.  The result lists each ``(src, dst)`` pair once,
+    in order of its first occurrence when the terms of ``terms`` are walked in order and
+    each is followed through the terms of ``following`` in their order; each coefficient
+    is summed in that same order, starting from zero (the library's host planner,
+    ``tnb_plan_compose``)."""
+    from tenet import _lib
+
+    a = np.ascontiguousarray(terms, dtype=np.float64).reshape(-1, 3)
+    b = np.ascontiguousarray(following, dtype=np.float64).reshape(-1, 3)
+    if not len(a) or not len(b):
+        return np.zeros((0, 3))
+    per_mid = np.bincount(b[:, 0].astype(np.int64))
+    mid = a[:, 1].astype(np.int64)
+    cap = int(per_mid[mid[mid < len(per_mid)]].sum())
+    out = np.empty((max(cap, 1), 3))
+    n = _lib.load().tnb_plan_compose(len(a), a.ctypes.data, len(b), b.ctypes.data,
+                                     out.ctypes.data, cap)
+    if n < 0:
+        raise RuntimeError(f"tnb_plan_compose failed ({n})")
+    return out[:n]
 
 
 @cache
@@ -187,7 +201,8 @@ def repartition_map(pat: Pattern, outputs: tuple, inputs: tuple):
     want = {ax: True for ax in outputs} | {ax: False for ax in inputs}
     crossing = [ax for ax in range(nd) if pat.legs[ax][1] != want[ax]]
     perm = tuple(range(nd))
-    terms = tuple((i, i, 1.0) for i in range(len(block_keys(pat))))
+    n = len(block_keys(pat))
+    terms = np.stack([np.arange(n), np.arange(n), np.ones(n)], axis=1).astype(np.float64)
     labels = list(range(nd))
     cur = pat
     for ax in crossing:

@@ -47,7 +47,8 @@ def _identity_plan(s: TensorStructure):
 class _Link:
     """One contraction of the chain, with its gathers and GEMM table."""
 
-    def __init__(self, src_struct, src_kind, a_plan, b_tensor, b_plan, axes, precision="f64"):
+    def __init__(self, src_struct, src_kind, a_plan, b_tensor, b_plan, axes, precision="f64",
+                 tc_min_flops=None):
         ca, cb = axes
         sa_logical = a_plan[0]
         sb_logical = b_plan[0]
@@ -84,7 +85,7 @@ class _Link:
             _exec.gather_rows(src_struct, src_kind, sa2, "matrix", pa, ta, 0, keep_a))
         self.b_gather = _exec.make_gather(
             _exec.gather_rows(b_tensor.structure, "arena", sb2, "matrix", pb, tb, 0, keep_b))
-        self.gemm = _exec.GemmGroup(products, precision)
+        self.gemm = _exec.GemmGroup(products, precision, tc_min_flops)
         self.c_struct = sc
         self.a_size, self.b_size, self.c_size = ma.size, mb.size, mc.size
         self.b_tensor = b_tensor
@@ -93,10 +94,13 @@ class _Link:
 class ChainProgram:
     """``y = chain(x)`` for a fixed input structure; see the module docstring."""
 
-    def __init__(self, in_struct: TensorStructure, precision: str = "f64") -> None:
-        """``precision``: "f64" (the plain FP64 form), or "tf32" / "3xbf16" to run every
-        coupled-sector product that is not tall-and-thin on the tcgen05 tensor cores."""
+    def __init__(self, in_struct: TensorStructure, precision: str = "f64",
+                 tc_min_flops: int | None = None) -> None:
+        """``precision``: "f64" (the plain FP64 form), or "tf32" / "3xbf16" to run the
+        coupled-sector products big enough to be dense contractions (at least
+        ``tc_min_flops``, default ``_exec.TC_MIN_FLOPS``) on the tcgen05 tensor cores."""
         self.precision = precision
+        self.tc_min_flops = tc_min_flops
         self.in_struct = in_struct
         self.src = (in_struct, "arena")
         self.pending = _identity_plan(in_struct)
@@ -119,7 +123,8 @@ class ChainProgram:
 
     def contract(self, b: SymmetricTensor, axes, b_plan=None) -> ChainProgram:
         b_plan = b_plan or _identity_plan(b.structure)
-        link = _Link(self.src[0], self.src[1], self.pending, b, b_plan, axes, self.precision)
+        link = _Link(self.src[0], self.src[1], self.pending, b, b_plan, axes, self.precision,
+                     self.tc_min_flops)
         self.links.append(link)
         self.src = (link.c_struct, "matrix")
         self.pending = link.after
@@ -184,6 +189,8 @@ class ChainProgram:
         """Allocate every buffer once and pack the fixed operands (needs the device)."""
         dev = _exec.device()
         f64 = dict(dtype=torch.float64, device=dev)
+        for lk in self.links:  # split-K scratch of this program's own
+            lk.gemm = lk.gemm.private()
         self.a_bufs = [torch.empty(max(1, lk.a_size), **f64) for lk in self.links]
         self.c_bufs = [torch.empty(max(1, lk.c_size), **f64) for lk in self.links]
         self.b_bufs = [torch.empty(max(1, lk.b_size), **f64) for lk in self.links]
@@ -209,7 +216,17 @@ class ChainProgram:
 
     @property
     def launches(self) -> int:
-        return 2 * len(self.links) + 1
+        return sum(lk.gemm.launches + 1 for lk in self.links) + 1
+
+    @property
+    def uses_tensor_cores(self) -> bool:
+        return any(lk.gemm.tensor_core for lk in self.links)
+
+    def tensor_core_candidates(self, min_flops: int | None = None) -> bool:
+        """Whether the precision form of this chain would put any product on the tensor
+        cores (``_exec.tc_worthy``)."""
+        return any(_exec.tc_worthy(p, min_flops) and not _exec._is_skinny(p)
+                   for lk in self.links for p in lk.gemm.products)
 
     def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         """``out = chain(x)`` on the current stream: one replay of the recorded sequence
@@ -269,19 +286,20 @@ _HEFF_TABLES_MAX = 512
 
 
 def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = True,
-                  precision: str = "f64") -> ChainProgram:
+                  precision: str = "f64", tc_min_flops: int | None = None) -> ChainProgram:
     """The site-tensor two-site matvec (``network/env.py:416-432``) as a chain program.
     ``fl``, ``w1``, ``w2``, ``fr`` need only ``.structure`` when ``allocate`` is False.
 
     The program's tables depend on the five structures and the precision only, so they
     are planned once per such key and shared: a later call with the same structures
     builds a fresh program (own buffers, bound to the given tensors) around them."""
-    key = (fl.structure, w1.structure, w2.structure, fr.structure, in_struct, precision)
+    key = (fl.structure, w1.structure, w2.structure, fr.structure, in_struct, precision,
+           tc_min_flops)
     cached = _HEFF_TABLES.get(key)
     if cached is not None:
         return cached.rebind(dict(zip(cached.operand_names, (fr, w2, w1, fl)))) \
             .finish_alloc(allocate)
-    p = ChainProgram(in_struct, precision)
+    p = ChainProgram(in_struct, precision, tc_min_flops)
     p.einsum("apqr,rys->apqys", fr)
     p.einsum("apqys,mQqy->apQms", w2, bend="q")
     p.einsum("apQms,xPpm->aPQxs", w1, bend="p")

@@ -350,14 +350,21 @@ def layout(s: TensorStructure) -> ArenaLayout:
     n, nd = len(keys), s.ndim
     oa, ia = s.out_axes, s.in_axes
     degs = [_space_degs(leg.space) for leg in s.legs]
-    shapes = np.zeros((n, nd), dtype=np.int64)
+    # the label each axis carries in each block, then its degeneracy, axis by axis
+    labels = np.zeros((n, nd), dtype=np.int64)
     coupled = np.zeros(n, dtype=np.int64)
     for b, (ot, it) in enumerate(keys):
-        for ax, u in zip(oa, ot[0]):
-            shapes[b, ax] = degs[ax][p._dual(u) if s.legs[ax].dual else u]
-        for ax, u in zip(ia, it[0]):
-            shapes[b, ax] = degs[ax][p._dual(u) if s.legs[ax].dual else u]
+        labels[b, list(oa)] = ot[0]
+        labels[b, list(ia)] = it[0]
         coupled[b] = ot[2]
+    shapes = np.zeros((n, nd), dtype=np.int64)
+    for ax, leg in enumerate(s.legs):
+        deg = degs[ax]
+        lab = labels[:, ax]
+        uniq, inv = np.unique(lab, return_inverse=True) if n else (lab, lab)
+        vals = np.array([deg[p._dual(int(u)) if leg.dual else int(u)] for u in uniq],
+                        dtype=np.int64)
+        shapes[:, ax] = vals[inv.reshape(-1)] if n else 0
     sizes = shapes.prod(axis=1) if n else np.zeros(0, dtype=np.int64)
     offsets = np.zeros(n, dtype=np.int64)
     if n:
@@ -390,46 +397,49 @@ def matrix_layout(s: TensorStructure) -> MatrixLayout:
     lay = layout(s)
     keys = s.keys
     oa, ia = s.out_axes, s.in_axes
+    n, nd = len(keys), s.ndim
+    shapes = lay.shapes
+    rsz = shapes[:, list(oa)].prod(axis=1) if oa else np.ones(n, dtype=np.int64)
+    csz = shapes[:, list(ia)].prod(axis=1) if ia else np.ones(n, dtype=np.int64)
     rows: dict = {}
     cols: dict = {}
     for b, (ot, it) in enumerate(keys):
-        rows.setdefault(ot[2], {}).setdefault(ot, int(np.prod(lay.shapes[b, list(oa)])) if oa else 1)
-        cols.setdefault(ot[2], {}).setdefault(it, int(np.prod(lay.shapes[b, list(ia)])) if ia else 1)
+        rows.setdefault(ot[2], {}).setdefault(ot, int(rsz[b]))
+        cols.setdefault(ot[2], {}).setdefault(it, int(csz[b]))
     sectors = tuple(sorted(rows))
     shape, base, roff, coff = {}, {}, {}, {}
     off = 0
     for c in sectors:
         r = 0
         for t in sorted(rows[c]):
-            roff[(c, t)] = r
+            roff[t] = r
             r += rows[c][t]
         q = 0
         for t in sorted(cols[c]):
-            coff[(c, t)] = q
+            coff[t] = q
             q += cols[c][t]
         shape[c] = (r, q)
         base[c] = off
         off += r * q
-    n, nd = len(keys), s.ndim
     block_sector = np.zeros(n, dtype=np.int64)
     block_off = np.zeros(n, dtype=np.int64)
     block_ld = np.zeros(n, dtype=np.int64)
-    rstride = np.zeros((n, nd), dtype=np.int64)
-    cstride = np.zeros((n, nd), dtype=np.int64)
     for b, (ot, it) in enumerate(keys):
         c = ot[2]
         ld = shape[c][1]
         block_sector[b] = c
         block_ld[b] = ld
-        block_off[b] = base[c] + roff[(c, ot)] * ld + coff[(c, it)]
-        acc = 1
-        for ax in reversed(oa):
-            rstride[b, ax] = acc
-            acc *= lay.shapes[b, ax]
-        acc = 1
-        for ax in reversed(ia):
-            cstride[b, ax] = acc
-            acc *= lay.shapes[b, ax]
+        block_off[b] = base[c] + roff[ot] * ld + coff[it]
+    rstride = np.zeros((n, nd), dtype=np.int64)
+    cstride = np.zeros((n, nd), dtype=np.int64)
+    acc = np.ones(n, dtype=np.int64)
+    for ax in reversed(oa):
+        rstride[:, ax] = acc
+        acc = acc * shapes[:, ax]
+    acc = np.ones(n, dtype=np.int64)
+    for ax in reversed(ia):
+        cstride[:, ax] = acc
+        acc = acc * shapes[:, ax]
     return MatrixLayout(sectors, shape, base, off, block_sector, block_off, block_ld, rstride,
                         cstride)
 

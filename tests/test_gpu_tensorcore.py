@@ -56,15 +56,19 @@ def test_tensorcore_gemm_kinds(kind):
             assert err < TOL[kind], f"{(M, N, K)}: relative error {err:.2e}"
 
 
-@pytest.mark.parametrize("precision,tol", [("3xbf16", 1e-4), ("tf32", 1e-2)])
-def test_mixed_precision_heff2_chain(precision, tol):
-    """The bench's SU(2) matvec with its sector products on the tensor cores."""
+@pytest.mark.parametrize("precision,tol,tc_min", [("3xbf16", 1e-4, None), ("tf32", 1e-2, None),
+                                                  ("3xbf16", 1e-4, 0), ("tf32", 1e-2, 0)])
+def test_mixed_precision_heff2_chain(precision, tol, tc_min):
+    """The bench's SU(2) matvec with its big sector products (or, with ``tc_min`` 0, all
+    of them) on the tensor cores."""
     import bench
     from tenet.program import heff2_program
 
     tensors = bench.build_workload()
     exact = heff2_program(*tensors[:4], tensors[4].structure)(tensors[4]).numpy_arena()
-    prog = heff2_program(*tensors[:4], tensors[4].structure, precision=precision)
+    prog = heff2_program(*tensors[:4], tensors[4].structure, precision=precision,
+                         tc_min_flops=tc_min)
+    assert prog.uses_tensor_cores
     got = prog(tensors[4]).numpy_arena()
     err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
     assert err < tol, f"{precision}: relative error {err:.2e}"
@@ -87,5 +91,6 @@ def test_mixed_precision_dmrg_energy(golden_dir, precision):
              for i in range(L + 1)]
     e, hist, _ = network.dmrg_(network.MPS.random(phys, bonds, seed=0),
                                network.heisenberg_mpo_su2(L), chi=chi, cutoff=1e-10, ncv=20,
-                               max_sweeps=g["sweeps"], energy_tol=0.0, precision=precision)
+                               max_sweeps=g["sweeps"], energy_tol=0.0, precision=precision,
+                               tc_min_flops=0)  # every product on the tensor cores
     assert abs(e - g["energy"]) / L <= 1e-8, f"|dE/L| = {abs(e - g['energy']) / L:.2e}"

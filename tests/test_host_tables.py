@@ -175,3 +175,68 @@ def test_heff2_chain_program_reproduces_reference(golden_dir):
     es, ex = T["heff_aa"]
     assert prog.out_struct == es
     np.testing.assert_allclose(out, ex, rtol=1e-12, atol=1e-12 * np.abs(ex).max())
+
+
+def _compose_spec(terms, following):
+    by_src: dict = {}
+    for s, d, c in following:
+        by_src.setdefault(s, []).append((d, c))
+    merged: dict = {}
+    for s, m, c in terms:
+        for d, o in by_src.get(m, ()):
+            merged[(s, d)] = merged.get((s, d), 0.0) + c * o
+    return [(s, d, c) for (s, d), c in merged.items()]
+
+
+def _normalise_spec(dims, dstr, rstr, cstr):
+    order = sorted(range(len(dims)), key=lambda k: (-dstr[k], -cstr[k], -rstr[k]))
+    out = []
+    for k in order:
+        if dims[k] == 1:
+            continue
+        d, a, b, c = dims[k], dstr[k], rstr[k], cstr[k]
+        if out and out[-1][1] == a * d and out[-1][2] == b * d and out[-1][3] == c * d:
+            out[-1] = (out[-1][0] * d, a, b, c)
+            continue
+        out.append((d, a, b, c))
+    return out or [(1, 1, 0, 0)]
+
+
+def test_native_compose_matches_the_sparse_product_rule():
+    from tenet.plan import compose_terms
+
+    rng = np.random.default_rng(7)
+    for trial in range(40):
+        na, nb, nm = rng.integers(0, 60), rng.integers(0, 60), rng.integers(1, 12)
+        a = [(int(rng.integers(0, 20)), int(rng.integers(0, nm)), float(rng.standard_normal()))
+             for _ in range(na)]
+        b = [(int(rng.integers(0, nm)), int(rng.integers(0, 20)), float(rng.choice([1.0, -1.0, 0.5])))
+             for _ in range(nb)]
+        got = compose_terms(a, b)
+        want = np.array(_compose_spec(a, b), dtype=np.float64).reshape(-1, 3)
+        assert got.shape == want.shape and np.array_equal(got, want)
+
+
+def test_native_gather_rows_match_the_normalisation_rule():
+    from tenet import _exec
+
+    rng = np.random.default_rng(3)
+    R, nd = 200, 5
+    D = rng.integers(1, 4, size=(R, nd))
+    DS, RS, CS = (rng.integers(0, 6, size=(R, nd)) for _ in range(3))
+    # contiguous runs so that merges happen
+    DS[:, -1], DS[:, -2] = 1, D[:, -1]
+    CS[:, -1], CS[:, -2] = 1, D[:, -1]
+    off, size = rng.integers(0, 1000, R), D.prod(axis=1)
+    tb = np.arange(R)
+    rows = _exec._plan_rows(D, DS, RS, CS, off, size, tb, tb + 1, 1)
+    for r in range(R):
+        segs = _normalise_spec(list(D[r]), list(DS[r]), list(RS[r]), list(CS[r]))
+        row = rows[r]
+        assert tuple(row[:6]) == (off[r], size[r], len(segs), r, r + 1, 1)
+        for k, (d, a, b, c) in enumerate(segs):
+            assert (row[8 + k], row[16 + k], row[24 + k], row[32 + k]) == (d, a, b, c)
+    with pytest.raises(ValueError):
+        big = np.full((1, 9), 2)
+        primes = np.array([[29, 23, 19, 17, 13, 11, 7, 5, 3]])  # no two dims merge
+        _exec._plan_rows(big, primes, big * 0, big * 0, [0], [512], [0], [0], 0)
