@@ -243,40 +243,67 @@ def cpu_baseline(flops: int, budget_s: float = 20.0) -> dict:
             "ms_per_matvec": med * 1e3}
 
 
-def dmrg_solves(args) -> dict:
-    """Time-to-solution of full DMRG solves on the device, plain FP64 form against the
-    precision form: SU(2) Heisenberg, ``L`` sites, dense ``chi``, ncv = 20, a fixed number
-    of sweeps, the reference's seeded start."""
+def serving(args) -> dict:
+    """Served DMRG solves against the plain FP64 form on the same seeded request sample
+    (SU(2) J1-J2 chains, 8 sweeps, ncv = 20, cutoff 1e-10).  Arms, each from empty plan
+    caches: the plain FP64 form (eager op-by-op matvec, host-driven Lanczos), the
+    compiled FP64 form one solve at a time, the serving loop in FP64 and in the
+    precision form with every request arriving at once, and the precision form again
+    at a Poisson arrival rate of 0.7 x the burst throughput for the latency point."""
     import torch
 
-    from tenet import network
-    from tenet.structure import GradedSpace
-    from tenet.symmetry import SU2
+    from tenet import serve
 
-    L, chi, sweeps = args.solve_L, args.solve_chi, args.solve_sweeps
-    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
-    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
-             for i in range(L + 1)]
-    h = network.heisenberg_mpo_su2(L)
-    out = {"workload": f"su2-heisenberg-L{L}-chi{chi}-{sweeps}sweeps-ncv20",
-           "timing": "median of the timed solves after one untimed warm-up solve per form "
-                     "(host plan caches warm, as a served stream of repeated shapes sees them)"}
-    for precision in ("f64", "3xbf16"):
-        times, energy = [], None
-        network.dmrg_(network.MPS.random(phys, bonds, seed=0), h, chi=chi, cutoff=1e-10, ncv=20,
-                      max_sweeps=sweeps, energy_tol=0.0, precision=precision)
-        for _ in range(args.solves):
+    kw = {} if args.serve_full else {"lengths": (16, 32), "chis": (32, 64)}
+    reqs = serve.request_stream(args.serve_requests, float("inf"), seed=0, **kw)
+    out = {"sample": (f"{len(reqs)} requests of the seeded config-5 stream (seed 0), "
+                      + ("full distribution" if args.serve_full else
+                         "L in {16, 32}, chi in {32, 64}") + ", J2/J1 in [0, 0.4], 8 sweeps"),
+           "requests": [{"rid": r.rid, "L": r.L, "chi": r.chi, "j2": round(r.j2, 4)}
+                        for r in reqs],
+           "timing": "wall clock from the first arrival to the last result; every arm starts "
+                     "with empty host plan caches"}
+    energies = {}
+
+    def sequential(name, **kw):
+        serve.clear_plan_caches()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done, en = [], {}
+        for r in reqs:
+            e, _ = serve.solve_alone(r, **kw)
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            energy, _, _ = network.dmrg_(network.MPS.random(phys, bonds, seed=0), h, chi=chi,
-                                         cutoff=1e-10, ncv=20, max_sweeps=sweeps,
-                                         energy_tol=0.0, precision=precision)
-            torch.cuda.synchronize()
-            times.append(time.perf_counter() - t0)
-        out[precision] = {"s_per_solve": float(np.median(times)),
-                          "solves_per_s": 1.0 / float(np.median(times)), "energy": energy,
-                          "runs": len(times)}
-    out["abs_dE_per_site"] = abs(out["3xbf16"]["energy"] - out["f64"]["energy"]) / L
+            done.append(time.perf_counter() - t0)
+            en[r.rid] = e
+        wall = time.perf_counter() - t0
+        energies[name] = en
+        out[name] = {"solves_per_s": len(reqs) / wall, "wall_s": wall,
+                     "p50_s": float(np.percentile(done, 50)), "p99_s": float(np.percentile(done, 99))}
+
+    def served(name, requests, **kw):
+        serve.clear_plan_caches()
+        srv = serve.Server(max_active=args.serve_slots, **kw)
+        t0 = time.perf_counter()
+        res = srv.run(requests)
+        wall = time.perf_counter() - t0
+        energies[name] = {r.rid: r.energy for r in res}
+        out[name] = serve.summarize(res, wall) | {"peak_active": srv.peak_active}
+
+    sequential("plain_f64_sequential", precision="f64", compiled=False)
+    sequential("compiled_f64_sequential", precision="f64")
+    served("served_f64", reqs, precision="f64")
+    served("served_3xbf16", reqs, precision="3xbf16")
+    rate = 0.7 * out["served_3xbf16"]["solves_per_s"]
+    poisson = serve.request_stream(len(reqs), rate, seed=0, **kw)
+    served("served_3xbf16_poisson", poisson, precision="3xbf16")
+    out["served_3xbf16_poisson"]["arrival_rate_per_s"] = rate
+    ref = energies["plain_f64_sequential"]
+    out["max_abs_dE_per_site_vs_plain_f64"] = {
+        k: max(abs(v[r.rid] - ref[r.rid]) / r.L for r in reqs) for k, v in energies.items()
+        if k != "plain_f64_sequential" and k != "served_3xbf16_poisson"}
+    base = out["plain_f64_sequential"]["solves_per_s"]
+    out["solves_per_s_vs_plain_f64"] = {k: out[k]["solves_per_s"] / base for k in
+                                        ("compiled_f64_sequential", "served_f64", "served_3xbf16")}
     return out
 
 
@@ -373,19 +400,23 @@ def run_tenet(args) -> None:
         gm_plain.replay()
     eager_ms["graph_chain_without_pdl"] = timed(gm_plain.replay, args.steps) / args.steps
 
-    # the precision form: every non-skinny sector product on the tcgen05 tensor cores
+    # the precision form: the sector products big enough to be dense contractions on the
+    # tcgen05 tensor cores (and, for comparison, every non-skinny product there)
     mixed = {}
     ref_out = prog(aa).numpy_arena()
-    for precision in ("3xbf16", "tf32"):
-        mprog = heff2_program(fl, w1, w2, fr, aa.structure, precision=precision)
+    for precision, tc_min in (("3xbf16", None), ("tf32", None), ("3xbf16", 0), ("tf32", 0)):
+        mprog = heff2_program(fl, w1, w2, fr, aa.structure, precision=precision,
+                              tc_min_flops=tc_min)
         mg = GraphMatvec(mprog)
         mg.x.copy_(aa.arena)
         for _ in range(args.warmup):
             mg.replay()
         mms = timed(mg.replay, args.steps) / args.steps
         got = mg(aa).numpy_arena()
-        mixed[precision] = {
+        mixed[precision + ("_all_products" if tc_min == 0 else "")] = {
             "ms_per_matvec": mms, "tflops": flops / (mms * 1e-3) / 1e12,
+            "tensor_core_products": sum(len(p.table) for lk in mprog.links
+                                        for p in lk.gemm.parts if p.kind in (3, 4)),
             "rel_error_vs_f64": float(np.linalg.norm(got - ref_out) / np.linalg.norm(ref_out))}
 
     for _ in range(args.warmup):
@@ -470,7 +501,7 @@ def run_tenet(args) -> None:
         }
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
-        solves = dmrg_solves(args) if args.solves > 0 else None
+        solves = serving(args) if args.serve_requests > 0 else None
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -491,7 +522,7 @@ def run_tenet(args) -> None:
                              **{k: flops / (v * 1e-3) / 1e12 for k, v in eager_ms.items()}},
             "launches_per_matvec_eager_ops": launches_eager,
             "mixed_precision_forms": mixed,
-            "dmrg_solves": solves,
+            "serving": solves,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),
@@ -509,10 +540,11 @@ def main() -> None:
     ap.add_argument("--impl", default="tenet", choices=["tenet", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--solves", type=int, default=1, help="DMRG solves per precision form")
-    ap.add_argument("--solve-L", type=int, default=32)
-    ap.add_argument("--solve-chi", type=int, default=64)
-    ap.add_argument("--solve-sweeps", type=int, default=4)
+    ap.add_argument("--serve-requests", type=int, default=6,
+                    help="served DMRG requests in the solves/s comparison (0: skip)")
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-full", action="store_true",
+                    help="draw the requests from the full L / chi distribution")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

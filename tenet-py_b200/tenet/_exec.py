@@ -97,6 +97,39 @@ _TORCH_DTYPE = {np.dtype(np.int64).str: torch.int64, np.dtype(np.int32).str: tor
                 np.dtype(np.float64).str: torch.float64}
 
 
+class _Staging:
+    """A pinned host ring through which plan tables reach the device: a table is packed
+    into the next free bytes of the ring and copied asynchronously, so an upload costs a
+    host memcpy and one queued copy.  Before the ring wraps, every copy still reading it
+    is waited for."""
+
+    def __init__(self, nbytes: int = 64 << 20) -> None:
+        self.nbytes = nbytes
+        self.buf = None
+        self.pos = 0
+        self.pending: list = []
+
+    def stage(self, packed: np.ndarray):
+        n = packed.nbytes
+        if n > self.nbytes // 4:
+            return None
+        if self.buf is None:
+            self.buf = torch.empty(self.nbytes, dtype=torch.uint8).pin_memory()
+            self.host = self.buf.numpy()
+        if self.pos + n > self.nbytes:
+            for ev in self.pending:
+                ev.synchronize()
+            self.pending.clear()
+            self.pos = 0
+        view = self.buf[self.pos:self.pos + n]
+        self.host[self.pos:self.pos + n] = packed
+        self.pos = -(-(self.pos + n) // 256) * 256
+        return view
+
+
+_STAGING = _Staging()
+
+
 class Uploaded:
     """Device copies of host arrays, made on the current stream.  A copy from pageable
     host memory may still be in flight when the call returns, so a kernel on another
@@ -116,7 +149,12 @@ class Uploaded:
         packed = np.zeros(max(total, 16), dtype=np.uint8)
         for x, o in zip(host_arrays, offs):
             packed[o:o + x.nbytes] = x.reshape(-1).view(np.uint8)
-        dev_buf = torch.from_numpy(packed).to(device())
+        staged = None if torch.cuda.is_current_stream_capturing() else _STAGING.stage(packed)
+        if staged is not None:
+            dev_buf = torch.empty(packed.nbytes, dtype=torch.uint8, device=device())
+            dev_buf.copy_(staged, non_blocking=True)
+        else:
+            dev_buf = torch.from_numpy(packed).to(device())
         views = []
         for x, o in zip(host_arrays, offs):
             t = dev_buf[o:o + x.nbytes].view(_TORCH_DTYPE[x.dtype.str])
@@ -125,6 +163,8 @@ class Uploaded:
         self.stream = stream_ptr()
         self.event = torch.cuda.Event()
         self.event.record()
+        if staged is not None:
+            _STAGING.pending.append(self.event)
 
     def ready(self) -> tuple:
         if self.event is not None and stream_ptr() != self.stream \

@@ -31,8 +31,8 @@ from tenet import network
 from tenet.structure import GradedSpace
 from tenet.symmetry import SU2
 
-__all__ = ["SolveRequest", "SolveResult", "Server", "footprint_bytes", "request_stream",
-           "solve_alone"]
+__all__ = ["SolveRequest", "SolveResult", "Server", "clear_plan_caches", "footprint_bytes",
+           "request_stream", "solve_alone"]
 
 
 @dataclass(frozen=True)
@@ -197,6 +197,22 @@ class Server:
                                            slot.admitted, clock() - t0, slot.footprint, slot.req))
         torch.cuda.synchronize()
         return results
+
+
+def clear_plan_caches() -> None:
+    """Empty every host plan cache (structures, block maps, descriptor tables, SU(2)
+    coefficients), so that a measurement starts cold."""
+    import sys
+
+    for name, mod in list(sys.modules.items()):
+        if not name.startswith("tenet.") or mod is None:
+            continue
+        for attr in list(vars(mod).values()):
+            if callable(getattr(attr, "cache_clear", None)):
+                attr.cache_clear()
+    from tenet import program
+
+    program._HEFF_TABLES.clear()
 
 
 def summarize(results, wall: float) -> dict:

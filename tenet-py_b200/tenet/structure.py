@@ -203,22 +203,23 @@ def coupled_of(p: Provider, uncoupled: tuple[int, ...]) -> tuple[int, ...]:
 
 @cache
 def block_keys(pat: Pattern) -> tuple:
-    """Every allowed key of a pattern, sorted (``structure.py:349-371``)."""
+    """Every allowed key of a pattern, sorted (``structure.py:349-371``): every OUT tree
+    over the OUT legs' labels paired with every IN tree over the IN legs' labels that
+    ends in the same coupled sector."""
     p = pat.provider
-    oa, ia = pat.out_axes, pat.in_axes
-    keys = set()
     fused = [tuple(p._dual(a) if dual else a for a in labels) for labels, _, dual in pat.legs]
-    for u in product(*fused):
-        ou = tuple(u[i] for i in oa)
-        iu = tuple(u[i] for i in ia)
-        for c in coupled_of(p, ou):
-            its = trees_to(p, iu, c)
-            if not its:
-                continue
-            for ot in trees_to(p, ou, c):
-                for it in its:
-                    keys.add((ot, it))
-    return tuple(sorted(keys))
+
+    def trees_by_coupled(axes):
+        by_c: dict = {}
+        for u in product(*(fused[i] for i in axes)):
+            for t in all_trees(p, u):
+                by_c.setdefault(t[2], []).append(t)
+        return by_c
+
+    outs, ins = trees_by_coupled(pat.out_axes), trees_by_coupled(pat.in_axes)
+    keys = [(ot, it) for c, ots in outs.items() if c in ins for ot in ots for it in ins[c]]
+    keys.sort()
+    return tuple(keys)
 
 
 @cache
@@ -349,22 +350,21 @@ def layout(s: TensorStructure) -> ArenaLayout:
     keys = s.keys
     n, nd = len(keys), s.ndim
     oa, ia = s.out_axes, s.in_axes
-    degs = [_space_degs(leg.space) for leg in s.legs]
-    # the label each axis carries in each block, then its degeneracy, axis by axis
-    labels = np.zeros((n, nd), dtype=np.int64)
+    # per axis: label -> degeneracy, the dual already applied
+    degs = []
+    for leg in s.legs:
+        d = _space_degs(leg.space)
+        degs.append({p._dual(u): m for u, m in d.items()} if leg.dual else d)
+    rows = [[0] * nd for _ in range(n)]
     coupled = np.zeros(n, dtype=np.int64)
     for b, (ot, it) in enumerate(keys):
-        labels[b, list(oa)] = ot[0]
-        labels[b, list(ia)] = it[0]
+        row = rows[b]
+        for ax, u in zip(oa, ot[0]):
+            row[ax] = degs[ax][u]
+        for ax, u in zip(ia, it[0]):
+            row[ax] = degs[ax][u]
         coupled[b] = ot[2]
-    shapes = np.zeros((n, nd), dtype=np.int64)
-    for ax, leg in enumerate(s.legs):
-        deg = degs[ax]
-        lab = labels[:, ax]
-        uniq, inv = np.unique(lab, return_inverse=True) if n else (lab, lab)
-        vals = np.array([deg[p._dual(int(u)) if leg.dual else int(u)] for u in uniq],
-                        dtype=np.int64)
-        shapes[:, ax] = vals[inv.reshape(-1)] if n else 0
+    shapes = np.array(rows, dtype=np.int64).reshape(n, nd)
     sizes = shapes.prod(axis=1) if n else np.zeros(0, dtype=np.int64)
     offsets = np.zeros(n, dtype=np.int64)
     if n:
