@@ -396,9 +396,14 @@ def run_tenet(args) -> None:
     lib.tnb_set_pdl(0)
     gm_plain = GraphMatvec(prog)
     lib.tnb_set_pdl(1)
-    for _ in range(args.warmup):
-        gm_plain.replay()
-    eager_ms["graph_chain_without_pdl"] = timed(gm_plain.replay, args.steps) / args.steps
+    # and the persistent one-launch form of the same chain (off by default, see _exec.FUSE)
+    _exec.FUSE = True
+    gm_fused = GraphMatvec(prog)
+    _exec.FUSE = False
+    for name, g in (("graph_chain_without_pdl", gm_plain), ("graph_fused_one_launch", gm_fused)):
+        for _ in range(args.warmup):
+            g.replay()
+        eager_ms[name] = timed(g.replay, args.steps) / args.steps
 
     # the precision form: the sector products big enough to be dense contractions on the
     # tcgen05 tensor cores (and, for comparison, every non-skinny product there)

@@ -258,6 +258,23 @@ int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
                      const double* a, int64_t n_a, const double* b, int64_t n_b, double* c,
                      int64_t n_c, void* work, int64_t work_bytes, int64_t n_counters);
 int tnb_seq_append(tnb_seq* dst, const tnb_seq* src);
+
+/*
+ * Fuse a recorded sequence of gathers and FP64 grouped GEMMs (kinds 64, 32, skinny; at
+ * most 24 ops) into ONE launch appended to `dst`: a persistent cooperative kernel, as
+ * many 256-thread CTAs as can be resident, that runs the stages in order with a
+ * grid-wide barrier between them (each stage's tables and arithmetic are those of its
+ * standalone kernel, so results are bit-identical).  Data-buffer pointers equal to
+ * x_slot / y_slot become the launch's input / output, which tnb_seq_run's patch list
+ * substitutes like any buffer.  `barrier` is 8 bytes of device memory, zero before the
+ * first launch, owned by this fused op alone: two launches of it must not overlap.  Its
+ * waits are bounded (about 2 s): past the limit the device error word reads
+ * TNB_ETIMEOUT and the counters must be zeroed again.  Tensor-core stages are refused
+ * (TNB_EINVAL).  Replaces no reference interface (the reference runs each block map and
+ * composition as its own Python loop); it is the one-launch form of a compiled chain.
+ */
+int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* y_slot, void* barrier,
+                 tnb_seq* dst);
 int tnb_seq_run(const tnb_seq* s, int32_t n_patch, const void* const* from, void* const* to,
                 void* stream);
 

@@ -9,9 +9,156 @@
 // reorthogonalisation -- from one host call; nothing in it waits on the host.
 #include <cstring>
 #include <new>
+#include <string>
 #include <vector>
 
-#include "tnb_common.cuh"
+#include "tnb_stages.cuh"
+
+namespace tnb {
+
+// ---------------------------------------------------------------------------------------
+// the persistent chain kernel: every stage of a recorded chain in one launch
+
+constexpr int kFusedThreads = 256;
+constexpr int kMaxStages = 24;
+constexpr long long kBarrierCycles = 4000000000LL;  // ~2 s at the boost clock
+
+// A stage is a recorded op's words; data-buffer words equal to kSlotX / kSlotY stand for
+// the launch's input and output vectors.
+constexpr int64_t kSlotX = 1, kSlotY = 2;
+
+// recorded op codes
+constexpr int32_t kOpGather = 1;
+constexpr int32_t kOpGemm = 2;
+constexpr int32_t kOpFused = 3;
+
+struct FStage {
+  int32_t code;
+  int32_t kind;
+  int64_t items;
+  int64_t w[16];
+};
+
+struct FChain {
+  int32_t n;
+  int32_t pad;
+  FStage st[kMaxStages];
+};
+
+// 32 x 32 tiles run as four independent 64-thread groups per CTA (one tile each, own
+// named barrier); gathers, skinny tiles and 64 x 64 tiles use the whole CTA.  (Gathers
+// and skinny tiles split into groups measured slower: more dependent load rounds per
+// item at the same number of loads in flight.)
+constexpr int kGroups = 4, kGroupThreads = kFusedThreads / kGroups;
+
+union FusedSmem {
+  GatherSmem gather;
+  GemmSmem<64, 64> g64;
+  GemmSmem<32, 32> g32[kGroups];
+  SkinnySmem skinny;
+};
+
+// Grid-wide barrier on two counters (arrivals, generation), zero before the first launch.
+// Every wait is bounded: past the limit the CTA reports TNB_ETIMEOUT and the kernel ends.
+__device__ bool grid_barrier(unsigned int* bar) {
+  __syncthreads();
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = bar + 1;
+    const unsigned int g = *gen;
+    __threadfence();
+    bool ok = true;
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*gen == g) {
+        if (clock64() - t0 > kBarrierCycles) {
+          ok = false;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+    if (!ok) atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__device__ __forceinline__ double* slot(int64_t w, const double* x, double* y) {
+  return w == kSlotX ? const_cast<double*>(x)
+                     : w == kSlotY ? y : reinterpret_cast<double*>(static_cast<intptr_t>(w));
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+chain_kernel(const FChain ch, const double* x, double* y, unsigned int* bar) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FusedSmem& sm = *reinterpret_cast<FusedSmem*>(smem_raw);
+  const int grp = threadIdx.x / kGroupThreads, gtid = threadIdx.x % kGroupThreads;
+  const GroupSync gsync{1 + grp, kGroupThreads};
+  for (int s = 0; s < ch.n; ++s) {
+    const FStage& st = ch.st[s];
+    const int64_t* w = st.w;
+    if (st.code == kOpGather) {
+      const GatherArgs g{reinterpret_cast<const int64_t*>(w[0]), w[1],
+                         reinterpret_cast<const int32_t*>(w[2]),
+                         reinterpret_cast<const int64_t*>(w[4]),
+                         reinterpret_cast<const double*>(w[5]),
+                         reinterpret_cast<const int64_t*>(w[6]), w[7], slot(w[8], x, y), w[9],
+                         slot(w[10], x, y), w[11], slot(w[12], x, y), w[13], slot(w[14], x, y),
+                         w[15]};
+      for (int64_t it = blockIdx.x; it < st.items; it += gridDim.x)
+        gather_chunk<kFusedThreads, true>(g, it, sm.gather, threadIdx.x, CtaSync{});
+    } else {
+      const int64_t poff = gemm_work_parts_offset(w[13]);
+      char* work = reinterpret_cast<char*>(static_cast<intptr_t>(w[11]));
+      const GemmArgs g{reinterpret_cast<const int64_t*>(w[0]), w[1],
+                       reinterpret_cast<const int32_t*>(w[2]), slot(w[5], x, y), w[6],
+                       slot(w[7], x, y), w[8], slot(w[9], x, y), w[10],
+                       reinterpret_cast<unsigned int*>(work), w[13],
+                       w[12] > poff ? reinterpret_cast<double*>(work + poff) : nullptr,
+                       w[12] > poff ? (w[12] - poff) / 8 : 0};
+      if (st.kind == TNB_TILE_64) {
+        for (int64_t it = blockIdx.x; it < st.items; it += gridDim.x)
+          gemm_tile<64, 64, true>(g, it, sm.g64, threadIdx.x, CtaSync{});
+      } else if (st.kind == TNB_TILE_32) {
+        for (int64_t it = static_cast<int64_t>(blockIdx.x) * kGroups + grp; it < st.items;
+             it += static_cast<int64_t>(gridDim.x) * kGroups)
+          gemm_tile<32, 32, true>(g, it, sm.g32[grp], gtid, gsync);
+      } else {
+        for (int64_t it = blockIdx.x; it < st.items; it += gridDim.x)
+          skinny_tile<kFusedThreads, true>(g, it, sm.skinny, threadIdx.x, CtaSync{});
+      }
+    }
+    if (s + 1 < ch.n && !grid_barrier(bar)) return;
+  }
+}
+
+// CTAs of one cooperative chain launch on `device`: as many as can be resident (0 when
+// the kernel cannot be configured).
+int fused_grid(int device) {
+  static int cached[64] = {0};
+  if (device < 0 || device >= 64) return 0;
+  if (cached[device]) return cached[device];
+  const size_t smem = sizeof(FusedSmem);
+  if (cudaFuncSetAttribute(chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return 0;
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel, kFusedThreads, smem) !=
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return 0;
+  cached[device] = per_sm * sms;
+  return cached[device];
+}
+
+}  // namespace tnb
 
 struct tnb_seq {
   struct Op {
@@ -19,13 +166,12 @@ struct tnb_seq {
     int64_t w[16];
   };
   std::vector<Op> ops;
+  std::vector<tnb::FChain> chains;  // the stages of this sequence's fused ops
 };
 
 namespace tnb {
 namespace {
 
-constexpr int32_t kOpGather = 1;
-constexpr int32_t kOpGemm = 2;
 
 // word positions of the data buffers a replay may substitute
 constexpr int kGatherBufs[] = {8, 10, 12, 14};  // src0, dst0, src1, dst1
@@ -62,6 +208,34 @@ int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* con
           w[3], static_cast<int32_t>(w[4]), static_cast<const double*>(as_ptr(w[5])), w[6],
           static_cast<const double*>(as_ptr(w[7])), w[8], static_cast<double*>(as_ptr(w[9])), w[10],
           as_ptr(w[11]), w[12], w[13], stream);
+    } else if (op.code == kOpFused) {
+      // w[0] chain index, w[1] input, w[2] output, w[3] barrier counters, w[4] grid
+      w[1] = patched(w[1], n_patch, from, to);
+      w[2] = patched(w[2], n_patch, from, to);
+      if (w[0] < 0 || w[0] >= static_cast<int64_t>(s->chains.size())) {
+        set_error("tnb_seq_run: corrupt fused op");
+      } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(static_cast<unsigned>(w[4]));
+        cfg.blockDim = dim3(kFusedThreads);
+        cfg.dynamicSmemBytes = sizeof(FusedSmem);
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(
+            &cfg, chain_kernel, s->chains[static_cast<size_t>(w[0])],
+            static_cast<const double*>(as_ptr(w[1])), static_cast<double*>(as_ptr(w[2])),
+            static_cast<unsigned int*>(as_ptr(w[3])));
+        if (e != cudaSuccess) {
+          set_error(std::string("tnb_seq_run: fused chain launch: ") + cudaGetErrorString(e));
+          rc = TNB_ECUDA;
+        } else {
+          rc = check_launch("tnb_seq_run: fused chain");
+        }
+      }
     } else {
       set_error("tnb_seq_run: corrupt sequence");
     }
@@ -123,7 +297,62 @@ extern "C" int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n
 extern "C" int tnb_seq_append(tnb_seq* dst, const tnb_seq* src) {
   TNB_REQUIRE(dst != nullptr && src != nullptr, "tnb_seq_append: null sequence");
   TNB_REQUIRE(dst != src, "tnb_seq_append: a sequence cannot append itself");
-  dst->ops.insert(dst->ops.end(), src->ops.begin(), src->ops.end());
+  const int64_t base = static_cast<int64_t>(dst->chains.size());
+  dst->chains.insert(dst->chains.end(), src->chains.begin(), src->chains.end());
+  for (auto op : src->ops) {
+    if (op.code == tnb::kOpFused) op.w[0] += base;  // the copied chain's new index
+    dst->ops.push_back(op);
+  }
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* y_slot,
+                            void* barrier, tnb_seq* dst) {
+  TNB_REQUIRE(src != nullptr && dst != nullptr && src != dst, "tnb_seq_fuse: bad sequences");
+  TNB_REQUIRE(x_slot != nullptr && y_slot != nullptr && barrier != nullptr,
+              "tnb_seq_fuse: null slot or barrier");
+  TNB_REQUIRE(!src->ops.empty(), "tnb_seq_fuse: empty sequence");
+  TNB_REQUIRE(src->ops.size() <= static_cast<size_t>(tnb::kMaxStages),
+              "tnb_seq_fuse: more stages than one fused launch holds");
+  tnb::FChain ch{};
+  ch.n = static_cast<int32_t>(src->ops.size());
+  const int64_t xw = tnb::as_word(x_slot), yw = tnb::as_word(y_slot);
+  for (size_t i = 0; i < src->ops.size(); ++i) {
+    const auto& op = src->ops[i];
+    tnb::FStage& st = ch.st[i];
+    TNB_REQUIRE(op.code == tnb::kOpGather || op.code == tnb::kOpGemm,
+                "tnb_seq_fuse: only gathers and grouped GEMMs fuse");
+    std::memcpy(st.w, op.w, sizeof(st.w));
+    st.code = op.code;
+    if (op.code == tnb::kOpGather) {
+      st.kind = 0;
+      st.items = op.w[3];  // chunks
+      for (int k : tnb::kGatherBufs)
+        st.w[k] = st.w[k] == xw ? tnb::kSlotX : st.w[k] == yw ? tnb::kSlotY : st.w[k];
+    } else {
+      st.kind = static_cast<int32_t>(op.w[4]);
+      TNB_REQUIRE(st.kind == TNB_TILE_64 || st.kind == TNB_TILE_32 || st.kind == TNB_TILE_SKINNY,
+                  "tnb_seq_fuse: tensor-core GEMM stages do not fuse");
+      st.items = op.w[3];  // tiles (a 32 x 32 tile goes to one of four groups of a CTA)
+      for (int k : tnb::kGemmBufs)
+        st.w[k] = st.w[k] == xw ? tnb::kSlotX : st.w[k] == yw ? tnb::kSlotY : st.w[k];
+    }
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) {
+    tnb::set_error("tnb_seq_fuse: no current device");
+    return TNB_ECUDA;
+  }
+  const int grid = tnb::fused_grid(device);
+  if (grid <= 0) {
+    tnb::set_error("tnb_seq_fuse: the chain kernel cannot be resident");
+    return TNB_ECUDA;
+  }
+  dst->chains.push_back(ch);
+  tnb_seq::Op op{tnb::kOpFused,
+                 {static_cast<int64_t>(dst->chains.size() - 1), xw, yw, tnb::as_word(barrier),
+                  grid, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+  dst->ops.push_back(op);
   return TNB_OK;
 }
 

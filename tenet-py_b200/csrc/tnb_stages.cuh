@@ -1,0 +1,416 @@
+// Device bodies of the table-driven stages -- a block-gather chunk, an FP64 GEMM tile, a
+// skinny GEMM tile -- shared by the standalone kernels (one launch per stage) and the
+// persistent chain kernel (every stage of a compiled chain in one launch).
+//
+// kFused selects how data buffers are read: a standalone launch reads its sources through
+// the read-only path (ld.global.nc), while inside the persistent kernel a source may have
+// been written by another CTA earlier in the same launch, so it is read through L2
+// (ld.global.cg), which the grid barrier's fences make coherent.  Descriptor tables never
+// change during a launch and are read through the read-only path in both.
+#pragma once
+
+#include "tnb_common.cuh"
+
+namespace tnb {
+
+// Synchronisation of the threads that share one work item: the whole CTA, or (several
+// items per CTA in the persistent kernel) one named barrier per group of threads.
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct GroupSync {
+  int id, count;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(count) : "memory");
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+// block gather
+
+constexpr int kGatherThreads = 256;
+constexpr int kGatherEpt = TNB_GATHER_CHUNK / kGatherThreads;
+constexpr int kStagedTerms = 64;
+
+struct GatherArgs {
+  const int64_t* segs;
+  int64_t n_seg;
+  const int32_t* chunk_map;
+  const int64_t* term_src;
+  const double* term_coeff;
+  const int64_t* term_ld;
+  int64_t n_term;
+  const double* src0;
+  int64_t n_src0;
+  double* dst0;
+  int64_t n_dst0;
+  const double* src1;
+  int64_t n_src1;
+  double* dst1;
+  int64_t n_dst1;
+};
+
+struct GatherSmem {
+  int64_t row[TNB_SEG_WIDTH];
+  int64_t t_src[kStagedTerms], t_ld[kStagedTerms];
+  double t_cf[kStagedTerms];
+};
+
+template <bool kFused>
+__device__ __forceinline__ double load_data(const double* p) {
+  if constexpr (kFused) {
+    return __ldcg(p);
+  } else {
+    return __ldg(p);
+  }
+}
+
+// One TNB_GATHER_CHUNK-element chunk of a gather by a group of NT threads (the whole
+// CTA standalone; a quarter of it in the persistent kernel); `tid` is the thread's index
+// within the group.
+template <int NT, bool kFused, class Sync>
+__device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm, int tid,
+                             Sync sync) {
+  constexpr int kEpt = TNB_GATHER_CHUNK / NT;
+  static_assert(NT >= TNB_SEG_WIDTH && NT >= kStagedTerms, "a group stages a row and its terms");
+  if constexpr (kFused) sync();  // the previous item's readers are done with sm
+  const int64_t seg = g.chunk_map[chunk];
+  if (seg < 0 || seg >= g.n_seg) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  if (tid < TNB_SEG_WIDTH) sm.row[tid] = g.segs[seg * TNB_SEG_WIDTH + tid];
+  sync();
+
+  const int64_t* row = sm.row;
+  const int64_t dst_off = row[0];
+  const int64_t size = row[1];
+  const int rank = static_cast<int>(row[2]);
+  const int64_t t0 = row[3], t1 = row[4];
+  const bool second = row[5] != 0;
+  const double* __restrict__ src = second ? g.src1 : g.src0;
+  double* __restrict__ dst = second ? g.dst1 : g.dst0;
+  const int64_t n_src = second ? g.n_src1 : g.n_src0;
+  const int64_t n_dst = second ? g.n_dst1 : g.n_dst0;
+  if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || rank > TNB_MAX_RANK) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  const int nt = static_cast<int>(t1 - t0);
+  const bool staged = nt <= kStagedTerms;
+  if (staged && tid < nt) {
+    sm.t_src[tid] = g.term_src[t0 + tid];
+    sm.t_ld[tid] = g.term_ld[t0 + tid];
+    sm.t_cf[tid] = g.term_coeff[t0 + tid];
+  }
+  sync();
+  if constexpr (!kFused) pdl_wait();  // tables are static; the source may be the previous kernel's output
+
+  uint32_t dims[TNB_MAX_RANK];
+  int64_t dstr[TNB_MAX_RANK], rstr[TNB_MAX_RANK], cstr[TNB_MAX_RANK];
+#pragma unroll
+  for (int d = 0; d < TNB_MAX_RANK; ++d) {
+    dims[d] = d < rank ? static_cast<uint32_t>(row[8 + d]) : 1u;
+    dstr[d] = d < rank ? row[16 + d] : 0;
+    rstr[d] = d < rank ? row[24 + d] : 0;
+    cstr[d] = d < rank ? row[32 + d] : 0;
+  }
+
+  const int64_t base = (chunk - row[6]) * TNB_GATHER_CHUNK;
+#pragma unroll
+  for (int k = 0; k < kEpt; ++k) {
+    const int64_t e = base + tid + k * NT;
+    if (e >= size) break;
+    uint32_t rem = static_cast<uint32_t>(e);
+    int64_t doff = 0, roff = 0, coff = 0;
+#pragma unroll
+    for (int d = TNB_MAX_RANK - 1; d >= 0; --d) {
+      if (d < rank) {
+        const uint32_t j = rem % dims[d];
+        rem /= dims[d];
+        doff += static_cast<int64_t>(j) * dstr[d];
+        roff += static_cast<int64_t>(j) * rstr[d];
+        coff += static_cast<int64_t>(j) * cstr[d];
+      }
+    }
+    double acc = 0.0;
+    if (staged) {
+      for (int t = 0; t < nt; ++t) {
+        const int64_t o = sm.t_src[t] + sm.t_ld[t] * roff + coff;
+        if (o < 0 || o >= n_src) { raise_bounds(); continue; }
+        acc = fma(sm.t_cf[t], load_data<kFused>(src + o), acc);
+      }
+    } else {
+      for (int64_t t = t0; t < t1; ++t) {
+        const int64_t o = __ldg(g.term_src + t) + __ldg(g.term_ld + t) * roff + coff;
+        if (o < 0 || o >= n_src) { raise_bounds(); continue; }
+        acc = fma(__ldg(g.term_coeff + t), load_data<kFused>(src + o), acc);
+      }
+    }
+    const int64_t w = dst_off + doff;
+    if (w < 0 || w >= n_dst) { raise_bounds(); continue; }
+    dst[w] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// grouped FP64 GEMM tiles
+
+constexpr int kBk = 16;
+constexpr int kSkinnyThreads = 256;
+constexpr int kSkinnyMax = 16;
+
+// Work-buffer layout of the split-K path: n_counters uint32 counters, padded to 256 bytes,
+// then the FP64 partial tiles.
+__host__ __device__ inline int64_t gemm_work_parts_offset(int64_t n_counters) {
+  return ((4 * n_counters + 255) / 256) * 256;
+}
+
+struct GemmArgs {
+  const int64_t* table;
+  int64_t n_gemm;
+  const int32_t* tile_map;
+  const double* a;
+  int64_t n_a;
+  const double* b;
+  int64_t n_b;
+  double* c;
+  int64_t n_c;
+  unsigned int* counters;
+  int64_t n_cnt;
+  double* parts;
+  int64_t n_parts;
+};
+
+struct GemmRow {
+  int64_t M, N, K, aoff, lda, boff, ldb, coff, ldc, tile_begin, tiles_n, splits, ksplit,
+      part_off, cnt_off;
+};
+
+__device__ __forceinline__ bool load_row(const int64_t* __restrict__ table, int64_t n_gemm,
+                                         const int32_t* __restrict__ tile_map, int64_t tile,
+                                         GemmRow& r) {
+  const int64_t g = tile_map[tile];
+  if (g < 0 || g >= n_gemm) return false;
+  const int64_t* t = table + g * TNB_GEMM_WIDTH;
+  r.M = t[0]; r.N = t[1]; r.K = t[2]; r.aoff = t[3]; r.lda = t[4]; r.boff = t[5];
+  r.ldb = t[6]; r.coff = t[7]; r.ldc = t[8]; r.tile_begin = t[9]; r.tiles_n = t[10];
+  r.splits = t[12] > 1 ? t[12] : 1; r.ksplit = t[13]; r.part_off = t[14]; r.cnt_off = t[15];
+  return true;
+}
+
+__device__ __forceinline__ bool footprint_ok(const GemmRow& r, int64_t n_a, int64_t n_b,
+                                             int64_t n_c) {
+  bool bad = r.M < 0 || r.N < 0 || r.K < 0 || r.coff < 0 || r.coff + (r.M - 1) * r.ldc + r.N > n_c;
+  if (r.K > 0)
+    bad = bad || r.aoff < 0 || r.boff < 0 || r.aoff + (r.M - 1) * r.lda + r.K > n_a ||
+          r.boff + (r.K - 1) * r.ldb + r.N > n_b;
+  return !bad;
+}
+
+template <int TM, int TN>
+struct GemmSmem {
+  double As[2][kBk][TM + 1];
+  double Bs[2][kBk][TN];
+  GemmRow row;
+  int ok;
+  int last;
+};
+
+// One TM x TN output tile (or one K split of it) by the NT = TM*TN/16 threads of a group;
+// `tid` is the thread's index within the group.
+template <int TM, int TN, bool kFused, class Sync>
+__device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN>& sm, int tid,
+                          Sync sync) {
+  constexpr int TX = TN / 4, TY = TM / 4, NT = TX * TY;
+  constexpr int LA = (TM * kBk) / NT, LB = (TN * kBk) / NT;
+  if constexpr (kFused) sync();  // the previous item's readers are done with sm
+  if (tid == 0) {
+    GemmRow r;
+    bool ok = load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+    ok = ok && footprint_ok(r, g.n_a, g.n_b, g.n_c);
+    if (ok && r.splits > 1) {
+      const int64_t nt = ((r.M + TM - 1) / TM) * r.tiles_n;
+      ok = r.ksplit > 0 && r.ksplit % kBk == 0 && r.cnt_off >= 0 && r.cnt_off + nt <= g.n_cnt &&
+           r.part_off >= 0 && r.part_off + nt * r.splits * TM * TN <= g.n_parts;
+    }
+    if (!ok) raise_bounds();
+    sm.row = r;
+    sm.ok = ok;
+  }
+  sync();
+  if (!sm.ok) return;
+  const GemmRow r = sm.row;
+  const int64_t local = tile - r.tile_begin;
+  const int64_t split = local % r.splits, t2 = local / r.splits;
+  const int64_t m0 = (t2 / r.tiles_n) * TM, n0 = (t2 % r.tiles_n) * TN;
+  if (m0 >= r.M || n0 >= r.N) return;
+  const int64_t kb = r.splits > 1 ? split * r.ksplit : 0;
+  const int64_t ke = r.splits > 1 ? min(r.K, kb + r.ksplit) : r.K;
+  if constexpr (!kFused) pdl_wait();  // A may be the previous kernel's output
+
+  const double* __restrict__ a = g.a;
+  const double* __restrict__ b = g.b;
+  const int tx = tid % TX, ty = tid / TX;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+  double ra[LA], rb[LB];
+  auto load_slab = [&](int64_t k0) {
+#pragma unroll
+    for (int q = 0; q < LA; ++q) {
+      const int idx = tid + q * NT;
+      const int am = idx / kBk, ak = idx % kBk;
+      const int64_t gm = m0 + am, gk = k0 + ak;
+      ra[q] = (gm < r.M && gk < ke) ? load_data<kFused>(a + r.aoff + gm * r.lda + gk) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < LB; ++q) {
+      const int idx = tid + q * NT;
+      const int bk = idx / TN, bn = idx % TN;
+      const int64_t gk = k0 + bk, gn = n0 + bn;
+      rb[q] = (gk < ke && gn < r.N) ? load_data<kFused>(b + r.boff + gk * r.ldb + gn) : 0.0;
+    }
+  };
+  auto store_slab = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < LA; ++q) {
+      const int idx = tid + q * NT;
+      sm.As[buf][idx % kBk][idx / kBk] = ra[q];
+    }
+#pragma unroll
+    for (int q = 0; q < LB; ++q) {
+      const int idx = tid + q * NT;
+      sm.Bs[buf][idx / TN][idx % TN] = rb[q];
+    }
+  };
+
+  const int64_t nk = ke > kb ? (ke - kb + kBk - 1) / kBk : 0;
+  if (nk > 0) {
+    load_slab(kb);
+    store_slab(0);
+    sync();
+  }
+  for (int64_t s = 0; s < nk; ++s) {
+    const int cur = static_cast<int>(s & 1);
+    if (s + 1 < nk) load_slab(kb + (s + 1) * kBk);
+#pragma unroll
+    for (int k = 0; k < kBk; ++k) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = sm.As[cur][k][ty + TY * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = sm.Bs[cur][k][tx + TX * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+    if (s + 1 < nk) store_slab(cur ^ 1);
+    sync();
+  }
+
+  if (r.splits > 1) {
+    // split K: park this partial tile, and let the last of the tile's splits to arrive
+    // sum all of them in split order (a fixed order, so the result is deterministic)
+    double* mine = g.parts + r.part_off + (t2 * r.splits + split) * (TM * TN);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mine[(ty + TY * i) * TN + tx + TX * j] = acc[i][j];
+    __threadfence();
+    sync();
+    if (tid == 0) {
+      const unsigned int prev = atomicAdd(g.counters + r.cnt_off + t2, 1u);
+      sm.last = (prev == static_cast<unsigned int>(r.splits - 1));
+    }
+    sync();
+    if (!sm.last) return;
+    __threadfence();
+    const double* base = g.parts + r.part_off + t2 * r.splits * (TM * TN);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int e = (ty + TY * i) * TN + tx + TX * j;
+        double v = 0.0;
+        for (int64_t q = 0; q < r.splits; ++q) v += __ldcg(base + q * (TM * TN) + e);
+        acc[i][j] = v;
+      }
+    if (tid == 0) g.counters[r.cnt_off + t2] = 0u;  // leave the counters zero for the next run
+  }
+
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int64_t gm = m0 + ty + TY * i;
+    if (gm >= r.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t gn = n0 + tx + TX * j;
+      if (gn < r.N) g.c[r.coff + gm * r.ldc + gn] = acc[i][j];
+    }
+  }
+}
+
+struct SkinnySmem {
+  double Bs[kSkinnyMax * kSkinnyMax];
+  GemmRow row;
+  int ok;
+};
+
+// kSkinnyThreads output rows, C[m, :] = A[m, :] * B for N, K <= 16, by a group of NT
+// threads (one row each standalone; kSkinnyThreads / NT rows each in the persistent
+// kernel, which gives every thread independent loads to overlap).
+template <int NT, bool kFused, class Sync>
+__device__ void skinny_tile(const GemmArgs& g, int64_t tile, SkinnySmem& sm, int tid, Sync sync) {
+  constexpr int kRows = kSkinnyThreads / NT;
+  if constexpr (kFused) sync();
+  if (tid == 0) {
+    GemmRow r;
+    bool ok = load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+    ok = ok && footprint_ok(r, g.n_a, g.n_b, g.n_c) && r.N <= kSkinnyMax && r.K <= kSkinnyMax;
+    if (!ok) raise_bounds();
+    sm.row = r;
+    sm.ok = ok;
+  }
+  sync();
+  if (!sm.ok) return;
+  const GemmRow r = sm.row;
+  const int K = static_cast<int>(r.K), N = static_cast<int>(r.N);
+  if constexpr (!kFused) pdl_wait();  // A may be the previous kernel's output
+  for (int i = tid; i < K * N; i += NT)
+    sm.Bs[i] = load_data<kFused>(g.b + r.boff + (i / N) * r.ldb + (i % N));
+  sync();
+  const int64_t m_base = (tile - r.tile_begin) * kSkinnyThreads + tid;
+  // rows in batches of up to two: both rows' loads are issued before either is used
+  constexpr int kBatch = kRows < 2 ? kRows : 2;
+#pragma unroll 1
+  for (int q0 = 0; q0 < kRows; q0 += kBatch) {
+    double av[kBatch][kSkinnyMax];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      const int64_t m = m_base + (q0 + q) * NT;
+#pragma unroll
+      for (int k = 0; k < kSkinnyMax; ++k)
+        av[q][k] = (m < r.M && k < K) ? load_data<kFused>(g.a + r.aoff + m * r.lda + k) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      const int64_t m = m_base + (q0 + q) * NT;
+      if (m >= r.M) break;
+#pragma unroll 1
+      for (int n = 0; n < N; ++n) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < kSkinnyMax; ++k)
+          if (k < K) s = fma(av[q][k], sm.Bs[k * N + n], s);
+        g.c[r.coff + m * r.ldc + n] = s;
+      }
+    }
+  }
+}
+
+}  // namespace tnb

@@ -92,6 +92,13 @@ class Seq:
 
 _REC: Seq | None = None
 
+#: Run compiled chains as one persistent launch when every stage fuses.  Off by default:
+#: on B200 the stage-by-stage replay (a CUDA graph, programmatic dependent launch) is
+#: faster at the sizes measured, because the FP64 tile holds the persistent kernel to one
+#: CTA per SM, which starves its latency-bound gather stages.  The fused launch gives
+#: bit-identical results and stays available for comparison.
+FUSE = False
+
 
 _TORCH_DTYPE = {np.dtype(np.int64).str: torch.int64, np.dtype(np.int32).str: torch.int32,
                 np.dtype(np.float64).str: torch.float64}

@@ -161,7 +161,7 @@ class DeviceLanczos:
         from tenet import _exec, _lib
 
         P, p, r = _exec.ptr, self.program, self.runs
-        _lib.call("tnb_lanczos_solve", p.seq.handle, P(p.x_slot), P(p.y_slot), self.n,
+        _lib.call("tnb_lanczos_solve", p.exec_seq.handle, P(p.x_slot), P(p.y_slot), self.n,
                   self.ncv, float(self.tol), int(self.reorth), P(x), P(self.V),
                   self.V.stride(0), P(self.W), P(self.state), P(self.scal),
                   P(self.ptrs), P(self.gs), P(r.start), P(r.weight), r.n_runs, P(self.work),
@@ -188,7 +188,7 @@ class DeviceLanczos:
         P, c, r = _exec.ptr, self.correct, self.runs
         self._host_coef.numpy()[:] = coef
         self.coef.copy_(self._host_coef, non_blocking=True)
-        _lib.call("tnb_lanczos_ritz", c.seq.handle if c is not None else None,
+        _lib.call("tnb_lanczos_ritz", c.exec_seq.handle if c is not None else None,
                   P(c.x_slot) if c is not None else None, P(c.y_slot) if c is not None else None,
                   self.n, self.ncv, P(self.coef), P(self.ptrs), P(out), P(self.W2),
                   P(self.scal), P(r.start), P(r.weight), r.n_runs, P(self.work),

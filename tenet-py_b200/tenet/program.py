@@ -30,6 +30,9 @@ from tenet.tensor import SymmetricTensor
 
 __all__ = ["ChainProgram", "heff2_program"]
 
+#: stage capacity of one fused launch (``tnb_seq_fuse``)
+FUSED_MAX_STAGES = 24
+
 
 class _StructureOnly:
     """Stand-in for a fixed operand in a shared program template: its structure only."""
@@ -202,7 +205,24 @@ class ChainProgram:
         self.seq = _exec.Seq()
         with self.seq:
             self._run_tables(self.x_slot, self.y_slot)
+        # the same stages as one persistent launch, when they all fuse (no tensor-core
+        # stage, at most the kernel's stage count)
+        self.fused = None
+        if not self.uses_tensor_cores and 0 < len(self.seq) <= FUSED_MAX_STAGES:
+            from tenet import _lib
+
+            self.barrier = torch.zeros(2, dtype=torch.int32, device=dev)
+            fused = _exec.Seq()
+            _lib.call("tnb_seq_fuse", self.seq.handle, self.x_slot.data_ptr(),
+                      self.y_slot.data_ptr(), self.barrier.data_ptr(), fused.handle)
+            self.fused = fused
         self._built = True
+
+    @property
+    def exec_seq(self) -> _exec.Seq:
+        """The sequence a replay runs: the fused launch when there is one (and fusing is
+        on), else the stage-by-stage sequence."""
+        return self.fused if (self.fused is not None and _exec.FUSE) else self.seq
 
     def refresh(self) -> None:
         """Re-pack the fixed operands (after their values changed, same structures)."""
@@ -229,11 +249,13 @@ class ChainProgram:
                    for lk in self.links for p in lk.gemm.products)
 
     def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
-        """``out = chain(x)`` on the current stream: one replay of the recorded sequence
-        (or launch by launch while a ``LaunchLog`` times each kernel)."""
+        """``out = chain(x)`` on the current stream: one replay of the recorded stages (or
+        of the fused one-launch chain when ``_exec.FUSE`` is on; launch by launch while a
+        ``LaunchLog`` times each kernel).  One program must not run on two streams at
+        once."""
         if _exec._LOG is None and _exec._REC is None:
-            self.seq.run({self.x_slot.data_ptr(): x.data_ptr(),
-                          self.y_slot.data_ptr(): out.data_ptr()})
+            self.exec_seq.run({self.x_slot.data_ptr(): x.data_ptr(),
+                               self.y_slot.data_ptr(): out.data_ptr()})
             return out
         return self._run_tables(x, out)
 

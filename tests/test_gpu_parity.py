@@ -470,6 +470,7 @@ def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
     T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
     prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
     assert len(prog.seq) == prog.launches
+    assert prog.fused is not None and len(prog.fused) == 1
     x = T["aa"].arena
     y_seq = torch.full_like(prog.y_slot, float("nan"))
     y_py = torch.full_like(prog.y_slot, float("nan"))
@@ -534,3 +535,34 @@ def test_j1j2_dmrg_matches_exact_diagonalisation(j2):
     e, hist, _ = network.dmrg_(network.MPS.random(phys, bonds, seed=0), h, chi=64,
                                cutoff=1e-14, ncv=20, max_sweeps=12, energy_tol=1e-12)
     assert e == pytest.approx(_ed_j1j2(L, 1.0, j2), abs=1e-9)
+
+
+def test_fused_chain_is_bit_identical_to_stage_by_stage(golden_dir):
+    """The persistent one-launch chain runs the same tables and arithmetic as the
+    stage-by-stage replay: identical bits on the golden heff2 and on the bench workload,
+    repeatedly (its grid barrier and split-K counters return to zero)."""
+    import bench
+    from tenet import _exec
+    from tenet.program import heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    w = bench.build_workload()
+    for ops4, aa in (((T["fl"], T["w1"], T["w2"], T["fr"]), T["aa"]), (w[:4], w[4])):
+        prog = heff2_program(*ops4, aa.structure)
+        assert prog.fused is not None and len(prog.fused) == 1
+        outs = []
+        default = _exec.FUSE
+        for fuse in (True, False, True, True):
+            _exec.FUSE = fuse
+            try:
+                y = torch.full_like(prog.y_slot, float("nan"))
+                prog.run(aa.arena, y)
+                torch.cuda.synchronize()
+                outs.append(y)
+            finally:
+                _exec.FUSE = default
+        for y in outs[1:]:
+            assert torch.equal(y, outs[0])
+        assert int(prog.barrier[0].item()) == 0
