@@ -810,3 +810,16 @@ def beta_free_energy(c: Tensor, e: Tensor, bulk: Tensor) -> float:
     z_a = full_trace(einsum("ab,acp,cd,edq,fe,gfr,gh,hks,spqr->kb",
                             cc, ec, ca, ea, cc, ea, ca, ec, bulk))
     return -float(np.log(z_a * z_c / z_h ** 2))
+
+
+def onsager_beta_f(beta: float, n: int = 20001) -> float:
+    """Onsager's exact ``beta f`` of the square-lattice Ising model (J = 1, no field), the
+    value ``examples/toy_codes/ctmrg.py``'s ``onsager`` quotes:
+    ``-beta f = ln(2 cosh 2b) + (1/2pi) int_0^pi ln[(1 + sqrt(1 - k^2 sin^2 t)) / 2] dt``
+    with ``k = 2 sinh 2b / cosh^2 2b``, the integral by Simpson's rule on ``n`` points."""
+    k = 2.0 * np.sinh(2.0 * beta) / np.cosh(2.0 * beta) ** 2
+    t = np.linspace(0.0, np.pi, n)
+    f = np.log((1.0 + np.sqrt(np.maximum(0.0, 1.0 - (k * np.sin(t)) ** 2))) / 2.0)
+    h = t[1] - t[0]
+    integral = h / 3.0 * (f[0] + f[-1] + 4.0 * f[1:-1:2].sum() + 2.0 * f[2:-1:2].sum())
+    return -float(np.log(2.0 * np.cosh(2.0 * beta)) + integral / (2.0 * np.pi))

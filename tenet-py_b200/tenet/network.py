@@ -662,25 +662,31 @@ def spectrum(s: SymmetricTensor) -> list[float]:
     return sorted(out, reverse=True)
 
 
-def move(c: SymmetricTensor, e: SymmetricTensor, absorb: Absorb, *, chi: int):
+def move(c: SymmetricTensor, e: SymmetricTensor, absorb: Absorb, *, chi: int,
+         precision: str = "f64", tc_min_flops: int | None = None):
     """One C4v move (``network/ctmrg.py:451-526``): the enlarged corner's truncated SVD;
-    the new corner is the singular-value tensor, the new edge is projected with ``u``."""
+    the new corner is the singular-value tensor, the new edge is projected with ``u``.
+    ``precision`` "tf32" / "3xbf16" runs the corner and edge contractions' sector
+    products on the tensor cores (``ops.precision``); the SVD and truncation stay FP64."""
     from tenet import linalg
 
-    big = absorb.corner(c, e)
+    with ops.precision(precision, tc_min_flops):
+        big = absorb.corner(c, e)
     n = big.ndim // 2
     p, s, _ = linalg.svd_truncated(big, (tuple(range(n)), tuple(range(n, 2 * n))), max_bond=chi)
-    e2 = absorb.edge(e, p)
+    with ops.precision(precision, tc_min_flops):
+        e2 = absorb.edge(e, p)
     return s / ops.norm(s), e2 / ops.norm(e2), p.legs[-1].space
 
 
 def ctmrg(absorb: Absorb, c: SymmetricTensor, e: SymmetricTensor, *, chi: int,
-          tol: float = 1e-10, max_sweeps: int = 100):
+          tol: float = 1e-10, max_sweeps: int = 100, precision: str = "f64",
+          tc_min_flops: int | None = None):
     """Moves until the corner spectrum changes by less than ``tol`` (``network/ctmrg.py:572-660``).
-    Returns ``(c, e, bond, history)``."""
+    Returns ``(c, e, bond, history)``.  ``precision``: see ``move``."""
     prev, history, bond = spectrum(c), [], None
     for _ in range(max_sweeps):
-        c, e, bond = move(c, e, absorb, chi=chi)
+        c, e, bond = move(c, e, absorb, chi=chi, precision=precision, tc_min_flops=tc_min_flops)
         cur = spectrum(c)
         n = max(len(prev), len(cur))
         a = np.array(prev + [0.0] * (n - len(prev)))

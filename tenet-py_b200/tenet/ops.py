@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import operator
 from collections import Counter
+from contextlib import contextmanager
 from dataclasses import dataclass
 from functools import cache
 
@@ -148,8 +149,30 @@ class ContractionExec:
         return self.gemm.flops
 
 
+#: arithmetic of the coupled-sector products of eager contractions: ("f64", None), or a
+#: tensor-core precision ("tf32" / "3xbf16") with its size rule (see ``precision``)
+_PRECISION: tuple = ("f64", None)
+
+
+@contextmanager
+def precision(kind: str = "f64", tc_min_flops: int | None = None):
+    """Run the coupled-sector products of eager contractions (``tensordot``, ``einsum``)
+    inside the block in ``kind``: "f64" (the plain form), or "tf32" / "3xbf16" on the
+    tcgen05 tensor cores for the products of at least ``tc_min_flops`` (default
+    ``_exec.TC_MIN_FLOPS``), FP64 in and out.  Gathers, SVDs and norms stay FP64."""
+    global _PRECISION
+    if kind != "f64" and kind not in _exec.TC_KINDS:
+        raise ValueError(f"unknown precision {kind!r}")
+    prev, _PRECISION = _PRECISION, (kind, tc_min_flops)
+    try:
+        yield
+    finally:
+        _PRECISION = prev
+
+
 @cache
-def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes) -> ContractionExec:
+def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes, precision: str = "f64",
+                     tc_min_flops: int | None = None) -> ContractionExec:
     ca, cb = axes
     if sa.provider != sb.provider:
         raise ValueError("tensordot: operands have different providers")
@@ -191,12 +214,14 @@ def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes) -> Contract
         _exec.gather_rows(sa, "arena", sa2, "matrix", perm_a, terms_a, 0, keep_a),
         _exec.gather_rows(sb, "arena", sb2, "matrix", perm_b, terms_b, 1, keep_b))
     unpack = _exec.make_gather(_exec.gather_rows(sc, "matrix", so, "arena", perm_u, terms_u))
-    return ContractionExec(so, ma.size, mb.size, mc.size, pack, _exec.GemmGroup(products), unpack)
+    return ContractionExec(so, ma.size, mb.size, mc.size, pack,
+                           _exec.GemmGroup(products, precision, tc_min_flops), unpack)
 
 
 def tensordot(a: SymmetricTensor, b: SymmetricTensor, axes) -> SymmetricTensor:
     """Contract ``axes[0]`` of ``a`` with ``axes[1]`` of ``b``; free legs come back unchanged."""
-    ex = contraction_exec(a.structure, b.structure, _validated_axes(a.structure, b.structure, axes))
+    ex = contraction_exec(a.structure, b.structure, _validated_axes(a.structure, b.structure, axes),
+                          *_PRECISION)
     return SymmetricTensor(ex.out, arena=ex.run(a.arena, b.arena))
 
 

@@ -94,3 +94,41 @@ def test_mixed_precision_dmrg_energy(golden_dir, precision):
                                max_sweeps=g["sweeps"], energy_tol=0.0, precision=precision,
                                tc_min_flops=0)  # every product on the tensor cores
     assert abs(e - g["energy"]) / L <= 1e-8, f"|dE/L| = {abs(e - g['energy']) / L:.2e}"
+
+
+@pytest.mark.parametrize("precision,rel", [("3xbf16", 1e-10), ("tf32", 1e-7)])
+def test_mixed_precision_ctmrg_free_energy(golden_dir, precision, rel):
+    """Z2 Ising CTMRG with every corner / edge sector product on the tensor cores (the SVD
+    and truncation in FP64): the free energy against the reference's converged FP64 run
+    (beta = 0.4, chi = 16) and the even/odd bond split unchanged."""
+    import json
+
+    import oracle.tenet_oracle as O
+    from tenet import network
+
+    r = json.loads((golden_dir / "ctmrg.json").read_text())["b040_chi16"]
+    bulk = network.ising_bulk(r["beta"])
+    c, e, bond, _ = network.ctmrg(*network.single_layer_ctm(bulk), chi=r["chi"], tol=r["tol"],
+                                  max_sweeps=r["max_sweeps"], precision=precision,
+                                  tc_min_flops=0)
+    bf = network.beta_free_energy(c, e, bulk)
+    assert abs(bf - r["beta_f"]) <= rel * abs(r["beta_f"])
+    assert abs(bf - O.onsager_beta_f(r["beta"])) <= max(rel, 1e-9) * abs(r["beta_f"])
+    assert [[a.parity, m] for a, m in bond.sectors] == r["bond"]
+
+
+def test_mixed_precision_ctmrg_chi128_near_criticality():
+    """beta = 0.44, chi = 128 (the even/odd split 64/64): 3xBF16 corner and edge products
+    give the FP64 free energy to 1e-8 and Onsager's to 1e-7."""
+    import oracle.tenet_oracle as O
+    from tenet import network
+
+    bulk = network.ising_bulk(0.44)
+    out = {}
+    for prec in ("f64", "3xbf16"):
+        c, e, bond, _ = network.ctmrg(*network.single_layer_ctm(bulk), chi=128, tol=1e-10,
+                                      max_sweeps=150, precision=prec, tc_min_flops=0)
+        out[prec] = network.beta_free_energy(c, e, bulk)
+        assert [m for _, m in bond.sectors] == [64, 64]
+    assert abs(out["3xbf16"] - out["f64"]) <= 1e-8 * abs(out["f64"])
+    assert abs(out["3xbf16"] - O.onsager_beta_f(0.44)) <= 1e-7 * abs(out["f64"])

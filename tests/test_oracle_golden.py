@@ -140,3 +140,10 @@ def test_ctmrg_matches_reference(golden_dir):
         if "beta_f" in r:
             assert O.beta_free_energy(c, e, bulk) == pytest.approx(r["beta_f"], rel=1e-10)
             assert O.beta_free_energy(c, e, bulk) == pytest.approx(r["onsager_beta_f"], rel=1e-6)
+
+
+def test_onsager_restatement_matches_the_reference_value(golden_dir):
+    import json
+
+    r = json.loads((golden_dir / "ctmrg.json").read_text())["b040_chi16"]
+    assert O.onsager_beta_f(r["beta"]) == pytest.approx(r["onsager_beta_f"], rel=1e-12)
