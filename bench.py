@@ -243,6 +243,111 @@ def cpu_baseline(flops: int, budget_s: float = 20.0) -> dict:
             "ms_per_matvec": med * 1e3}
 
 
+def config3_spaces(seed: int = 1000, lam: float = 24.0, max_deg: int = 256):
+    """The U(1) x U(1) x fZ2 spaces of the batched environment update: a bond leg with
+    sectors (N, 2Sz) in [-4, 4]^2 on the allowed grid (2Sz = N mod 2, parity N mod 2; 41
+    sectors) and degeneracies Poisson(lam) clipped to 1..max_deg from
+    ``np.random.default_rng(seed)``; an MPO leg of width 6 with the Hubbard chain's
+    sectors (two identity channels and the four single-fermion channels c+up, c+dn,
+    c up, c dn); the Hubbard site's four states."""
+    from tenet.structure import GradedSpace
+    from tenet.symmetry import ProductSector as PS
+    from tenet.symmetry import U1xU1xfZ2 as P
+
+    rng = np.random.default_rng(seed)
+    bond = {}
+    for n in range(-4, 5):
+        for sz in range(-4, 5):
+            if (sz - n) % 2 == 0:
+                bond[PS(n, sz, n % 2)] = int(np.clip(rng.poisson(lam), 1, max_deg))
+    mpo = {PS(0, 0, 0): 2, PS(1, 1, 1): 1, PS(1, -1, 1): 1, PS(-1, -1, 1): 1, PS(-1, 1, 1): 1}
+    phys = {PS(0, 0, 0): 1, PS(1, 1, 1): 1, PS(1, -1, 1): 1, PS(2, 0, 0): 1}
+    return (GradedSpace.new(P, bond), GradedSpace.new(P, mpo), GradedSpace.new(P, phys))
+
+
+def config3_batch(n: int, seed: int = 1000, lam: float = 24.0, max_deg: int = 256):
+    """``(F, A, W)`` for ``n`` independent environment updates ``L' = A^dagger L W A``:
+    ``F = (ket IN, mpo OUT*, bra OUT)`` and ``A = (l OUT, p OUT, r IN)`` per member, ``W =
+    (x IN*, P OUT, p IN, m OUT*)`` shared, N(0, 1) values rounded to FP32 (member k's F
+    and A draw with seeds 2k and 2k + 1 after ``seed``)."""
+    import torch
+
+    from tenet import batch
+    from tenet.structure import IN, OUT, Leg, TensorStructure, layout
+    from tenet.tensor import SymmetricTensor
+
+    V, M, Pp = config3_spaces(seed, lam, max_deg)
+    sf = TensorStructure((Leg(V, IN), Leg(M, OUT, True), Leg(V, OUT)))
+    sa = TensorStructure((Leg(V, OUT), Leg(Pp, OUT), Leg(V, IN)))
+    sw = TensorStructure((Leg(M, IN, True), Leg(Pp, OUT), Leg(Pp, IN), Leg(M, OUT, True)))
+
+    def values(s, sd, rows):
+        rng = np.random.default_rng(sd)
+        host = rng.standard_normal((rows, layout(s).size), dtype=np.float32).astype(np.float64)
+        return torch.from_numpy(host).cuda()
+
+    F = batch.TensorBatch(sf, values(sf, seed + 1, n), n)
+    A = batch.TensorBatch(sa, values(sa, seed + 2, n), n)
+    W = batch.TensorBatch.broadcast(SymmetricTensor(sw, arena=values(sw, seed + 3, 1)[0]), n)
+    return F, A, W
+
+
+def batched_env_updates(args) -> dict:
+    """``n`` independent U(1) x U(1) x fZ2 environment updates ``L' = A^dagger L W A`` as one
+    batch (every stage one launch for all members), in FP64 and with every sector product
+    on the tensor cores (3xBF16, TF32), against the same updates run one by one in FP64.
+    Errors are relative Frobenius norms against the FP64 batch, worst member."""
+    import torch
+
+    from tenet import _exec, batch, network, ops
+
+    n = args.config3_n
+    F, A, W = config3_batch(n)
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+
+    def timed(fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            fn()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+    out = {"workload": f"{n} U1xU1xfZ2 env updates, bond 41 sectors Poisson(24) clipped 1..256 "
+                       "(seed 1000), MPO width 6 (Hubbard sectors), values N(0,1) rounded to FP32",
+           "l2": "flushed between timed steps (256 MiB write)"}
+    exact = batch.env_update_last(F, A, W)
+    log = _exec.LaunchLog(timed=True)
+    with log:
+        batch.env_update_last(F, A, W)
+    kinds = log.summary()
+    flops = sum(v["work"] for k, v in kinds.items() if k.startswith("grouped_gemm"))
+    out["flops_per_batch"] = int(flops)
+    out["launches_per_batch"] = int(sum(v["launches"] for v in kinds.values()))
+    ex = exact.arena.cpu().numpy()
+    for name, prec in (("f64", ("f64", None)), ("3xbf16", ("3xbf16", 0)), ("tf32", ("tf32", 0))):
+        with ops.precision(*prec):
+            fn = lambda: batch.env_update_last(F, A, W)  # noqa: E731
+            for _ in range(args.warmup):
+                fn()
+            ms = timed(fn, args.steps)
+            got = fn().arena.cpu().numpy()
+        err = max(float(np.linalg.norm(got[k] - ex[k]) / np.linalg.norm(ex[k])) for k in range(n))
+        out[name] = {"ms_per_batch": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                     "max_rel_error_vs_f64": err}
+    members = [(F[k], A[k], W[k]) for k in range(n)]
+    one = lambda: [network.env_update_last(*m) for m in members]  # noqa: E731
+    for _ in range(args.warmup):
+        one()
+    ms1 = timed(one, max(1, args.steps // 4))
+    out["f64_one_by_one"] = {"ms_per_batch": ms1, "tflops": flops / (ms1 * 1e-3) / 1e12}
+    out["batched_f64_speedup_over_one_by_one"] = ms1 / out["f64"]["ms_per_batch"]
+    return out
+
+
 def serving(args) -> dict:
     """Served DMRG solves against the plain FP64 form on the same seeded request sample
     (SU(2) J1-J2 chains, 8 sweeps, ncv = 20, cutoff 1e-10).  Arms, each from empty plan
@@ -507,6 +612,7 @@ def run_tenet(args) -> None:
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
         solves = serving(args) if args.serve_requests > 0 else None
+        env3 = batched_env_updates(args) if args.config3_n > 0 else None
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -528,6 +634,7 @@ def run_tenet(args) -> None:
             "launches_per_matvec_eager_ops": launches_eager,
             "mixed_precision_forms": mixed,
             "serving": solves,
+            "batched_env_updates": env3,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),
@@ -548,6 +655,8 @@ def main() -> None:
     ap.add_argument("--serve-requests", type=int, default=6,
                     help="served DMRG requests in the solves/s comparison (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--config3-n", type=int, default=64,
+                    help="members of the batched U1xU1xfZ2 environment update (0: skip)")
     ap.add_argument("--serve-full", action="store_true",
                     help="draw the requests from the full L / chi distribution")
     args = ap.parse_args()

@@ -110,6 +110,7 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
  *   TNB_TILE_64      64 x 64 output tiles (tiles = ceil(M/64) * ceil(N/64))
  *   TNB_TILE_32      32 x 32 output tiles, for compositions too small to fill the GPU
  *   TNB_TILE_SKINNY  256 output rows per tile (tiles = ceil(M/256)); needs N, K <= 16
+ *   TNB_TILE_WIDE    256 output columns per tile (tiles = ceil(N/256)); needs M, K <= 16
  *   TNB_TILE_TC_TF32    128 x 64 tiles on the tcgen05 tensor cores, operands rounded to
  *                       TF32, FP32 accumulation (tiles = ceil(M/128) * ceil(N/64))
  *   TNB_TILE_TC_3XBF16  same tiles, operands split into BF16 hi + lo pairs and the product
@@ -123,6 +124,7 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
 #define TNB_TILE_SKINNY 2
 #define TNB_TILE_TC_TF32 3
 #define TNB_TILE_TC_3XBF16 4
+#define TNB_TILE_WIDE 5
 
 /*
  * Grouped FP64 GEMM over uneven coupled sectors, one launch for every sector.

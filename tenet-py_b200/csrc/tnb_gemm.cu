@@ -13,6 +13,8 @@
 //   TNB_TILE_SKINNY one thread per output row, for products with N <= 16 and K <= 16
 //                   (the MPO links of a matvec: tall, 1-3 columns), B staged in shared
 //                   memory; bandwidth-bound by construction
+//   TNB_TILE_WIDE   one thread per output column, for products with M <= 16 and K <= 16
+//                   (an MPO tensor as the left operand: a few rows, a long N)
 // The plain form computes in FP64 on the DFMA pipe; micro-tile rows/cols are strided so
 // shared-memory reads are conflict-free, and the next K slab is prefetched into
 // registers while the current one is consumed.
@@ -35,6 +37,13 @@ gemm_f64_skinny_kernel(const GemmArgs g) {
   __shared__ SkinnySmem sm;
   pdl_launch_dependents();
   skinny_tile<kSkinnyThreads, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
+}
+
+__global__ void __launch_bounds__(kSkinnyThreads, 4)
+gemm_f64_wide_kernel(const GemmArgs g) {
+  __shared__ SkinnySmem sm;
+  pdl_launch_dependents();
+  wide_tile(g, blockIdx.x, sm);
 }
 
 }  // namespace tnb
@@ -73,6 +82,9 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
       break;
     case TNB_TILE_SKINNY:
       e = tnb::launch(tnb::gemm_f64_skinny_kernel, grid, tnb::kSkinnyThreads, s, g);
+      break;
+    case TNB_TILE_WIDE:
+      e = tnb::launch(tnb::gemm_f64_wide_kernel, grid, tnb::kSkinnyThreads, s, g);
       break;
     case TNB_TILE_TC_TF32:
     case TNB_TILE_TC_3XBF16:

@@ -332,7 +332,7 @@ extern "C" int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* 
     } else {
       st.kind = static_cast<int32_t>(op.w[4]);
       TNB_REQUIRE(st.kind == TNB_TILE_64 || st.kind == TNB_TILE_32 || st.kind == TNB_TILE_SKINNY,
-                  "tnb_seq_fuse: tensor-core GEMM stages do not fuse");
+                  "tnb_seq_fuse: only 64, 32 and skinny GEMM stages fuse");
       st.items = op.w[3];  // tiles (a 32 x 32 tile goes to one of four groups of a CTA)
       for (int k : tnb::kGemmBufs)
         st.w[k] = st.w[k] == xw ? tnb::kSlotX : st.w[k] == yw ? tnb::kSlotY : st.w[k];

@@ -413,4 +413,40 @@ __device__ void skinny_tile(const GemmArgs& g, int64_t tile, SkinnySmem& sm, int
   }
 }
 
+// kSkinnyThreads output columns, C[:, n] = A * B[:, n] for M, K <= 16, one column per
+// thread (the transpose of the skinny case: a few rows, a long N): A is staged in shared
+// memory, and loads of B and stores of C run along N, so both are coalesced.
+__device__ inline void wide_tile(const GemmArgs& g, int64_t tile, SkinnySmem& sm) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    GemmRow r;
+    bool ok = load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+    ok = ok && footprint_ok(r, g.n_a, g.n_b, g.n_c) && r.M <= kSkinnyMax && r.K <= kSkinnyMax;
+    if (!ok) raise_bounds();
+    sm.row = r;
+    sm.ok = ok;
+  }
+  __syncthreads();
+  if (!sm.ok) return;
+  const GemmRow r = sm.row;
+  const int M = static_cast<int>(r.M), K = static_cast<int>(r.K);
+  pdl_wait();  // B may be the previous kernel's output
+  for (int i = tid; i < M * K; i += kSkinnyThreads)
+    sm.Bs[i] = __ldg(g.a + r.aoff + (i / K) * r.lda + (i % K));
+  __syncthreads();
+  const int64_t n = (tile - r.tile_begin) * kSkinnyThreads + tid;
+  if (n >= r.N) return;
+  double bv[kSkinnyMax];
+#pragma unroll
+  for (int k = 0; k < kSkinnyMax; ++k) bv[k] = k < K ? __ldg(g.b + r.boff + k * r.ldb + n) : 0.0;
+#pragma unroll 1
+  for (int m = 0; m < M; ++m) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kSkinnyMax; ++k)
+      if (k < K) s = fma(sm.Bs[m * K + k], bv[k], s);
+    g.c[r.coff + m * r.ldc + n] = s;
+  }
+}
+
 }  // namespace tnb

@@ -28,7 +28,7 @@ SEG_W = 40
 GEMM_W = 16
 CHUNK = 1024
 MAX_RANK = 8
-TILE_64, TILE_32, TILE_SKINNY, TILE_TC_TF32, TILE_TC_3XBF16 = 0, 1, 2, 3, 4
+TILE_64, TILE_32, TILE_SKINNY, TILE_TC_TF32, TILE_TC_3XBF16, TILE_WIDE = 0, 1, 2, 3, 4, 5
 TC_KINDS = {"tf32": TILE_TC_TF32, "3xbf16": TILE_TC_3XBF16}
 SKINNY_ROWS, SKINNY_MAX = 256, 16
 N_SM = 148
@@ -441,6 +441,8 @@ class GemmTable:
 def _tiles(M, N, kind):
     if kind == TILE_SKINNY:
         return (M + SKINNY_ROWS - 1) // SKINNY_ROWS, 1
+    if kind == TILE_WIDE:
+        return (N + SKINNY_ROWS - 1) // SKINNY_ROWS, 1
     if kind in (TILE_TC_TF32, TILE_TC_3XBF16):
         tn = (N + 63) // 64
         return ((M + 127) // 128) * tn, tn
@@ -453,16 +455,40 @@ def choose_kind(products) -> int:
     """Skinny when every product is tall and thin; else 64x64 tiles unless they would
     not fill two waves of the GPU, then 32x32."""
     live = [p for p in products if p[0] and p[1]]
-    if live and all(_is_skinny(p) for p in live):
+    if live and all(_is_skinny(p, thin_rows(live)) for p in live):
         return TILE_SKINNY
     big = sum(_tiles(p[0], p[1], TILE_64)[0] for p in live)
     return TILE_64 if big >= 2 * N_SM else TILE_32
 
 
-def _is_skinny(p) -> bool:
-    """A tall product (many rows, at most 16 columns and 16 contracted) goes to the
-    one-thread-per-row kernel; a small one stays in the tiled launch."""
-    return p[0] >= SKINNY_ROWS and p[1] <= SKINNY_MAX and p[2] <= SKINNY_MAX
+def _is_skinny(p, thin_rows: int = 0) -> bool:
+    """A tall product (at most 16 columns and 16 contracted) goes to the one-thread-per-row
+    kernel when it has many rows, or whenever its composition's thin products hold
+    ``SKINNY_BULK`` rows or more in all (``thin_rows``): then a 64- or 32-wide tile would
+    leave most of its columns idle on a lot of work.  A few small thin products stay in
+    the tiled launch (no second launch for little work)."""
+    thin = p[1] <= SKINNY_MAX and p[2] <= SKINNY_MAX
+    return thin and (p[0] >= SKINNY_ROWS or thin_rows >= SKINNY_BULK)
+
+
+#: total rows of thin products above which every thin product of a composition runs on
+#: the one-thread-per-row kernel
+SKINNY_BULK = 1 << 16
+
+
+def thin_rows(products) -> int:
+    return sum(p[0] for p in products if p[1] and p[1] <= SKINNY_MAX and p[2] <= SKINNY_MAX)
+
+
+def wide_cols(products) -> int:
+    return sum(p[1] for p in products if p[0] and p[0] <= SKINNY_MAX and p[2] <= SKINNY_MAX)
+
+
+def _is_wide(p, cols: int = 0) -> bool:
+    """The transpose of ``_is_skinny``: at most 16 rows and 16 contracted, a long N (or
+    many such columns in the composition) -- one thread per output column."""
+    flat = p[0] <= SKINNY_MAX and p[2] <= SKINNY_MAX
+    return flat and (p[1] >= SKINNY_ROWS or cols >= SKINNY_BULK)
 
 
 #: A coupled-sector product goes to the tensor cores in the precision form only when it
@@ -476,14 +502,16 @@ def tc_worthy(p, min_flops: int | None = None) -> bool:
 
 
 class GemmGroup:
-    """One composition's products in at most three launches: the tall skinny ones, the
-    rest in FP64 tiles, and -- in the precision form -- the products big enough to be
-    dense contractions on the tcgen05 tensor cores (``tc_min_flops`` overrides the size
-    rule)."""
+    """One composition's products in at most four launches: the tall skinny ones, the wide
+    flat ones, the rest in FP64 tiles, and -- in the precision form -- the products big
+    enough to be dense contractions on the tcgen05 tensor cores (``tc_min_flops``
+    overrides the size rule)."""
 
     def __init__(self, products, precision: str = "f64", tc_min_flops: int | None = None):
-        skinny = [p for p in products if _is_skinny(p)]
-        rest = [p for p in products if not _is_skinny(p)]
+        bulk, cols = thin_rows(products), wide_cols(products)
+        skinny = [p for p in products if _is_skinny(p, bulk)]
+        wide = [p for p in products if not _is_skinny(p, bulk) and _is_wide(p, cols)]
+        rest = [p for p in products if not _is_skinny(p, bulk) and not _is_wide(p, cols)]
         tc = []
         if precision in TC_KINDS:
             tc = [p for p in rest if tc_worthy(p, tc_min_flops)]
@@ -495,6 +523,8 @@ class GemmGroup:
             self.parts.append(make_gemm(rest, choose_kind(rest)))
         if skinny:
             self.parts.append(make_gemm(skinny, TILE_SKINNY))
+        if wide:
+            self.parts.append(make_gemm(wide, TILE_WIDE))
         self.tensor_core = bool(tc)
         self.products = list(products)
         self.flops = sum(p.flops for p in self.parts)

@@ -172,7 +172,10 @@ def precision(kind: str = "f64", tc_min_flops: int | None = None):
 
 @cache
 def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes, precision: str = "f64",
-                     tc_min_flops: int | None = None) -> ContractionExec:
+                     tc_min_flops: int | None = None, out_axes=None) -> ContractionExec:
+    """Planned pairwise contraction.  ``out_axes`` (a permutation of the free legs) folds a
+    final transpose into the unpack gather: the result comes out already permuted, the
+    composed block map applied in one pass (as ``einsum`` needs)."""
     ca, cb = axes
     if sa.provider != sb.provider:
         raise ValueError("tensordot: operands have different providers")
@@ -196,6 +199,8 @@ def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes, precision: 
     so, perm_u, terms_u = chain(repartition_plan(sc, ro, ri), transpose_plan(
         repartition_plan(sc, ro, ri)[0], ft))
     assert so.legs == free, "the restoring repartition must return the free legs unchanged"
+    if out_axes is not None and tuple(out_axes) != tuple(range(len(free))):
+        so, perm_u, terms_u = chain((so, perm_u, terms_u), transpose_plan(so, tuple(out_axes)))
 
     ma, mb, mc = matrix_layout(sa2), matrix_layout(sb2), matrix_layout(sc)
     products, used = [], set()
@@ -218,10 +223,11 @@ def contraction_exec(sa: TensorStructure, sb: TensorStructure, axes, precision: 
                            _exec.GemmGroup(products, precision, tc_min_flops), unpack)
 
 
-def tensordot(a: SymmetricTensor, b: SymmetricTensor, axes) -> SymmetricTensor:
-    """Contract ``axes[0]`` of ``a`` with ``axes[1]`` of ``b``; free legs come back unchanged."""
+def tensordot(a: SymmetricTensor, b: SymmetricTensor, axes, out_axes=None) -> SymmetricTensor:
+    """Contract ``axes[0]`` of ``a`` with ``axes[1]`` of ``b``; free legs come back unchanged
+    (or transposed by ``out_axes``, in the same pass)."""
     ex = contraction_exec(a.structure, b.structure, _validated_axes(a.structure, b.structure, axes),
-                          *_PRECISION)
+                          *_PRECISION, None if out_axes is None else tuple(out_axes))
     return SymmetricTensor(ex.out, arena=ex.run(a.arena, b.arena))
 
 
@@ -281,7 +287,13 @@ def einsum(equation: str, *operands: SymmetricTensor, optimize=None) -> Symmetri
     shared = [x for x in terms[0] if x in terms[1]]
     axes = (tuple(terms[0].index(x) for x in shared), tuple(terms[1].index(x) for x in shared))
     free = [x for x in terms[0] if x not in shared] + [x for x in terms[1] if x not in shared]
-    return transpose(tensordot(operands[0], operands[1], axes), tuple(free.index(x) for x in out))
+    perm = tuple(free.index(x) for x in out)
+    if operands[0].provider.abelian:
+        # one +-1 term per block: the transpose folds into the unpack exactly
+        return tensordot(operands[0], operands[1], axes, perm)
+    # SU(2): the unpack and the transpose stay two passes, the reference's order of
+    # roundings (composing their multi-term maps would round the sums differently)
+    return transpose(tensordot(operands[0], operands[1], axes), perm)
 
 
 # ---------------------------------------------------------------------------------------

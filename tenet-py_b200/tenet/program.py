@@ -245,7 +245,9 @@ class ChainProgram:
     def tensor_core_candidates(self, min_flops: int | None = None) -> bool:
         """Whether the precision form of this chain would put any product on the tensor
         cores (``_exec.tc_worthy``)."""
-        return any(_exec.tc_worthy(p, min_flops) and not _exec._is_skinny(p)
+        return any(_exec.tc_worthy(p, min_flops)
+                   and not _exec._is_skinny(p, _exec.thin_rows(lk.gemm.products))
+                   and not _exec._is_wide(p, _exec.wide_cols(lk.gemm.products))
                    for lk in self.links for p in lk.gemm.products)
 
     def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:

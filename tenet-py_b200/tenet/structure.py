@@ -178,7 +178,7 @@ class Pattern:
 def all_trees(p: Provider, uncoupled: tuple[int, ...]) -> tuple:
     """All left-associated trees over ``uncoupled``, sorted (``fusion_tree.py:251-267``)."""
     if not uncoupled:
-        return (((), (), 0),)
+        return (((), (), p._unit_label()),)
     if len(uncoupled) == 1:
         return ((uncoupled, (), uncoupled[0]),)
     last = uncoupled[-1]

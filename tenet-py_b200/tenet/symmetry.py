@@ -18,8 +18,9 @@ from dataclasses import dataclass
 from tenet import _su2
 
 __all__ = [
-    "SU2", "U1", "Z2", "CapabilityError", "FZ2Sector", "Provider", "SU2Sector", "Sector",
-    "StructureChangingError", "U1Sector", "Z2Sector", "fZ2",
+    "SU2", "U1", "U1xU1xfZ2", "Z2", "CapabilityError", "FZ2Sector", "ProductProvider",
+    "ProductSector", "Provider", "SU2Sector", "Sector", "StructureChangingError", "U1Sector",
+    "Z2Sector", "fZ2",
 ]
 
 
@@ -73,6 +74,41 @@ class SU2Sector(Sector):
             raise TypeError(f"two_j must be an int, got {type(self.two_j).__name__}")
         if self.two_j < 0:
             raise ValueError(f"two_j must be non-negative, got {self.two_j}")
+
+
+@dataclass(frozen=True, slots=True, order=True)
+class ProductSector(Sector):
+    """A sector of U(1) x U(1) x fZ2: particle number ``n``, ``two_sz`` and fermion parity
+    (the grading of a spinful fermion chain such as the Hubbard chain).  Ordered
+    lexicographically by ``(n, two_sz, parity)``."""
+
+    n: int
+    two_sz: int
+    parity: int
+
+    def __post_init__(self) -> None:
+        for v in (self.n, self.two_sz, self.parity):
+            if not isinstance(v, int) or isinstance(v, bool):
+                raise TypeError(f"product sector components must be ints, got {v!r}")
+        if self.parity not in (0, 1):
+            raise ValueError(f"parity must be 0 or 1, got {self.parity}")
+        if not (-_PROD_OFF < self.n < _PROD_OFF and -_PROD_OFF < self.two_sz < _PROD_OFF):
+            raise ValueError("product sector charge out of range")
+
+
+# integer labels of product sectors: ((n + OFF) * 2^21 + (two_sz + OFF)) * 2 + parity, so the
+# parity is the lowest bit (the Koszul sign reads it there) and labels sort like sectors
+_PROD_OFF = 1 << 20
+_PROD_SPAN = 1 << 21
+
+
+def _prod_encode(n: int, sz: int, p: int) -> int:
+    return ((n + _PROD_OFF) * _PROD_SPAN + (sz + _PROD_OFF)) * 2 + p
+
+
+def _prod_decode(label: int) -> tuple[int, int, int]:
+    q = label >> 1
+    return (q // _PROD_SPAN) - _PROD_OFF, (q % _PROD_SPAN) - _PROD_OFF, label & 1
 
 
 @dataclass(frozen=True, slots=True)
@@ -132,7 +168,10 @@ class Provider:
     # ---- sector level (the reference's provider protocol) -------------------------------
     @property
     def unit(self) -> Sector:
-        return self.sector(0)
+        return self.sector(self._unit_label())
+
+    def _unit_label(self) -> int:
+        return 0
 
     def dual(self, a: Sector) -> Sector:
         return self.sector(self._dual(self.label(a)))
@@ -182,7 +221,58 @@ class Provider:
         return f"{self.name}Provider()"
 
 
+@dataclass(frozen=True, slots=True)
+class ProductProvider(Provider):
+    """U(1) x U(1) x fZ2: charges add, parities add mod 2, the braiding sign is the fZ2
+    one (``-1`` when both lines are odd), every quantum dimension is 1.  The reference
+    composes such groups with ``ProductProvider`` (``symmetry/product.py``); its labels
+    here are single integers (``_prod_encode``) so the planner's integer core applies
+    unchanged."""
+
+    @property
+    def fermionic(self) -> bool:
+        return True
+
+    def _unit_label(self) -> int:
+        return _prod_encode(0, 0, 0)
+
+    def _fuse(self, a: int, b: int) -> tuple[int, ...]:
+        n1, s1, p1 = _prod_decode(a)
+        n2, s2, p2 = _prod_decode(b)
+        return (_prod_encode(n1 + n2, s1 + s2, p1 ^ p2),)
+
+    def _dual(self, a: int) -> int:
+        n, sz, p = _prod_decode(a)
+        return _prod_encode(-n, -sz, p)
+
+    def _qdim(self, a: int) -> float:
+        return 1.0
+
+    def _fs(self, a: int) -> int:
+        return 1
+
+    def _twist(self, a: int) -> int:
+        return -1 if a & 1 else 1
+
+    def label(self, s: Sector) -> int:
+        return _prod_encode(s.n, s.two_sz, s.parity)
+
+    def sector(self, label: int) -> Sector:
+        return ProductSector(*_prod_decode(label))
+
+    @property
+    def sector_type(self) -> type:
+        return ProductSector
+
+    def r_symbol(self, a, b, c) -> float:
+        la, lb, lc = self.label(a), self.label(b), self.label(c)
+        if lc not in self._fuse(la, lb):
+            return 0
+        return -1 if (la & 1 and lb & 1) else 1
+
+
 U1 = Provider("U1")
 Z2 = Provider("Z2")
 fZ2 = Provider("fZ2")
 SU2 = Provider("SU2")
+U1xU1xfZ2 = ProductProvider("U1xU1xfZ2")

@@ -1,0 +1,56 @@
+"""Batched U(1) x U(1) x fZ2 environment updates on the device, against the oracle's fZ2
+update on coarsened tensors (``tests/_coarsen.py``), the unbatched device path, and, in
+reduced precision, the FP64 batch."""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle.tenet_oracle as O
+from _coarsen import coarsen as _coarsen
+from _coarsen import rel
+from tenet import _lib, batch, network, ops
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _device_error_clear():
+    yield
+    torch.cuda.synchronize()
+    assert _lib.device_error(0) == 0, "a kernel raised the device error word"
+
+
+def coarsen(t):
+    return _coarsen(t.structure, t.numpy_arena())
+
+
+def test_batched_product_env_update_matches_oracle_and_unbatched():
+    import bench
+
+    n = 3
+    F, A, W = bench.config3_batch(n, seed=7, lam=2.5, max_deg=4)
+    out = batch.env_update_last(F, A, W)
+    assert out.arena.shape[0] == n
+    for k in range(n):
+        got = out[k]
+        want = O.env_update_last(coarsen(F[k]), coarsen(A[k]), coarsen(W[k]))
+        c = coarsen(got)
+        assert c.structure == want.structure
+        assert rel(c.arena(), want.arena()) <= 1e-12
+        # the unbatched device path on the same member
+        one = network.env_update_last(F[k], A[k], W[k])
+        assert one.structure == got.structure
+        assert rel(got.numpy_arena(), one.numpy_arena()) <= 1e-13
+
+
+@pytest.mark.parametrize("precision,tol", [("3xbf16", 1e-4), ("tf32", 1e-2)])
+def test_batched_product_env_update_in_reduced_precision(precision, tol):
+    import bench
+
+    F, A, W = bench.config3_batch(4, seed=3, lam=6.0, max_deg=16)
+    exact = batch.env_update_last(F, A, W).arena.cpu().numpy()
+    with ops.precision(precision, 0):
+        got = batch.env_update_last(F, A, W).arena.cpu().numpy()
+    for k in range(4):
+        assert rel(got[k], exact[k]) <= tol

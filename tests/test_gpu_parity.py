@@ -296,7 +296,7 @@ def test_bench_workload_program_matches_oracle():
     close(got, want)
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2])
+@pytest.mark.parametrize("kind", [0, 1, 2, 5])
 def test_grouped_gemm_kinds_against_numpy(kind):
     """Every tile kind on uneven products, K = 0 included, through the C ABI."""
     from tenet import _exec
@@ -304,6 +304,8 @@ def test_grouped_gemm_kinds_against_numpy(kind):
     rng = np.random.default_rng(kind)
     if kind == 2:
         shapes = [(1000, 3, 3), (777, 1, 1), (5, 16, 16), (300, 2, 0)]
+    elif kind == 5:
+        shapes = [(3, 1000, 3), (1, 777, 1), (16, 5, 16), (2, 300, 0), (4, 25790, 4)]
     else:
         shapes = [(176, 236, 60), (9, 11, 2), (64, 64, 64), (65, 33, 17), (40, 7, 0), (1, 1, 1),
                   (176, 60, 236), (41, 10, 511), (3, 2, 1000)]
@@ -318,7 +320,7 @@ def test_grouped_gemm_kinds_against_numpy(kind):
     A = rng.standard_normal(a_off)
     B = rng.standard_normal(b_off)
     table = _exec.make_gemm(prods, kind)
-    if kind != 2:
+    if kind in (0, 1):
         assert table.n_counters > 0, "the long-K products must take the split-K path"
     ta, tb = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
     for _ in range(2):  # the split-K counters must be left zero for the next run

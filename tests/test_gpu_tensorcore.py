@@ -118,8 +118,9 @@ def test_mixed_precision_ctmrg_free_energy(golden_dir, precision, rel):
 
 
 def test_mixed_precision_ctmrg_chi128_near_criticality():
-    """beta = 0.44, chi = 128 (the even/odd split 64/64): 3xBF16 corner and edge products
-    give the FP64 free energy to 1e-8 and Onsager's to 1e-7."""
+    """beta = 0.44, chi = 128 (the even/odd split 64/64), 150 moves: 3xBF16 corner and edge
+    products give the FP64 free energy to 1e-8, both within 1e-6 of Onsager's (the bound
+    of the reference's own CTMRG test; near criticality 150 moves are not converged)."""
     import oracle.tenet_oracle as O
     from tenet import network
 
@@ -131,4 +132,4 @@ def test_mixed_precision_ctmrg_chi128_near_criticality():
         out[prec] = network.beta_free_energy(c, e, bulk)
         assert [m for _, m in bond.sectors] == [64, 64]
     assert abs(out["3xbf16"] - out["f64"]) <= 1e-8 * abs(out["f64"])
-    assert abs(out["3xbf16"] - O.onsager_beta_f(0.44)) <= 1e-7 * abs(out["f64"])
+    assert abs(out["3xbf16"] - O.onsager_beta_f(0.44)) <= 1e-6 * abs(out["f64"])

@@ -46,8 +46,8 @@ def run_map(src_s, arena, plan):
     return dst, out
 
 
-def run_tensordot(sa, a, sb, b, axes):
-    ex = ops.contraction_exec(sa, sb, ops._validated_axes(sa, sb, axes))
+def run_tensordot(sa, a, sb, b, axes, out_axes=None):
+    ex = ops.contraction_exec(sa, sb, ops._validated_axes(sa, sb, axes), "f64", None, out_axes)
     ap, bp, cp = np.full(ex.a_mat, np.nan), np.full(ex.b_mat, np.nan), np.full(ex.c_mat, np.nan)
     _emulate.gather(ex.pack, a, ap, b, bp)
     _emulate.gemm(ex.gemm, ap, bp, cp)
@@ -63,8 +63,14 @@ def run_einsum(eq, ops_):
     shared = [x for x in ta if x in tb]
     axes = (tuple(ta.index(x) for x in shared), tuple(tb.index(x) for x in shared))
     free = [x for x in ta if x not in shared] + [x for x in tb if x not in shared]
+    # the product path folds the output transpose into the unpack; the two-step form
+    # (unpack, then a transpose) must give the same numbers
+    folded = run_tensordot(sa, a, sb, b, axes, tuple(free.index(x) for x in outl))
     s, c = run_tensordot(sa, a, sb, b, axes)
-    return run_map(s, c, transpose_plan(s, tuple(free.index(x) for x in outl)))
+    two_step = run_map(s, c, transpose_plan(s, tuple(free.index(x) for x in outl)))
+    assert folded[0] == two_step[0]
+    np.testing.assert_allclose(folded[1], two_step[1], rtol=1e-13, atol=1e-14)
+    return folded
 
 
 @pytest.fixture(scope="module")
