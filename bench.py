@@ -659,9 +659,22 @@ def main() -> None:
                     help="members of the batched U1xU1xfZ2 environment update (0: skip)")
     ap.add_argument("--serve-full", action="store_true",
                     help="draw the requests from the full L / chi distribution")
+    ap.add_argument("--profile-config3", action="store_true",
+                    help="only run the batched environment update a few times (a small, "
+                         "fixed launch sequence for profiling its kernels) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile_config3:
+        import torch
+
+        from tenet import batch
+
+        F, A, W = config3_batch(args.config3_n)
+        for _ in range(3):
+            batch.env_update_last(F, A, W)
+        torch.cuda.synchronize()
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
