@@ -338,6 +338,16 @@ def batched_env_updates(args) -> dict:
         err = max(float(np.linalg.norm(got[k] - ex[k]) / np.linalg.norm(ex[k])) for k in range(n))
         out[name] = {"ms_per_batch": ms, "tflops": flops / (ms * 1e-3) / 1e12,
                      "max_rel_error_vs_f64": err}
+    # the same FP64 batch with the size heuristic instead of the autotuned tile kinds
+    batch.AUTOTUNE = False
+    try:
+        fn = lambda: batch.env_update_last(F, A, W)  # noqa: E731
+        for _ in range(args.warmup):
+            fn()
+        out["f64_heuristic_tiles"] = {"ms_per_batch": timed(fn, args.steps)}
+    finally:
+        batch.AUTOTUNE = True
+    out["autotuned_kinds"] = {str(k): list(v) for k, v in _exec.AUTOTUNE_CACHE.items()}
     members = [(F[k], A[k], W[k]) for k in range(n)]
     one = lambda: [network.env_update_last(*m) for m in members]  # noqa: E731
     for _ in range(args.warmup):

@@ -501,13 +501,68 @@ def tc_worthy(p, min_flops: int | None = None) -> bool:
     return K >= 16 and 2 * M * N * K >= (TC_MIN_FLOPS if min_flops is None else min_flops)
 
 
+# ---------------------------------------------------------------------------------------
+# autotuning of the FP64 tile kind
+
+
+AUTOTUNE_CACHE: dict = {}
+
+
+def histogram_key(products) -> tuple:
+    """The block-size histogram of a composition: product counts per (log2 M, log2 N,
+    log2 K) bin.  Compositions with the same histogram share a tuning decision."""
+    from collections import Counter
+
+    c = Counter((int(p[0]).bit_length(), int(p[1]).bit_length(), int(p[2]).bit_length())
+                for p in products if p[0] and p[1])
+    return tuple(sorted(c.items()))
+
+
+def autotune(products) -> tuple[int, bool]:
+    """``(tile kind, split-K)`` for the FP64 products of a composition, measured: each
+    candidate -- 64 x 64 or 32 x 32 tiles, with or without split-K -- runs three times
+    on scratch operands of the composition's extents (CUDA events on the current
+    stream, after one untimed run), and the fastest is cached under the block-size
+    histogram.  Every candidate computes the same products; split-K changes the order
+    in which a long K is summed, so results are reproducible for a fixed decision."""
+    key = histogram_key(products)
+    hit = AUTOTUNE_CACHE.get(key)
+    if hit is not None:
+        return hit
+    live = [p for p in products if p[0] and p[1]]
+    dev = device()
+    f64 = dict(dtype=torch.float64, device=dev)
+    na = max([p[3] + (p[0] - 1) * p[4] + p[2] for p in live if p[2]] + [1])
+    nb = max([p[5] + (p[2] - 1) * p[6] + p[1] for p in live if p[2]] + [1])
+    nc = max([p[7] + (p[0] - 1) * p[8] + p[1] for p in live] + [1])
+    a, b, c = torch.zeros(na, **f64), torch.zeros(nb, **f64), torch.empty(nc, **f64)
+    best, best_ms = (choose_kind(live), True), float("inf")
+    for kind in (TILE_64, TILE_32):
+        for split in (True, False):
+            t = make_gemm(live, kind, split_k=split)
+            t.run(a, b, c)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record()
+            for _ in range(3):
+                t.run(a, b, c)
+            ev[1].record()
+            ev[1].synchronize()
+            ms = ev[0].elapsed_time(ev[1])
+            if ms < best_ms:
+                best, best_ms = (kind, split), ms
+    AUTOTUNE_CACHE[key] = best
+    return best
+
+
 class GemmGroup:
     """One composition's products in at most four launches: the tall skinny ones, the wide
     flat ones, the rest in FP64 tiles, and -- in the precision form -- the products big
     enough to be dense contractions on the tcgen05 tensor cores (``tc_min_flops``
-    overrides the size rule)."""
+    overrides the size rule).  ``tuned`` picks the FP64 tile kind by ``autotune``
+    instead of the size heuristic."""
 
-    def __init__(self, products, precision: str = "f64", tc_min_flops: int | None = None):
+    def __init__(self, products, precision: str = "f64", tc_min_flops: int | None = None,
+                 tuned: bool = False):
         bulk, cols = thin_rows(products), wide_cols(products)
         skinny = [p for p in products if _is_skinny(p, bulk)]
         wide = [p for p in products if not _is_skinny(p, bulk) and _is_wide(p, cols)]
@@ -520,7 +575,11 @@ class GemmGroup:
         if tc:
             self.parts.append(make_gemm(tc, TC_KINDS[precision]))
         if rest:
-            self.parts.append(make_gemm(rest, choose_kind(rest)))
+            if tuned:  # the measured tile kind for this block-size histogram
+                kind, split = autotune(rest)
+                self.parts.append(make_gemm(rest, kind, split_k=split))
+            else:
+                self.parts.append(make_gemm(rest, choose_kind(rest)))
         if skinny:
             self.parts.append(make_gemm(skinny, TILE_SKINNY))
         if wide:

@@ -28,6 +28,10 @@ from tenet.tensor import SymmetricTensor
 
 __all__ = ["TensorBatch", "adjoint", "einsum", "env_update_last", "tensordot", "transpose"]
 
+#: pick the FP64 tile kind of batched products by measurement (``_exec.autotune``), keyed
+#: on the block-size histogram; False uses the size heuristic
+AUTOTUNE = True
+
 
 class TensorBatch:
     """``n`` tensors of one structure, or one tensor shared by every member of a batch."""
@@ -117,7 +121,7 @@ class _BatchedContraction:
     coupled-sector matrices and every member's products read that one copy."""
 
     def __init__(self, ex: ops.ContractionExec, n: int, sa_stride: int, sb_stride: int,
-                 precision: str, tc_min_flops) -> None:
+                 precision: str, tc_min_flops, tuned: bool = False) -> None:
         self.out, self.n = ex.out, n
         self.a_mat, self.b_mat, self.c_mat = ex.a_mat, ex.b_mat, ex.c_mat
         self.a_shared, self.b_shared = sa_stride == 0, sb_stride == 0
@@ -129,7 +133,7 @@ class _BatchedContraction:
         self.gemm = _exec.GemmGroup(
             _batch_products(ex.gemm.products, n, 0 if self.a_shared else ex.a_mat,
                             0 if self.b_shared else ex.b_mat, ex.c_mat),
-            precision, tc_min_flops)
+            precision, tc_min_flops, tuned=tuned)
         self.out_size = layout(ex.out).size
         self.unpack = _batch_gather(ex.unpack, n, (ex.c_mat, 0), (self.out_size, 0))
 
@@ -163,10 +167,12 @@ def _rows_of_buf(table: _exec.GatherTable, buf: int):
 
 
 @cache
-def _contraction(sa, sb, axes, n, a_shared, b_shared, precision, tc_min_flops, out_axes=None):
+def _contraction(sa, sb, axes, n, a_shared, b_shared, precision, tc_min_flops, out_axes=None,
+                 tuned=None):
     ex = ops.contraction_exec(sa, sb, axes, precision, tc_min_flops, out_axes)
     return _BatchedContraction(ex, n, 0 if a_shared else layout(sa).size,
-                               0 if b_shared else layout(sb).size, precision, tc_min_flops)
+                               0 if b_shared else layout(sb).size, precision, tc_min_flops,
+                               bool(tuned))
 
 
 def tensordot(a: TensorBatch, b: TensorBatch, axes, out_axes=None) -> TensorBatch:
@@ -175,7 +181,7 @@ def tensordot(a: TensorBatch, b: TensorBatch, axes, out_axes=None) -> TensorBatc
         raise ValueError("batch: operands of different batch sizes")
     ax = ops._validated_axes(a.structure, b.structure, axes)
     bc = _contraction(a.structure, b.structure, ax, a.n, a.shared, b.shared, *ops._PRECISION,
-                      None if out_axes is None else tuple(out_axes))
+                      None if out_axes is None else tuple(out_axes), AUTOTUNE)
     return TensorBatch(bc.out, bc.run(a.arena, b.arena), a.n)
 
 

@@ -54,3 +54,18 @@ def test_batched_product_env_update_in_reduced_precision(precision, tol):
         got = batch.env_update_last(F, A, W).arena.cpu().numpy()
     for k in range(4):
         assert rel(got[k], exact[k]) <= tol
+
+
+def test_autotuned_tiles_compute_the_same_products():
+    """The autotuner only chooses among tile kinds that compute the same products: the
+    tuned batch agrees with the heuristic one to rounding."""
+    import bench
+
+    F, A, W = bench.config3_batch(4, seed=5, lam=6.0, max_deg=16)
+    batch.AUTOTUNE = False
+    try:
+        ref = batch.env_update_last(F, A, W).arena.cpu().numpy()
+    finally:
+        batch.AUTOTUNE = True
+    got = batch.env_update_last(F, A, W).arena.cpu().numpy()
+    assert rel(got, ref) <= 1e-13
