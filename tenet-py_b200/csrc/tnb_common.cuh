@@ -53,6 +53,23 @@ cudaError_t launch(void (*kernel)(KArgs...), unsigned grid, unsigned block, cuda
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
 
+// The same with `smem` bytes of dynamic shared memory.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dyn(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                       cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Tensor-core grouped GEMM launcher (tnb_gemm_tc.cu).
 cudaError_t launch_gemm_tc(int kind, unsigned grid, cudaStream_t s, const int64_t* table,
                            int64_t n_gemm, const int32_t* tile_map, const double* a,

@@ -14,10 +14,13 @@
 // memory in the canonical K-major, no-swizzle UMMA layout -- 8-row x 16-byte core
 // matrices, LBO = 128 B between the two core matrices of one K step, SBO between 8-row
 // groups -- then one elected thread issues the MMAs into a 128-lane x 64-column TMEM
-// accumulator and commits them to an mbarrier that every thread waits on before the
-// slab is overwritten.  The epilogue reads TMEM with tcgen05.ld (warp w owns lanes
-// 32w..32w+31) and writes FP64.  Every wait is bounded: past the limit the kernel raises
-// TNB_ETIMEOUT, stops issuing, and still frees its TMEM before returning.
+// accumulator and commits them to the stage's mbarrier.  Two shared-memory stages make a
+// pipeline: slab s + 1 is loaded from global memory into registers while slab s is
+// converted, stored and issued, and a stage is overwritten only after the mbarrier of
+// the MMAs that read it (two slabs back) has completed.  The epilogue reads TMEM with
+// tcgen05.ld (warp w owns lanes 32w..32w+31) and writes FP64.  Every wait is bounded:
+// past the limit the kernel raises TNB_ETIMEOUT, stops issuing, and still frees its TMEM
+// before returning.
 #include <cuda_bf16.h>
 
 #include <string>
@@ -76,19 +79,30 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
   }
 }
 
+template <int MODE>
+struct TcLayout {
+  static constexpr int kEsz = MODE == 0 ? 4 : 2;
+  static constexpr int kRowBytes = kTcBk * kEsz;
+  static constexpr int kParts = MODE == 0 ? 1 : 2;
+  static constexpr int kABytes = kTcM * kRowBytes, kBBytes = kTcN * kRowBytes;
+  // one pipeline stage: A parts, then B parts (TF32 16 + 8 KB; 3xBF16 2 x 8 + 2 x 4 KB)
+  static constexpr int kStageBytes = kParts * (kABytes + kBBytes);
+  static constexpr int kSmemBytes = 2 * kStageBytes + 1024;  // two stages + alignment slack
+};
+
 template <int MODE>  // 0 = TF32, 1 = 3 x BF16
 __global__ void __launch_bounds__(kTcThreads)
 gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
                const int32_t* __restrict__ tile_map, const double* __restrict__ a, int64_t n_a,
                const double* __restrict__ b, int64_t n_b, double* __restrict__ c, int64_t n_c) {
-  // TF32: A 128x32x4 = 16 KB, B 64x32x4 = 8 KB.  3xBF16: A hi/lo 2 x 8 KB, B hi/lo 2 x 4 KB.
-  constexpr int kEsz = MODE == 0 ? 4 : 2;
-  constexpr int kRowBytes = kTcBk * kEsz;
-  constexpr int kParts = MODE == 0 ? 1 : 2;
-  constexpr int kABytes = kTcM * kRowBytes, kBBytes = kTcN * kRowBytes;
-  __shared__ __align__(1024) uint8_t sa[kParts][kABytes];
-  __shared__ __align__(1024) uint8_t sb[kParts][kBBytes];
-  __shared__ __align__(8) uint64_t mbar;
+  using L = TcLayout<MODE>;
+  constexpr int kEsz = L::kEsz, kRowBytes = L::kRowBytes;
+  constexpr int kLA = (kTcM * kTcBk) / kTcThreads, kLB = (kTcN * kTcBk) / kTcThreads;
+  extern __shared__ uint8_t smem_dyn[];
+  // 1024-byte aligned base of the two stages
+  uint8_t* const smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t s_tmem;
   __shared__ GemmRowTc s_row;
   __shared__ int s_ok;
@@ -116,7 +130,8 @@ gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
     s_row = r;
     s_ok = ok;
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {  // one warp owns the TMEM allocation
@@ -134,49 +149,75 @@ gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   const int64_t m0 = ok ? (local / r.tiles_n) * kTcM : 0, n0 = ok ? (local % r.tiles_n) * kTcN : 0;
   pdl_wait();  // A may be the previous kernel's output
 
-  const uint32_t mb = smem_u32(&mbar);
-  uint32_t phase = 0;
-  const int64_t nk = ok ? (r.K + kTcBk - 1) / kTcBk : 0;
-  for (int64_t s = 0; s < nk; ++s) {
-    const int64_t k0 = s * kTcBk;
-    // A slab: 128 x 32, coalesced along K
-#pragma unroll 4
-    for (int i = 0; i < (kTcM * kTcBk) / kTcThreads; ++i) {
+  double ra[kLA], rb[kLB];
+  auto load_slab = [&](int64_t k0) {
+#pragma unroll
+    for (int i = 0; i < kLA; ++i) {
       const int idx = tid + i * kTcThreads;
       const int rr = idx / kTcBk, kk = idx % kTcBk;
       const int64_t gm = m0 + rr, gk = k0 + kk;
-      const double x = (gm < r.M && gk < r.K) ? a[r.aoff + gm * r.lda + gk] : 0.0;
-      const uint32_t off = kmajor(rr, kk, kEsz, kRowBytes);
-      if constexpr (MODE == 0) {
-        *reinterpret_cast<uint32_t*>(&sa[0][off]) = to_tf32(x);
-      } else {
-        const __nv_bfloat16 hi = __double2bfloat16(x);
-        const __nv_bfloat16 lo = __double2bfloat16(x - static_cast<double>(__bfloat162float(hi)));
-        *reinterpret_cast<__nv_bfloat16*>(&sa[0][off]) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(&sa[1][off]) = lo;
-      }
+      ra[i] = (gm < r.M && gk < r.K) ? a[r.aoff + gm * r.lda + gk] : 0.0;
     }
-    // B slab: 32 x 64 from row-major B, stored transposed (N x K, K-major)
-#pragma unroll 4
-    for (int i = 0; i < (kTcN * kTcBk) / kTcThreads; ++i) {
+#pragma unroll
+    for (int i = 0; i < kLB; ++i) {
       const int idx = tid + i * kTcThreads;
       const int kk = idx / kTcN, nn = idx % kTcN;
       const int64_t gk = k0 + kk, gn = n0 + nn;
-      const double x = (gk < r.K && gn < r.N) ? b[r.boff + gk * r.ldb + gn] : 0.0;
-      const uint32_t off = kmajor(nn, kk, kEsz, kRowBytes);
+      rb[i] = (gk < r.K && gn < r.N) ? b[r.boff + gk * r.ldb + gn] : 0.0;
+    }
+  };
+  auto store_slab = [&](int stage) {
+    uint8_t* sa0 = smem + stage * L::kStageBytes;
+    uint8_t* sb0 = sa0 + L::kParts * L::kABytes;
+#pragma unroll
+    for (int i = 0; i < kLA; ++i) {
+      const int idx = tid + i * kTcThreads;
+      const uint32_t off = kmajor(idx / kTcBk, idx % kTcBk, kEsz, kRowBytes);
       if constexpr (MODE == 0) {
-        *reinterpret_cast<uint32_t*>(&sb[0][off]) = to_tf32(x);
+        *reinterpret_cast<uint32_t*>(sa0 + off) = to_tf32(ra[i]);
       } else {
-        const __nv_bfloat16 hi = __double2bfloat16(x);
-        const __nv_bfloat16 lo = __double2bfloat16(x - static_cast<double>(__bfloat162float(hi)));
-        *reinterpret_cast<__nv_bfloat16*>(&sb[0][off]) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(&sb[1][off]) = lo;
+        const __nv_bfloat16 hi = __double2bfloat16(ra[i]);
+        const __nv_bfloat16 lo = __double2bfloat16(ra[i] - static_cast<double>(__bfloat162float(hi)));
+        *reinterpret_cast<__nv_bfloat16*>(sa0 + off) = hi;
+        *reinterpret_cast<__nv_bfloat16*>(sa0 + L::kABytes + off) = lo;
       }
     }
+#pragma unroll
+    for (int i = 0; i < kLB; ++i) {
+      const int idx = tid + i * kTcThreads;
+      const uint32_t off = kmajor(idx % kTcN, idx / kTcN, kEsz, kRowBytes);
+      if constexpr (MODE == 0) {
+        *reinterpret_cast<uint32_t*>(sb0 + off) = to_tf32(rb[i]);
+      } else {
+        const __nv_bfloat16 hi = __double2bfloat16(rb[i]);
+        const __nv_bfloat16 lo = __double2bfloat16(rb[i] - static_cast<double>(__bfloat162float(hi)));
+        *reinterpret_cast<__nv_bfloat16*>(sb0 + off) = hi;
+        *reinterpret_cast<__nv_bfloat16*>(sb0 + L::kBBytes + off) = lo;
+      }
+    }
+  };
+
+  uint32_t phase[2] = {0u, 0u};
+  const int64_t nk = ok ? (r.K + kTcBk - 1) / kTcBk : 0;
+  if (nk > 0) load_slab(0);
+  for (int64_t s = 0; s < nk; ++s) {
+    const int stage = static_cast<int>(s & 1);
+    // the stage is free once the MMAs of slab s - 2 (its last readers) have completed
+    if (s >= 2 && !s_fail && !mbar_wait(smem_u32(&mbar[stage]), phase[stage])) {
+      if (lane == 0) {
+        atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
+        s_fail = 1;
+      }
+    }
+    if (s >= 2) phase[stage] ^= 1u;
+    __syncthreads();
+    if (s_fail) break;
+    store_slab(stage);
+    if (s + 1 < nk) load_slab((s + 1) * kTcBk);  // in flight while slab s is issued
     // make the generic-proxy stores visible to the tensor cores, then issue
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    if (tid == 0 && !s_fail) {
+    if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       constexpr uint32_t kLbo = 128, kSbo = (kRowBytes / 16) * 128;
       constexpr uint32_t kIdesc = umma_idesc(MODE == 0 ? 2u : 1u);
@@ -184,12 +225,14 @@ gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
       // (A part, B part) pairs: TF32 one product; 3xBF16 hi.hi, hi.lo, lo.hi
       constexpr int kProducts = MODE == 0 ? 1 : 3;
       const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+      const uint32_t sa = smem_u32(smem + stage * L::kStageBytes);
+      const uint32_t sb = sa + L::kParts * L::kABytes;
 #pragma unroll
       for (int p = 0; p < kProducts; ++p) {
 #pragma unroll
         for (int st = 0; st < kSteps; ++st) {
-          const uint64_t ad = umma_desc(smem_u32(&sa[pa[p]][0]) + st * 256, kLbo, kSbo);
-          const uint64_t bd = umma_desc(smem_u32(&sb[pb[p]][0]) + st * 256, kLbo, kSbo);
+          const uint64_t ad = umma_desc(sa + pa[p] * L::kABytes + st * 256, kLbo, kSbo);
+          const uint64_t bd = umma_desc(sb + pb[p] * L::kBBytes + st * 256, kLbo, kSbo);
           const uint32_t acc = (s > 0 || p > 0 || st > 0) ? 1u : 0u;
           if constexpr (MODE == 0) {
             asm volatile(
@@ -205,19 +248,20 @@ gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
         }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   :: "r"(mb) : "memory");
+                   :: "r"(smem_u32(&mbar[stage])) : "memory");
     }
-    // every thread waits for this slab's MMAs before the slab is overwritten
-    if (!s_fail && !mbar_wait(mb, phase)) {
+  }
+  // the last commit covers every MMA issued before it
+  if (nk > 0 && !s_fail) {
+    const int last = static_cast<int>((nk - 1) & 1);
+    if (!mbar_wait(smem_u32(&mbar[last]), phase[last])) {
       if (lane == 0) {
         atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
         s_fail = 1;
       }
     }
-    phase ^= 1u;
-    __syncthreads();
-    if (s_fail) break;
   }
+  __syncthreads();
 
   // epilogue: TMEM -> registers -> FP64 C (zeros when K == 0 or the MMAs timed out)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -262,10 +306,22 @@ namespace tnb {
 cudaError_t launch_gemm_tc(int kind, unsigned grid, cudaStream_t s, const int64_t* table,
                            int64_t n_gemm, const int32_t* tile_map, const double* a,
                            int64_t n_a, const double* b, int64_t n_b, double* c, int64_t n_c) {
-  if (kind == TNB_TILE_TC_TF32)
-    return launch(gemm_tc_kernel<0>, grid, kTcThreads, s, table, n_gemm, tile_map, a, n_a, b,
-                  n_b, c, n_c);
-  return launch(gemm_tc_kernel<1>, grid, kTcThreads, s, table, n_gemm, tile_map, a, n_a, b, n_b,
-                c, n_c);
+  // the two-stage pipeline needs more than the default 48 KB of shared memory per CTA
+  static bool opted[2] = {false, false};
+  const int mode = kind == TNB_TILE_TC_TF32 ? 0 : 1;
+  if (!opted[mode]) {
+    const cudaError_t e = mode == 0
+        ? cudaFuncSetAttribute(gemm_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               TcLayout<0>::kSmemBytes)
+        : cudaFuncSetAttribute(gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               TcLayout<1>::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    opted[mode] = true;
+  }
+  if (mode == 0)
+    return launch_dyn(gemm_tc_kernel<0>, grid, kTcThreads, TcLayout<0>::kSmemBytes, s, table,
+                      n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
+  return launch_dyn(gemm_tc_kernel<1>, grid, kTcThreads, TcLayout<1>::kSmemBytes, s, table,
+                    n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
 }
 }  // namespace tnb
