@@ -39,6 +39,10 @@ for _p in (ROOT, ROOT / "tenet-py_b200"):
         sys.path.insert(0, str(_p))
 
 METRIC = "Heff matvec TFLOP/s (SU(2) Heisenberg two-site, FP64)"
+# dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload (ncu captures of
+# two launches each, mean), in bytes
+NCU_TRAFFIC = {"block_gather": (502_528 + 413_184) // 2,
+               "grouped_gemm_f64": (781_568 + 1_981_952) // 2}
 # multiplets per bond sector, half-integer bond spins 2j = 1, 3, ..., 17 (sum 256)
 BOND = {1: 60, 3: 56, 5: 46, 7: 36, 9: 25, 11: 16, 13: 10, 15: 5, 17: 2}
 MPO = {0: 2, 2: 1}
@@ -417,8 +421,9 @@ def serving(args) -> dict:
         k: max(abs(v[r.rid] - ref[r.rid]) / r.L for r in reqs) for k, v in energies.items()
         if k != "plain_f64_sequential" and k != "served_3xbf16_poisson"}
     base = out["plain_f64_sequential"]["solves_per_s"]
-    out["solves_per_s_vs_plain_f64"] = {k: out[k]["solves_per_s"] / base for k in
-                                        ("compiled_f64_sequential", "served_f64", "served_3xbf16")}
+    out["solves_per_s_vs_plain_f64"] = {
+        k: out[k]["solves_per_s"] / base for k in
+        ("compiled_f64_sequential", "served_f64", "served_3xbf16")}
     return out
 
 
@@ -609,7 +614,12 @@ def run_tenet(args) -> None:
             "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in "
                             "MEASURED_PEAKS.json)") if dominant_is_gemm
             else f"MEASURED_PEAKS.json hbm_gbs ({pk['src']})",
-            "traffic": None,
+            # DRAM bytes per launch (read + write) of the same kernel from the ncu captures of
+            # this workload, mean of the two captured launches: the operands sit in L2
+            "traffic": NCU_TRAFFIC["grouped_gemm_f64" if dominant_is_gemm else "block_gather"],
+            "traffic_source": "ncu --set full captures, profiles/"
+                              + ("gemm_f64_heff2_su2_256mult.md" if dominant_is_gemm
+                                 else "gather_heff2_su2_256mult.md"),
             "kernels": {
                 "grouped_gemm_f64": {"launches": g["launches"], "ms": g["ms"],
                                      "share": g["ms"] / total_kernel_ms if total_kernel_ms else 0,

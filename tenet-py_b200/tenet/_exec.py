@@ -16,6 +16,7 @@ costs one ctypes launch per kernel.
 from __future__ import annotations
 
 import ctypes
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -70,13 +71,12 @@ class Seq:
         return int(_lib.load().tnb_seq_length(self.handle))
 
     def __enter__(self):
-        global _REC
-        self._prev, _REC = _REC, self
+        self._prev = recording()
+        _TLS.rec = self
         return self
 
     def __exit__(self, *exc):
-        global _REC
-        _REC = self._prev
+        _TLS.rec = self._prev
 
     def run(self, patch: dict | None = None) -> None:
         """Replay on the current stream; ``patch`` maps recorded buffer addresses to the
@@ -90,7 +90,14 @@ class Seq:
             _lib.call("tnb_seq_run", self.handle, 0, None, None, stream_ptr())
 
 
-_REC: Seq | None = None
+# per host thread: the sequence being recorded, if any (threads of the serving loop record
+# their own programs concurrently)
+_TLS = threading.local()
+
+
+def recording() -> Seq | None:
+    """The sequence launches are being recorded into on this thread (None: launch)."""
+    return getattr(_TLS, "rec", None)
 
 #: Run compiled chains as one persistent launch when every stage fuses.  Off by default:
 #: on B200 the stage-by-stage replay (a CUDA graph, programmatic dependent launch) is
@@ -115,8 +122,13 @@ class _Staging:
         self.buf = None
         self.pos = 0
         self.pending: list = []
+        self.lock = threading.Lock()
 
     def stage(self, packed: np.ndarray):
+        with self.lock:
+            return self._stage(packed)
+
+    def _stage(self, packed: np.ndarray):
         n = packed.nbytes
         if n > self.nbytes // 4:
             return None
@@ -335,8 +347,9 @@ class GatherTable:
         if self.n_seg == 0:
             return
         seg, tsrc, tcf, tld, cmap = self.device_arrays()
-        if _REC is not None:
-            _lib.call("tnb_seq_add_gather", _REC.handle, ptr(seg), self.n_seg, ptr(cmap),
+        rec = recording()
+        if rec is not None:
+            _lib.call("tnb_seq_add_gather", rec.handle, ptr(seg), self.n_seg, ptr(cmap),
                       self.chunks, ptr(tsrc), ptr(tcf), ptr(tld), self.n_term,
                       ptr(src0), src0.numel(), ptr(dst0), dst0.numel(),
                       ptr(src1), 0 if src1 is None else src1.numel(),
@@ -424,8 +437,9 @@ class GemmTable:
             self._dev = Uploaded((self.table, self.tile_map))
         table, tile_map = self._dev.ready()
         work = self.work()
-        if _REC is not None:
-            _lib.call("tnb_seq_add_gemm", _REC.handle, ptr(table), self.n_gemm, ptr(tile_map),
+        rec = recording()
+        if rec is not None:
+            _lib.call("tnb_seq_add_gemm", rec.handle, ptr(table), self.n_gemm, ptr(tile_map),
                       self.tiles, self.kind, ptr(a), a.numel(), ptr(b), b.numel(), ptr(c),
                       c.numel(), ptr(work), self.work_bytes, self.n_counters)
             return

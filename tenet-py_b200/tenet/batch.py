@@ -180,7 +180,7 @@ def tensordot(a: TensorBatch, b: TensorBatch, axes, out_axes=None) -> TensorBatc
     if a.n != b.n:
         raise ValueError("batch: operands of different batch sizes")
     ax = ops._validated_axes(a.structure, b.structure, axes)
-    bc = _contraction(a.structure, b.structure, ax, a.n, a.shared, b.shared, *ops._PRECISION,
+    bc = _contraction(a.structure, b.structure, ax, a.n, a.shared, b.shared, *ops.current_precision(),
                       None if out_axes is None else tuple(out_axes), AUTOTUNE)
     return TensorBatch(bc.out, bc.run(a.arena, b.arena), a.n)
 

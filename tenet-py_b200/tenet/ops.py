@@ -17,6 +17,7 @@ composed into a single block map).
 from __future__ import annotations
 
 import operator
+import threading
 from collections import Counter
 from contextlib import contextmanager
 from dataclasses import dataclass
@@ -149,9 +150,14 @@ class ContractionExec:
         return self.gemm.flops
 
 
-#: arithmetic of the coupled-sector products of eager contractions: ("f64", None), or a
-#: tensor-core precision ("tf32" / "3xbf16") with its size rule (see ``precision``)
-_PRECISION: tuple = ("f64", None)
+# per host thread: the arithmetic of the coupled-sector products of eager contractions,
+# ("f64", None) or a tensor-core precision ("tf32" / "3xbf16") with its size rule
+_PREC = threading.local()
+
+
+def current_precision() -> tuple:
+    """``(precision, tc_min_flops)`` of eager contractions on this thread."""
+    return getattr(_PREC, "value", ("f64", None))
 
 
 @contextmanager
@@ -160,14 +166,14 @@ def precision(kind: str = "f64", tc_min_flops: int | None = None):
     inside the block in ``kind``: "f64" (the plain form), or "tf32" / "3xbf16" on the
     tcgen05 tensor cores for the products of at least ``tc_min_flops`` (default
     ``_exec.TC_MIN_FLOPS``), FP64 in and out.  Gathers, SVDs and norms stay FP64."""
-    global _PRECISION
     if kind != "f64" and kind not in _exec.TC_KINDS:
         raise ValueError(f"unknown precision {kind!r}")
-    prev, _PRECISION = _PRECISION, (kind, tc_min_flops)
+    prev = current_precision()
+    _PREC.value = (kind, tc_min_flops)
     try:
         yield
     finally:
-        _PRECISION = prev
+        _PREC.value = prev
 
 
 @cache
@@ -227,7 +233,7 @@ def tensordot(a: SymmetricTensor, b: SymmetricTensor, axes, out_axes=None) -> Sy
     """Contract ``axes[0]`` of ``a`` with ``axes[1]`` of ``b``; free legs come back unchanged
     (or transposed by ``out_axes``, in the same pass)."""
     ex = contraction_exec(a.structure, b.structure, _validated_axes(a.structure, b.structure, axes),
-                          *_PRECISION, None if out_axes is None else tuple(out_axes))
+                          *current_precision(), None if out_axes is None else tuple(out_axes))
     return SymmetricTensor(ex.out, arena=ex.run(a.arena, b.arena))
 
 

@@ -255,7 +255,7 @@ class ChainProgram:
         of the fused one-launch chain when ``_exec.FUSE`` is on; launch by launch while a
         ``LaunchLog`` times each kernel).  One program must not run on two streams at
         once."""
-        if _exec._LOG is None and _exec._REC is None:
+        if _exec._LOG is None and _exec.recording() is None:
             self.exec_seq.run({self.x_slot.data_ptr(): x.data_ptr(),
                                self.y_slot.data_ptr(): out.data_ptr()})
             return out
