@@ -48,8 +48,10 @@ extern "C" {
  *   [3]  t_begin       first term index (into term_src / term_coeff / term_ld)
  *   [4]  t_end         one past the last term index (t_end == t_begin: write zeros)
  *   [5]  buf           0 or 1: which (src, dst) buffer pair the segment uses
- *   [6]  chunk_begin   prefix sum of ceil(size / TNB_GATHER_CHUNK) over earlier rows
- *   [7]  reserved, 0
+ *   [6]  chunk_begin   prefix sum of ceil(size / chunk) over earlier rows
+ *   [7]  chunk         elements per work chunk of this row: 256, 512, 768 or 1024
+ *                      (0 means TNB_GATHER_CHUNK); the host picks small chunks for small
+ *                      tables (more CTAs on latency-bound work), large ones for big tables
  *   [8..15]  dims        iteration extents, outermost first
  *   [16..23] dst_stride  element stride of each dim in the destination
  *   [24..31] src_rstride source stride of each dim, in units of the term's ld

@@ -116,11 +116,18 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
     cstr[d] = d < rank ? row[32 + d] : 0;
   }
 
-  const int64_t base = (chunk - row[6]) * TNB_GATHER_CHUNK;
+  // the row's chunk size (a multiple of kGatherThreads up to TNB_GATHER_CHUNK)
+  const int64_t ce = row[7] ? row[7] : TNB_GATHER_CHUNK;
+  if (ce <= 0 || ce > TNB_GATHER_CHUNK || ce % kGatherThreads) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  const int64_t base = (chunk - row[6]) * ce;
+  const int64_t lim = min(size, base + ce);
 #pragma unroll
   for (int k = 0; k < kEpt; ++k) {
     const int64_t e = base + tid + k * NT;
-    if (e >= size) break;
+    if (e >= lim) break;
     uint32_t rem = static_cast<uint32_t>(e);
     int64_t doff = 0, roff = 0, coff = 0;
 #pragma unroll

@@ -325,10 +325,11 @@ class GatherTable:
         self.tld = np.asarray(tld, dtype=np.int64)
         self.n_seg = len(seg)
         self.n_term = len(self.tsrc)
-        self.chunks = int(((seg[:, 1] + CHUNK - 1) // CHUNK).sum()) if len(seg) else 0
+        ce = np.where(seg[:, 7] > 0, seg[:, 7], CHUNK) if len(seg) else np.zeros(0, np.int64)
+        per = (seg[:, 1] + ce - 1) // ce if len(seg) else np.zeros(0, np.int64)
+        self.chunks = int(per.sum()) if len(seg) else 0
         self.elems = int(seg[:, 1].sum()) if len(seg) else 0
         self.term_elems = int((seg[:, 1] * (seg[:, 4] - seg[:, 3])).sum()) if len(seg) else 0
-        per = (seg[:, 1] + CHUNK - 1) // CHUNK if len(seg) else np.zeros(0, np.int64)
         self.chunk_map = np.repeat(np.arange(len(seg), dtype=np.int32), per)
         self._dev = None
 
@@ -365,6 +366,17 @@ class GatherTable:
             _LOG.end("block_gather", mark, self.bytes_moved)
 
 
+def chunk_size(elems: int) -> int:
+    """Elements per gather chunk for a table of ``elems`` destination elements: the largest
+    of 1024, 512, 256 that still gives about four CTAs per SM -- small chunks put more
+    CTAs (more independent load chains) on a small, latency-bound table, large chunks
+    keep a big, bandwidth-bound one at four elements per thread."""
+    for ce in (CHUNK, CHUNK // 2, CHUNK // 4):
+        if elems >= ce * 4 * N_SM:
+            return ce
+    return CHUNK // 4
+
+
 def make_gather(*parts) -> GatherTable:
     """Concatenate one or more ``gather_rows`` results into a single table."""
     rows, tsrc, tcf, tld = [], [], [], []
@@ -378,7 +390,8 @@ def make_gather(*parts) -> GatherTable:
         tld.append(np.asarray(tl, np.int64))
         base += len(ts)
     seg = np.concatenate(rows) if rows else np.zeros((0, SEG_W), np.int64)
-    per = (seg[:, 1] + CHUNK - 1) // CHUNK
+    seg[:, 7] = chunk_size(int(seg[:, 1].sum()) if len(seg) else 0)
+    per = (seg[:, 1] + seg[:, 7] - 1) // seg[:, 7]
     seg[:, 6] = np.cumsum(per) - per
     return GatherTable(seg, np.concatenate(tsrc) if tsrc else np.zeros(0, np.int64),
                        np.concatenate(tcf) if tcf else np.zeros(0),
