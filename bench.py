@@ -366,9 +366,10 @@ def serving(args) -> dict:
     """Served DMRG solves against the plain FP64 form on the same seeded request sample
     (SU(2) J1-J2 chains, 8 sweeps, ncv = 20, cutoff 1e-10).  Arms, each from empty plan
     caches: the plain FP64 form (eager op-by-op matvec, host-driven Lanczos), the
-    compiled FP64 form one solve at a time, the serving loop in FP64 and in the
-    precision form with every request arriving at once, and the precision form again
-    at a Poisson arrival rate of 0.7 x the burst throughput for the latency point."""
+    compiled FP64 form one solve at a time, the single-process serving loop in FP64 and
+    in the precision form, the same with host-parallel worker processes (started and
+    warmed before the timed run), every request arriving at once, and the worker form
+    again at a Poisson arrival rate of 0.7 x its burst throughput for the latency point."""
     import torch
 
     from tenet import serve
@@ -399,12 +400,17 @@ def serving(args) -> dict:
         out[name] = {"solves_per_s": len(reqs) / wall, "wall_s": wall,
                      "p50_s": float(np.percentile(done, 50)), "p99_s": float(np.percentile(done, 99))}
 
-    def served(name, requests, **kw):
+    def served(name, requests, workers=0, **kw):
         serve.clear_plan_caches()
-        srv = serve.Server(max_active=args.serve_slots, **kw)
+        if workers:  # worker processes, started and warmed before the timed run
+            srv = serve.ProcessServer(workers=workers, **kw)
+        else:
+            srv = serve.Server(max_active=args.serve_slots, **kw)
         t0 = time.perf_counter()
         res = srv.run(requests)
         wall = time.perf_counter() - t0
+        if workers:
+            srv.close()
         energies[name] = {r.rid: r.energy for r in res}
         out[name] = serve.summarize(res, wall) | {"peak_active": srv.peak_active}
 
@@ -412,18 +418,22 @@ def serving(args) -> dict:
     sequential("compiled_f64_sequential", precision="f64")
     served("served_f64", reqs, precision="f64")
     served("served_3xbf16", reqs, precision="3xbf16")
-    rate = 0.7 * out["served_3xbf16"]["solves_per_s"]
+    w = args.serve_workers
+    served(f"served_f64_{w}workers", reqs, workers=w, precision="f64")
+    served(f"served_3xbf16_{w}workers", reqs, workers=w, precision="3xbf16")
+    rate = 0.7 * out[f"served_3xbf16_{w}workers"]["solves_per_s"]
     poisson = serve.request_stream(len(reqs), rate, seed=0, **kw)
-    served("served_3xbf16_poisson", poisson, precision="3xbf16")
-    out["served_3xbf16_poisson"]["arrival_rate_per_s"] = rate
+    served(f"served_3xbf16_{w}workers_poisson", poisson, workers=w, precision="3xbf16")
+    out[f"served_3xbf16_{w}workers_poisson"]["arrival_rate_per_s"] = rate
     ref = energies["plain_f64_sequential"]
     out["max_abs_dE_per_site_vs_plain_f64"] = {
         k: max(abs(v[r.rid] - ref[r.rid]) / r.L for r in reqs) for k, v in energies.items()
-        if k != "plain_f64_sequential" and k != "served_3xbf16_poisson"}
+        if k != "plain_f64_sequential" and not k.endswith("poisson")}
     base = out["plain_f64_sequential"]["solves_per_s"]
     out["solves_per_s_vs_plain_f64"] = {
         k: out[k]["solves_per_s"] / base for k in
-        ("compiled_f64_sequential", "served_f64", "served_3xbf16")}
+        ("compiled_f64_sequential", "served_f64", "served_3xbf16", f"served_f64_{w}workers",
+         f"served_3xbf16_{w}workers")}
     return out
 
 
@@ -675,6 +685,8 @@ def main() -> None:
     ap.add_argument("--serve-requests", type=int, default=6,
                     help="served DMRG requests in the solves/s comparison (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-workers", type=int, default=4,
+                    help="worker processes of the host-parallel serving arms")
     ap.add_argument("--config3-n", type=int, default=64,
                     help="members of the batched U1xU1xfZ2 environment update (0: skip)")
     ap.add_argument("--serve-full", action="store_true",

@@ -145,8 +145,9 @@ class DeviceLanczos:
         self.state = torch.zeros(3 * ncv + 2, **f64)
         self.scal = torch.zeros(2, **f64)  # [0] a squared norm, [1] the corrected energy
         self.coef = torch.zeros(ncv, **f64)
-        self.ptrs = torch.tensor([self.V[k].data_ptr() for k in range(ncv)], dtype=torch.int64,
-                                 device=dev)
+        # the rows' addresses, computed on the device (no host -> device copy, no sync)
+        self.ptrs = self.V.data_ptr() + torch.arange(ncv, dtype=torch.int64, device=dev) \
+            * (self.V.stride(0) * self.V.element_size())
         lib = _lib.load()
         self.work = torch.zeros(int(lib.tnb_dot_work_bytes(n)), dtype=torch.uint8, device=dev)
         self.mwork = torch.zeros(int(lib.tnb_multi_dot_work_bytes(n, ncv)) if self.reorth

@@ -31,8 +31,8 @@ from tenet import network
 from tenet.structure import GradedSpace
 from tenet.symmetry import SU2
 
-__all__ = ["SolveRequest", "SolveResult", "Server", "clear_plan_caches", "footprint_bytes",
-           "request_stream", "solve_alone"]
+__all__ = ["ProcessServer", "SolveRequest", "SolveResult", "Server", "clear_plan_caches",
+           "footprint_bytes", "request_stream", "solve_alone"]
 
 
 @dataclass(frozen=True)
@@ -196,6 +196,108 @@ class Server:
                 results.append(SolveResult(slot.req.rid, energy, history, slot.req.arrival,
                                            slot.admitted, clock() - t0, slot.footprint, slot.req))
         torch.cuda.synchronize()
+        return results
+
+
+# ---------------------------------------------------------------------------------------
+# host-parallel serving: worker processes on one GPU
+
+_WORKER: dict = {}
+
+
+def _worker_init(precision: str, ncv: int, cutoff: float, tc_min_flops) -> None:
+    torch.cuda.set_device(0)
+    _WORKER.update(precision=precision, ncv=ncv, cutoff=cutoff, tc_min_flops=tc_min_flops)
+    # load the library and the CUDA context now, not inside the first timed request
+    solve_alone(SolveRequest(-1, 8, 0.1, 16, sweeps=1), precision=precision, ncv=ncv,
+                cutoff=cutoff, tc_min_flops=tc_min_flops)
+    torch.cuda.synchronize()
+
+
+def _worker_ready(_: int) -> int:
+    import os
+
+    time.sleep(0.2)  # long enough that every worker of the pool takes one
+    return os.getpid()
+
+
+def _worker_solve(req: SolveRequest):
+    w = _WORKER
+    e, hist = solve_alone(req, precision=w["precision"], ncv=w["ncv"], cutoff=w["cutoff"],
+                          tc_min_flops=w["tc_min_flops"])
+    torch.cuda.synchronize()
+    return e, hist
+
+
+class ProcessServer:
+    """Continuous batching over host-parallel workers: ``workers`` processes (spawned,
+    each with its own CUDA context on the same GPU) solve the admitted requests, so the
+    per-bond host work of one solve -- planning, the SVD decision, launches -- runs beside
+    the others' instead of after it.  Admission is the same as ``Server``'s: arrival
+    order, a free worker, and the summed footprint estimates within ``hbm_budget``.  The
+    workers start and warm up (library, CUDA context) when the server is built; a
+    long-running server keeps them.  Kernels of different workers share the GPU by time
+    slicing."""
+
+    def __init__(self, *, workers: int = 4, hbm_budget: int | None = None,
+                 precision: str = "3xbf16", ncv: int = 20, cutoff: float = 1e-10,
+                 tc_min_flops=None) -> None:
+        import multiprocessing
+        from concurrent.futures import ProcessPoolExecutor
+
+        if workers < 1:
+            raise ValueError("workers must be at least 1")
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info()
+            hbm_budget = int(0.6 * free)
+        self.workers, self.hbm_budget, self.ncv = workers, hbm_budget, ncv
+        self.pool = ProcessPoolExecutor(
+            max_workers=workers, mp_context=multiprocessing.get_context("spawn"),
+            initializer=_worker_init, initargs=(precision, ncv, cutoff, tc_min_flops))
+        self.pids = set(self.pool.map(_worker_ready, range(2 * workers)))
+        self.peak_active = 0
+
+    def close(self) -> None:
+        self.pool.shutdown()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, requests, clock=time.perf_counter) -> list[SolveResult]:
+        from concurrent.futures import FIRST_COMPLETED, wait
+
+        pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        for r in pending:
+            if footprint_bytes(r, self.ncv) > self.hbm_budget:
+                raise ValueError(f"request {r.rid} needs more HBM than the whole budget")
+        results: list[SolveResult] = []
+        active: dict = {}
+        used = 0
+        t0 = clock()
+        while pending or active:
+            now = clock() - t0
+            while pending and pending[0].arrival <= now and len(active) < self.workers:
+                fp = footprint_bytes(pending[0], self.ncv)
+                if used + fp > self.hbm_budget:
+                    break
+                req = pending.pop(0)
+                used += fp
+                active[self.pool.submit(_worker_solve, req)] = (req, now, fp)
+            self.peak_active = max(self.peak_active, len(active))
+            if not active:
+                time.sleep(max(0.0, min(pending[0].arrival - (clock() - t0), 0.01)))
+                continue
+            timeout = max(0.0, pending[0].arrival - now) if pending else None
+            done, _ = wait(list(active), timeout=timeout, return_when=FIRST_COMPLETED)
+            for f in done:
+                req, admitted, fp = active.pop(f)
+                energy, history = f.result()
+                used -= fp
+                results.append(SolveResult(req.rid, energy, history, req.arrival, admitted,
+                                           clock() - t0, fp, req))
         return results
 
 

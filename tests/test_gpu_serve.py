@@ -52,3 +52,18 @@ def test_admission_by_footprint_serialises_what_does_not_fit_together():
     assert len(results) == 3
     for r in results:
         assert r.admitted >= 0.0 and r.finished >= r.admitted
+
+
+def test_solves_served_by_worker_processes_equal_the_same_solves_alone():
+    """Host-parallel serving (two spawned workers on the same GPU): every result is the
+    same as the solve alone in this process."""
+    with serve.ProcessServer(workers=2, hbm_budget=8 << 30, precision="f64") as srv:
+        assert len(srv.pids) == 2
+        results = srv.run(REQUESTS[:4])
+    assert sorted(r.rid for r in results) == [0, 1, 2, 3]
+    assert srv.peak_active == 2
+    for r in results:
+        e, hist = serve.solve_alone(r.request, precision="f64")
+        assert len(hist) == len(r.history)
+        for a, b in zip(hist, r.history):
+            assert abs(a - b) / r.request.L <= TOL_PER_SITE
