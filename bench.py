@@ -296,6 +296,70 @@ def config3_batch(n: int, seed: int = 1000, lam: float = 24.0, max_deg: int = 25
     return F, A, W
 
 
+def batched_matvecs(args, plain_ms: float, graph_ms: float) -> dict:
+    """``n`` independent two-site matvecs of the bench workload's structures (own
+    environments and Krylov vectors, shared MPO sites) as one batch, every stage one
+    launch for all members: FP64 (autotuned tile kinds), and the precision forms with the
+    default tensor-core size rule and with every product on the tensor cores.  Reported
+    per matvec against the plain FP64 form (one eager op-by-op matvec) and the compiled
+    single matvec of the same run; errors are relative Frobenius norms against the FP64
+    batch, worst member."""
+    import torch
+
+    from tenet import _exec, batch, ops
+
+    n = args.batch_n
+    members = [build_workload(seed=10 * k) for k in range(n)]
+    fl, fr, aa = (batch.TensorBatch.stack([m[i] for m in members]) for i in (0, 3, 4))
+    w1 = batch.TensorBatch.broadcast(members[0][1], n)
+    w2 = batch.TensorBatch.broadcast(members[0][2], n)
+    flops = heff2_flops() * n
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+
+    def timed(fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        for k in range(steps):
+            flush.fill_(float(k))
+            ev[k][0].record()
+            fn()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+    out = {"workload": f"{n} SU(2) heff2 matvecs, 256 multiplets per bond (seeds 0, 10, ...), "
+                       "shared MPO sites; compiled batched chain (BatchedHeff2) unless named "
+                       "eager", "flops_per_batch": flops,
+           "l2": "flushed between timed steps (256 MiB write)"}
+    exact = batch.heff2(fl, w1, w2, fr, aa).arena.cpu().numpy()
+    for name, prec in (("f64", ("f64", None)), ("3xbf16", ("3xbf16", None)),
+                       ("3xbf16_all_products", ("3xbf16", 0)), ("tf32_all_products", ("tf32", 0)),
+                       ("f64_eager_batch", None)):
+        if prec is None:  # the same batch through the eager batched ops (no compiled chain)
+            fn = lambda: batch.heff2(fl, w1, w2, fr, aa)  # noqa: E731
+        else:
+            prog = batch.BatchedHeff2(fl, w1, w2, fr, aa.structure, precision=prec[0],
+                                      tc_min_flops=prec[1])
+            y = torch.empty((n, prog.out_size), dtype=torch.float64, device="cuda")
+            fn = lambda: prog.run(aa.arena, y)  # noqa: E731
+        for _ in range(args.warmup):
+            fn()
+        ms = timed(fn, args.steps)
+        if prec is None:
+            got = fn().arena.cpu().numpy()
+        else:
+            fn()
+            got = y.cpu().numpy()
+        err = max(float(np.linalg.norm(got[k] - exact[k]) / np.linalg.norm(exact[k]))
+                  for k in range(n))
+        per = ms / n
+        out[name] = {"ms_per_batch": ms, "us_per_matvec": per * 1e3,
+                     "tflops": flops / (ms * 1e-3) / 1e12, "max_rel_error_vs_f64": err,
+                     "matvec_throughput_vs_plain_f64": plain_ms / per,
+                     "matvec_throughput_vs_compiled_single": graph_ms / per}
+    return out
+
+
 def batched_env_updates(args) -> dict:
     """``n`` independent U(1) x U(1) x fZ2 environment updates ``L' = A^dagger L W A`` as one
     batch (every stage one launch for all members), in FP64 and with every sector product
@@ -643,6 +707,8 @@ def run_tenet(args) -> None:
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
         solves = serving(args) if args.serve_requests > 0 else None
         env3 = batched_env_updates(args) if args.config3_n > 0 else None
+        bmv = (batched_matvecs(args, eager_ms["eager_ops"], ms / args.steps)
+               if args.batch_n > 0 else None)
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -665,6 +731,7 @@ def run_tenet(args) -> None:
             "mixed_precision_forms": mixed,
             "serving": solves,
             "batched_env_updates": env3,
+            "batched_matvecs": bmv,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),
@@ -687,6 +754,8 @@ def main() -> None:
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-workers", type=int, default=4,
                     help="worker processes of the host-parallel serving arms")
+    ap.add_argument("--batch-n", type=int, default=32,
+                    help="members of the batched heff2 matvec (0: skip)")
     ap.add_argument("--config3-n", type=int, default=64,
                     help="members of the batched U1xU1xfZ2 environment update (0: skip)")
     ap.add_argument("--serve-full", action="store_true",

@@ -23,10 +23,11 @@ import numpy as np
 import torch
 
 from tenet import _exec, ops
-from tenet.structure import TensorStructure, layout
+from tenet.structure import OUT, TensorStructure, layout
 from tenet.tensor import SymmetricTensor
 
-__all__ = ["TensorBatch", "adjoint", "einsum", "env_update_last", "tensordot", "transpose"]
+__all__ = ["BatchedHeff2", "TensorBatch", "adjoint", "composed", "einsum", "env_update_last",
+           "heff2", "repartition", "tensordot", "transpose"]
 
 #: pick the FP64 tile kind of batched products by measurement (``_exec.autotune``), keyed
 #: on the block-size histogram; False uses the size heuristic
@@ -195,7 +196,8 @@ def _unary(s: TensorStructure, kind: str, x, y, n: int):
 def _apply(t: TensorBatch, kind: str, x=None, y=None) -> TensorBatch:
     if t.shared:
         src = t[0]
-        one = ops.transpose(src, x) if kind == "t" else ops.adjoint(src)
+        one = (ops.transpose(src, x) if kind == "t" else
+               ops.repartition(src, x, y) if kind == "r" else ops.adjoint(src))
         return TensorBatch.broadcast(one, t.n)
     dst, table = _unary(t.structure, kind, x, y, t.n)
     if table is None:
@@ -211,6 +213,10 @@ def transpose(t: TensorBatch, axes) -> TensorBatch:
 
 def adjoint(t: TensorBatch) -> TensorBatch:
     return _apply(t, "a")
+
+
+def repartition(t: TensorBatch, outputs, inputs) -> TensorBatch:
+    return _apply(t, "r", tuple(outputs), tuple(inputs))
 
 
 def einsum(equation: str, a: TensorBatch, b: TensorBatch) -> TensorBatch:
@@ -235,3 +241,96 @@ def env_update_last(f: TensorBatch, a: TensorBatch, w: TensorBatch) -> TensorBat
     t = einsum("axB,apr->xBpr", f, a)
     t = einsum("xPpm,xBpr->BrPm", w, t)
     return einsum("BPs,BrPm->rms", bra, t)
+
+
+def composed(equation: str, a: TensorBatch, b: TensorBatch, bend: str = "") -> TensorBatch:
+    """Member-wise ``network.composed``: the wires named in ``bend`` bent first."""
+    if bend:
+        lhs, out = equation.split("->")
+        ta, tb = lhs.split(",")
+
+        def bent(t: TensorBatch, term: str):
+            flip = set(bend)
+            outs = tuple(i for i, ch in enumerate(term)
+                         if (t.legs[i].side is OUT) != (ch in flip))
+            ins = tuple(i for i in range(len(term)) if i not in outs)
+            return repartition(t, outs, ins), "".join(term[i] for i in (*outs, *ins))
+
+        a, ta = bent(a, ta)
+        b, tb = bent(b, tb)
+        equation = f"{ta},{tb}->{out}"
+    return einsum(equation, a, b)
+
+
+def heff2(fl: TensorBatch, w1: TensorBatch, w2: TensorBatch, fr: TensorBatch,
+          aa: TensorBatch) -> TensorBatch:
+    """Member-wise ``network.heff2``: ``n`` two-site matvecs, every stage one launch."""
+    t = einsum("apqr,rys->apqys", aa, fr)
+    t = composed("apqys,mQqy->apQms", t, w2, bend="q")
+    t = composed("apQms,xPpm->aPQxs", t, w1, bend="p")
+    return composed("aPQxs,axB->BPQs", t, fl, bend="a")
+
+
+class BatchedHeff2:
+    """The compiled two-site matvec (``program.heff2_program``: 5 gathers, one grouped GEMM
+    launch set per link) for ``n`` members at once: every table of the single-member
+    chain replicated across the batch, every fixed operand packed once (per member, or
+    once for a shared operand), so one ``run`` is about ten launches for all ``n``
+    matvecs.  ``precision`` / ``tc_min_flops`` as in ``ChainProgram``; the FP64 tile kinds
+    of the batched products are autotuned when ``tuned``."""
+
+    def __init__(self, fl: TensorBatch, w1: TensorBatch, w2: TensorBatch, fr: TensorBatch,
+                 in_struct: TensorStructure, precision: str = "f64", tc_min_flops=None,
+                 tuned: bool = True) -> None:
+        from tenet import program
+
+        class _S:
+            def __init__(self, s):
+                self.structure = s
+
+        n = fl.n
+        tmpl = program.heff2_program(*(_S(t.structure) for t in (fl, w1, w2, fr)), in_struct,
+                                     allocate=False, precision=precision,
+                                     tc_min_flops=tc_min_flops)
+        operands = {"fr": fr, "w2": w2, "w1": w1, "fl": fl}
+        dev = _exec.device()
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.n, self.in_struct, self.out_struct = n, in_struct, tmpl.out_struct
+        self.in_size, self.out_size = layout(in_struct).size, layout(tmpl.out_struct).size
+        self.links = []
+        src_stride = self.in_size
+        for lk, name in zip(tmpl.links, tmpl.operand_names):
+            op = operands[name]
+            m = 1 if op.shared else n
+            a_g = _batch_gather(lk.a_gather, n, (src_stride, 0), (lk.a_size, 0))
+            b_g = _batch_gather(lk.b_gather, m, (layout(op.structure).size, 0), (lk.b_size, 0))
+            gemm = _exec.GemmGroup(
+                _batch_products(lk.gemm.products, n, lk.a_size, 0 if op.shared else lk.b_size,
+                                lk.c_size), precision, tc_min_flops, tuned=tuned)
+            bufs = (torch.empty(max(1, n * lk.a_size), **f64),
+                    torch.empty(max(1, m * lk.b_size), **f64),
+                    torch.empty(max(1, n * lk.c_size), **f64))
+            if b_g is not None:
+                b_g.run(op.arena.reshape(-1), bufs[1])
+            self.links.append((a_g, gemm, bufs, op))
+            src_stride = lk.c_size
+        self.out_gather = _batch_gather(tmpl.out_gather, n, (src_stride, 0), (self.out_size, 0))
+        self.flops = sum(g.flops for _, g, _, _ in self.links)
+
+    def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+        """``out[k] = H_k x[k]`` for the ``(n, size)`` arenas ``x`` and ``out``."""
+        src = x.reshape(-1)
+        for a_g, gemm, (ab, bb, cb), _ in self.links:
+            if a_g is not None:
+                a_g.run(src, ab)
+            gemm.run(ab, bb, cb)
+            src = cb
+        if self.out_gather is not None:
+            self.out_gather.run(src, out.reshape(-1))
+        return out
+
+    def __call__(self, aa: TensorBatch) -> TensorBatch:
+        if aa.structure != self.in_struct or aa.n != self.n:
+            raise ValueError("BatchedHeff2: the batch's structure or size differs")
+        out = torch.empty((self.n, self.out_size), dtype=torch.float64, device=aa.arena.device)
+        return TensorBatch(self.out_struct, self.run(aa.arena, out), self.n)

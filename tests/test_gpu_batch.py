@@ -69,3 +69,22 @@ def test_autotuned_tiles_compute_the_same_products():
         batch.AUTOTUNE = True
     got = batch.env_update_last(F, A, W).arena.cpu().numpy()
     assert rel(got, ref) <= 1e-13
+
+
+def test_batched_heff2_matches_each_member():
+    """n two-site matvecs of the bench workload's structures (own environments and
+    vectors, shared MPO) in one batch: each member equals ``network.heff2`` on it."""
+    import bench
+
+    n = 3
+    members = [bench.build_workload(seed=10 * k) for k in range(n)]
+    fl, w1, w2, fr, aa = (batch.TensorBatch.stack([m[i] for m in members]) for i in range(5))
+    w1 = batch.TensorBatch.broadcast(members[0][1], n)
+    w2 = batch.TensorBatch.broadcast(members[0][2], n)
+    out = batch.heff2(fl, w1, w2, fr, aa)
+    compiled = batch.BatchedHeff2(fl, w1, w2, fr, aa.structure)(aa)
+    for k, (f, _, _, r, a) in enumerate(members):
+        want = network.heff2(f, members[0][1], members[0][2], r, a)
+        assert out.structure == want.structure == compiled.structure
+        assert rel(out[k].numpy_arena(), want.numpy_arena()) <= 1e-13
+        assert rel(compiled[k].numpy_arena(), want.numpy_arena()) <= 1e-13
