@@ -8,6 +8,7 @@ path; the host only plans.
 """
 
 from tenet import linalg, network, symmetry
+from tenet.serialize import load, save
 from tenet.ops import add, adjoint, compose, contractible, divide, einsum, inner, multiply, \
     norm, outward_dual, repartition, subtract, tensordot, transpose
 from tenet.structure import IN, OUT, FusionBlockKey, FusionTree, GradedSpace, Leg, Side, \
@@ -17,6 +18,6 @@ from tenet.tensor import SymmetricTensor
 __all__ = [
     "IN", "OUT", "FusionBlockKey", "FusionTree", "GradedSpace", "Leg", "Side",
     "SymmetricTensor", "TensorStructure", "add", "adjoint", "compose", "contractible",
-    "divide", "einsum", "inner", "linalg", "multiply", "network", "norm", "outward_dual",
-    "repartition", "subtract", "symmetry", "tensordot", "transpose",
+    "divide", "einsum", "inner", "linalg", "load", "multiply", "network", "norm",
+    "outward_dual", "repartition", "save", "subtract", "symmetry", "tensordot", "transpose",
 ]

@@ -258,6 +258,20 @@ class MPS:
                                            Leg(bonds[i + 1], IN)), seed=seed + i)
                    for i in range(len(bonds) - 1))
 
+    def save(self, path) -> None:
+        """Write a directory: one ``NNN.npz`` per site plus ``mps.json``
+        (``network/mps.py:567-607``; ``tenet.serialize``)."""
+        from tenet import serialize
+
+        serialize.save_mps(self, path)
+
+    @classmethod
+    def load(cls, path) -> "MPS":
+        """Read a directory written by ``save`` (``network/mps.py:609-676``)."""
+        from tenet import serialize
+
+        return serialize.load_mps(path)
+
     def canonize_(self, to: int = 0) -> "MPS":
         """Right-canonicalise by one LQ per site from the right (``network/mps.py:312-352``)."""
         from tenet import linalg, ops

@@ -8,6 +8,7 @@ keys must be identical.  After each test the sticky device error word must be cl
 """
 
 import json
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -568,3 +569,28 @@ def test_fused_chain_is_bit_identical_to_stage_by_stage(golden_dir):
         for y in outs[1:]:
             assert torch.equal(y, outs[0])
         assert int(prog.barrier[0].item()) == 0
+
+
+def test_save_load_round_trip_on_the_device(tmp_path):
+    """``tenet.save`` / ``tenet.load`` and ``MPS.save`` / ``MPS.load`` through the device."""
+    import tenet
+    from tenet.structure import GradedSpace
+    from tenet.symmetry import SU2
+
+    m = json.loads((Path(__file__).resolve().parent / "golden" / "heff.json").read_text())
+    h = np.load(Path(__file__).resolve().parent / "golden" / "heff.npz")
+    t = load(h, m["aa"])
+    tenet.save(t, tmp_path / "aa.npz")
+    back = tenet.load(tmp_path / "aa.npz")
+    assert back.structure == t.structure
+    assert torch.equal(back.arena, t.arena)
+    L = 6
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
+             for i in range(L + 1)]
+    psi = network.MPS.random(phys, bonds, seed=2).canonize_(0)
+    psi.save(tmp_path / "psi")
+    psi2 = network.MPS.load(tmp_path / "psi")
+    assert psi2.center == psi.center == 0
+    for n in range(L):
+        assert torch.equal(psi2[n].arena, psi[n].arena)
