@@ -113,12 +113,16 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
  *   TNB_TILE_32      32 x 32 output tiles, for compositions too small to fill the GPU
  *   TNB_TILE_SKINNY  256 output rows per tile (tiles = ceil(M/256)); needs N, K <= 16
  *   TNB_TILE_WIDE    256 output columns per tile (tiles = ceil(N/256)); needs M, K <= 16
- *   TNB_TILE_TC_TF32    128 x 64 tiles on the tcgen05 tensor cores, operands rounded to
- *                       TF32, FP32 accumulation (tiles = ceil(M/128) * ceil(N/64))
+ *   TNB_TILE_TC_TF32    128 x 128 tiles on the tcgen05 tensor cores, operands rounded to
+ *                       TF32, FP32 accumulation (tiles = ceil(M/128) * ceil(N/128))
  *   TNB_TILE_TC_3XBF16  same tiles, operands split into BF16 hi + lo pairs and the product
  *                       taken as hi.hi + hi.lo + lo.hi, FP32 accumulation
  * The tensor-core kinds read and write FP64 like the others; only the arithmetic inside
- * is reduced, and they take no split-K.
+ * is reduced, and they take no split-K.  They pack each operand once into 16 KB slabs
+ * (one 128-row x 32-K slab of A, or of B transposed, per slab) in the work buffer, so for
+ * them columns [12] and [13] are the row's first A slab and first B slab (rows in slab
+ * order, A slabs of a row m-tile-major then K), n_counters = A slabs | (B slabs << 32),
+ * and work_bytes >= 16384 * (A slabs + B slabs); the work buffer needs no zeroing.
  */
 #define TNB_GEMM_WIDTH 16
 #define TNB_TILE_64 0

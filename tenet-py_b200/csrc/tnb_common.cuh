@@ -73,7 +73,8 @@ cudaError_t launch_dyn(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
 // Tensor-core grouped GEMM launcher (tnb_gemm_tc.cu).
 cudaError_t launch_gemm_tc(int kind, unsigned grid, cudaStream_t s, const int64_t* table,
                            int64_t n_gemm, const int32_t* tile_map, const double* a,
-                           int64_t n_a, const double* b, int64_t n_b, double* c, int64_t n_c);
+                           int64_t n_a, const double* b, int64_t n_b, double* c, int64_t n_c,
+                           void* work, int64_t work_bytes, int64_t n_counters);
 
 }  // namespace tnb
 

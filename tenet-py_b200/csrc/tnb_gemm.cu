@@ -59,10 +59,13 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
   TNB_REQUIRE(gemm_table != nullptr && tile_map != nullptr && c != nullptr,
               "tnb_grouped_gemm_f64: null table, tile map or C");
   TNB_REQUIRE(total_tiles < (int64_t(1) << 31), "tnb_grouped_gemm_f64: too many tiles");
-  TNB_REQUIRE(work_bytes >= 0 && n_counters >= 0 &&
-              (work_bytes == 0 || work != nullptr) &&
-              tnb::gemm_work_parts_offset(n_counters) <= work_bytes,
+  const bool tc = tile_kind == TNB_TILE_TC_TF32 || tile_kind == TNB_TILE_TC_3XBF16;
+  TNB_REQUIRE(work_bytes >= 0 && n_counters >= 0 && (work_bytes == 0 || work != nullptr),
+              "tnb_grouped_gemm_f64: bad work buffer");
+  TNB_REQUIRE(tc || tnb::gemm_work_parts_offset(n_counters) <= work_bytes,
               "tnb_grouped_gemm_f64: work buffer too small for its counters");
+  TNB_REQUIRE(!tc || ((n_counters & 0xFFFFFFFFll) + (n_counters >> 32)) * 16384 <= work_bytes,
+              "tnb_grouped_gemm_f64: work buffer too small for the packed operands");
   auto* counters = static_cast<unsigned int*>(work);
   const int64_t poff = tnb::gemm_work_parts_offset(n_counters);
   double* parts = work_bytes > poff
@@ -89,7 +92,7 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
     case TNB_TILE_TC_TF32:
     case TNB_TILE_TC_3XBF16:
       e = tnb::launch_gemm_tc(tile_kind, grid, s, gemm_table, n_gemm, tile_map, a, n_a, b, n_b,
-                              c, n_c);
+                              c, n_c, work, work_bytes, n_counters);
       break;
     default:
       tnb::set_error("tnb_grouped_gemm_f64: unknown tile kind");

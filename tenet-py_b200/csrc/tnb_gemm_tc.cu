@@ -3,24 +3,25 @@
 // The precision form of the block GEMMs: the same descriptor table as the FP64 kernels,
 // FP64 operands in and FP64 results out, but every product runs as tcgen05.mma with FP32
 // accumulators held in tensor memory:
-//   TNB_TILE_TC_TF32    A, B rounded to TF32 (kind::tf32), one MMA per K step of 8;
+//   TNB_TILE_TC_TF32    A, B rounded to TF32 (kind::tf32);
 //   TNB_TILE_TC_3XBF16  A = A_hi + A_lo, B = B_hi + B_lo split into BF16 pairs and the
 //                       product taken as A_hi B_hi + A_hi B_lo + A_lo B_hi (kind::f16 with
-//                       BF16 inputs, K step 16), which keeps about 16 significand bits of
-//                       every operand instead of 8.
+//                       BF16 inputs), which keeps about 16 significand bits of every
+//                       operand instead of 8.
 //
-// One CTA of 128 threads owns one 128 x 64 output tile.  Per K slab of 32 the threads
-// convert their share of A (128 x 32) and B (32 x 64, transposed on the way) into shared
-// memory in the canonical K-major, no-swizzle UMMA layout -- 8-row x 16-byte core
+// Three launches per table.  Two pack kernels convert each operand once: every 128-row x
+// 32 slab of A (and of B^T) becomes one 16 KB chunk of the work buffer, already in the
+// canonical K-major, no-swizzle UMMA shared-memory layout (8-row x 16-byte core
 // matrices, LBO = 128 B between the two core matrices of one K step, SBO between 8-row
-// groups -- then one elected thread issues the MMAs into a 128-lane x 64-column TMEM
-// accumulator and commits them to the stage's mbarrier.  Two shared-memory stages make a
-// pipeline: slab s + 1 is loaded from global memory into registers while slab s is
-// converted, stored and issued, and a stage is overwritten only after the mbarrier of
-// the MMAs that read it (two slabs back) has completed.  The epilogue reads TMEM with
-// tcgen05.ld (warp w owns lanes 32w..32w+31) and writes FP64.  Every wait is bounded:
-// past the limit the kernel raises TNB_ETIMEOUT, stops issuing, and still frees its TMEM
-// before returning.
+// groups), parts (BF16 hi, lo) back to back.  The MMA kernel gives each CTA a 128 x 128
+// output tile and runs a three-stage pipeline: one producer thread copies the next A and
+// B slabs with cp.async.bulk (global -> shared, completion counted in bytes on the
+// stage's "full" mbarrier), one issuer thread waits for "full", issues the MMAs into a
+// 128-lane x 128-column TMEM accumulator and commits them to the stage's "empty"
+// mbarrier, which the producer waits on before refilling the stage.  The epilogue reads
+// TMEM with tcgen05.ld (warp w owns lanes 32w..32w+31) and writes FP64.  Every wait is
+// bounded: past the limit the kernel raises TNB_ETIMEOUT, stops, and still frees its
+// TMEM before returning.  No copy uses cluster multicast.
 #include <cuda_bf16.h>
 
 #include <string>
@@ -29,12 +30,13 @@
 
 namespace tnb {
 
-constexpr int kTcM = 128, kTcN = 64, kTcBk = 32, kTcThreads = 128;
-constexpr unsigned kTcTmemCols = 64;
-constexpr long long kTcWaitCycles = 4000000000LL;  // ~2 s at the boost clock
+constexpr int kT2M = 128, kT2N = 128, kT2Bk = 32, kT2Threads = 128, kT2Stages = 3;
+constexpr int kT2Slab = 16384;  // bytes of one packed operand slab, all parts
+constexpr unsigned kT2TmemCols = 128;
+constexpr long long kT2WaitCycles = 4000000000LL;  // ~2 s at the boost clock
 
-struct GemmRowTc {
-  int64_t M, N, K, aoff, lda, boff, ldb, coff, ldc, tile_begin, tiles_n;
+struct T2Row {
+  int64_t M, N, K, aoff, lda, boff, ldb, coff, ldc, tile_begin, tiles_n, a_chunk, b_chunk;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -48,9 +50,9 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
          (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor: FP32 accumulate, both operands K-major, M = 128, N = 64.
+// Instruction descriptor: FP32 accumulate, both operands K-major, M = 128, N = 128.
 __host__ __device__ constexpr uint32_t umma_idesc(uint32_t fmt) {
-  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((kTcN >> 3) << 17) | ((kTcM >> 4) << 24);
+  return (1u << 4) | (fmt << 7) | (fmt << 10) | ((kT2N >> 3) << 17) | ((kT2M >> 4) << 24);
 }
 
 // Byte offset of element (r, k) of a K-major tile whose rows hold `row_bytes` bytes.
@@ -75,165 +77,212 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
         "selp.b32 %0, 1, 0, p;\n\t}"
         : "=r"(done) : "r"(mbar), "r"(phase) : "memory");
     if (done) return true;
-    if (clock64() - t0 > kTcWaitCycles) return false;
+    if (clock64() - t0 > kT2WaitCycles) return false;
   }
 }
 
 template <int MODE>
-struct TcLayout {
+struct T2Layout {
   static constexpr int kEsz = MODE == 0 ? 4 : 2;
-  static constexpr int kRowBytes = kTcBk * kEsz;
+  static constexpr int kRowBytes = kT2Bk * kEsz;      // one 32-wide K row of one part
   static constexpr int kParts = MODE == 0 ? 1 : 2;
-  static constexpr int kABytes = kTcM * kRowBytes, kBBytes = kTcN * kRowBytes;
-  // one pipeline stage: A parts, then B parts (TF32 16 + 8 KB; 3xBF16 2 x 8 + 2 x 4 KB)
-  static constexpr int kStageBytes = kParts * (kABytes + kBBytes);
-  static constexpr int kSmemBytes = 2 * kStageBytes + 1024;  // two stages + alignment slack
+  static constexpr int kPartBytes = kT2M * kRowBytes;  // 16 KB (TF32) or 8 KB (BF16)
+  static_assert(kParts * kPartBytes == kT2Slab, "a slab is 16 KB");
+  static constexpr int kStageBytes = 2 * kT2Slab;      // A slab + B slab
+  static constexpr int kSmemBytes = kT2Stages * kStageBytes + 1024;
 };
 
-template <int MODE>  // 0 = TF32, 1 = 3 x BF16
-__global__ void __launch_bounds__(kTcThreads)
-gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
-               const int32_t* __restrict__ tile_map, const double* __restrict__ a, int64_t n_a,
-               const double* __restrict__ b, int64_t n_b, double* __restrict__ c, int64_t n_c) {
-  using L = TcLayout<MODE>;
-  constexpr int kEsz = L::kEsz, kRowBytes = L::kRowBytes;
-  constexpr int kLA = (kTcM * kTcBk) / kTcThreads, kLB = (kTcN * kTcBk) / kTcThreads;
+__device__ __forceinline__ bool load_t2row(const int64_t* table, int64_t g, T2Row& r) {
+  const int64_t* t = table + g * TNB_GEMM_WIDTH;
+  r.M = t[0]; r.N = t[1]; r.K = t[2]; r.aoff = t[3]; r.lda = t[4]; r.boff = t[5];
+  r.ldb = t[6]; r.coff = t[7]; r.ldc = t[8]; r.tile_begin = t[9]; r.tiles_n = t[10];
+  r.a_chunk = t[12]; r.b_chunk = t[13];
+  return r.M >= 0 && r.N >= 0 && r.K >= 0 && r.a_chunk >= 0 && r.b_chunk >= 0;
+}
+
+// The table row owning packed chunk `chunk` of operand A (which == 0) or B (which == 1):
+// the last row whose first chunk is <= chunk (rows in chunk order).
+__device__ int64_t owner_row(const int64_t* table, int64_t n_gemm, int64_t chunk, int which) {
+  int64_t lo = 0, hi = n_gemm - 1;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (table[mid * TNB_GEMM_WIDTH + 12 + which] <= chunk) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Pack one 128 x 32 slab of A (which == 0: rows = M, read along K) or of B^T (which == 1:
+// rows = N, read along N) into its work-buffer chunk in the UMMA layout.
+template <int MODE>
+__global__ void __launch_bounds__(kT2Threads)
+tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* __restrict__ src,
+               int64_t n_src, uint8_t* __restrict__ work, int64_t work_bytes, int64_t chunk0,
+               int which) {
+  using L = T2Layout<MODE>;
+  __shared__ T2Row s_row;
+  __shared__ int s_ok;
+  pdl_launch_dependents();
+  const int tid = threadIdx.x;
+  const int64_t chunk = blockIdx.x;
+  if (tid == 0) {
+    T2Row r{};
+    const int64_t g = owner_row(table, n_gemm, chunk, which);
+    bool ok = load_t2row(table, g, r);
+    const int64_t rows = which == 0 ? r.M : r.N;
+    const int64_t ks = (r.K + kT2Bk - 1) / kT2Bk;
+    ok = ok && ks > 0 && (chunk0 + chunk + 1) * kT2Slab <= work_bytes;
+    if (ok) {  // the row's operand footprint
+      ok = which == 0 ? (r.aoff >= 0 && r.aoff + (r.M - 1) * r.lda + r.K <= n_src)
+                      : (r.boff >= 0 && r.boff + (r.K - 1) * r.ldb + r.N <= n_src);
+      ok = ok && rows > 0;
+    }
+    if (!ok) raise_bounds();
+    s_row = r;
+    s_ok = ok;
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  const T2Row r = s_row;
+  const int64_t ks = (r.K + kT2Bk - 1) / kT2Bk;
+  const int64_t local = chunk - (which == 0 ? r.a_chunk : r.b_chunk);
+  const int64_t t0 = (local / ks) * kT2M, k0 = (local % ks) * kT2Bk;
+  uint8_t* dst = work + (chunk0 + chunk) * kT2Slab;
+  pdl_wait();  // the operand may be the previous kernel's output
+#pragma unroll 4
+  for (int i = 0; i < (kT2M * kT2Bk) / kT2Threads; ++i) {
+    const int idx = tid + i * kT2Threads;
+    int rr, kk;
+    double x;
+    if (which == 0) {  // A: consecutive threads along K
+      rr = idx / kT2Bk;
+      kk = idx % kT2Bk;
+      const int64_t gm = t0 + rr, gk = k0 + kk;
+      x = (gm < r.M && gk < r.K) ? src[r.aoff + gm * r.lda + gk] : 0.0;
+    } else {  // B: consecutive threads along N
+      kk = idx / kT2N;
+      rr = idx % kT2N;
+      const int64_t gn = t0 + rr, gk = k0 + kk;
+      x = (gk < r.K && gn < r.N) ? src[r.boff + gk * r.ldb + gn] : 0.0;
+    }
+    const uint32_t off = kmajor(rr, kk, L::kEsz, L::kRowBytes);
+    if constexpr (MODE == 0) {
+      *reinterpret_cast<uint32_t*>(dst + off) = to_tf32(x);
+    } else {
+      const __nv_bfloat16 hi = __double2bfloat16(x);
+      const __nv_bfloat16 lo = __double2bfloat16(x - static_cast<double>(__bfloat162float(hi)));
+      *reinterpret_cast<__nv_bfloat16*>(dst + off) = hi;
+      *reinterpret_cast<__nv_bfloat16*>(dst + L::kPartBytes + off) = lo;
+    }
+  }
+}
+
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kT2Threads)
+tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
+              const int32_t* __restrict__ tile_map, const uint8_t* __restrict__ work,
+              int64_t work_bytes, int64_t b_chunk0, double* __restrict__ c, int64_t n_c) {
+  using L = T2Layout<MODE>;
   extern __shared__ uint8_t smem_dyn[];
-  // 1024-byte aligned base of the two stages
   uint8_t* const smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_dyn) + 1023) & ~static_cast<uintptr_t>(1023));
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t full[kT2Stages], empty[kT2Stages], done;
   __shared__ uint32_t s_tmem;
-  __shared__ GemmRowTc s_row;
-  __shared__ int s_ok;
-  __shared__ int s_fail;
+  __shared__ T2Row s_row;
+  __shared__ int s_ok, s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   pdl_launch_dependents();
   if (tid == 0) {
-    bool ok = true;
+    T2Row r{};
     const int64_t g = tile_map[blockIdx.x];
-    GemmRowTc r{};
-    if (g < 0 || g >= n_gemm) {
-      ok = false;
-    } else {
-      const int64_t* t = table + g * TNB_GEMM_WIDTH;
-      r.M = t[0]; r.N = t[1]; r.K = t[2]; r.aoff = t[3]; r.lda = t[4]; r.boff = t[5];
-      r.ldb = t[6]; r.coff = t[7]; r.ldc = t[8]; r.tile_begin = t[9]; r.tiles_n = t[10];
-      ok = r.M > 0 && r.N > 0 && r.K >= 0 && r.tiles_n > 0 && r.coff >= 0 &&
-           r.coff + (r.M - 1) * r.ldc + r.N <= n_c;
-      if (r.K > 0)
-        ok = ok && r.aoff >= 0 && r.boff >= 0 && r.aoff + (r.M - 1) * r.lda + r.K <= n_a &&
-             r.boff + (r.K - 1) * r.ldb + r.N <= n_b;
+    bool ok = g >= 0 && g < n_gemm && load_t2row(table, g, r);
+    const int64_t ks = ok ? (r.K + kT2Bk - 1) / kT2Bk : 0;
+    if (ok) {
+      const int64_t mt = (r.M + kT2M - 1) / kT2M, nt = (r.N + kT2N - 1) / kT2N;
+      ok = r.M > 0 && r.N > 0 && r.tiles_n == nt && r.coff >= 0 &&
+           r.coff + (r.M - 1) * r.ldc + r.N <= n_c &&
+           (ks == 0 || ((r.a_chunk + mt * ks) * kT2Slab <= work_bytes &&
+                        (b_chunk0 + r.b_chunk + nt * ks) * kT2Slab <= work_bytes));
     }
     if (!ok) raise_bounds();
     s_row = r;
     s_ok = ok;
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    for (int st = 0; st < kT2Stages; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&full[st])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&empty[st])) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&done)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {  // one warp owns the TMEM allocation
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 :: "r"(smem_u32(&s_tmem)), "r"(kTcTmemCols) : "memory");
+                 :: "r"(smem_u32(&s_tmem)), "r"(kT2TmemCols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
-  const GemmRowTc r = s_row;
+  const T2Row r = s_row;
   const bool ok = s_ok;
   const int64_t local = blockIdx.x - r.tile_begin;
-  const int64_t m0 = ok ? (local / r.tiles_n) * kTcM : 0, n0 = ok ? (local % r.tiles_n) * kTcN : 0;
-  pdl_wait();  // A may be the previous kernel's output
+  const int64_t mtile = ok ? local / r.tiles_n : 0, ntile = ok ? local % r.tiles_n : 0;
+  const int64_t nk = ok ? (r.K + kT2Bk - 1) / kT2Bk : 0;
+  const uint8_t* a_src = work + (r.a_chunk + mtile * nk) * kT2Slab;
+  const uint8_t* b_src = work + (b_chunk0 + r.b_chunk + ntile * nk) * kT2Slab;
+  pdl_wait();  // the packed operands are the pack kernels' output
 
-  double ra[kLA], rb[kLB];
-  auto load_slab = [&](int64_t k0) {
-#pragma unroll
-    for (int i = 0; i < kLA; ++i) {
-      const int idx = tid + i * kTcThreads;
-      const int rr = idx / kTcBk, kk = idx % kTcBk;
-      const int64_t gm = m0 + rr, gk = k0 + kk;
-      ra[i] = (gm < r.M && gk < r.K) ? a[r.aoff + gm * r.lda + gk] : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < kLB; ++i) {
-      const int idx = tid + i * kTcThreads;
-      const int kk = idx / kTcN, nn = idx % kTcN;
-      const int64_t gk = k0 + kk, gn = n0 + nn;
-      rb[i] = (gk < r.K && gn < r.N) ? b[r.boff + gk * r.ldb + gn] : 0.0;
-    }
-  };
-  auto store_slab = [&](int stage) {
-    uint8_t* sa0 = smem + stage * L::kStageBytes;
-    uint8_t* sb0 = sa0 + L::kParts * L::kABytes;
-#pragma unroll
-    for (int i = 0; i < kLA; ++i) {
-      const int idx = tid + i * kTcThreads;
-      const uint32_t off = kmajor(idx / kTcBk, idx % kTcBk, kEsz, kRowBytes);
-      if constexpr (MODE == 0) {
-        *reinterpret_cast<uint32_t*>(sa0 + off) = to_tf32(ra[i]);
-      } else {
-        const __nv_bfloat16 hi = __double2bfloat16(ra[i]);
-        const __nv_bfloat16 lo = __double2bfloat16(ra[i] - static_cast<double>(__bfloat162float(hi)));
-        *reinterpret_cast<__nv_bfloat16*>(sa0 + off) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(sa0 + L::kABytes + off) = lo;
+  if (tid == 0 && nk > 0) {  // producer
+    uint32_t ephase[kT2Stages] = {0u, 0u, 0u};
+    for (int64_t s = 0; s < nk; ++s) {
+      const int st = static_cast<int>(s % kT2Stages);
+      if (s >= kT2Stages) {
+        if (!mbar_wait(smem_u32(&empty[st]), ephase[st])) {
+          atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
+          s_fail = 1;
+          break;
+        }
+        ephase[st] ^= 1u;
       }
+      const uint32_t fb = smem_u32(&full[st]);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                   :: "r"(fb), "r"(static_cast<uint32_t>(2 * kT2Slab)) : "memory");
+      const uint32_t sa = smem_u32(smem + st * L::kStageBytes);
+      bulk_copy(sa, a_src + s * kT2Slab, kT2Slab, fb);
+      bulk_copy(sa + kT2Slab, b_src + s * kT2Slab, kT2Slab, fb);
     }
-#pragma unroll
-    for (int i = 0; i < kLB; ++i) {
-      const int idx = tid + i * kTcThreads;
-      const uint32_t off = kmajor(idx % kTcN, idx / kTcN, kEsz, kRowBytes);
-      if constexpr (MODE == 0) {
-        *reinterpret_cast<uint32_t*>(sb0 + off) = to_tf32(rb[i]);
-      } else {
-        const __nv_bfloat16 hi = __double2bfloat16(rb[i]);
-        const __nv_bfloat16 lo = __double2bfloat16(rb[i] - static_cast<double>(__bfloat162float(hi)));
-        *reinterpret_cast<__nv_bfloat16*>(sb0 + off) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(sb0 + L::kBBytes + off) = lo;
-      }
-    }
-  };
-
-  uint32_t phase[2] = {0u, 0u};
-  const int64_t nk = ok ? (r.K + kTcBk - 1) / kTcBk : 0;
-  if (nk > 0) load_slab(0);
-  for (int64_t s = 0; s < nk; ++s) {
-    const int stage = static_cast<int>(s & 1);
-    // the stage is free once the MMAs of slab s - 2 (its last readers) have completed
-    if (s >= 2 && !s_fail && !mbar_wait(smem_u32(&mbar[stage]), phase[stage])) {
-      if (lane == 0) {
+  } else if (tid == 32 && nk > 0) {  // MMA issuer
+    uint32_t fphase[kT2Stages] = {0u, 0u, 0u};
+    constexpr uint32_t kLbo = 128, kSbo = (L::kRowBytes / 16) * 128;
+    constexpr uint32_t kIdesc = umma_idesc(MODE == 0 ? 2u : 1u);
+    constexpr int kSteps = L::kRowBytes / 32;  // one MMA consumes 32 bytes of K
+    constexpr int kProducts = MODE == 0 ? 1 : 3;  // 3xBF16: hi.hi, hi.lo, lo.hi
+    for (int64_t s = 0; s < nk; ++s) {
+      const int st = static_cast<int>(s % kT2Stages);
+      if (!mbar_wait(smem_u32(&full[st]), fphase[st])) {
         atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
         s_fail = 1;
+        break;
       }
-    }
-    if (s >= 2) phase[stage] ^= 1u;
-    __syncthreads();
-    if (s_fail) break;
-    store_slab(stage);
-    if (s + 1 < nk) load_slab((s + 1) * kTcBk);  // in flight while slab s is issued
-    // make the generic-proxy stores visible to the tensor cores, then issue
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
+      fphase[st] ^= 1u;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      constexpr uint32_t kLbo = 128, kSbo = (kRowBytes / 16) * 128;
-      constexpr uint32_t kIdesc = umma_idesc(MODE == 0 ? 2u : 1u);
-      constexpr int kSteps = kRowBytes / 32;  // one MMA consumes 32 bytes of K
-      // (A part, B part) pairs: TF32 one product; 3xBF16 hi.hi, hi.lo, lo.hi
-      constexpr int kProducts = MODE == 0 ? 1 : 3;
-      const int pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
-      const uint32_t sa = smem_u32(smem + stage * L::kStageBytes);
-      const uint32_t sb = sa + L::kParts * L::kABytes;
+      const uint32_t sa = smem_u32(smem + st * L::kStageBytes), sb = sa + kT2Slab;
 #pragma unroll
       for (int p = 0; p < kProducts; ++p) {
+        const int pa = p == 2 ? 1 : 0, pb = p == 1 ? 1 : 0;
 #pragma unroll
-        for (int st = 0; st < kSteps; ++st) {
-          const uint64_t ad = umma_desc(sa + pa[p] * L::kABytes + st * 256, kLbo, kSbo);
-          const uint64_t bd = umma_desc(sb + pb[p] * L::kBBytes + st * 256, kLbo, kSbo);
-          const uint32_t acc = (s > 0 || p > 0 || st > 0) ? 1u : 0u;
+        for (int k = 0; k < kSteps; ++k) {
+          const uint64_t ad = umma_desc(sa + pa * L::kPartBytes + k * 256, kLbo, kSbo);
+          const uint64_t bd = umma_desc(sb + pb * L::kPartBytes + k * 256, kLbo, kSbo);
+          const uint32_t acc = (s > 0 || p > 0 || k > 0) ? 1u : 0u;
           if constexpr (MODE == 0) {
             asm volatile(
                 "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %4, 0;\n\t"
@@ -248,27 +297,28 @@ gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
         }
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   :: "r"(smem_u32(&mbar[stage])) : "memory");
+                   :: "r"(smem_u32(&empty[st])) : "memory");
     }
+    // the last commit covers every MMA issued before it
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(smem_u32(&done)) : "memory");
   }
-  // the last commit covers every MMA issued before it
-  if (nk > 0 && !s_fail) {
-    const int last = static_cast<int>((nk - 1) & 1);
-    if (!mbar_wait(smem_u32(&mbar[last]), phase[last])) {
-      if (lane == 0) {
-        atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
-        s_fail = 1;
-      }
+  __syncthreads();
+  if (nk > 0 && !s_fail && !mbar_wait(smem_u32(&done), 0u)) {
+    if (lane == 0) {
+      atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
+      s_fail = 1;
     }
   }
   __syncthreads();
 
-  // epilogue: TMEM -> registers -> FP64 C (zeros when K == 0 or the MMAs timed out)
+  // epilogue: TMEM -> registers -> FP64 C (zeros when K == 0 or a wait gave up)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const int64_t row = m0 + warp * 32 + lane;
+  const int64_t row = mtile * kT2M + warp * 32 + lane;
+  const int64_t n0 = ntile * kT2N;
   const bool live = ok && nk > 0 && !s_fail;
-#pragma unroll
-  for (int chunk = 0; chunk < kTcN / 16; ++chunk) {
+#pragma unroll 1
+  for (int chunk = 0; chunk < kT2N / 16; ++chunk) {
     uint32_t v[16];
     if (live) {
       const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + chunk * 16;
@@ -296,32 +346,50 @@ gemm_tc_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
-                 :: "r"(tmem), "r"(kTcTmemCols) : "memory");
+                 :: "r"(tmem), "r"(kT2TmemCols) : "memory");
   }
 }
 
-}  // namespace tnb
+template <int MODE>
+cudaError_t launch_tc_mode(unsigned grid, cudaStream_t s, const int64_t* table, int64_t n_gemm,
+                           const int32_t* tile_map, const double* a, int64_t n_a,
+                           const double* b, int64_t n_b, double* c, int64_t n_c, void* work,
+                           int64_t work_bytes, int64_t a_chunks, int64_t b_chunks) {
+  using L = T2Layout<MODE>;
+  static bool opted = false;
+  if (!opted) {
+    const cudaError_t e = cudaFuncSetAttribute(tc_mma_kernel<MODE>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               L::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
+  auto* w = static_cast<uint8_t*>(work);
+  cudaError_t e = cudaSuccess;
+  if (a_chunks > 0)
+    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(a_chunks), kT2Threads, s, table,
+               n_gemm, a, n_a, w, work_bytes, int64_t{0}, 0);
+  if (e == cudaSuccess && b_chunks > 0)
+    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(b_chunks), kT2Threads, s, table,
+               n_gemm, b, n_b, w, work_bytes, a_chunks, 1);
+  if (e == cudaSuccess)
+    e = launch_dyn(tc_mma_kernel<MODE>, grid, kT2Threads, L::kSmemBytes, s, table, n_gemm,
+                   tile_map, static_cast<const uint8_t*>(w), work_bytes, a_chunks, c, n_c);
+  return e;
+}
 
-namespace tnb {
 cudaError_t launch_gemm_tc(int kind, unsigned grid, cudaStream_t s, const int64_t* table,
                            int64_t n_gemm, const int32_t* tile_map, const double* a,
-                           int64_t n_a, const double* b, int64_t n_b, double* c, int64_t n_c) {
-  // the two-stage pipeline needs more than the default 48 KB of shared memory per CTA
-  static bool opted[2] = {false, false};
-  const int mode = kind == TNB_TILE_TC_TF32 ? 0 : 1;
-  if (!opted[mode]) {
-    const cudaError_t e = mode == 0
-        ? cudaFuncSetAttribute(gemm_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               TcLayout<0>::kSmemBytes)
-        : cudaFuncSetAttribute(gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               TcLayout<1>::kSmemBytes);
-    if (e != cudaSuccess) return e;
-    opted[mode] = true;
-  }
-  if (mode == 0)
-    return launch_dyn(gemm_tc_kernel<0>, grid, kTcThreads, TcLayout<0>::kSmemBytes, s, table,
-                      n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
-  return launch_dyn(gemm_tc_kernel<1>, grid, kTcThreads, TcLayout<1>::kSmemBytes, s, table,
-                    n_gemm, tile_map, a, n_a, b, n_b, c, n_c);
+                           int64_t n_a, const double* b, int64_t n_b, double* c, int64_t n_c,
+                           void* work, int64_t work_bytes, int64_t n_counters) {
+  const int64_t a_chunks = n_counters & 0xFFFFFFFFll, b_chunks = (n_counters >> 32) & 0xFFFFFFFFll;
+  if ((a_chunks + b_chunks) * kT2Slab > work_bytes || ((a_chunks + b_chunks) > 0 && !work))
+    return cudaErrorInvalidValue;
+  if (kind == TNB_TILE_TC_TF32)
+    return launch_tc_mode<0>(grid, s, table, n_gemm, tile_map, a, n_a, b, n_b, c, n_c, work,
+                             work_bytes, a_chunks, b_chunks);
+  return launch_tc_mode<1>(grid, s, table, n_gemm, tile_map, a, n_a, b, n_b, c, n_c, work,
+                           work_bytes, a_chunks, b_chunks);
 }
+
 }  // namespace tnb

@@ -32,6 +32,9 @@ MAX_RANK = 8
 TILE_64, TILE_32, TILE_SKINNY, TILE_TC_TF32, TILE_TC_3XBF16, TILE_WIDE = 0, 1, 2, 3, 4, 5
 TC_KINDS = {"tf32": TILE_TC_TF32, "3xbf16": TILE_TC_3XBF16}
 SKINNY_ROWS, SKINNY_MAX = 256, 16
+# tensor-core tiles: 128 x 128 outputs, K slabs of 32; each packed operand slab (one
+# 128-row x 32 chunk, every part: BF16 hi + lo, or one TF32) is 16 KB
+TC_TILE, TC_BK, TC_SLAB_BYTES = 128, 32, 16384
 N_SM = 148
 
 
@@ -420,6 +423,15 @@ class GemmTable:
         self._work: dict = {}
         self._private = False
 
+    @property
+    def launches(self) -> int:
+        """Kernels one ``run`` launches: tensor-core tables pack A and B first."""
+        if self.n_gemm == 0:
+            return 0
+        if self.kind in (TILE_TC_TF32, TILE_TC_3XBF16):
+            return 1 + int((self.n_counters & 0xFFFFFFFF) > 0) + int((self.n_counters >> 32) > 0)
+        return 1
+
     def private(self) -> GemmTable:
         """The same table with a split-K work buffer of its own (a compiled program's
         copy, so that programs sharing a cached table can run on different streams)."""
@@ -471,8 +483,8 @@ def _tiles(M, N, kind):
     if kind == TILE_WIDE:
         return (N + SKINNY_ROWS - 1) // SKINNY_ROWS, 1
     if kind in (TILE_TC_TF32, TILE_TC_3XBF16):
-        tn = (N + 63) // 64
-        return ((M + 127) // 128) * tn, tn
+        tn = (N + TC_TILE - 1) // TC_TILE
+        return ((M + TC_TILE - 1) // TC_TILE) * tn, tn
     t = 64 if kind == TILE_64 else 32
     tn = (N + t - 1) // t
     return ((M + t - 1) // t) * tn, tn
@@ -616,7 +628,7 @@ class GemmGroup:
         self.flops = sum(p.flops for p in self.parts)
         self.tiles = sum(p.tiles for p in self.parts)
         self.n_gemm = sum(p.n_gemm for p in self.parts)
-        self.launches = len(self.parts)
+        self.launches = sum(p.launches for p in self.parts)
 
     @property
     def table(self):
@@ -669,6 +681,20 @@ def make_gemm(products, kind: int | None = None, split_k: bool = True) -> GemmTa
         tile += out_tiles * S
         flops += 2 * M * N * K
     arr = np.array(rows, dtype=np.int64).reshape(-1, GEMM_W)
+    if kind in (TILE_TC_TF32, TILE_TC_3XBF16):
+        # operand packing: per row the first A slab (M tiles x K slabs) and B slab (N tiles
+        # x K slabs) in the packed work buffer; the counts travel in n_counters
+        a_tot = b_tot = 0
+        for row in arr:
+            M, N, K = int(row[0]), int(row[1]), int(row[2])
+            ks = (K + TC_BK - 1) // TC_BK
+            row[12], row[13] = a_tot, b_tot
+            a_tot += ((M + TC_TILE - 1) // TC_TILE) * ks
+            b_tot += ((N + TC_TILE - 1) // TC_TILE) * ks
+        t = GemmTable(arr, tile, flops, kind)
+        t.n_counters = a_tot | (b_tot << 32)
+        t.work_bytes = (a_tot + b_tot) * TC_SLAB_BYTES
+        return t
     return GemmTable(arr, tile, flops, kind, n_cnt, n_parts)
 
 
