@@ -202,6 +202,56 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "src": "fallback"}
 
 
+def gemm_probe(n: int, dgemm: float | None, reps: int = 5) -> dict:
+    """The grouped GEMM's tile kinds on one n x n x n product (each operand n^2 doubles,
+    128 MiB at n = 4096, so nothing stays in L2 between repetitions): FP64 64 x 64 tiles
+    against cuBLAS DGEMM, the tensor-core kinds against the measured dense BF16 peak
+    (3xBF16 issues three BF16 products per product, TF32 runs at half the BF16 rate).
+    The tensor-core times include packing the operands (two of the three launches)."""
+    import torch
+
+    from tenet import _exec
+
+    p = ROOT / "MEASURED_PEAKS.json"
+    bf16 = json.loads(p.read_text()).get("bf16_tflops") if p.exists() else None
+    src = "MEASURED_PEAKS.json bf16_tflops (measured)" if bf16 else "fallback 1590"
+    bf16 = bf16 or 1590.0
+    g = torch.Generator(device="cuda").manual_seed(5)
+    a = torch.randn(n * n, dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn(n * n, dtype=torch.float64, device="cuda", generator=g)
+    prod = [(n, n, n, 0, n, 0, n, 0, n)]
+    out = {"workload": f"one {n}^3 FP64-in/FP64-out product", "flops": 2 * n ** 3,
+           "peak_bf16_tflops": bf16, "peak_source": src, "dgemm_tflops": dgemm}
+    ref = None
+    for name, kind in (("f64_64x64", _exec.TILE_64), ("tf32", _exec.TILE_TC_TF32),
+                       ("3xbf16", _exec.TILE_TC_3XBF16)):
+        t = _exec.make_gemm(prod, kind, split_k=False)
+        c = torch.empty(n * n, dtype=torch.float64, device="cuda")
+        t.run(a, b, c)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            t.run(a, b, c)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = float(np.median(times))
+        tf = 2 * n ** 3 / (ms * 1e-3) / 1e12
+        d = {"ms": ms, "tflops": tf, "launches": t.launches}
+        if ref is None:
+            ref = c.clone()
+            d["frac_of_cublas_dgemm"] = tf / dgemm if dgemm else None
+        else:
+            d["rel_error_vs_f64"] = float((c - ref).norm() / ref.norm())
+            mult = 3 if name == "3xbf16" else 2
+            d["bf16_equivalent_tflops"] = tf * mult
+            d["frac_of_bf16_peak"] = tf * mult / bf16
+        out[name] = d
+    return out
+
+
 def measure_dgemm_peak(torch) -> float:
     """cuBLAS DGEMM throughput on this GPU (TFLOP/s), the FP64 roofline denominator."""
     n = 8192
@@ -709,6 +759,7 @@ def run_tenet(args) -> None:
         env3 = batched_env_updates(args) if args.config3_n > 0 else None
         bmv = (batched_matvecs(args, eager_ms["eager_ops"], ms / args.steps)
                if args.batch_n > 0 else None)
+        gprobe = gemm_probe(args.gemm_n, dgemm) if args.gemm_n > 0 else None
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -732,6 +783,7 @@ def run_tenet(args) -> None:
             "serving": solves,
             "batched_env_updates": env3,
             "batched_matvecs": bmv,
+            "gemm_probe": gprobe,
             "roofline": roofline,
             "cpu_baseline": base,
             "clocks": clk.summary(),
@@ -760,12 +812,20 @@ def main() -> None:
                     help="members of the batched U1xU1xfZ2 environment update (0: skip)")
     ap.add_argument("--serve-full", action="store_true",
                     help="draw the requests from the full L / chi distribution")
+    ap.add_argument("--gemm-n", type=int, default=4096,
+                    help="size of the square product of the GEMM tile-kind probe (0: skip)")
+    ap.add_argument("--profile-gemm", type=int, default=0,
+                    help="only run each GEMM tile kind once on this square size (for "
+                         "profiling the tensor-core kernels) and exit")
     ap.add_argument("--profile-config3", action="store_true",
                     help="only run the batched environment update a few times (a small, "
                          "fixed launch sequence for profiling its kernels) and exit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile_gemm > 0:
+        gemm_probe(args.profile_gemm, None, reps=1)
+        return
     if args.profile_config3:
         import torch
 

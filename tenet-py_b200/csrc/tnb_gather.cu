@@ -22,7 +22,7 @@ namespace tnb {
 
 // Four CTAs per SM: the bound keeps the kernel at 56 registers (no spills), twice the
 // warps of an unbounded build, for more loads in flight on this latency-bound work.
-__global__ void __launch_bounds__(kGatherThreads, 4)
+__global__ void __launch_bounds__(kGatherThreads, 3)
 gather_kernel(const GatherArgs g) {
   __shared__ GatherSmem sm;
   pdl_launch_dependents();

@@ -16,20 +16,39 @@
 //   TNB_TILE_WIDE   one thread per output column, for products with M <= 16 and K <= 16
 //                   (an MPO tensor as the left operand: a few rows, a long N)
 // The plain form computes in FP64 on the DFMA pipe; micro-tile rows/cols are strided so
-// shared-memory reads are conflict-free, and the next K slab is prefetched into
-// registers while the current one is consumed.
+// shared-memory reads are conflict-free, and the next K slabs stream into shared memory
+// with cp.async (three ahead for 32 x 32 tiles, two for 64 x 64) while one is consumed.
 #include <string>
 
 #include "tnb_stages.cuh"
 
 namespace tnb {
 
+// K slabs in shared memory per tile shape: 32 x 32 keeps three in flight (33 KB, six CTAs
+// per SM), 64 x 64 two (50 KB, dynamic shared memory).
+template <int TM>
+constexpr int kGemmStages = TM == 64 ? 3 : 4;
+
 template <int TM, int TN>
 __global__ void __launch_bounds__((TM / 4) * (TN / 4), (TM == 64 ? 1 : 6))
 gemm_f64_kernel(const GemmArgs g) {
-  __shared__ GemmSmem<TM, TN> sm;
+  extern __shared__ __align__(16) uint8_t gemm_smem[];
+  auto& sm = *reinterpret_cast<GemmSmem<TM, TN, kGemmStages<TM>>*>(gemm_smem);
   pdl_launch_dependents();
   gemm_tile<TM, TN, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
+}
+
+template <int TM, int TN>
+cudaError_t launch_gemm_f64(unsigned grid, cudaStream_t s, const GemmArgs& g) {
+  constexpr size_t kSmem = sizeof(GemmSmem<TM, TN, kGemmStages<TM>>);
+  static bool opted = false;
+  if (!opted) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        gemm_f64_kernel<TM, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
+  return launch_dyn(gemm_f64_kernel<TM, TN>, grid, (TM / 4) * (TN / 4), kSmem, s, g);
 }
 
 __global__ void __launch_bounds__(kSkinnyThreads, 4)
@@ -78,10 +97,10 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
                         n_counters, parts, n_parts};
   switch (tile_kind) {
     case TNB_TILE_64:
-      e = tnb::launch(tnb::gemm_f64_kernel<64, 64>, grid, 256, s, g);
+      e = tnb::launch_gemm_f64<64, 64>(grid, s, g);
       break;
     case TNB_TILE_32:
-      e = tnb::launch(tnb::gemm_f64_kernel<32, 32>, grid, 64, s, g);
+      e = tnb::launch_gemm_f64<32, 32>(grid, s, g);
       break;
     case TNB_TILE_SKINNY:
       e = tnb::launch(tnb::gemm_f64_skinny_kernel, grid, tnb::kSkinnyThreads, s, g);

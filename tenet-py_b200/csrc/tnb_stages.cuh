@@ -65,6 +65,101 @@ __device__ __forceinline__ double load_data(const double* p) {
   }
 }
 
+struct GatherElems {
+  const double* __restrict__ src;
+  double* __restrict__ dst;
+  int64_t n_src, n_dst, dst_off, base, lim, t0, t1;
+  bool staged;
+};
+
+// The KE elements base + tid + k * NT (k < KE) of one segment.  Offsets first, then the
+// terms in table order, 4 / KE at a time: the four loads (terms x elements) are
+// independent and in flight together, and each element still sums its terms in table
+// order with one FMA chain.
+template <int KE, int NT, bool kFused>
+__device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSmem& sm,
+                                             const GatherElems& ge, int tid, int rank,
+                                             const uint32_t* dims, const int64_t* dstr,
+                                             const int64_t* rstr, const int64_t* cstr) {
+  int64_t roff[KE], coff[KE], doff[KE];
+  bool live[KE];
+  double acc[KE];
+#pragma unroll
+  for (int k = 0; k < KE; ++k) {
+    const int64_t e = ge.base + tid + k * NT;
+    live[k] = e < ge.lim;
+    uint32_t rem = live[k] ? static_cast<uint32_t>(e) : 0u;
+    int64_t dd = 0, rr = 0, cc = 0;
+#pragma unroll
+    for (int d = TNB_MAX_RANK - 1; d >= 0; --d) {
+      if (d < rank) {
+        const uint32_t j = rem % dims[d];
+        rem /= dims[d];
+        dd += static_cast<int64_t>(j) * dstr[d];
+        rr += static_cast<int64_t>(j) * rstr[d];
+        cc += static_cast<int64_t>(j) * cstr[d];
+      }
+    }
+    roff[k] = rr;
+    coff[k] = cc;
+    doff[k] = ge.dst_off + dd;
+    acc[k] = 0.0;
+  }
+  bool bad = false;
+  auto term = [&](int64_t t, int64_t& ts, int64_t& tl, double& cf) {
+    if (ge.staged) {
+      ts = sm.t_src[t - ge.t0];
+      tl = sm.t_ld[t - ge.t0];
+      cf = sm.t_cf[t - ge.t0];
+    } else {
+      ts = __ldg(g.term_src + t);
+      tl = __ldg(g.term_ld + t);
+      cf = __ldg(g.term_coeff + t);
+    }
+  };
+  auto fetch = [&](int64_t ts, int64_t tl, int k) -> double {
+    const int64_t o = ts + tl * roff[k] + coff[k];
+    const bool ok = live[k] && o >= 0 && o < ge.n_src;
+    bad |= live[k] && !ok;
+    return ok ? load_data<kFused>(ge.src + o) : 0.0;
+  };
+  constexpr int kU = KE >= 4 ? 1 : 4 / KE;  // four loads in flight per thread
+  int64_t t = ge.t0;
+  for (; t + kU <= ge.t1; t += kU) {
+    int64_t ts[kU], tl[kU];
+    double cf[kU], v[kU][KE];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) term(t + u, ts[u], tl[u], cf[u]);
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+#pragma unroll
+      for (int k = 0; k < KE; ++k) v[u][k] = fetch(ts[u], tl[u], k);
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+#pragma unroll
+      for (int k = 0; k < KE; ++k) acc[k] = fma(cf[u], v[u][k], acc[k]);
+  }
+  for (; t < ge.t1; ++t) {
+    int64_t ts, tl;
+    double cf, v[KE];
+    term(t, ts, tl, cf);
+#pragma unroll
+    for (int k = 0; k < KE; ++k) v[k] = fetch(ts, tl, k);
+#pragma unroll
+    for (int k = 0; k < KE; ++k) acc[k] = fma(cf, v[k], acc[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < KE; ++k) {
+    if (!live[k]) continue;
+    if (doff[k] < 0 || doff[k] >= ge.n_dst) {
+      bad = true;
+      continue;
+    }
+    ge.dst[doff[k]] = acc[k];
+  }
+  if (bad) raise_bounds();
+}
+
 // One TNB_GATHER_CHUNK-element chunk of a gather by a group of NT threads (the whole
 // CTA standalone; a quarter of it in the persistent kernel); `tid` is the thread's index
 // within the group.
@@ -124,39 +219,13 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   }
   const int64_t base = (chunk - row[6]) * ce;
   const int64_t lim = min(size, base + ce);
-#pragma unroll
-  for (int k = 0; k < kEpt; ++k) {
-    const int64_t e = base + tid + k * NT;
-    if (e >= lim) break;
-    uint32_t rem = static_cast<uint32_t>(e);
-    int64_t doff = 0, roff = 0, coff = 0;
-#pragma unroll
-    for (int d = TNB_MAX_RANK - 1; d >= 0; --d) {
-      if (d < rank) {
-        const uint32_t j = rem % dims[d];
-        rem /= dims[d];
-        doff += static_cast<int64_t>(j) * dstr[d];
-        roff += static_cast<int64_t>(j) * rstr[d];
-        coff += static_cast<int64_t>(j) * cstr[d];
-      }
-    }
-    double acc = 0.0;
-    if (staged) {
-      for (int t = 0; t < nt; ++t) {
-        const int64_t o = sm.t_src[t] + sm.t_ld[t] * roff + coff;
-        if (o < 0 || o >= n_src) { raise_bounds(); continue; }
-        acc = fma(sm.t_cf[t], load_data<kFused>(src + o), acc);
-      }
-    } else {
-      for (int64_t t = t0; t < t1; ++t) {
-        const int64_t o = __ldg(g.term_src + t) + __ldg(g.term_ld + t) * roff + coff;
-        if (o < 0 || o >= n_src) { raise_bounds(); continue; }
-        acc = fma(__ldg(g.term_coeff + t), load_data<kFused>(src + o), acc);
-      }
-    }
-    const int64_t w = dst_off + doff;
-    if (w < 0 || w >= n_dst) { raise_bounds(); continue; }
-    dst[w] = acc;
+  const GatherElems ge{src, dst, n_src, n_dst, dst_off, base, lim, t0, t1, staged};
+  if (ce <= NT) {
+    gather_elems<1, NT, kFused>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
+  } else if (ce <= 2 * NT) {
+    gather_elems<(2 <= kEpt ? 2 : kEpt), NT, kFused>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
+  } else {
+    gather_elems<kEpt, NT, kFused>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
   }
 }
 
@@ -215,20 +284,39 @@ __device__ __forceinline__ bool footprint_ok(const GemmRow& r, int64_t n_a, int6
   return !bad;
 }
 
-template <int TM, int TN>
+// S K slabs of both operands.  The persistent chain kernel uses S = 2 with the next slab
+// prefetched through registers (its sources may have been written earlier in the same
+// launch and are read through L2); a standalone launch keeps S - 1 slabs in flight with
+// cp.async (operands are fixed for the launch), which the DFMA loop needs at the few warps
+// per SM that small coupled sectors give.
+template <int TM, int TN, int S = 2>
 struct GemmSmem {
-  double As[2][kBk][TM + 1];
-  double Bs[2][kBk][TN];
+  double As[S][kBk][TM + 1];
+  double Bs[S][kBk][TN];
   GemmRow row;
   int ok;
   int last;
 };
 
+__device__ __forceinline__ void cp_async8(void* smem_dst, const double* src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+               :: "r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst))), "l"(src),
+                  "r"(ok ? 8u : 0u) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
+
 // One TM x TN output tile (or one K split of it) by the NT = TM*TN/16 threads of a group;
 // `tid` is the thread's index within the group.
-template <int TM, int TN, bool kFused, class Sync>
-__device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN>& sm, int tid,
+template <int TM, int TN, bool kFused, class Sync, int S>
+__device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN, S>& sm, int tid,
                           Sync sync) {
+  static_assert(!kFused || S == 2, "the persistent kernel double-buffers through registers");
   constexpr int TX = TN / 4, TY = TM / 4, NT = TX * TY;
   constexpr int LA = (TM * kBk) / NT, LB = (TN * kBk) / NT;
   if constexpr (kFused) sync();  // the previous item's readers are done with sm
@@ -265,6 +353,23 @@ __device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN>& sm,
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
 
+  auto slab_fma = [&](int buf) {
+#pragma unroll
+    for (int k = 0; k < kBk; ++k) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = sm.As[buf][k][ty + TY * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = sm.Bs[buf][k][tx + TX * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  };
+  const int64_t nk = ke > kb ? (ke - kb + kBk - 1) / kBk : 0;
+
+  if constexpr (kFused) {
   double ra[LA], rb[LB];
   auto load_slab = [&](int64_t k0) {
 #pragma unroll
@@ -295,7 +400,6 @@ __device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN>& sm,
     }
   };
 
-  const int64_t nk = ke > kb ? (ke - kb + kBk - 1) / kBk : 0;
   if (nk > 0) {
     load_slab(kb);
     store_slab(0);
@@ -304,20 +408,47 @@ __device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN>& sm,
   for (int64_t s = 0; s < nk; ++s) {
     const int cur = static_cast<int>(s & 1);
     if (s + 1 < nk) load_slab(kb + (s + 1) * kBk);
-#pragma unroll
-    for (int k = 0; k < kBk; ++k) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = sm.As[cur][k][ty + TY * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = sm.Bs[cur][k][tx + TX * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-    }
+    slab_fma(cur);
     if (s + 1 < nk) store_slab(cur ^ 1);
     sync();
+  }
+  } else {
+  // slab s lands in buffer s % S; S - 1 slabs are in flight while one is consumed
+  const double* const a0 = a + r.aoff;
+  const double* const b0 = b + r.boff;
+  auto issue = [&](int64_t s) {
+    const int buf = static_cast<int>(s % S);
+    const int64_t k0 = kb + s * kBk;
+#pragma unroll
+    for (int q = 0; q < LA; ++q) {
+      const int idx = tid + q * NT;
+      const int am = idx / kBk, ak = idx % kBk;
+      const int64_t gm = m0 + am, gk = k0 + ak;
+      const bool ok = gm < r.M && gk < ke;
+      cp_async8(&sm.As[buf][ak][am], ok ? a0 + gm * r.lda + gk : a0, ok);
+    }
+#pragma unroll
+    for (int q = 0; q < LB; ++q) {
+      const int idx = tid + q * NT;
+      const int bk = idx / TN, bn = idx % TN;
+      const int64_t gk = k0 + bk, gn = n0 + bn;
+      const bool ok = gk < ke && gn < r.N;
+      cp_async8(&sm.Bs[buf][bk][bn], ok ? b0 + gk * r.ldb + gn : b0, ok);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < S - 1; ++s) {
+    if (s < nk) issue(s);
+    cp_async_commit();
+  }
+  for (int64_t s = 0; s < nk; ++s) {
+    cp_async_wait<S - 2>();  // this thread's copies of slab s have landed
+    sync();                  // everyone's have, and slab s - 1 is consumed
+    if (s + S - 1 < nk) issue(s + S - 1);
+    cp_async_commit();
+    slab_fma(static_cast<int>(s % S));
+  }
+  cp_async_wait<0>();
   }
 
   if (r.splits > 1) {

@@ -369,13 +369,20 @@ class GatherTable:
             _LOG.end("block_gather", mark, self.bytes_moved)
 
 
-def chunk_size(elems: int) -> int:
-    """Elements per gather chunk for a table of ``elems`` destination elements: the largest
-    of 1024, 512, 256 that still gives about four CTAs per SM -- small chunks put more
-    CTAs (more independent load chains) on a small, latency-bound table, large chunks
-    keep a big, bandwidth-bound one at four elements per thread."""
-    for ce in (CHUNK, CHUNK // 2, CHUNK // 4):
-        if elems >= ce * 4 * N_SM:
+#: resident gather CTAs per SM (the kernel's launch bounds)
+GATHER_CTAS_PER_SM = 3
+
+
+def chunk_size(sizes) -> int:
+    """Elements per gather chunk for a table whose segments hold ``sizes`` elements: the
+    largest of 1024, 512, 256 whose chunks still fill one wave of resident CTAs.  Every
+    CTA pays a chain of dependent loads (chunk map, row, terms) before its data loads, so
+    a small, latency-bound table wants one wave of CTAs with two or four elements per
+    thread rather than two waves of one; a big table keeps four elements per thread."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    wave = GATHER_CTAS_PER_SM * N_SM
+    for ce in (CHUNK, CHUNK // 2):
+        if int(((sizes + ce - 1) // ce).sum()) >= wave:
             return ce
     return CHUNK // 4
 
@@ -393,7 +400,7 @@ def make_gather(*parts) -> GatherTable:
         tld.append(np.asarray(tl, np.int64))
         base += len(ts)
     seg = np.concatenate(rows) if rows else np.zeros((0, SEG_W), np.int64)
-    seg[:, 7] = chunk_size(int(seg[:, 1].sum()) if len(seg) else 0)
+    seg[:, 7] = chunk_size(seg[:, 1])
     per = (seg[:, 1] + seg[:, 7] - 1) // seg[:, 7]
     seg[:, 6] = np.cumsum(per) - per
     return GatherTable(seg, np.concatenate(tsrc) if tsrc else np.zeros(0, np.int64),

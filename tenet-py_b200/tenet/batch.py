@@ -302,28 +302,34 @@ class BatchedHeff2:
         for lk, name in zip(tmpl.links, tmpl.operand_names):
             op = operands[name]
             m = 1 if op.shared else n
-            a_g = _batch_gather(lk.a_gather, n, (src_stride, 0), (lk.a_size, 0))
+            # a link whose products read their source in place reads each member's source
+            a_g = None if lk.a_direct else _batch_gather(lk.a_gather, n, (src_stride, 0),
+                                                         (lk.a_size, 0))
             b_g = _batch_gather(lk.b_gather, m, (layout(op.structure).size, 0), (lk.b_size, 0))
             gemm = _exec.GemmGroup(
-                _batch_products(lk.gemm.products, n, lk.a_size, 0 if op.shared else lk.b_size,
-                                lk.c_size), precision, tc_min_flops, tuned=tuned)
+                _batch_products(lk.gemm.products, n, src_stride if lk.a_direct else lk.a_size,
+                                0 if op.shared else lk.b_size, lk.c_size),
+                precision, tc_min_flops, tuned=tuned)
             bufs = (torch.empty(max(1, n * lk.a_size), **f64),
                     torch.empty(max(1, m * lk.b_size), **f64),
                     torch.empty(max(1, n * lk.c_size), **f64))
             if b_g is not None:
                 b_g.run(op.arena.reshape(-1), bufs[1])
-            self.links.append((a_g, gemm, bufs, op))
+            self.links.append((a_g, gemm, bufs, op, lk.a_direct))
             src_stride = lk.c_size
         self.out_gather = _batch_gather(tmpl.out_gather, n, (src_stride, 0), (self.out_size, 0))
-        self.flops = sum(g.flops for _, g, _, _ in self.links)
+        self.flops = sum(lk[1].flops for lk in self.links)
 
     def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         """``out[k] = H_k x[k]`` for the ``(n, size)`` arenas ``x`` and ``out``."""
         src = x.reshape(-1)
-        for a_g, gemm, (ab, bb, cb), _ in self.links:
-            if a_g is not None:
-                a_g.run(src, ab)
-            gemm.run(ab, bb, cb)
+        for a_g, gemm, (ab, bb, cb), _, direct in self.links:
+            if direct:
+                gemm.run(src, bb, cb)
+            else:
+                if a_g is not None:
+                    a_g.run(src, ab)
+                gemm.run(ab, bb, cb)
             src = cb
         if self.out_gather is not None:
             self.out_gather.run(src, out.reshape(-1))

@@ -16,11 +16,14 @@ during a Lanczos solve (an environment or an MPO site).  In the reference every 
 * every buffer is allocated once, so ``run`` is a fixed launch sequence that a CUDA
   graph captures and replays.
 
-For ``heff2`` that is 5 gathers and 4 grouped GEMMs per matvec.
+For ``heff2`` that is 5 gathers and 4 grouped GEMMs per matvec, and 4 gathers in the
+FP64 form: the first link's A gather only permutes whole rows of the input's blocks, so
+its products read the input in place (``_direct_products``).
 """
 
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 from tenet import _exec
@@ -45,6 +48,50 @@ class _StructureOnly:
 
 def _identity_plan(s: TensorStructure):
     return s, tuple(range(s.ndim)), tuple((i, i, 1.0) for i in range(s.num_blocks))
+
+
+def _direct_products(g, products):
+    """The link's products reading its source in place, or None.
+
+    When the A gather only moves whole rows of the coupled-sector matrices -- every
+    segment a contiguous run (rank 1, unit strides) copied with one term of coefficient 1,
+    covering complete rows of one product's A -- the gather is a row permutation, and a
+    product whose A rows come from several runs is the same product split by rows: one
+    product per run (runs contiguous in the source merged), A read from the source where
+    the run lies, C rows where they were.  Every C element keeps its FMA chain over K."""
+    if g is None or g.n_seg == 0:
+        return None
+    seg = g.seg
+    t0 = seg[:, 3]
+    single = seg[:, 1] == 1  # a one-element run has no stride
+    if (np.any(seg[:, 2] != 1) or np.any(seg[:, 4] - t0 != 1) or np.any(seg[:, 5] != 0)
+            or np.any((seg[:, 16] != 1) & ~single) or np.any((seg[:, 32] != 1) & ~single)):
+        return None
+    if np.any(g.tcf[t0] != 1.0) or np.any((g.tld[t0] * seg[:, 24] != 0) & ~single):
+        return None
+    runs = sorted(zip(seg[:, 0].tolist(), seg[:, 1].tolist(), g.tsrc[t0].tolist()))
+    out, r = [], 0
+    for M, N, K, ao, lda, bo, ldb, co, ldc in sorted(products, key=lambda p: (p[2] == 0, p[3])):
+        if K == 0:
+            out.append((M, N, K, ao, lda, bo, ldb, co, ldc))
+            continue
+        if lda != K:
+            return None
+        end, pos, mine = ao + M * K, ao, []
+        while r < len(runs) and runs[r][0] < end:
+            d, size, src = runs[r]
+            if d != pos or size % K or d + size > end:
+                return None
+            if mine and mine[-1][2] + mine[-1][1] == src:  # contiguous in the source too
+                mine[-1] = (mine[-1][0], mine[-1][1] + size, mine[-1][2])
+            else:
+                mine.append((d, size, src))
+            pos, r = d + size, r + 1
+        if pos != end:
+            return None
+        for d, size, src in mine:
+            out.append((size // K, N, K, src, K, bo, ldb, co + ((d - ao) // K) * ldc, ldc))
+    return out if r == len(runs) else None
 
 
 class _Link:
@@ -88,9 +135,16 @@ class _Link:
             _exec.gather_rows(src_struct, src_kind, sa2, "matrix", pa, ta, 0, keep_a))
         self.b_gather = _exec.make_gather(
             _exec.gather_rows(b_tensor.structure, "arena", sb2, "matrix", pb, tb, 0, keep_b))
+        self.a_size = ma.size
+        # the FP64 form reads a row-permuting A gather's source in place (the tensor-core
+        # form keeps the packed A: its 128-row tiles would run half empty on split rows)
+        direct = _direct_products(self.a_gather, products) if precision == "f64" else None
+        self.a_direct = direct is not None
+        if self.a_direct:
+            products, self.a_gather, self.a_size = direct, None, 0
         self.gemm = _exec.GemmGroup(products, precision, tc_min_flops)
         self.c_struct = sc
-        self.a_size, self.b_size, self.c_size = ma.size, mb.size, mc.size
+        self.b_size, self.c_size = mb.size, mc.size
         self.b_tensor = b_tensor
 
 
@@ -236,7 +290,7 @@ class ChainProgram:
 
     @property
     def launches(self) -> int:
-        return sum(lk.gemm.launches + 1 for lk in self.links) + 1
+        return sum(lk.gemm.launches + (not lk.a_direct) for lk in self.links) + 1
 
     @property
     def uses_tensor_cores(self) -> bool:
@@ -264,8 +318,11 @@ class ChainProgram:
     def _run_tables(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         src = x
         for lk, ab, bb, cb in zip(self.links, self.a_bufs, self.b_bufs, self.c_bufs):
-            lk.a_gather.run(src, ab)
-            lk.gemm.run(ab, bb, cb)
+            if lk.a_direct:
+                lk.gemm.run(src, bb, cb)
+            else:
+                lk.a_gather.run(src, ab)
+                lk.gemm.run(ab, bb, cb)
             src = cb
         self.out_gather.run(src, out)
         return out

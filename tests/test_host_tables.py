@@ -166,14 +166,20 @@ def test_heff2_chain_program_reproduces_reference(golden_dir):
     ops_ = {k: SimpleNamespace(structure=T[k][0]) for k in ("fl", "w1", "w2", "fr")}
     prog = heff2_program(ops_["fl"], ops_["w1"], ops_["w2"], ops_["fr"], T["aa"][0],
                          allocate=False)
-    assert prog.launches == 9
+    # the first link's A gather permutes whole rows only: its products read the input
+    assert [lk.a_direct for lk in prog.links] == [True, False, False, False]
+    assert prog.launches == 8
     src = T["aa"][1]
     for lk in prog.links:
         name = next(k for k in ("fl", "w1", "w2", "fr") if ops_[k] is lk.b_tensor)
         bbuf = np.full(lk.b_size, np.nan)
         _emulate.gather(lk.b_gather, T[name][1], bbuf)
-        abuf, cbuf = np.full(lk.a_size, np.nan), np.full(lk.c_size, np.nan)
-        _emulate.gather(lk.a_gather, src, abuf)
+        cbuf = np.full(lk.c_size, np.nan)
+        if lk.a_direct:
+            abuf = src
+        else:
+            abuf = np.full(lk.a_size, np.nan)
+            _emulate.gather(lk.a_gather, src, abuf)
         _emulate.gemm(lk.gemm, abuf, bbuf, cbuf)
         src = cbuf
     out = np.full(layout(prog.out_struct).size, np.nan)
