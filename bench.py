@@ -207,7 +207,7 @@ def gemm_probe(n: int, dgemm: float | None, reps: int = 5) -> dict:
     128 MiB at n = 4096, so nothing stays in L2 between repetitions): FP64 64 x 64 tiles
     against cuBLAS DGEMM, the tensor-core kinds against the measured dense BF16 peak
     (3xBF16 issues three BF16 products per product, TF32 runs at half the BF16 rate).
-    The tensor-core times include packing the operands (two of the three launches)."""
+    The tensor-core times include packing the operands (the first of two launches)."""
     import torch
 
     from tenet import _exec

@@ -9,7 +9,7 @@
 //                       BF16 inputs), which keeps about 16 significand bits of every
 //                       operand instead of 8.
 //
-// Three launches per table.  Two pack kernels convert each operand once: every 128-row x
+// Two launches per table.  A pack kernel converts each operand once: every 128-row x
 // 32 slab of A (and of B^T) becomes one 16 KB chunk of the work buffer, already in the
 // canonical K-major, no-swizzle UMMA shared-memory layout (8-row x 16-byte core
 // matrices, LBO = 128 B between the two core matrices of one K step, SBO between 8-row
@@ -111,29 +111,33 @@ __device__ int64_t owner_row(const int64_t* table, int64_t n_gemm, int64_t chunk
   return lo;
 }
 
-// Pack one 128 x 32 slab of A (which == 0: rows = M, read along K) or of B^T (which == 1:
-// rows = N, read along N) into its work-buffer chunk in the UMMA layout.
+// Pack one 128 x 32 slab of A (blocks [0, a_chunks): rows = M, read along K) or of B^T
+// (blocks after them: rows = N, read along N) into its work-buffer chunk in the UMMA
+// layout.  Reads are coalesced along the operand's contiguous dimension; the slab is
+// assembled in shared memory and leaves as 16-byte stores.
 template <int MODE>
 __global__ void __launch_bounds__(kT2Threads)
-tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* __restrict__ src,
-               int64_t n_src, uint8_t* __restrict__ work, int64_t work_bytes, int64_t chunk0,
-               int which) {
+tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* __restrict__ a,
+               int64_t n_a, const double* __restrict__ b, int64_t n_b,
+               uint8_t* __restrict__ work, int64_t work_bytes, int64_t a_chunks) {
   using L = T2Layout<MODE>;
+  __shared__ __align__(16) uint8_t slab[kT2Slab];
   __shared__ T2Row s_row;
   __shared__ int s_ok;
   pdl_launch_dependents();
   const int tid = threadIdx.x;
-  const int64_t chunk = blockIdx.x;
+  const int which = blockIdx.x < a_chunks ? 0 : 1;
+  const int64_t chunk = which == 0 ? blockIdx.x : blockIdx.x - a_chunks;
   if (tid == 0) {
     T2Row r{};
     const int64_t g = owner_row(table, n_gemm, chunk, which);
     bool ok = load_t2row(table, g, r);
     const int64_t rows = which == 0 ? r.M : r.N;
     const int64_t ks = (r.K + kT2Bk - 1) / kT2Bk;
-    ok = ok && ks > 0 && (chunk0 + chunk + 1) * kT2Slab <= work_bytes;
+    ok = ok && ks > 0 && (static_cast<int64_t>(blockIdx.x) + 1) * kT2Slab <= work_bytes;
     if (ok) {  // the row's operand footprint
-      ok = which == 0 ? (r.aoff >= 0 && r.aoff + (r.M - 1) * r.lda + r.K <= n_src)
-                      : (r.boff >= 0 && r.boff + (r.K - 1) * r.ldb + r.N <= n_src);
+      ok = which == 0 ? (r.aoff >= 0 && r.aoff + (r.M - 1) * r.lda + r.K <= n_a)
+                      : (r.boff >= 0 && r.boff + (r.K - 1) * r.ldb + r.N <= n_b);
       ok = ok && rows > 0;
     }
     if (!ok) raise_bounds();
@@ -146,7 +150,6 @@ tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* 
   const int64_t ks = (r.K + kT2Bk - 1) / kT2Bk;
   const int64_t local = chunk - (which == 0 ? r.a_chunk : r.b_chunk);
   const int64_t t0 = (local / ks) * kT2M, k0 = (local % ks) * kT2Bk;
-  uint8_t* dst = work + (chunk0 + chunk) * kT2Slab;
   pdl_wait();  // the operand may be the previous kernel's output
 #pragma unroll 4
   for (int i = 0; i < (kT2M * kT2Bk) / kT2Threads; ++i) {
@@ -157,23 +160,28 @@ tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* 
       rr = idx / kT2Bk;
       kk = idx % kT2Bk;
       const int64_t gm = t0 + rr, gk = k0 + kk;
-      x = (gm < r.M && gk < r.K) ? src[r.aoff + gm * r.lda + gk] : 0.0;
+      x = (gm < r.M && gk < r.K) ? a[r.aoff + gm * r.lda + gk] : 0.0;
     } else {  // B: consecutive threads along N
       kk = idx / kT2N;
       rr = idx % kT2N;
       const int64_t gn = t0 + rr, gk = k0 + kk;
-      x = (gk < r.K && gn < r.N) ? src[r.boff + gk * r.ldb + gn] : 0.0;
+      x = (gk < r.K && gn < r.N) ? b[r.boff + gk * r.ldb + gn] : 0.0;
     }
     const uint32_t off = kmajor(rr, kk, L::kEsz, L::kRowBytes);
     if constexpr (MODE == 0) {
-      *reinterpret_cast<uint32_t*>(dst + off) = to_tf32(x);
+      *reinterpret_cast<uint32_t*>(slab + off) = to_tf32(x);
     } else {
       const __nv_bfloat16 hi = __double2bfloat16(x);
       const __nv_bfloat16 lo = __double2bfloat16(x - static_cast<double>(__bfloat162float(hi)));
-      *reinterpret_cast<__nv_bfloat16*>(dst + off) = hi;
-      *reinterpret_cast<__nv_bfloat16*>(dst + L::kPartBytes + off) = lo;
+      *reinterpret_cast<__nv_bfloat16*>(slab + off) = hi;
+      *reinterpret_cast<__nv_bfloat16*>(slab + L::kPartBytes + off) = lo;
     }
   }
+  __syncthreads();
+  uint4* dst = reinterpret_cast<uint4*>(work + static_cast<int64_t>(blockIdx.x) * kT2Slab);
+  const uint4* from = reinterpret_cast<const uint4*>(slab);
+#pragma unroll
+  for (int i = 0; i < kT2Slab / 16 / kT2Threads; ++i) dst[tid + i * kT2Threads] = from[tid + i * kT2Threads];
 }
 
 __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes,
@@ -312,11 +320,15 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   }
   __syncthreads();
 
-  // epilogue: TMEM -> registers -> FP64 C (zeros when K == 0 or a wait gave up)
+  // epilogue: TMEM -> registers -> shared memory -> FP64 C, 16 columns at a time (zeros
+  // when K == 0 or a wait gave up).  Warp w owns TMEM lanes (tile rows) 32w..32w+31; its
+  // 32 x 16 block is transposed through shared memory (the drained pipeline stages) so
+  // that each store instruction writes two rows' 16 consecutive columns.
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const int64_t row = mtile * kT2M + warp * 32 + lane;
+  const int64_t row0 = mtile * kT2M + warp * 32;
   const int64_t n0 = ntile * kT2N;
   const bool live = ok && nk > 0 && !s_fail;
+  double* const stage = reinterpret_cast<double*>(smem) + warp * (32 * 17);
 #pragma unroll 1
   for (int chunk = 0; chunk < kT2N / 16; ++chunk) {
     uint32_t v[16];
@@ -334,11 +346,16 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
 #pragma unroll
       for (int j = 0; j < 16; ++j) v[j] = 0u;
     }
-    if (ok && row < r.M) {
+    __syncwarp();  // the previous chunk's reads of the stage are done
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int64_t col = n0 + chunk * 16 + j;
-        if (col < r.N) c[r.coff + row * r.ldc + col] = static_cast<double>(__uint_as_float(v[j]));
+    for (int j = 0; j < 16; ++j) stage[lane * 17 + j] = static_cast<double>(__uint_as_float(v[j]));
+    __syncwarp();
+    if (ok) {
+#pragma unroll
+      for (int it = 0; it < 16; ++it) {
+        const int e = it * 32 + lane, rr = e >> 4, cc = e & 15;
+        const int64_t row = row0 + rr, col = n0 + chunk * 16 + cc;
+        if (row < r.M && col < r.N) c[r.coff + row * r.ldc + col] = stage[rr * 17 + cc];
       }
     }
   }
@@ -366,12 +383,9 @@ cudaError_t launch_tc_mode(unsigned grid, cudaStream_t s, const int64_t* table, 
   }
   auto* w = static_cast<uint8_t*>(work);
   cudaError_t e = cudaSuccess;
-  if (a_chunks > 0)
-    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(a_chunks), kT2Threads, s, table,
-               n_gemm, a, n_a, w, work_bytes, int64_t{0}, 0);
-  if (e == cudaSuccess && b_chunks > 0)
-    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(b_chunks), kT2Threads, s, table,
-               n_gemm, b, n_b, w, work_bytes, a_chunks, 1);
+  if (a_chunks + b_chunks > 0)
+    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(a_chunks + b_chunks), kT2Threads, s,
+               table, n_gemm, a, n_a, b, n_b, w, work_bytes, a_chunks);
   if (e == cudaSuccess)
     e = launch_dyn(tc_mma_kernel<MODE>, grid, kT2Threads, L::kSmemBytes, s, table, n_gemm,
                    tile_map, static_cast<const uint8_t*>(w), work_bytes, a_chunks, c, n_c);

@@ -436,7 +436,7 @@ class GemmTable:
         if self.n_gemm == 0:
             return 0
         if self.kind in (TILE_TC_TF32, TILE_TC_3XBF16):
-            return 1 + int((self.n_counters & 0xFFFFFFFF) > 0) + int((self.n_counters >> 32) > 0)
+            return 1 + int(self.n_counters > 0)
         return 1
 
     def private(self) -> GemmTable:
