@@ -640,11 +640,15 @@ def run_tenet(args) -> None:
     lib.tnb_set_pdl(0)
     gm_plain = GraphMatvec(prog)
     lib.tnb_set_pdl(1)
-    # and the persistent one-launch form of the same chain (off by default, see _exec.FUSE)
+    # the persistent one-launch form of the chain (off by default, see _exec.FUSE), and
+    # the six-launch form whose gathers compute the MPO links' products (off by default)
     _exec.FUSE = True
     gm_fused = GraphMatvec(prog)
     _exec.FUSE = False
-    for name, g in (("graph_chain_without_pdl", gm_plain), ("graph_fused_one_launch", gm_fused)):
+    gm_defer = GraphMatvec(heff2_program(fl, w1, w2, fr, aa.structure, defer=True))
+    gm_defer.x.copy_(aa.arena)
+    for name, g in (("graph_chain_without_pdl", gm_plain), ("graph_fused_one_launch", gm_fused),
+                    ("graph_chain_product_gathers", gm_defer)):
         for _ in range(args.warmup):
             g.replay()
         eager_ms[name] = timed(g.replay, args.steps) / args.steps

@@ -90,6 +90,30 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
                      void* stream);
 
 /*
+ * Block gather whose source is a product with a short K, never materialised: the source
+ * is C = A * B over the grouped-GEMM table prod_table (n_prod rows in the TNB_GEMM_WIDTH
+ * layout below, K at most 4).  The segment rows are those of tnb_block_gather, with one
+ * buffer pair (buf = 0); the terms address C by row and column instead of by offset:
+ * term t of an element with row and column sums R and C (as above) reads
+ *   C[m, n] = sum_{k < K} A[a_off + m * lda + k] * B[b_off + k * ldb + n],
+ *   m = term_src[t] + R,  n = term_ld[t] + C,
+ * of product row term_prod[t].  The product is computed where the gather reads it, with
+ * the FMA chain of the FP64 GEMM kernels (from zero, k ascending), so the result is
+ * bit-identical to tnb_grouped_gemm_f64 (any FP64 kind, no split-K) into a buffer
+ * followed by tnb_block_gather over it -- one launch and one round trip of C fewer.  An
+ * element outside its row's M x N block, or an operand access outside A or B, raises
+ * the bounds error and reads 0.  No counterpart in the reference: its MPO links are a
+ * matmul then a repartition (ops/map.py:155-172, ops/repartition.py:458-476).
+ */
+int tnb_block_gather_product(const int64_t* seg_table, int64_t n_seg,
+                             const int32_t* chunk_map, int64_t total_chunks,
+                             const int64_t* term_src, const double* term_coeff,
+                             const int64_t* term_ld, const int64_t* term_prod, int64_t n_term,
+                             const int64_t* prod_table, int64_t n_prod, const double* a,
+                             int64_t n_a, const double* b, int64_t n_b, double* dst,
+                             int64_t n_dst, void* stream);
+
+/*
  * Grouped GEMM descriptor: one row of 16 int64 per product C = A * B (row-major).
  *
  *   [0] M  [1] N  [2] K  [3] a_off  [4] lda  [5] b_off  [6] ldb  [7] c_off  [8] ldc
@@ -265,6 +289,13 @@ int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
                      const int32_t* tile_map, int64_t total_tiles, int32_t tile_kind,
                      const double* a, int64_t n_a, const double* b, int64_t n_b, double* c,
                      int64_t n_c, void* work, int64_t work_bytes, int64_t n_counters);
+int tnb_seq_add_gather_product(tnb_seq* s, const int64_t* seg_table, int64_t n_seg,
+                               const int32_t* chunk_map, int64_t total_chunks,
+                               const int64_t* term_src, const double* term_coeff,
+                               const int64_t* term_ld, const int64_t* term_prod,
+                               int64_t n_term, const int64_t* prod_table, int64_t n_prod,
+                               const double* a, int64_t n_a, const double* b, int64_t n_b,
+                               double* dst, int64_t n_dst);
 int tnb_seq_append(tnb_seq* dst, const tnb_seq* src);
 
 /*

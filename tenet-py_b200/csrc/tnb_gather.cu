@@ -20,13 +20,24 @@
 
 namespace tnb {
 
-// Four CTAs per SM: the bound keeps the kernel at 56 registers (no spills), twice the
-// warps of an unbounded build, for more loads in flight on this latency-bound work.
+// Three CTAs per SM: the bound keeps the kernel under 80 registers with no spills while
+// each thread keeps four loads in flight on this latency-bound work.
 __global__ void __launch_bounds__(kGatherThreads, 3)
 gather_kernel(const GatherArgs g) {
   __shared__ GatherSmem sm;
   pdl_launch_dependents();
   gather_chunk<kGatherThreads, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
+}
+
+// The product-source form: every source element is an element of C = A x B of a GEMM
+// table with K <= 4 (an MPO link), computed where it is read instead of being written by
+// a GEMM launch and read back.  Two CTAs per SM: the product's 2K operand loads per term need
+// the registers.
+__global__ void __launch_bounds__(kGatherThreads, 2)
+gather_product_kernel(const GatherArgs g) {
+  __shared__ GatherSmem sm;
+  pdl_launch_dependents();
+  gather_chunk<kGatherThreads, false, CtaSync, true>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
 }
 
 }  // namespace tnb
@@ -54,4 +65,43 @@ extern "C" int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const i
     return TNB_ECUDA;
   }
   return tnb::check_launch("tnb_block_gather");
+}
+
+extern "C" int tnb_block_gather_product(const int64_t* seg_table, int64_t n_seg,
+                                        const int32_t* chunk_map, int64_t total_chunks,
+                                        const int64_t* term_src, const double* term_coeff,
+                                        const int64_t* term_ld, const int64_t* term_prod,
+                                        int64_t n_term, const int64_t* prod_table,
+                                        int64_t n_prod, const double* a, int64_t n_a,
+                                        const double* b, int64_t n_b, double* dst,
+                                        int64_t n_dst, void* stream) {
+  TNB_REQUIRE(n_seg >= 0 && total_chunks >= 0 && n_term >= 0 && n_prod >= 0 && n_a >= 0 &&
+                  n_b >= 0 && n_dst >= 0,
+              "tnb_block_gather_product: negative size");
+  if (n_seg == 0 || total_chunks == 0) return TNB_OK;
+  TNB_REQUIRE(seg_table != nullptr && chunk_map != nullptr && dst != nullptr,
+              "tnb_block_gather_product: seg_table, chunk_map or dst is null");
+  TNB_REQUIRE(n_term == 0 || (term_src != nullptr && term_coeff != nullptr &&
+                              term_ld != nullptr && term_prod != nullptr),
+              "tnb_block_gather_product: term arrays are null");
+  TNB_REQUIRE(n_prod > 0 && prod_table != nullptr && a != nullptr && b != nullptr,
+              "tnb_block_gather_product: no product table or operands");
+  TNB_REQUIRE(total_chunks < (int64_t(1) << 31),
+              "tnb_block_gather_product: too many chunks for one launch");
+  tnb::GatherArgs g{seg_table, n_seg, chunk_map, term_src, term_coeff, term_ld, n_term,
+                    nullptr, 0, dst, n_dst, nullptr, 0, nullptr, 0};
+  g.term_prod = term_prod;
+  g.prod = prod_table;
+  g.n_prod = n_prod;
+  g.pa = a;
+  g.n_pa = n_a;
+  g.pb = b;
+  g.n_pb = n_b;
+  cudaError_t e = tnb::launch(tnb::gather_product_kernel, static_cast<unsigned>(total_chunks),
+                              tnb::kGatherThreads, tnb::as_stream(stream), g);
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_block_gather_product: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  return tnb::check_launch("tnb_block_gather_product");
 }

@@ -31,6 +31,7 @@ constexpr int64_t kSlotX = 1, kSlotY = 2;
 constexpr int32_t kOpGather = 1;
 constexpr int32_t kOpGemm = 2;
 constexpr int32_t kOpFused = 3;
+constexpr int32_t kOpGatherProduct = 4;
 
 struct FStage {
   int32_t code;
@@ -163,7 +164,7 @@ int fused_grid(int device) {
 struct tnb_seq {
   struct Op {
     int32_t code;
-    int64_t w[16];
+    int64_t w[20];
   };
   std::vector<Op> ops;
   std::vector<tnb::FChain> chains;  // the stages of this sequence's fused ops
@@ -176,6 +177,7 @@ namespace {
 // word positions of the data buffers a replay may substitute
 constexpr int kGatherBufs[] = {8, 10, 12, 14};  // src0, dst0, src1, dst1
 constexpr int kGemmBufs[] = {5, 7, 9};          // a, b, c
+constexpr int kGatherProductBufs[] = {11, 13, 15};  // a, b, dst
 
 inline void* as_ptr(int64_t w) { return reinterpret_cast<void*>(static_cast<intptr_t>(w)); }
 inline int64_t as_word(const void* p) { return static_cast<int64_t>(reinterpret_cast<intptr_t>(p)); }
@@ -189,7 +191,7 @@ int64_t patched(int64_t w, int32_t n_patch, const void* const* from, void* const
 int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* const* to,
            cudaStream_t stream) {
   for (const auto& op : s->ops) {
-    int64_t w[16];
+    int64_t w[20];
     std::memcpy(w, op.w, sizeof(w));
     int rc = TNB_EINVAL;
     if (op.code == kOpGather) {
@@ -208,6 +210,16 @@ int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* con
           w[3], static_cast<int32_t>(w[4]), static_cast<const double*>(as_ptr(w[5])), w[6],
           static_cast<const double*>(as_ptr(w[7])), w[8], static_cast<double*>(as_ptr(w[9])), w[10],
           as_ptr(w[11]), w[12], w[13], stream);
+    } else if (op.code == kOpGatherProduct) {
+      for (int k : kGatherProductBufs) w[k] = patched(w[k], n_patch, from, to);
+      rc = tnb_block_gather_product(
+          static_cast<const int64_t*>(as_ptr(w[0])), w[1], static_cast<const int32_t*>(as_ptr(w[2])),
+          w[3], static_cast<const int64_t*>(as_ptr(w[4])), static_cast<const double*>(as_ptr(w[5])),
+          static_cast<const int64_t*>(as_ptr(w[6])), static_cast<const int64_t*>(as_ptr(w[7])),
+          w[8], static_cast<const int64_t*>(as_ptr(w[9])), w[10],
+          static_cast<const double*>(as_ptr(w[11])), w[12],
+          static_cast<const double*>(as_ptr(w[13])), w[14],
+          static_cast<double*>(as_ptr(w[15])), w[16], stream);
     } else if (op.code == kOpFused) {
       // w[0] chain index, w[1] input, w[2] output, w[3] barrier counters, w[4] grid
       w[1] = patched(w[1], n_patch, from, to);
@@ -294,6 +306,27 @@ extern "C" int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n
   return TNB_OK;
 }
 
+extern "C" int tnb_seq_add_gather_product(tnb_seq* s, const int64_t* seg_table, int64_t n_seg,
+                                          const int32_t* chunk_map, int64_t total_chunks,
+                                          const int64_t* term_src, const double* term_coeff,
+                                          const int64_t* term_ld, const int64_t* term_prod,
+                                          int64_t n_term, const int64_t* prod_table,
+                                          int64_t n_prod, const double* a, int64_t n_a,
+                                          const double* b, int64_t n_b, double* dst,
+                                          int64_t n_dst) {
+  TNB_REQUIRE(s != nullptr, "tnb_seq_add_gather_product: null sequence");
+  TNB_REQUIRE(n_seg >= 0 && total_chunks >= 0 && n_term >= 0 && n_prod >= 0,
+              "tnb_seq_add_gather_product: negative size");
+  using tnb::as_word;
+  tnb_seq::Op op{tnb::kOpGatherProduct,
+                 {as_word(seg_table), n_seg, as_word(chunk_map), total_chunks, as_word(term_src),
+                  as_word(term_coeff), as_word(term_ld), as_word(term_prod), n_term,
+                  as_word(prod_table), n_prod, as_word(a), n_a, as_word(b), n_b,
+                  as_word(dst), n_dst, 0, 0, 0}};
+  s->ops.push_back(op);
+  return TNB_OK;
+}
+
 extern "C" int tnb_seq_append(tnb_seq* dst, const tnb_seq* src) {
   TNB_REQUIRE(dst != nullptr && src != nullptr, "tnb_seq_append: null sequence");
   TNB_REQUIRE(dst != src, "tnb_seq_append: a sequence cannot append itself");
@@ -321,7 +354,8 @@ extern "C" int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* 
     const auto& op = src->ops[i];
     tnb::FStage& st = ch.st[i];
     TNB_REQUIRE(op.code == tnb::kOpGather || op.code == tnb::kOpGemm,
-                "tnb_seq_fuse: only gathers and grouped GEMMs fuse");
+                "tnb_seq_fuse: only gathers and grouped GEMMs fuse (not product-source "
+                "gathers or fused ops)");
     std::memcpy(st.w, op.w, sizeof(st.w));
     st.code = op.code;
     if (op.code == tnb::kOpGather) {

@@ -29,6 +29,8 @@ struct GroupSync {
 // block gather
 
 constexpr int kGatherThreads = 256;
+// longest K of a product-source gather's products (the host defers only those)
+constexpr int kSkinnyMaxK = 4;
 constexpr int kGatherEpt = TNB_GATHER_CHUNK / kGatherThreads;
 constexpr int kStagedTerms = 64;
 
@@ -48,13 +50,51 @@ struct GatherArgs {
   int64_t n_src1;
   double* dst1;
   int64_t n_dst1;
+  // product-source gathers only: the source is C = A x B over the GEMM table `prod`
+  // (TNB_GEMM_WIDTH words per row, K <= 4); term t reads C[term_src[t] + R, term_ld[t] + C]
+  // of row term_prod[t] (R, C the element's row and column strides summed)
+  const int64_t* term_prod;
+  const int64_t* prod;
+  int64_t n_prod;
+  const double* pa;
+  int64_t n_pa;
+  const double* pb;
+  int64_t n_pb;
 };
 
 struct GatherSmem {
   int64_t row[TNB_SEG_WIDTH];
-  int64_t t_src[kStagedTerms], t_ld[kStagedTerms];
+  int64_t t_src[kStagedTerms], t_ld[kStagedTerms], t_prod[kStagedTerms];
   double t_cf[kStagedTerms];
 };
+
+// C[m, n] of a product-source gather, computed as the FP64 GEMM kernels compute it: one
+// FMA chain over k from zero, so the value is bit-identical to the materialised product.
+// An element outside the product row's block, or an operand access outside A or B,
+// raises the bounds error and gives 0.
+__device__ __forceinline__ double product_element(const GatherArgs& g, const int64_t* pr,
+                                                  int64_t m, int64_t n, bool& bad) {
+  const int64_t M = __ldg(pr + 0), N = __ldg(pr + 1), K = __ldg(pr + 2), aoff = __ldg(pr + 3),
+                lda = __ldg(pr + 4), boff = __ldg(pr + 5), ldb = __ldg(pr + 6);
+  const int64_t a0 = aoff + m * lda, b_last = boff + (K - 1) * ldb + n;
+  if (m < 0 || m >= M || n < 0 || n >= N || K > kSkinnyMaxK ||
+      (K > 0 && (aoff < 0 || boff < 0 || lda < 0 || ldb < 0 || a0 + K > g.n_pa ||
+                 b_last >= g.n_pb))) {
+    bad = true;
+    return 0.0;
+  }
+  double av[kSkinnyMaxK], bv[kSkinnyMaxK];
+#pragma unroll
+  for (int k = 0; k < kSkinnyMaxK; ++k) {
+    av[k] = k < K ? __ldg(g.pa + a0 + k) : 0.0;
+    bv[k] = k < K ? __ldg(g.pb + boff + k * ldb + n) : 0.0;
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kSkinnyMaxK; ++k)
+    if (k < K) s = fma(av[k], bv[k], s);
+  return s;
+}
 
 template <bool kFused>
 __device__ __forceinline__ double load_data(const double* p) {
@@ -76,7 +116,7 @@ struct GatherElems {
 // terms in table order, 4 / KE at a time: the four loads (terms x elements) are
 // independent and in flight together, and each element still sums its terms in table
 // order with one FMA chain.
-template <int KE, int NT, bool kFused>
+template <int KE, int NT, bool kFused, bool kProd>
 __device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSmem& sm,
                                              const GatherElems& ge, int tid, int rank,
                                              const uint32_t* dims, const int64_t* dstr,
@@ -106,45 +146,59 @@ __device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSm
     acc[k] = 0.0;
   }
   bool bad = false;
-  auto term = [&](int64_t t, int64_t& ts, int64_t& tl, double& cf) {
+  auto term = [&](int64_t t, int64_t& ts, int64_t& tl, double& cf, int64_t& tp) {
     if (ge.staged) {
       ts = sm.t_src[t - ge.t0];
       tl = sm.t_ld[t - ge.t0];
       cf = sm.t_cf[t - ge.t0];
+      tp = kProd ? sm.t_prod[t - ge.t0] : 0;
     } else {
       ts = __ldg(g.term_src + t);
       tl = __ldg(g.term_ld + t);
       cf = __ldg(g.term_coeff + t);
+      tp = kProd ? __ldg(g.term_prod + t) : 0;
     }
   };
-  auto fetch = [&](int64_t ts, int64_t tl, int k) -> double {
-    const int64_t o = ts + tl * roff[k] + coff[k];
-    const bool ok = live[k] && o >= 0 && o < ge.n_src;
-    bad |= live[k] && !ok;
-    return ok ? load_data<kFused>(ge.src + o) : 0.0;
+  auto fetch = [&](int64_t ts, int64_t tl, int64_t tp, int k) -> double {
+    if constexpr (kProd) {
+      // term_src / term_ld hold the term's first product row and column (m0, n0): the
+      // element is C[m0 + R, n0 + C] of product row tp
+      if (!live[k]) return 0.0;
+      if (tp < 0 || tp >= g.n_prod) {
+        bad = true;
+        return 0.0;
+      }
+      return product_element(g, g.prod + tp * TNB_GEMM_WIDTH, ts + roff[k], tl + coff[k], bad);
+    } else {
+      const int64_t o = ts + tl * roff[k] + coff[k];
+      const bool ok = live[k] && o >= 0 && o < ge.n_src;
+      bad |= live[k] && !ok;
+      return ok ? load_data<kFused>(ge.src + o) : 0.0;
+    }
   };
-  constexpr int kU = KE >= 4 ? 1 : 4 / KE;  // four loads in flight per thread
+  // four loads in flight per thread (a product-source term costs 2K loads: one term)
+  constexpr int kU = kProd ? 1 : (KE >= 4 ? 1 : 4 / KE);
   int64_t t = ge.t0;
   for (; t + kU <= ge.t1; t += kU) {
-    int64_t ts[kU], tl[kU];
+    int64_t ts[kU], tl[kU], tp[kU];
     double cf[kU], v[kU][KE];
 #pragma unroll
-    for (int u = 0; u < kU; ++u) term(t + u, ts[u], tl[u], cf[u]);
+    for (int u = 0; u < kU; ++u) term(t + u, ts[u], tl[u], cf[u], tp[u]);
 #pragma unroll
     for (int u = 0; u < kU; ++u)
 #pragma unroll
-      for (int k = 0; k < KE; ++k) v[u][k] = fetch(ts[u], tl[u], k);
+      for (int k = 0; k < KE; ++k) v[u][k] = fetch(ts[u], tl[u], tp[u], k);
 #pragma unroll
     for (int u = 0; u < kU; ++u)
 #pragma unroll
       for (int k = 0; k < KE; ++k) acc[k] = fma(cf[u], v[u][k], acc[k]);
   }
   for (; t < ge.t1; ++t) {
-    int64_t ts, tl;
+    int64_t ts, tl, tp;
     double cf, v[KE];
-    term(t, ts, tl, cf);
+    term(t, ts, tl, cf, tp);
 #pragma unroll
-    for (int k = 0; k < KE; ++k) v[k] = fetch(ts, tl, k);
+    for (int k = 0; k < KE; ++k) v[k] = fetch(ts, tl, tp, k);
 #pragma unroll
     for (int k = 0; k < KE; ++k) acc[k] = fma(cf, v[k], acc[k]);
   }
@@ -163,9 +217,10 @@ __device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSm
 // One TNB_GATHER_CHUNK-element chunk of a gather by a group of NT threads (the whole
 // CTA standalone; a quarter of it in the persistent kernel); `tid` is the thread's index
 // within the group.
-template <int NT, bool kFused, class Sync>
+template <int NT, bool kFused, class Sync, bool kProd = false>
 __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm, int tid,
                              Sync sync) {
+  static_assert(!(kFused && kProd), "product-source gathers run standalone only");
   constexpr int kEpt = TNB_GATHER_CHUNK / NT;
   static_assert(NT >= TNB_SEG_WIDTH && NT >= kStagedTerms, "a group stages a row and its terms");
   if constexpr (kFused) sync();  // the previous item's readers are done with sm
@@ -185,9 +240,11 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   const bool second = row[5] != 0;
   const double* __restrict__ src = second ? g.src1 : g.src0;
   double* __restrict__ dst = second ? g.dst1 : g.dst0;
+  // (a product-source gather checks its elements against its product rows instead)
   const int64_t n_src = second ? g.n_src1 : g.n_src0;
   const int64_t n_dst = second ? g.n_dst1 : g.n_dst0;
-  if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || rank > TNB_MAX_RANK) {
+  if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || rank > TNB_MAX_RANK ||
+      (kProd && second)) {
     if (tid == 0) raise_bounds();
     return;
   }
@@ -197,6 +254,7 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
     sm.t_src[tid] = g.term_src[t0 + tid];
     sm.t_ld[tid] = g.term_ld[t0 + tid];
     sm.t_cf[tid] = g.term_coeff[t0 + tid];
+    if constexpr (kProd) sm.t_prod[tid] = g.term_prod[t0 + tid];
   }
   sync();
   if constexpr (!kFused) pdl_wait();  // tables are static; the source may be the previous kernel's output
@@ -221,11 +279,12 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   const int64_t lim = min(size, base + ce);
   const GatherElems ge{src, dst, n_src, n_dst, dst_off, base, lim, t0, t1, staged};
   if (ce <= NT) {
-    gather_elems<1, NT, kFused>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
+    gather_elems<1, NT, kFused, kProd>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
   } else if (ce <= 2 * NT) {
-    gather_elems<(2 <= kEpt ? 2 : kEpt), NT, kFused>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
+    gather_elems<(2 <= kEpt ? 2 : kEpt), NT, kFused, kProd>(g, sm, ge, tid, rank, dims, dstr,
+                                                            rstr, cstr);
   } else {
-    gather_elems<kEpt, NT, kFused>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
+    gather_elems<kEpt, NT, kFused, kProd>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
   }
 }
 

@@ -369,22 +369,127 @@ class GatherTable:
             _LOG.end("block_gather", mark, self.bytes_moved)
 
 
-#: resident gather CTAs per SM (the kernel's launch bounds)
+#: resident gather CTAs per SM (the kernels' launch bounds): plain, product-source
 GATHER_CTAS_PER_SM = 3
+PRODUCT_GATHER_CTAS_PER_SM = 2
 
 
-def chunk_size(sizes) -> int:
+def chunk_size(sizes, ctas_per_sm: int = GATHER_CTAS_PER_SM) -> int:
     """Elements per gather chunk for a table whose segments hold ``sizes`` elements: the
     largest of 1024, 512, 256 whose chunks still fill one wave of resident CTAs.  Every
     CTA pays a chain of dependent loads (chunk map, row, terms) before its data loads, so
     a small, latency-bound table wants one wave of CTAs with two or four elements per
     thread rather than two waves of one; a big table keeps four elements per thread."""
     sizes = np.asarray(sizes, dtype=np.int64)
-    wave = GATHER_CTAS_PER_SM * N_SM
+    wave = ctas_per_sm * N_SM
     for ce in (CHUNK, CHUNK // 2):
         if int(((sizes + ce - 1) // ce).sum()) >= wave:
             return ce
     return CHUNK // 4
+
+
+def _chunked(seg: np.ndarray, ctas_per_sm: int = GATHER_CTAS_PER_SM) -> np.ndarray:
+    """``seg`` with the chunk size (column 7) and chunk prefix sums (column 6) set."""
+    seg = seg.copy()
+    if len(seg):
+        seg[:, 7] = chunk_size(seg[:, 1], ctas_per_sm)
+        per = (seg[:, 1] + seg[:, 7] - 1) // seg[:, 7]
+        seg[:, 6] = np.cumsum(per) - per
+    return seg
+
+
+class ProductGather(GatherTable):
+    """A gather whose source is the product C = A x B of an FP64 GEMM table with K <= 4
+    (an MPO link's products), never materialised: each source element is computed where
+    it is read (``tnb_block_gather_product``), so the GEMM launch and the round trip of C
+    through memory disappear.  ``base`` is the plain gather over a materialised C; term
+    ``t`` reads C[m0[t] + R, n0[t] + C] of product row ``tprod[t]`` (its ``tsrc`` and
+    ``tld`` hold m0 and n0).  Built by ``product_gather``."""
+
+    def __init__(self, base: GatherTable, gemm: "GemmTable", tprod, m0, n0) -> None:
+        super().__init__(_chunked(base.seg, PRODUCT_GATHER_CTAS_PER_SM), m0, base.tcf, n0)
+        self.base, self.gemm = base, gemm
+        self.tprod = np.asarray(tprod, dtype=np.int64)
+
+    @property
+    def bytes_moved(self) -> int:
+        """Algorithmic bytes: every destination element written once and the product's
+        operands read once (A is M x K, B is K x N per product row); the re-reads of an A
+        row for the N columns and the terms that share it hit in cache."""
+        r = self.gemm.table
+        return 8 * (self.elems + int((r[:, 0] * r[:, 2] + r[:, 2] * r[:, 1]).sum()))
+
+    def device_arrays(self):
+        if self._dev is None:
+            self._dev = Uploaded((self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map,
+                                  self.tprod))
+        return self._dev.ready()
+
+    def run(self, a, b, dst) -> None:
+        """``dst`` = the gather of C = A x B (``a``, ``b``: the product's operand buffers)
+        on the current stream."""
+        if self.n_seg == 0:
+            return
+        seg, tsrc, tcf, tld, cmap, tprod = self.device_arrays()
+        table, _ = self.gemm.device_tables()
+        args = (ptr(seg), self.n_seg, ptr(cmap), self.chunks, ptr(tsrc), ptr(tcf), ptr(tld),
+                ptr(tprod), self.n_term, ptr(table), self.gemm.n_gemm, ptr(a), a.numel(),
+                ptr(b), b.numel(), ptr(dst), dst.numel())
+        rec = recording()
+        if rec is not None:
+            _lib.call("tnb_seq_add_gather_product", rec.handle, *args)
+            return
+        mark = _LOG.begin() if _LOG is not None else None
+        _lib.call("tnb_block_gather_product", *args, stream_ptr())
+        if _LOG is not None:
+            _LOG.end("block_gather", mark, self.bytes_moved)
+
+
+#: longest K of a skinny product that a gather computes where it reads it
+PRODUCT_MAX_K = 4
+
+
+def product_gather(g: GatherTable, part):
+    """``g`` (a gather over the C arena of the FP64 GEMM table ``part``) as a
+    ``ProductGather``, or None when it cannot be one: ``part`` is a tensor-core or split-K
+    table or has a product with K > ``PRODUCT_MAX_K``, a row uses the second buffer pair,
+    or a term's window is not a window of one product's M x N block.  Every FP64 kind
+    without split-K sums k ascending from zero in one FMA chain, as the product-source
+    gather does, so the values are bit-identical.
+
+    Term t reads offsets tsrc + tld R + C with R = sum_d j_d rstride_d and C = sum_d j_d
+    cstride_d over the box 0 <= j_d < dims_d.  When tld is the block's ldc and, with
+    tsrc - c_off = m0 ldc + n0, every C stays in [-n0, N - n0) and every R in [-m0, M - m0),
+    the element is exactly C[m0 + R, n0 + C] of that product; R and C are linear over the
+    box, so their extremes follow from the strides' signs."""
+    if (g is None or g.n_seg == 0 or part.n_gemm == 0
+            or part.kind not in (TILE_64, TILE_32, TILE_SKINNY, TILE_WIDE)):
+        return None
+    rows, seg = part.table, g.seg
+    if np.any(rows[:, 2] > PRODUCT_MAX_K) or np.any(rows[:, 12] > 1) or np.any(seg[:, 5] != 0):
+        return None
+    if seg[0, 3] != 0 or seg[-1, 4] != g.n_term or np.any(seg[1:, 3] != seg[:-1, 4]):
+        return None  # terms are not stored row by row
+    owner = np.repeat(np.arange(g.n_seg), seg[:, 4] - seg[:, 3])  # term -> its row
+    rk = seg[owner, 2][:, None]
+    span = np.where(np.arange(8)[None, :] < rk, np.maximum(seg[owner, 8:16] - 1, 0), 0)
+    rs, cs = span * seg[owner, 24:32], span * seg[owner, 32:40]
+    r_lo, r_hi = np.minimum(rs, 0).sum(1), np.maximum(rs, 0).sum(1)
+    c_lo, c_hi = np.minimum(cs, 0).sum(1), np.maximum(cs, 0).sum(1)
+    coff = rows[:, 7]
+    order = np.argsort(coff, kind="stable")
+    pos = np.searchsorted(coff[order], g.tsrc, side="right") - 1
+    if np.any(pos < 0):
+        return None
+    tprod = order[pos]
+    M, N, ldc = rows[tprod, 0], rows[tprod, 1], rows[tprod, 8]
+    if np.any(g.tld != ldc) or np.any(ldc <= 0):
+        return None
+    m0, n0 = np.divmod(g.tsrc - coff[tprod], ldc)
+    if (np.any(m0 + r_lo < 0) or np.any(m0 + r_hi >= M)
+            or np.any(n0 + c_lo < 0) or np.any(n0 + c_hi >= N)):
+        return None
+    return ProductGather(g, part, tprod, m0, n0)
 
 
 def make_gather(*parts) -> GatherTable:
@@ -399,10 +504,7 @@ def make_gather(*parts) -> GatherTable:
         tcf.append(np.asarray(tc, np.float64))
         tld.append(np.asarray(tl, np.int64))
         base += len(ts)
-    seg = np.concatenate(rows) if rows else np.zeros((0, SEG_W), np.int64)
-    seg[:, 7] = chunk_size(seg[:, 1])
-    per = (seg[:, 1] + seg[:, 7] - 1) // seg[:, 7]
-    seg[:, 6] = np.cumsum(per) - per
+    seg = _chunked(np.concatenate(rows) if rows else np.zeros((0, SEG_W), np.int64))
     return GatherTable(seg, np.concatenate(tsrc) if tsrc else np.zeros(0, np.int64),
                        np.concatenate(tcf) if tcf else np.zeros(0),
                        np.concatenate(tld) if tld else np.zeros(0, np.int64))
@@ -460,14 +562,18 @@ class GemmTable:
             self._work[key] = buf
         return buf
 
+    def device_tables(self):
+        """(table, tile_map) on the current device, uploaded on first use."""
+        if self._dev is None:
+            self._dev = Uploaded((self.table, self.tile_map))
+        return self._dev.ready()
+
     def run(self, a, b, c) -> None:
         """Launch on the current stream.  The split-K counters of a private table belong
         to it, so one private table must not run on two streams at once."""
         if self.n_gemm == 0:
             return
-        if self._dev is None:
-            self._dev = Uploaded((self.table, self.tile_map))
-        table, tile_map = self._dev.ready()
+        table, tile_map = self.device_tables()
         work = self.work()
         rec = recording()
         if rec is not None:

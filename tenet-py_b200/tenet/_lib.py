@@ -21,6 +21,8 @@ _i64, _i32, _f64, _vp = ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_
 SIGNATURES = {
     "tnb_block_gather": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
                                 _i64, _vp, _i64, _vp, _i64, _vp]),
+    "tnb_block_gather_product": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp,
+                                        _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
     "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
                                     _i64, _vp, _i64, _i64, _vp]),
     "tnb_dot_work_bytes": (_i64, [_i64]),
@@ -37,6 +39,8 @@ SIGNATURES = {
     "tnb_seq_create": (_i32, [ctypes.POINTER(_vp)]),
     "tnb_seq_destroy": (None, [_vp]),
     "tnb_seq_length": (_i64, [_vp]),
+    "tnb_seq_add_gather_product": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64,
+                                          _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64]),
     "tnb_seq_add_gather": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64,
                                   _vp, _i64, _vp, _i64, _vp, _i64]),
     "tnb_seq_add_gemm": (_i32, [_vp, _vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,

@@ -271,17 +271,29 @@ def heff2(fl: TensorBatch, w1: TensorBatch, w2: TensorBatch, fr: TensorBatch,
     return composed("aPQxs,axB->BPQs", t, fl, bend="a")
 
 
+class _BLink:
+    """One link of ``BatchedHeff2``: its replicated A gather (None when the products read
+    the source in place), GEMM group, buffers, fixed operand, and whether the next gather
+    computes its product (``deferred``)."""
+
+    __slots__ = ("a_g", "gemm", "bufs", "op", "direct", "c_elems", "deferred")
+
+    def __init__(self, a_g, gemm, bufs, op, direct, c_elems) -> None:
+        self.a_g, self.gemm, self.bufs, self.op = a_g, gemm, bufs, op
+        self.direct, self.c_elems, self.deferred = direct, c_elems, False
+
+
 class BatchedHeff2:
-    """The compiled two-site matvec (``program.heff2_program``: 5 gathers, one grouped GEMM
-    launch set per link) for ``n`` members at once: every table of the single-member
-    chain replicated across the batch, every fixed operand packed once (per member, or
-    once for a shared operand), so one ``run`` is about ten launches for all ``n``
-    matvecs.  ``precision`` / ``tc_min_flops`` as in ``ChainProgram``; the FP64 tile kinds
+    """The compiled two-site matvec (``program.heff2_program``: six launches in the FP64
+    form) for ``n`` members at once: every table of the single-member chain replicated
+    across the batch, every fixed operand packed once (per member, or once for a shared
+    operand), so one ``run`` is the same few launches for all ``n`` matvecs.  ``defer`` as
+    in ``ChainProgram``.  ``precision`` / ``tc_min_flops`` as in ``ChainProgram``; the FP64 tile kinds
     of the batched products are autotuned when ``tuned``."""
 
     def __init__(self, fl: TensorBatch, w1: TensorBatch, w2: TensorBatch, fr: TensorBatch,
                  in_struct: TensorStructure, precision: str = "f64", tc_min_flops=None,
-                 tuned: bool = True) -> None:
+                 tuned: bool = True, defer: bool = False) -> None:
         from tenet import program
 
         class _S:
@@ -291,20 +303,23 @@ class BatchedHeff2:
         n = fl.n
         tmpl = program.heff2_program(*(_S(t.structure) for t in (fl, w1, w2, fr)), in_struct,
                                      allocate=False, precision=precision,
-                                     tc_min_flops=tc_min_flops)
+                                     tc_min_flops=tc_min_flops, defer=defer)
         operands = {"fr": fr, "w2": w2, "w1": w1, "fl": fl}
         dev = _exec.device()
         f64 = dict(dtype=torch.float64, device=dev)
         self.n, self.in_struct, self.out_struct = n, in_struct, tmpl.out_struct
         self.in_size, self.out_size = layout(in_struct).size, layout(tmpl.out_struct).size
+        def plain(g):  # the replicated table starts from the materialised-product form
+            return g.base if isinstance(g, _exec.ProductGather) else g
+
         self.links = []
         src_stride = self.in_size
         for lk, name in zip(tmpl.links, tmpl.operand_names):
             op = operands[name]
             m = 1 if op.shared else n
             # a link whose products read their source in place reads each member's source
-            a_g = None if lk.a_direct else _batch_gather(lk.a_gather, n, (src_stride, 0),
-                                                         (lk.a_size, 0))
+            a_g = None if lk.a_direct else _batch_gather(plain(lk.a_gather), n,
+                                                         (src_stride, 0), (lk.a_size, 0))
             b_g = _batch_gather(lk.b_gather, m, (layout(op.structure).size, 0), (lk.b_size, 0))
             gemm = _exec.GemmGroup(
                 _batch_products(lk.gemm.products, n, src_stride if lk.a_direct else lk.a_size,
@@ -315,23 +330,51 @@ class BatchedHeff2:
                     torch.empty(max(1, n * lk.c_size), **f64))
             if b_g is not None:
                 b_g.run(op.arena.reshape(-1), bufs[1])
-            self.links.append((a_g, gemm, bufs, op, lk.a_direct))
+            self.links.append(_BLink(a_g, gemm, bufs, op, lk.a_direct, n * lk.c_size))
             src_stride = lk.c_size
-        self.out_gather = _batch_gather(tmpl.out_gather, n, (src_stride, 0), (self.out_size, 0))
-        self.flops = sum(lk[1].flops for lk in self.links)
+        self.out_gather = _batch_gather(plain(tmpl.out_gather), n, (src_stride, 0),
+                                        (self.out_size, 0))
+        # the links the single-member chain folds into their consumer gathers, replicated
+        for i, lk in enumerate(tmpl.links):
+            bl = self.links[i]
+            if not lk.deferred or len(bl.gemm.parts) != 1:
+                continue
+            last = i + 1 == len(self.links)
+            consumer = self.out_gather if last else self.links[i + 1].a_g
+            pg = _exec.product_gather(consumer, bl.gemm.parts[0])
+            if pg is None:
+                continue
+            bl.deferred = True
+            if last:
+                self.out_gather = pg
+            else:
+                self.links[i + 1].a_g = pg
+        self.flops = sum(bl.gemm.flops for bl in self.links)
+
+    @property
+    def launches(self) -> int:
+        return (sum((0 if bl.deferred else bl.gemm.launches)
+                    + (bl.a_g is not None and bl.a_g.n_seg > 0) for bl in self.links)
+                + (self.out_gather is not None))
 
     def run(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         """``out[k] = H_k x[k]`` for the ``(n, size)`` arenas ``x`` and ``out``."""
-        src = x.reshape(-1)
-        for a_g, gemm, (ab, bb, cb), _, direct in self.links:
-            if direct:
-                gemm.run(src, bb, cb)
+        src, pending = x.reshape(-1), None
+        for bl in self.links:
+            ab, bb, cb = bl.bufs
+            a = src if bl.direct else ab
+            if isinstance(bl.a_g, _exec.ProductGather):
+                bl.a_g.run(*pending, ab)
+            elif bl.a_g is not None:
+                bl.a_g.run(src, ab)
+            if bl.deferred:
+                pending = (a, bb)
             else:
-                if a_g is not None:
-                    a_g.run(src, ab)
-                gemm.run(ab, bb, cb)
+                bl.gemm.run(a, bb, cb)
             src = cb
-        if self.out_gather is not None:
+        if isinstance(self.out_gather, _exec.ProductGather):
+            self.out_gather.run(*pending, out.reshape(-1))
+        elif self.out_gather is not None:
             self.out_gather.run(src, out.reshape(-1))
         return out
 

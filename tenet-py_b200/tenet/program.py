@@ -16,9 +16,11 @@ during a Lanczos solve (an environment or an MPO site).  In the reference every 
 * every buffer is allocated once, so ``run`` is a fixed launch sequence that a CUDA
   graph captures and replays.
 
-For ``heff2`` that is 5 gathers and 4 grouped GEMMs per matvec, and 4 gathers in the
-FP64 form: the first link's A gather only permutes whole rows of the input's blocks, so
-its products read the input in place (``_direct_products``).
+For ``heff2`` that is 5 gathers and 4 grouped GEMMs per matvec, 8 launches in the FP64
+form: the first link's A gather only permutes whole rows of the input's blocks, so its
+products read the input in place (``_direct_products``).  Optionally (``defer``) the two
+MPO links' products (K <= 4) are computed by the gathers that read them
+(``_defer_skinny``): 6 launches, the same bits.
 """
 
 from __future__ import annotations
@@ -140,6 +142,7 @@ class _Link:
         # form keeps the packed A: its 128-row tiles would run half empty on split rows)
         direct = _direct_products(self.a_gather, products) if precision == "f64" else None
         self.a_direct = direct is not None
+        self.deferred = False  # the consumer gather computes this link's skinny product
         if self.a_direct:
             products, self.a_gather, self.a_size = direct, None, 0
         self.gemm = _exec.GemmGroup(products, precision, tc_min_flops)
@@ -152,11 +155,17 @@ class ChainProgram:
     """``y = chain(x)`` for a fixed input structure; see the module docstring."""
 
     def __init__(self, in_struct: TensorStructure, precision: str = "f64",
-                 tc_min_flops: int | None = None) -> None:
+                 tc_min_flops: int | None = None, defer: bool = False) -> None:
         """``precision``: "f64" (the plain FP64 form), or "tf32" / "3xbf16" to run the
         coupled-sector products big enough to be dense contractions (at least
-        ``tc_min_flops``, default ``_exec.TC_MIN_FLOPS``) on the tcgen05 tensor cores."""
+        ``tc_min_flops``, default ``_exec.TC_MIN_FLOPS``) on the tcgen05 tensor cores.
+        ``defer``: let the gather that consumes a short-K link's product compute it where
+        it reads it (``_exec.ProductGather``) instead of launching the GEMM.  Off by
+        default: bit-identical and two launches fewer on heff2, but slower there (65.5
+        against 57.4 us per SU(2) matvec on B200), because each product element is read
+        by 2.4 gather terms on average and is recomputed for each."""
         self.precision = precision
+        self.defer = defer
         self.tc_min_flops = tc_min_flops
         self.in_struct = in_struct
         self.src = (in_struct, "arena")
@@ -216,9 +225,39 @@ class ChainProgram:
         self.out_struct = dst
         self.out_gather = _exec.make_gather(
             _exec.gather_rows(self.src[0], self.src[1], dst, "arena", perm, terms))
+        if self.defer:
+            self._defer_skinny()
         if allocate:
             self.allocate()
         return self
+
+    def _consumer(self, i: int):
+        """The gather that reads link ``i``'s product, or None (a GEMM reads it)."""
+        if i + 1 < len(self.links):
+            nxt = self.links[i + 1]
+            return None if nxt.a_direct else nxt.a_gather
+        return self.out_gather
+
+    def _set_consumer(self, i: int, g) -> None:
+        if i + 1 < len(self.links):
+            self.links[i + 1].a_gather = g
+        else:
+            self.out_gather = g
+
+    def _defer_skinny(self) -> None:
+        """Fold every link whose products all have K <= 4 (the MPO links) into the gather
+        that consumes its product, when that gather's terms each read inside one product
+        block (``_exec.product_gather``): one launch and one round trip of the product
+        fewer per such link, bit-identical results."""
+        for i, lk in enumerate(self.links):
+            parts = lk.gemm.parts
+            consumer = self._consumer(i)
+            if len(parts) != 1 or consumer is None:
+                continue
+            pg = _exec.product_gather(consumer, parts[0])
+            if pg is not None:
+                lk.deferred = True
+                self._set_consumer(i, pg)
 
     def rebind(self, operands: dict) -> ChainProgram:
         """A new program sharing this one's tables, with the fixed operands replaced by
@@ -260,9 +299,10 @@ class ChainProgram:
         with self.seq:
             self._run_tables(self.x_slot, self.y_slot)
         # the same stages as one persistent launch, when they all fuse (no tensor-core
-        # stage, at most the kernel's stage count)
+        # stage, no product-source gather, at most the kernel's stage count)
         self.fused = None
-        if not self.uses_tensor_cores and 0 < len(self.seq) <= FUSED_MAX_STAGES:
+        if (not self.uses_tensor_cores and not any(lk.deferred for lk in self.links)
+                and 0 < len(self.seq) <= FUSED_MAX_STAGES):
             from tenet import _lib
 
             self.barrier = torch.zeros(2, dtype=torch.int32, device=dev)
@@ -290,7 +330,8 @@ class ChainProgram:
 
     @property
     def launches(self) -> int:
-        return sum(lk.gemm.launches + (not lk.a_direct) for lk in self.links) + 1
+        return sum((0 if lk.deferred else lk.gemm.launches) + (not lk.a_direct)
+                   for lk in self.links) + 1
 
     @property
     def uses_tensor_cores(self) -> bool:
@@ -316,15 +357,22 @@ class ChainProgram:
         return self._run_tables(x, out)
 
     def _run_tables(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
-        src = x
+        src, pending = x, None  # pending: the operands of a deferred link's product
         for lk, ab, bb, cb in zip(self.links, self.a_bufs, self.b_bufs, self.c_bufs):
-            if lk.a_direct:
-                lk.gemm.run(src, bb, cb)
-            else:
+            a = src if lk.a_direct else ab
+            if isinstance(lk.a_gather, _exec.ProductGather):
+                lk.a_gather.run(*pending, ab)
+            elif not lk.a_direct:
                 lk.a_gather.run(src, ab)
-                lk.gemm.run(ab, bb, cb)
+            if lk.deferred:
+                pending = (a, bb)
+            else:
+                lk.gemm.run(a, bb, cb)
             src = cb
-        self.out_gather.run(src, out)
+        if isinstance(self.out_gather, _exec.ProductGather):
+            self.out_gather.run(*pending, out)
+        else:
+            self.out_gather.run(src, out)
         return out
 
     def __call__(self, x: SymmetricTensor) -> SymmetricTensor:
@@ -367,7 +415,8 @@ _HEFF_TABLES_MAX = 512
 
 
 def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = True,
-                  precision: str = "f64", tc_min_flops: int | None = None) -> ChainProgram:
+                  precision: str = "f64", tc_min_flops: int | None = None,
+                  defer: bool = False) -> ChainProgram:
     """The site-tensor two-site matvec (``network/env.py:416-432``) as a chain program.
     ``fl``, ``w1``, ``w2``, ``fr`` need only ``.structure`` when ``allocate`` is False.
 
@@ -375,12 +424,12 @@ def heff2_program(fl, w1, w2, fr, in_struct: TensorStructure, allocate: bool = T
     are planned once per such key and shared: a later call with the same structures
     builds a fresh program (own buffers, bound to the given tensors) around them."""
     key = (fl.structure, w1.structure, w2.structure, fr.structure, in_struct, precision,
-           tc_min_flops)
+           tc_min_flops, defer)
     cached = _HEFF_TABLES.get(key)
     if cached is not None:
         return cached.rebind(dict(zip(cached.operand_names, (fr, w2, w1, fl)))) \
             .finish_alloc(allocate)
-    p = ChainProgram(in_struct, precision, tc_min_flops)
+    p = ChainProgram(in_struct, precision, tc_min_flops, defer)
     p.einsum("apqr,rys->apqys", fr)
     p.einsum("apqys,mQqy->apQms", w2, bend="q")
     p.einsum("apQms,xPpm->aPQxs", w1, bend="p")

@@ -27,6 +27,33 @@ def gather(table, src0, dst0, src1=None, dst1=None):
         dsts[buf][doff] = acc
 
 
+def gather_product(table, a, b, dst):
+    """``tnb_block_gather_product``: the gather of C = A x B over ``table.gemm``; term t
+    reads C[tsrc[t] + R, tld[t] + C] of product row ``table.tprod[t]``."""
+    rows = table.gemm.table
+    for row in table.seg:
+        dst_off, size, rank, t0, t1, buf = (int(x) for x in row[:6])
+        assert buf == 0, "a product-source gather has one buffer pair"
+        dims = [int(x) for x in row[8:8 + rank]]
+        dstr, rstr, cstr = (np.array(row[o:o + rank], dtype=np.int64) for o in (16, 24, 32))
+        J = np.indices(dims).reshape(rank, -1)
+        doff = dst_off + (J * dstr[:, None]).sum(0)
+        R = (J * rstr[:, None]).sum(0)
+        C = (J * cstr[:, None]).sum(0)
+        acc = np.zeros(J.shape[1])
+        for t in range(t0, t1):
+            M, N, K, ao, lda, bo, ldb = (int(x) for x in rows[table.tprod[t], :7])
+            m, n = table.tsrc[t] + R, table.tld[t] + C
+            assert m.min() >= 0 and m.max() < M and n.min() >= 0 and n.max() < N, \
+                "term reads outside its product"
+            v = np.zeros(len(m))
+            for k in range(K):
+                v = v + a[ao + m * lda + k] * b[bo + k * ldb + n]
+            acc = acc + table.tcf[t] * v
+        assert doff.min() >= 0 and doff.max() < dst.size, "destination out of bounds"
+        dst[doff] = acc
+
+
 def gemm(table, a, b, c):
     parts = getattr(table, "parts", None)
     if parts is not None:

@@ -83,6 +83,10 @@ def test_batched_heff2_matches_each_member():
     w2 = batch.TensorBatch.broadcast(members[0][2], n)
     out = batch.heff2(fl, w1, w2, fr, aa)
     compiled = batch.BatchedHeff2(fl, w1, w2, fr, aa.structure)(aa)
+    # the MPO links' products computed by the gathers that read them: the same bits
+    deferred = batch.BatchedHeff2(fl, w1, w2, fr, aa.structure, defer=True)
+    assert sum(bl.deferred for bl in deferred.links) == 2
+    assert torch.equal(deferred(aa).arena, compiled.arena)
     for k, (f, _, _, r, a) in enumerate(members):
         want = network.heff2(f, members[0][1], members[0][2], r, a)
         assert out.structure == want.structure == compiled.structure

@@ -471,9 +471,9 @@ def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
     m = json.loads((golden_dir / "heff.json").read_text())
     h = np.load(golden_dir / "heff.npz")
     T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
-    prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
-    assert len(prog.seq) == prog.launches
-    assert prog.fused is not None and len(prog.fused) == 1
+    prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure, defer=True)
+    assert len(prog.seq) == prog.launches == 6
+    assert [lk.deferred for lk in prog.links] == [False, True, True, False]
     x = T["aa"].arena
     y_seq = torch.full_like(prog.y_slot, float("nan"))
     y_py = torch.full_like(prog.y_slot, float("nan"))
@@ -481,6 +481,12 @@ def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
     prog._run_tables(x, y_py)
     assert torch.equal(y_seq, y_py)
     close(y_seq.cpu().numpy(), load(h, m["heff_aa"]).numpy_arena(), 1e-12)
+    # the product-source gathers give the bits of the GEMM-then-gather chain they replace
+    plain = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure, defer=False)
+    assert plain.launches == 8 and not any(lk.deferred for lk in plain.links)
+    y_plain = torch.full_like(prog.y_slot, float("nan"))
+    plain.run(x, y_plain)
+    assert torch.equal(y_plain, y_seq)
     # a sequence appended to itself twice replays both copies
     s2 = _exec.Seq()
     _lib.call("tnb_seq_append", s2.handle, prog.seq.handle)
@@ -543,7 +549,9 @@ def test_j1j2_dmrg_matches_exact_diagonalisation(j2):
 def test_fused_chain_is_bit_identical_to_stage_by_stage(golden_dir):
     """The persistent one-launch chain runs the same tables and arithmetic as the
     stage-by-stage replay: identical bits on the golden heff2 and on the bench workload,
-    repeatedly (its grid barrier and split-K counters return to zero)."""
+    repeatedly (its grid barrier and split-K counters return to zero).  It runs gathers
+    and GEMMs only, so its programs are planned without product-source gathers; the
+    six-launch chain with them gives the same bits."""
     import bench
     from tenet import _exec
     from tenet.program import heff2_program
@@ -553,9 +561,13 @@ def test_fused_chain_is_bit_identical_to_stage_by_stage(golden_dir):
     T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
     w = bench.build_workload()
     for ops4, aa in (((T["fl"], T["w1"], T["w2"], T["fr"]), T["aa"]), (w[:4], w[4])):
-        prog = heff2_program(*ops4, aa.structure)
+        prog = heff2_program(*ops4, aa.structure, defer=False)
         assert prog.fused is not None and len(prog.fused) == 1
-        outs = []
+        default_prog = heff2_program(*ops4, aa.structure, defer=True)
+        assert default_prog.fused is None
+        y_default = torch.full_like(prog.y_slot, float("nan"))
+        default_prog.run(aa.arena, y_default)
+        outs = [y_default]
         default = _exec.FUSE
         for fuse in (True, False, True, True):
             _exec.FUSE = fuse

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import _emulate
-from tenet import ops
+from tenet import _exec, ops
 from tenet.plan import repartition_plan, transpose_plan
 from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure, layout
 from tenet._exec import gather_rows, make_gather
@@ -154,8 +154,10 @@ def test_config1_plan_sizes(golden_dir):
     assert ex.flops == 215_736_784 or abs(ex.flops - 2.157e8) / 2.157e8 < 1e-3
 
 
-def test_heff2_chain_program_reproduces_reference(golden_dir):
-    """The compiled chain (5 gathers + 4 GEMMs, fixed operands pre-packed) on CPU."""
+@pytest.mark.parametrize("defer", [False, True])
+def test_heff2_chain_program_reproduces_reference(golden_dir, defer):
+    """The compiled chain (5 gathers + 4 GEMMs, fixed operands pre-packed) on CPU, with
+    and without the MPO links' products computed by the gathers that read them."""
     from types import SimpleNamespace
 
     from tenet.program import heff2_program
@@ -165,11 +167,13 @@ def test_heff2_chain_program_reproduces_reference(golden_dir):
     T = {k: _load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2", "heff_aa")}
     ops_ = {k: SimpleNamespace(structure=T[k][0]) for k in ("fl", "w1", "w2", "fr")}
     prog = heff2_program(ops_["fl"], ops_["w1"], ops_["w2"], ops_["fr"], T["aa"][0],
-                         allocate=False)
-    # the first link's A gather permutes whole rows only: its products read the input
+                         allocate=False, defer=defer)
+    # the first link's A gather permutes whole rows only: its products read the input;
+    # the two MPO links' skinny products are computed by the gathers that read them
     assert [lk.a_direct for lk in prog.links] == [True, False, False, False]
-    assert prog.launches == 8
-    src = T["aa"][1]
+    assert [lk.deferred for lk in prog.links] == [False, defer, defer, False]
+    assert prog.launches == (6 if defer else 8)
+    src, pending = T["aa"][1], None
     for lk in prog.links:
         name = next(k for k in ("fl", "w1", "w2", "fr") if ops_[k] is lk.b_tensor)
         bbuf = np.full(lk.b_size, np.nan)
@@ -179,11 +183,20 @@ def test_heff2_chain_program_reproduces_reference(golden_dir):
             abuf = src
         else:
             abuf = np.full(lk.a_size, np.nan)
-            _emulate.gather(lk.a_gather, src, abuf)
-        _emulate.gemm(lk.gemm, abuf, bbuf, cbuf)
+            if isinstance(lk.a_gather, _exec.ProductGather):
+                _emulate.gather_product(lk.a_gather, *pending, abuf)
+            else:
+                _emulate.gather(lk.a_gather, src, abuf)
+        if lk.deferred:
+            pending = (abuf, bbuf)
+        else:
+            _emulate.gemm(lk.gemm, abuf, bbuf, cbuf)
         src = cbuf
     out = np.full(layout(prog.out_struct).size, np.nan)
-    _emulate.gather(prog.out_gather, src, out)
+    if isinstance(prog.out_gather, _exec.ProductGather):
+        _emulate.gather_product(prog.out_gather, *pending, out)
+    else:
+        _emulate.gather(prog.out_gather, src, out)
     es, ex = T["heff_aa"]
     assert prog.out_struct == es
     np.testing.assert_allclose(out, ex, rtol=1e-12, atol=1e-12 * np.abs(ex).max())
