@@ -113,10 +113,13 @@ __device__ int64_t owner_row(const int64_t* table, int64_t n_gemm, int64_t chunk
 
 // Pack one 128 x 32 slab of A (blocks [0, a_chunks): rows = M, read along K) or of B^T
 // (blocks after them: rows = N, read along N) into its work-buffer chunk in the UMMA
-// layout.  Reads are coalesced along the operand's contiguous dimension; the slab is
-// assembled in shared memory and leaves as 16-byte stores.
+// layout.  Each of the 256 threads loads its 16 elements at once (coalesced along the
+// operand's contiguous dimension), the slab is assembled in shared memory and leaves as
+// 16-byte stores.
+constexpr int kPackThreads = 256, kPackPer = (kT2M * kT2Bk) / kPackThreads;
+
 template <int MODE>
-__global__ void __launch_bounds__(kT2Threads)
+__global__ void __launch_bounds__(kPackThreads)
 tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* __restrict__ a,
                int64_t n_a, const double* __restrict__ b, int64_t n_b,
                uint8_t* __restrict__ work, int64_t work_bytes, int64_t a_chunks) {
@@ -151,28 +154,30 @@ tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* 
   const int64_t local = chunk - (which == 0 ? r.a_chunk : r.b_chunk);
   const int64_t t0 = (local / ks) * kT2M, k0 = (local % ks) * kT2Bk;
   pdl_wait();  // the operand may be the previous kernel's output
-#pragma unroll 4
-  for (int i = 0; i < (kT2M * kT2Bk) / kT2Threads; ++i) {
-    const int idx = tid + i * kT2Threads;
-    int rr, kk;
-    double x;
+  double x[kPackPer];
+#pragma unroll
+  for (int i = 0; i < kPackPer; ++i) {
+    const int idx = tid + i * kPackThreads;
     if (which == 0) {  // A: consecutive threads along K
-      rr = idx / kT2Bk;
-      kk = idx % kT2Bk;
-      const int64_t gm = t0 + rr, gk = k0 + kk;
-      x = (gm < r.M && gk < r.K) ? a[r.aoff + gm * r.lda + gk] : 0.0;
+      const int64_t gm = t0 + idx / kT2Bk, gk = k0 + idx % kT2Bk;
+      x[i] = (gm < r.M && gk < r.K) ? __ldg(a + r.aoff + gm * r.lda + gk) : 0.0;
     } else {  // B: consecutive threads along N
-      kk = idx / kT2N;
-      rr = idx % kT2N;
-      const int64_t gn = t0 + rr, gk = k0 + kk;
-      x = (gk < r.K && gn < r.N) ? b[r.boff + gk * r.ldb + gn] : 0.0;
+      const int64_t gk = k0 + idx / kT2N, gn = t0 + idx % kT2N;
+      x[i] = (gk < r.K && gn < r.N) ? __ldg(b + r.boff + gk * r.ldb + gn) : 0.0;
     }
+  }
+#pragma unroll
+  for (int i = 0; i < kPackPer; ++i) {
+    const int idx = tid + i * kPackThreads;
+    const int rr = which == 0 ? idx / kT2Bk : idx % kT2N;
+    const int kk = which == 0 ? idx % kT2Bk : idx / kT2N;
     const uint32_t off = kmajor(rr, kk, L::kEsz, L::kRowBytes);
     if constexpr (MODE == 0) {
-      *reinterpret_cast<uint32_t*>(slab + off) = to_tf32(x);
+      *reinterpret_cast<uint32_t*>(slab + off) = to_tf32(x[i]);
     } else {
-      const __nv_bfloat16 hi = __double2bfloat16(x);
-      const __nv_bfloat16 lo = __double2bfloat16(x - static_cast<double>(__bfloat162float(hi)));
+      const __nv_bfloat16 hi = __double2bfloat16(x[i]);
+      const __nv_bfloat16 lo =
+          __double2bfloat16(x[i] - static_cast<double>(__bfloat162float(hi)));
       *reinterpret_cast<__nv_bfloat16*>(slab + off) = hi;
       *reinterpret_cast<__nv_bfloat16*>(slab + L::kPartBytes + off) = lo;
     }
@@ -181,7 +186,8 @@ tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* 
   uint4* dst = reinterpret_cast<uint4*>(work + static_cast<int64_t>(blockIdx.x) * kT2Slab);
   const uint4* from = reinterpret_cast<const uint4*>(slab);
 #pragma unroll
-  for (int i = 0; i < kT2Slab / 16 / kT2Threads; ++i) dst[tid + i * kT2Threads] = from[tid + i * kT2Threads];
+  for (int i = 0; i < kT2Slab / 16 / kPackThreads; ++i)
+    dst[tid + i * kPackThreads] = from[tid + i * kPackThreads];
 }
 
 __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes,
@@ -329,8 +335,13 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   const int64_t n0 = ntile * kT2N;
   const bool live = ok && nk > 0 && !s_fail;
   double* const stage = reinterpret_cast<double*>(smem) + warp * (32 * 17);
+  // columns past N and warps whose rows all lie past M have nothing to store (both
+  // conditions are uniform across the warp, as tcgen05.ld requires)
+  const int64_t cols = ok ? r.N - n0 : 0;
+  const int n_chunks = cols >= kT2N ? kT2N / 16 : static_cast<int>((cols + 15) / 16);
+  const int warp_chunks = ok && row0 < r.M ? n_chunks : 0;
 #pragma unroll 1
-  for (int chunk = 0; chunk < kT2N / 16; ++chunk) {
+  for (int chunk = 0; chunk < warp_chunks; ++chunk) {
     uint32_t v[16];
     if (live) {
       const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + chunk * 16;
@@ -384,7 +395,7 @@ cudaError_t launch_tc_mode(unsigned grid, cudaStream_t s, const int64_t* table, 
   auto* w = static_cast<uint8_t*>(work);
   cudaError_t e = cudaSuccess;
   if (a_chunks + b_chunks > 0)
-    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(a_chunks + b_chunks), kT2Threads, s,
+    e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(a_chunks + b_chunks), kPackThreads, s,
                table, n_gemm, a, n_a, b, n_b, w, work_bytes, a_chunks);
   if (e == cudaSuccess)
     e = launch_dyn(tc_mma_kernel<MODE>, grid, kT2Threads, L::kSmemBytes, s, table, n_gemm,

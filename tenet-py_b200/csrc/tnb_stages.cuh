@@ -528,15 +528,24 @@ __device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN, S>& 
     if (!sm.last) return;
     __threadfence();
     const double* base = g.parts + r.part_off + t2 * r.splits * (TM * TN);
+    // splits outermost: each element still sums its splits in split order from zero, and
+    // the 16 loads of one split are in flight together
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int e = (ty + TY * i) * TN + tx + TX * j;
-        double v = 0.0;
-        for (int64_t q = 0; q < r.splits; ++q) v += __ldcg(base + q * (TM * TN) + e);
-        acc[i][j] = v;
-      }
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    for (int64_t q = 0; q < r.splits; ++q) {
+      double v[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          v[i][j] = __ldcg(base + q * (TM * TN) + (ty + TY * i) * TN + tx + TX * j);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += v[i][j];
+    }
     if (tid == 0) g.counters[r.cnt_off + t2] = 0u;  // leave the counters zero for the next run
   }
 
