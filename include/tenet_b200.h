@@ -206,6 +206,23 @@ int tnb_weighted_dot_noalloc(const double* x, const double* y, int64_t n,
                              double* out, void* stream);
 
 /*
+ * dst[i] = src[i], i < n, by a kernel: either buffer may be pinned host memory (read or
+ * written through its mapped device pointer), so a host caller's input and output move
+ * inside the same stream -- or CUDA graph -- as the kernels around them, at about one
+ * link latency per copy.  Pageable host memory is refused.  No counterpart in the
+ * reference (its arrays live on one device already).
+ */
+int tnb_copy_f64(int64_t n, const double* src, double* dst, void* stream);
+
+/*
+ * *out = the address kernels use for `p`: `p` itself for device or managed memory, the
+ * mapped device pointer for pinned host memory (so any kernel of this library may read
+ * or write a pinned host buffer, e.g. the last gather of a matvec writing its result to
+ * the host directly).  TNB_EINVAL for pageable host memory.
+ */
+int tnb_mapped_address(const void* p, void** out);
+
+/*
  * out[i] = alpha * x[i] + beta * y[i], i < n.  `out` may alias `x` or `y`.
  * Replaces add / subtract / multiply / divide over aligned blocks
  * (ops/basic.py:81-236) and Lanczos' vector updates (network/dmrg.py:207-227).

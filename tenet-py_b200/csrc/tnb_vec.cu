@@ -91,6 +91,26 @@ __global__ void axpby_kernel(int64_t n, double alpha, const double* x, double be
     out[i] = fma(alpha, x[i], beta * y[i]);
 }
 
+// dst[i] = src[i]: one 16-byte (or, unaligned, 8-byte) element per thread, all loads in
+// flight at once, so a copy that reads or writes pinned host memory through its mapped
+// pointer pays the link's latency about once.  It waits for the previous kernel first
+// (its source may be that kernel's output, its destination that kernel's input).
+__global__ void copy_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ dst,
+                            int vec) {
+  pdl_launch_dependents();
+  pdl_wait();
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (vec) {
+    if (2 * i + 1 < n) {
+      reinterpret_cast<double2*>(dst)[i] = reinterpret_cast<const double2*>(src)[i];
+    } else if (2 * i < n) {
+      dst[2 * i] = src[2 * i];
+    }
+  } else if (i < n) {
+    dst[i] = src[i];
+  }
+}
+
 __global__ void lincomb_kernel(int64_t n, int64_t k, const double* __restrict__ coeffs,
                                const double* const* __restrict__ vecs, double* out) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -428,6 +448,54 @@ extern "C" int tnb_axpby(int64_t n, double alpha, const double* x, double beta, 
   tnb::axpby_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(n, alpha, x,
                                                                                   beta, y, out);
   return tnb::check_launch("tnb_axpby");
+}
+
+namespace {
+// The address a kernel uses for `p`: device and managed memory as is, pinned host
+// memory through its mapped device pointer; pageable host memory is refused (nullptr).
+const void* kernel_address(const void* p) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) return p;
+  if (at.type == cudaMemoryTypeHost && at.devicePointer != nullptr) {
+    const auto off = static_cast<const char*>(p) - static_cast<const char*>(at.hostPointer);
+    return static_cast<const char*>(at.devicePointer) + off;
+  }
+  return nullptr;
+}
+}  // namespace
+
+extern "C" int tnb_mapped_address(const void* p, void** out) {
+  TNB_REQUIRE(p != nullptr && out != nullptr, "tnb_mapped_address: null pointer");
+  const void* k = kernel_address(p);
+  TNB_REQUIRE(k != nullptr,
+              "tnb_mapped_address: neither device memory nor pinned host memory");
+  *out = const_cast<void*>(k);
+  return TNB_OK;
+}
+
+extern "C" int tnb_copy_f64(int64_t n, const double* src, double* dst, void* stream) {
+  TNB_REQUIRE(n >= 0, "tnb_copy_f64: negative size");
+  if (n == 0) return TNB_OK;
+  TNB_REQUIRE(src != nullptr && dst != nullptr, "tnb_copy_f64: null pointer");
+  const auto* ks = static_cast<const double*>(kernel_address(src));
+  auto* kd = static_cast<double*>(const_cast<void*>(kernel_address(dst)));
+  TNB_REQUIRE(ks != nullptr && kd != nullptr,
+              "tnb_copy_f64: a buffer is neither device memory nor pinned host memory");
+  const int vec = (reinterpret_cast<uintptr_t>(ks) % 16 == 0 &&
+                   reinterpret_cast<uintptr_t>(kd) % 16 == 0) ? 1 : 0;
+  const int64_t items = vec ? (n + 1) / 2 : n;
+  TNB_REQUIRE(items < (int64_t(1) << 31) * 256, "tnb_copy_f64: too large for one launch");
+  const cudaError_t e = tnb::launch(tnb::copy_kernel, static_cast<unsigned>((items + 255) / 256),
+                                    256, tnb::as_stream(stream), n, ks, kd, vec);
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_copy_f64: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  return tnb::check_launch("tnb_copy_f64");
 }
 
 extern "C" int tnb_lincomb(int64_t n, int64_t k, const double* coeffs,

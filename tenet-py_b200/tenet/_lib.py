@@ -21,6 +21,8 @@ _i64, _i32, _f64, _vp = ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_
 SIGNATURES = {
     "tnb_block_gather": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
                                 _i64, _vp, _i64, _vp, _i64, _vp]),
+    "tnb_copy_f64": (_i32, [_i64, _vp, _vp, _vp]),
+    "tnb_mapped_address": (_i32, [_vp, ctypes.POINTER(_vp)]),
     "tnb_block_gather_product": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp,
                                         _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
     "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
@@ -97,4 +99,12 @@ def call(name: str, *args) -> None:
 def device_error(stream) -> int:
     out = ctypes.c_int(0)
     call("tnb_device_error", ctypes.byref(out), stream)
+    return int(out.value)
+
+
+def mapped_address(p: int) -> int:
+    """The address kernels use for ``p`` (``tnb_mapped_address``): pinned host memory
+    through its mapped device pointer; raises for pageable memory."""
+    out = _vp()
+    call("tnb_mapped_address", p, ctypes.byref(out))
     return int(out.value)

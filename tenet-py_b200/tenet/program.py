@@ -28,7 +28,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from tenet import _exec
+from tenet import _exec, _lib
 from tenet.plan import chain, repartition_plan, transpose_plan
 from tenet.structure import IN, OUT, TensorStructure, layout, matrix_layout
 from tenet.tensor import SymmetricTensor
@@ -383,23 +383,72 @@ class ChainProgram:
         return out
 
 
-class GraphMatvec:
-    """A ``ChainProgram`` captured in a CUDA graph: copy in, replay, copy out."""
+class _Mapped:
+    """A pinned host tensor seen through its kernel address (``_lib.mapped_address``):
+    the two methods a chain program's ``run`` reads of its output."""
 
-    def __init__(self, program: ChainProgram, warmup: int = 2) -> None:
+    __slots__ = ("_ptr", "_n")
+
+    def __init__(self, host: torch.Tensor) -> None:
+        self._ptr, self._n = _lib.mapped_address(host.data_ptr()), host.numel()
+
+    def data_ptr(self) -> int:
+        return self._ptr
+
+    def numel(self) -> int:
+        return self._n
+
+
+class GraphMatvec:
+    """A ``ChainProgram`` captured in a CUDA graph: copy in, replay, copy out.
+
+    With ``host_io`` the graph also moves the data between pinned host buffers and the
+    device: ``host_x`` -> device, the chain, the result -> ``host_y``, so a host caller
+    pays one graph launch per matvec (``replay_host``).  ``host_copy`` "kernel" reads
+    ``host_x`` with a copy kernel (``tnb_copy_f64``) and lets the chain's last gather
+    write its result straight into ``host_y`` through the buffer's mapped address
+    (every output element is written once); "dma" uses the copy engines
+    (``cudaMemcpyAsync``) both ways."""
+
+    def __init__(self, program: ChainProgram, warmup: int = 2, host_io: bool = False,
+                 host_copy: str = "kernel") -> None:
+        if host_copy not in ("kernel", "dma"):
+            raise ValueError(f"GraphMatvec: host_copy {host_copy!r} is not 'kernel' or 'dma'")
         self.program = program
         dev = _exec.device()
         self.x = torch.zeros(layout(program.in_struct).size, dtype=torch.float64, device=dev)
         self.y = torch.empty(layout(program.out_struct).size, dtype=torch.float64, device=dev)
+        self.host_x = self.host_y = None
+        if host_io:
+            self.host_x = torch.zeros(self.x.numel(), dtype=torch.float64).pin_memory()
+            self.host_y = torch.zeros(self.y.numel(), dtype=torch.float64).pin_memory()
+
+        def move(src, dst):
+            if host_copy == "kernel":
+                _lib.call("tnb_copy_f64", src.numel(), src.data_ptr(), dst.data_ptr(),
+                          _exec.stream_ptr())
+            else:
+                dst.copy_(src, non_blocking=True)
+
+        direct_out = host_io and host_copy == "kernel"
+        out = _Mapped(self.host_y) if direct_out else self.y
+
+        def body():
+            if host_io:
+                move(self.host_x, self.x)
+            program.run(self.x, out)
+            if host_io and not direct_out:
+                move(self.y, self.host_y)
+
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
             for _ in range(warmup):
-                program.run(self.x, self.y)
+                body()
         torch.cuda.current_stream().wait_stream(side)
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
-            program.run(self.x, self.y)
+            body()
 
     def __call__(self, x: SymmetricTensor) -> SymmetricTensor:
         self.x.copy_(x.arena)
@@ -408,6 +457,14 @@ class GraphMatvec:
 
     def replay(self) -> None:
         self.graph.replay()
+
+    def replay_host(self) -> torch.Tensor:
+        """``host_y`` = H ``host_x`` (host_io graphs): enqueue on the current stream; the
+        result is in ``host_y`` once the stream reaches this point."""
+        if self.host_x is None:
+            raise ValueError("GraphMatvec.replay_host: built without host_io")
+        self.graph.replay()
+        return self.host_y
 
 
 _HEFF_TABLES: dict = {}

@@ -506,6 +506,14 @@ def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(y_g, y_py)
+    # the host-buffer graph: pinned input in, the chain, pinned output back, one launch
+    from tenet.program import GraphMatvec
+
+    gh = GraphMatvec(prog, host_io=True)
+    gh.host_x.copy_(x.cpu())
+    gh.replay_host()
+    torch.cuda.synchronize()
+    assert torch.equal(gh.host_y, y_py.cpu())
 
 
 def _ed_j1j2(L: int, j1: float, j2: float) -> float:
