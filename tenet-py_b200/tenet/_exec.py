@@ -760,12 +760,16 @@ class GemmGroup:
         return q
 
 
+#: CTAs a composition's split-K tiles aim for (two per SM)
+SPLITK_TARGET_CTAS = 2 * N_SM
+
+
 def _splits(K: int, out_tiles_total: int) -> tuple[int, int]:
     """K splits for a long-K product when the composition's output tiles cannot fill two
     waves: (splits, ksplit) with ksplit a multiple of 16 and at least 32."""
-    if K <= 64 or out_tiles_total >= 2 * N_SM:
+    if K <= 64 or out_tiles_total >= SPLITK_TARGET_CTAS:
         return 1, 0
-    want = max(1, -(-2 * N_SM // max(out_tiles_total, 1)))
+    want = max(1, -(-SPLITK_TARGET_CTAS // max(out_tiles_total, 1)))
     ks = max(32, -(-K // want))
     ks = -(-ks // 16) * 16
     return -(-K // ks), ks
