@@ -265,3 +265,52 @@ def test_native_gather_rows_match_the_normalisation_rule():
         big = np.full((1, 9), 2)
         primes = np.array([[29, 23, 19, 17, 13, 11, 7, 5, 3]])  # no two dims merge
         _exec._plan_rows(big, primes, big * 0, big * 0, [0], [512], [0], [0], 0)
+
+
+def _seg(dst_off, dims, dstr, rstr, cstr, t0, t1):
+    row = np.zeros(_exec.SEG_W, np.int64)
+    rank = len(dims)
+    row[0], row[1], row[2], row[3], row[4] = dst_off, int(np.prod(dims)), rank, t0, t1
+    row[8:8 + rank], row[16:16 + rank] = dims, dstr
+    row[24:24 + rank], row[32:32 + rank] = rstr, cstr
+    return row
+
+
+def test_product_gather_plans_windows_and_refuses_the_rest():
+    """``product_gather`` maps each term of a gather over a product's C arena to its
+    product row and first (row, column); computing the elements from A and B (the
+    kernel's semantics, emulated) gives what the gather gives over the materialised C.
+    It refuses long K, split-K and tensor-core tables, and windows that leave a block."""
+    prods = [(5, 3, 2, 0, 2, 0, 3, 0, 3), (4, 2, 3, 10, 3, 6, 2, 15, 2)]
+    table = _exec.make_gemm(prods, _exec.TILE_SKINNY)
+    rng = np.random.default_rng(3)
+    a, b = rng.standard_normal(22), rng.standard_normal(12)
+    # one destination block, the sum of a 3 x 2 window of product 0 (rows 1-3, columns
+    # 1-2) and a 3 x 2 window of product 1 (rows 0-2), transposed into the destination
+    rows = np.array([_seg(0, (3, 2), (1, 3), (1, 0), (0, 1), 0, 2)])
+    g = make_gather((rows, np.array([4, 15]), np.array([0.5, -2.0]), np.array([3, 2])))
+    pg = _exec.product_gather(g, table)
+    assert pg is not None
+    assert pg.tprod.tolist() == [0, 1] and pg.tsrc.tolist() == [1, 0] and pg.tld.tolist() == [1, 0]
+    c = np.full(23, np.nan)
+    _emulate.gemm(table, a, b, c)
+    want, got = np.full(6, np.nan), np.full(6, np.nan)
+    _emulate.gather(g, c, want)
+    _emulate.gather_product(pg, a, b, got)
+    np.testing.assert_allclose(got, want, rtol=1e-14, atol=1e-14)
+    # a contiguous run across rows of product 1 is not a (row, column) window
+    run = make_gather((np.array([_seg(0, (4,), (1,), (0,), (1,), 0, 1)]), np.array([17]),
+                       np.array([1.0]), np.array([0])))
+    assert _exec.product_gather(run, table) is None
+    # a window reaching past its block's last row
+    tall = make_gather((np.array([_seg(0, (3, 2), (1, 3), (1, 0), (0, 1), 0, 1)]),
+                        np.array([15 + 2 * 2]), np.array([1.0]), np.array([2])))
+    assert _exec.product_gather(tall, table) is None
+    # long K, tensor-core and split-K tables
+    assert _exec.product_gather(g, _exec.make_gemm(
+        [(5, 3, 5, 0, 5, 0, 3, 0, 3), (4, 2, 3, 25, 3, 15, 2, 15, 2)], _exec.TILE_SKINNY)) is None
+    assert _exec.product_gather(g, _exec.make_gemm(prods, _exec.TILE_TC_3XBF16)) is None
+    split = _exec.make_gemm(prods, _exec.TILE_SKINNY)
+    split.table = split.table.copy()
+    split.table[0, 12] = 2
+    assert _exec.product_gather(g, split) is None
