@@ -41,8 +41,8 @@ for _p in (ROOT, ROOT / "tenet-py_b200"):
 METRIC = "Heff matvec TFLOP/s (SU(2) Heisenberg two-site, FP64)"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload (ncu captures of
 # two launches each, mean), in bytes
-NCU_TRAFFIC = {"block_gather": (502_528 + 413_184) // 2,
-               "grouped_gemm_f64": (781_568 + 1_981_952) // 2}
+NCU_TRAFFIC = {"block_gather": (480_000 + 1_625_856) // 2,
+               "grouped_gemm_f64": (786_432 + 1_986_816) // 2}
 # multiplets per bond sector, half-integer bond spins 2j = 1, 3, ..., 17 (sum 256)
 BOND = {1: 60, 3: 56, 5: 46, 7: 36, 9: 25, 11: 16, 13: 10, 15: 5, 17: 2}
 MPO = {0: 2, 2: 1}
