@@ -214,24 +214,14 @@ __device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSm
   if (bad) raise_bounds();
 }
 
-// One TNB_GATHER_CHUNK-element chunk of a gather by a group of NT threads (the whole
-// CTA standalone; a quarter of it in the persistent kernel); `tid` is the thread's index
-// within the group.
-template <int NT, bool kFused, class Sync, bool kProd = false>
-__device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm, int tid,
-                             Sync sync) {
-  static_assert(!(kFused && kProd), "product-source gathers run standalone only");
+// Chunk `chunk` of the row staged in `sm` (row words, and its terms when there are at
+// most kStagedTerms of them), by a group of NT threads; `tid` is the thread's index within
+// the group.  Every check that depends on the row is made here, so a caller that staged
+// the row ahead of time (the range kernel) gets the same validation.
+template <int NT, bool kFused, bool kProd = false>
+__device__ void gather_staged(const GatherArgs& g, int64_t chunk, const GatherSmem& sm,
+                              int tid) {
   constexpr int kEpt = TNB_GATHER_CHUNK / NT;
-  static_assert(NT >= TNB_SEG_WIDTH && NT >= kStagedTerms, "a group stages a row and its terms");
-  if constexpr (kFused) sync();  // the previous item's readers are done with sm
-  const int64_t seg = g.chunk_map[chunk];
-  if (seg < 0 || seg >= g.n_seg) {
-    if (tid == 0) raise_bounds();
-    return;
-  }
-  if (tid < TNB_SEG_WIDTH) sm.row[tid] = g.segs[seg * TNB_SEG_WIDTH + tid];
-  sync();
-
   const int64_t* row = sm.row;
   const int64_t dst_off = row[0];
   const int64_t size = row[1];
@@ -243,21 +233,15 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   // (a product-source gather checks its elements against its product rows instead)
   const int64_t n_src = second ? g.n_src1 : g.n_src0;
   const int64_t n_dst = second ? g.n_dst1 : g.n_dst0;
+  // the row's chunk size (a multiple of kGatherThreads up to TNB_GATHER_CHUNK)
+  const int64_t ce = row[7] ? row[7] : TNB_GATHER_CHUNK;
   if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || rank > TNB_MAX_RANK ||
-      (kProd && second)) {
+      (kProd && second) || ce <= 0 || ce > TNB_GATHER_CHUNK || ce % kGatherThreads ||
+      chunk < row[6] || (chunk - row[6]) * ce >= size) {
     if (tid == 0) raise_bounds();
     return;
   }
-  const int nt = static_cast<int>(t1 - t0);
-  const bool staged = nt <= kStagedTerms;
-  if (staged && tid < nt) {
-    sm.t_src[tid] = g.term_src[t0 + tid];
-    sm.t_ld[tid] = g.term_ld[t0 + tid];
-    sm.t_cf[tid] = g.term_coeff[t0 + tid];
-    if constexpr (kProd) sm.t_prod[tid] = g.term_prod[t0 + tid];
-  }
-  sync();
-  if constexpr (!kFused) pdl_wait();  // tables are static; the source may be the previous kernel's output
+  const bool staged = t1 - t0 <= kStagedTerms;
 
   uint32_t dims[TNB_MAX_RANK];
   int64_t dstr[TNB_MAX_RANK], rstr[TNB_MAX_RANK], cstr[TNB_MAX_RANK];
@@ -267,13 +251,6 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
     dstr[d] = d < rank ? row[16 + d] : 0;
     rstr[d] = d < rank ? row[24 + d] : 0;
     cstr[d] = d < rank ? row[32 + d] : 0;
-  }
-
-  // the row's chunk size (a multiple of kGatherThreads up to TNB_GATHER_CHUNK)
-  const int64_t ce = row[7] ? row[7] : TNB_GATHER_CHUNK;
-  if (ce <= 0 || ce > TNB_GATHER_CHUNK || ce % kGatherThreads) {
-    if (tid == 0) raise_bounds();
-    return;
   }
   const int64_t base = (chunk - row[6]) * ce;
   const int64_t lim = min(size, base + ce);
@@ -286,6 +263,47 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   } else {
     gather_elems<kEpt, NT, kFused, kProd>(g, sm, ge, tid, rank, dims, dstr, rstr, cstr);
   }
+}
+
+// Stage the terms of the row in `sm` (when there are at most kStagedTerms), one term per
+// thread of the group.  False when the row's term range is invalid.
+template <bool kProd>
+__device__ __forceinline__ bool stage_terms(const GatherArgs& g, GatherSmem& sm, int tid) {
+  const int64_t t0 = sm.row[3], t1 = sm.row[4];
+  if (t0 < 0 || t1 > g.n_term || t0 > t1) return false;
+  if (t1 - t0 <= kStagedTerms && tid < t1 - t0) {
+    sm.t_src[tid] = g.term_src[t0 + tid];
+    sm.t_ld[tid] = g.term_ld[t0 + tid];
+    sm.t_cf[tid] = g.term_coeff[t0 + tid];
+    if constexpr (kProd) sm.t_prod[tid] = g.term_prod[t0 + tid];
+  }
+  return true;
+}
+
+// One chunk of a gather with its tables staged on the spot (chunk map -> row -> terms) by
+// a group of NT threads (the whole CTA standalone; a quarter of it in the persistent
+// kernel); `tid` is the thread's index within the group.
+template <int NT, bool kFused, class Sync, bool kProd = false>
+__device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm, int tid,
+                             Sync sync) {
+  static_assert(!(kFused && kProd), "product-source gathers run standalone only");
+  static_assert(NT >= TNB_SEG_WIDTH && NT >= kStagedTerms, "a group stages a row and its terms");
+  if constexpr (kFused) sync();  // the previous item's readers are done with sm
+  const int64_t seg = g.chunk_map[chunk];
+  if (seg < 0 || seg >= g.n_seg) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  if (tid < TNB_SEG_WIDTH) sm.row[tid] = g.segs[seg * TNB_SEG_WIDTH + tid];
+  sync();
+  const bool ok = stage_terms<kProd>(g, sm, tid);
+  sync();
+  if (!ok) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  if constexpr (!kFused) pdl_wait();  // tables are static; the source may be the previous kernel's output
+  gather_staged<NT, kFused, kProd>(g, chunk, sm, tid);
 }
 
 // ---------------------------------------------------------------------------------------
