@@ -28,10 +28,16 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // own static tables, and only then waits for the previous kernel's results (wait).  The
 // next kernel's table prologue therefore overlaps this kernel's work.  Both instructions
 // are no-ops for a kernel launched without the attribute.
-__device__ __forceinline__ void pdl_launch_dependents() {
+// Programmatic dependent launch: wait for the previous kernel's results, then let the
+// next kernel launch, whose CTAs become resident and load their static tables while this
+// kernel moves its data.  Releasing the next kernel at this kernel's first instruction
+// instead was measured slower on the heff2 chain (49.2 against 45-47 us per matvec): the
+// early dependents held SM slots this kernel's own CTAs still needed.  A kernel that
+// returns before waiting releases its dependents when it completes.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Whether table-driven kernels are launched with the programmatic-serialisation
 // attribute (tnb_set_pdl).

@@ -29,7 +29,6 @@ template <int kMinBlocks>
 __global__ void __launch_bounds__(kGatherThreads, kMinBlocks)
 gather_kernel(const GatherArgs g) {
   __shared__ GatherSmem sm;
-  pdl_launch_dependents();
   gather_chunk<kGatherThreads, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
 }
 
@@ -57,7 +56,6 @@ int device_sms() {
 __global__ void __launch_bounds__(kGatherThreads, 2)
 gather_product_kernel(const GatherArgs g) {
   __shared__ GatherSmem sm;
-  pdl_launch_dependents();
   gather_chunk<kGatherThreads, false, CtaSync, true>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
 }
 

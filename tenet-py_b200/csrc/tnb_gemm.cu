@@ -34,7 +34,6 @@ __global__ void __launch_bounds__((TM / 4) * (TN / 4), (TM == 64 ? 1 : 6))
 gemm_f64_kernel(const GemmArgs g) {
   extern __shared__ __align__(16) uint8_t gemm_smem[];
   auto& sm = *reinterpret_cast<GemmSmem<TM, TN, kGemmStages<TM>>*>(gemm_smem);
-  pdl_launch_dependents();
   gemm_tile<TM, TN, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
 }
 
@@ -54,14 +53,12 @@ cudaError_t launch_gemm_f64(unsigned grid, cudaStream_t s, const GemmArgs& g) {
 __global__ void __launch_bounds__(kSkinnyThreads, 4)
 gemm_f64_skinny_kernel(const GemmArgs g) {
   __shared__ SkinnySmem sm;
-  pdl_launch_dependents();
   skinny_tile<kSkinnyThreads, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
 }
 
 __global__ void __launch_bounds__(kSkinnyThreads, 4)
 gemm_f64_wide_kernel(const GemmArgs g) {
   __shared__ SkinnySmem sm;
-  pdl_launch_dependents();
   wide_tile(g, blockIdx.x, sm);
 }
 

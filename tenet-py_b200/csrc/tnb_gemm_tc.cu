@@ -127,7 +127,6 @@ tc_pack_kernel(const int64_t* __restrict__ table, int64_t n_gemm, const double* 
   __shared__ __align__(16) uint8_t slab[kT2Slab];
   __shared__ T2Row s_row;
   __shared__ int s_ok;
-  pdl_launch_dependents();
   const int tid = threadIdx.x;
   const int which = blockIdx.x < a_chunks ? 0 : 1;
   const int64_t chunk = which == 0 ? blockIdx.x : blockIdx.x - a_chunks;
@@ -212,7 +211,6 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   __shared__ int s_ok, s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  pdl_launch_dependents();
   if (tid == 0) {
     T2Row r{};
     const int64_t g = tile_map[blockIdx.x];

@@ -97,7 +97,6 @@ __global__ void axpby_kernel(int64_t n, double alpha, const double* x, double be
 // (its source may be that kernel's output, its destination that kernel's input).
 __global__ void copy_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ dst,
                             int vec) {
-  pdl_launch_dependents();
   pdl_wait();
   const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   if (vec) {
