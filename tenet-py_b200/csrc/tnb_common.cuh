@@ -32,11 +32,14 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // next kernel launch, whose CTAs become resident and load their static tables while this
 // kernel moves its data.  Releasing the next kernel at this kernel's first instruction
 // instead was measured slower on the heff2 chain (49.2 against 45-47 us per matvec): the
-// early dependents held SM slots this kernel's own CTAs still needed.  A kernel that
-// returns before waiting releases its dependents when it completes.
+// early dependents held SM slots this kernel's own CTAs still needed.  A kernel of many
+// waves (kRelease = false) releases nothing early: its later waves would share the SMs
+// with the dependents (the batched U(1)xU(1)xfZ2 update: 2.68 against 2.76 ms).  A kernel
+// that returns before waiting releases its dependents when it completes.
+template <bool kRelease = true>
 __device__ __forceinline__ void pdl_wait() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  if constexpr (kRelease) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // Whether table-driven kernels are launched with the programmatic-serialisation

@@ -25,11 +25,13 @@ namespace tnb {
 // spilled) for larger tables, where more resident warps keep more loads in flight
 // (measured on the batched U(1)xU(1)xfZ2 update: 2.02 against 2.27 ms for its gathers;
 // on the single heff2 matvec's one-wave gathers the three-CTA build is as fast or faster).
+// The four-CTA build, always many waves, does not release the next kernel early.
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kGatherThreads, kMinBlocks)
 gather_kernel(const GatherArgs g) {
   __shared__ GatherSmem sm;
-  gather_chunk<kGatherThreads, false>(g, blockIdx.x, sm, threadIdx.x, CtaSync{});
+  gather_chunk<kGatherThreads, false, CtaSync, false, (kMinBlocks == 3)>(g, blockIdx.x, sm,
+                                                                         threadIdx.x, CtaSync{});
 }
 
 // SMs of the current device (0 when it cannot be queried), cached per device.

@@ -283,7 +283,7 @@ __device__ __forceinline__ bool stage_terms(const GatherArgs& g, GatherSmem& sm,
 // One chunk of a gather with its tables staged on the spot (chunk map -> row -> terms) by
 // a group of NT threads (the whole CTA standalone; a quarter of it in the persistent
 // kernel); `tid` is the thread's index within the group.
-template <int NT, bool kFused, class Sync, bool kProd = false>
+template <int NT, bool kFused, class Sync, bool kProd = false, bool kRelease = true>
 __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm, int tid,
                              Sync sync) {
   static_assert(!(kFused && kProd), "product-source gathers run standalone only");
@@ -302,7 +302,7 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
     if (tid == 0) raise_bounds();
     return;
   }
-  if constexpr (!kFused) pdl_wait();  // tables are static; the source may be the previous kernel's output
+  if constexpr (!kFused) pdl_wait<kRelease>();  // tables are static; the source may be the previous kernel's output
   gather_staged<NT, kFused, kProd>(g, chunk, sm, tid);
 }
 
