@@ -644,7 +644,8 @@ def _is_wide(p, cols: int = 0) -> bool:
 
 
 #: A coupled-sector product goes to the tensor cores in the precision form only when it
-#: is at least one full 128 x 64 x 64 tile of work; smaller ones stay on the FP64 path.
+#: is at least 2 x 128 x 64 x 64 flops (half a 128 x 128 x 64 tile's work); smaller ones
+#: stay on the FP64 path.
 TC_MIN_FLOPS = 2 * 128 * 64 * 64
 
 
