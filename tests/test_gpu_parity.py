@@ -614,3 +614,29 @@ def test_save_load_round_trip_on_the_device(tmp_path):
     assert psi2.center == psi.center == 0
     for n in range(L):
         assert torch.equal(psi2[n].arena, psi[n].arena)
+
+
+def test_host_copies_refuse_pageable_memory():
+    """``tnb_copy_f64`` and ``tnb_mapped_address`` reach host memory only through pinned
+    buffers' mapped addresses: a pageable buffer is refused on the host, before any
+    launch, with the library's error status; pinned and device buffers work."""
+    import ctypes
+
+    lib = _lib.load()
+    n = 1000
+    pageable = np.arange(n, dtype=np.float64)
+    dev = torch.zeros(n, dtype=torch.float64, device="cuda")
+    pinned = torch.arange(n, dtype=torch.float64).pin_memory()
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.tnb_copy_f64(n, pageable.ctypes.data, dev.data_ptr(), s) != 0
+    assert b"pinned" in lib.tnb_last_error()
+    out = ctypes.c_void_p()
+    assert lib.tnb_mapped_address(pageable.ctypes.data, ctypes.byref(out)) != 0
+    assert lib.tnb_copy_f64(n, pinned.data_ptr(), dev.data_ptr(), s) == 0
+    back = torch.zeros(n, dtype=torch.float64).pin_memory()
+    assert lib.tnb_copy_f64(n - 1, dev.data_ptr() + 8, back.data_ptr(), s) == 0  # unaligned
+    torch.cuda.synchronize()
+    assert torch.equal(dev.cpu(), pinned)
+    assert torch.equal(back[:n - 1], pinned[1:])
+    assert lib.tnb_mapped_address(dev.data_ptr(), ctypes.byref(out)) == 0
+    assert out.value == dev.data_ptr()
