@@ -551,6 +551,25 @@ def serving(args) -> dict:
     return out
 
 
+def max_over_ranks(ms: float, device) -> float:
+    """The slowest rank's time: every rank of an initialised process group calls this at
+    the same point (one all-reduce); a single process gets its own time back."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(flops: int, steps: int, world: int, ms: float) -> float:
+    """Whole-job TFLOP/s: every rank's ``steps`` matvecs of ``flops`` each over the slowest
+    rank's time ``ms``."""
+    return flops * steps * world / (ms * 1e-3) / 1e12
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -686,12 +705,10 @@ def run_tenet(args) -> None:
             for _ in range(50):
                 gm.replay()
             torch.cuda.synchronize()
+    ms = max_over_ranks(ms, "cuda")
     if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = flops * args.steps * world / (ms * 1e-3) / 1e12
+    value = job_value(flops, args.steps, world, ms)
     launches_per_step = prog.launches
 
     # kernel timing pass: the same steps, each enqueued behind a GPU-side head start so
@@ -716,12 +733,8 @@ def run_tenet(args) -> None:
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
-    e_ms = timed(e2e_step, args.steps)
-    if world > 1:
-        t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
-    e2e_value = flops * args.steps * world / (e_ms * 1e-3) / 1e12
+    e_ms = max_over_ranks(timed(e2e_step, args.steps), "cuda")
+    e2e_value = job_value(flops, args.steps, world, e_ms)
     torch.cuda.synchronize()
     gm.replay()
     torch.cuda.synchronize()
