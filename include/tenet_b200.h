@@ -369,6 +369,17 @@ int tnb_lanczos_ritz(const tnb_seq* correct, const void* x_slot, const void* y_s
  *   stable), extent-1 dims dropped, dims contiguous in destination and source merged,
  *   a rank-1 unit row when nothing is left.  TNB_EINVAL when a row keeps more than
  *   TNB_MAX_RANK dims.
+ * tnb_plan_gather_table: the whole gather table of a block map: terms (t_src, t_dst,
+ *   t_coef; n_terms) over source blocks (n_src: offset, leading dimension, and nd row / column
+ *   strides each) and destination blocks (n_dst: offset, nd strides, nd dims, size, keep
+ *   flag), `perm` giving for each destination axis its source axis.  The terms of kept
+ *   destination blocks, grouped by destination block in block order (their given order
+ *   kept), become one row each per block (tnb_plan_gather_rows' rules, the first term's
+ *   source strides permuted) and fill out_src / out_coef / out_ld (source offset,
+ *   coefficient, leading dimension per term); every kept block without terms then gets a
+ *   zero-writing row.  rows holds n_dst rows, the term outputs n_terms entries; counts[0]
+ *   = rows written, counts[1] = terms written.  TNB_EINVAL on an out-of-range index or a
+ *   row above TNB_MAX_RANK dims.
  * tnb_plan_compose: the sparse product of block maps a (n_a x 3: src, mid, coeff) and
  *   b (n_b x 3: mid, dst, coeff): each (src, dst) pair once, in order of first occurrence
  *   walking a in order and b's terms of each mid in their order, coefficients summed in
@@ -379,6 +390,13 @@ int tnb_plan_gather_rows(int64_t n_rows, int32_t nd, const int64_t* dims, const 
                          const int64_t* rstr, const int64_t* cstr, const int64_t* d_off,
                          const int64_t* sizes, const int64_t* t_begin, const int64_t* t_end,
                          int64_t buf, int64_t* rows);
+int tnb_plan_gather_table(int64_t n_terms, const int64_t* t_src, const int64_t* t_dst,
+                          const double* t_coef, int64_t n_src, const int64_t* s_off,
+                          const int64_t* s_ld, const int64_t* s_rs, const int64_t* s_cs,
+                          int64_t n_dst, const int64_t* d_off, const int64_t* d_str,
+                          const int64_t* d_shape, const int64_t* d_size, const uint8_t* keep,
+                          int32_t nd, const int64_t* perm, int64_t buf, int64_t* rows,
+                          int64_t* out_src, double* out_coef, int64_t* out_ld, int64_t* counts);
 int64_t tnb_plan_compose(int64_t n_a, const double* a, int64_t n_b, const double* b, double* out,
                          int64_t cap);
 

@@ -110,9 +110,6 @@ def recording() -> Seq | None:
 FUSE = False
 
 
-_TORCH_DTYPE = {np.dtype(np.int64).str: torch.int64, np.dtype(np.int32).str: torch.int32,
-                np.dtype(np.float64).str: torch.float64}
-
 
 class _Staging:
     """A pinned host ring through which plan tables reach the device: a table is packed
@@ -152,13 +149,31 @@ class _Staging:
 _STAGING = _Staging()
 
 
+class _DevArray:
+    """One array of an upload as the library's calls take it: a device address and an
+    element count (``ptr`` reads both).  The upload's buffer keeps the memory alive."""
+
+    __slots__ = ("_ptr", "_n")
+
+    def __init__(self, address: int, n: int) -> None:
+        self._ptr, self._n = address, n
+
+    def data_ptr(self) -> int:
+        return self._ptr
+
+    def numel(self) -> int:
+        return self._n
+
+
 class Uploaded:
     """Device copies of host arrays, made on the current stream.  A copy from pageable
     host memory may still be in flight when the call returns, so a kernel on another
     stream waits for the upload's event before first reading them (the serving loop runs
-    requests that share plan tables on different streams)."""
+    requests that share plan tables on different streams).  The arrays come back as
+    address-and-count holders over one device buffer (tables are only ever handed to
+    the library), which spares a torch view per array on every upload."""
 
-    __slots__ = ("arrays", "stream", "event")
+    __slots__ = ("arrays", "stream", "event", "buf")
 
     def __init__(self, host_arrays) -> None:
         # one host->device copy: the arrays packed at 16-byte aligned offsets of one
@@ -177,11 +192,9 @@ class Uploaded:
             dev_buf.copy_(staged, non_blocking=True)
         else:
             dev_buf = torch.from_numpy(packed).to(device())
-        views = []
-        for x, o in zip(host_arrays, offs):
-            t = dev_buf[o:o + x.nbytes].view(_TORCH_DTYPE[x.dtype.str])
-            views.append(t.view(x.shape) if x.ndim > 1 else t)
-        self.arrays = tuple(views)
+        base = dev_buf.data_ptr()
+        self.buf = dev_buf
+        self.arrays = tuple(_DevArray(base + o, x.size) for x, o in zip(host_arrays, offs))
         self.stream = stream_ptr()
         self.event = torch.cuda.Event()
         self.event.record()
@@ -250,20 +263,6 @@ _LOG: LaunchLog | None = None
 # gather tables
 
 
-def _plan_rows(D, DS, RS, CS, d_off, sizes, tb, te, buf):
-    """Descriptor rows by the library's host planner (``tnb_plan_gather_rows``)."""
-    R, nd = D.shape
-    rows = np.zeros((R, SEG_W), np.int64)
-    if not R:
-        return rows
-    arrs = [np.ascontiguousarray(x, dtype=np.int64) for x in (D, DS, RS, CS, d_off, sizes, tb, te)]
-    status = _lib.load().tnb_plan_gather_rows(R, nd, *(x.ctypes.data for x in arrs), buf,
-                                              rows.ctypes.data)
-    if status != 0:
-        raise ValueError(f"a block of rank above the kernel's {MAX_RANK} in a gather plan")
-    return rows
-
-
 def gather_rows(src_s: TensorStructure, src_kind: str, dst_s: TensorStructure, dst_kind: str,
                 perm, terms, buf: int = 0, dst_keep=None):
     """Rows + term arrays executing ``dst[j] = sum c * transpose(src[i], perm)``: one row
@@ -271,50 +270,60 @@ def gather_rows(src_s: TensorStructure, src_kind: str, dst_s: TensorStructure, d
     then one zero-writing row per destination block without any.  ``dst_keep``
     optionally restricts the emitted destination blocks (a boolean mask).  Returns
     ``(rows (R, SEG_W), term sources, term coefficients, term leading dimensions)`` as
-    arrays, term ranges relative to this part."""
+    arrays, term ranges relative to this part.  The grouping and the rows are built by
+    the library's host planner (``tnb_plan_gather_table``)."""
     sl, dl = layout(src_s), layout(dst_s)
     if src_kind == "matrix":
         sm = matrix_layout(src_s)
         s_off, s_ld, s_rs, s_cs = sm.block_off, sm.block_ld, sm.rstride, sm.cstride
     else:
-        s_off, s_ld = sl.offsets, np.zeros_like(sl.offsets)
-        s_rs, s_cs = np.zeros_like(sl.strides), sl.strides
+        s_off, s_ld = sl.offsets, _zeros_like_cached(sl.offsets)
+        s_rs, s_cs = _zeros_like_cached(sl.strides), sl.strides
     if dst_kind == "matrix":
         dm = matrix_layout(dst_s)
         d_off = dm.block_off
         d_str = dm.rstride * dm.block_ld[:, None] + dm.cstride
     else:
         d_off, d_str = dl.offsets, dl.strides
-    perm = np.asarray(perm, dtype=np.int64)
-    n_dst = len(dl.sizes)
-    keep = np.ones(n_dst, bool) if dst_keep is None else np.asarray(dst_keep, bool)
+    n_dst, nd = dl.shapes.shape
+    keep = np.ones(n_dst, np.uint8) if dst_keep is None else np.asarray(dst_keep, np.uint8)
     if len(terms):
         tarr = np.asarray(terms, dtype=np.float64).reshape(-1, 3)
-        ts, td, tc = tarr[:, 0].astype(np.int64), tarr[:, 1].astype(np.int64), tarr[:, 2]
+        ts, td, tc = tarr[:, 0].astype(np.int64), tarr[:, 1].astype(np.int64), tarr[:, 2].copy()
     else:
         ts = td = np.zeros(0, np.int64)
         tc = np.zeros(0)
-    covered = np.zeros(n_dst, bool)
-    covered[td] = True
-    sel = keep[td]
-    ts, td, tc = ts[sel], td[sel], tc[sel]
-    o = np.argsort(td, kind="stable")
-    ts, td, tc = ts[o], td[o], tc[o]
-    js, first, counts = np.unique(td, return_index=True, return_counts=True)
-    i0 = ts[first]
-    if perm.size:
-        RS, CS = s_rs[i0][:, perm], s_cs[i0][:, perm]
-    else:
-        RS = CS = np.zeros((len(js), 0), np.int64)
-    parts = [(js, dl.shapes[js], d_str[js], RS, CS, first, first + counts)]
-    zj = np.nonzero(~covered & keep)[0]
     nt = len(ts)
-    z = np.zeros((len(zj), dl.shapes.shape[1]), np.int64)
-    parts.append((zj, dl.shapes[zj], d_str[zj], z, z, np.full(len(zj), nt), np.full(len(zj), nt)))
-    rows = [_plan_rows(D, DS, RS_, CS_, d_off[j], dl.sizes[j], tb, te, buf)
-            for j, D, DS, RS_, CS_, tb, te in parts]
-    return (np.concatenate(rows), s_off[ts].astype(np.int64), tc.astype(np.float64),
-            s_ld[ts].astype(np.int64))
+    c = lambda x, t=np.int64: np.ascontiguousarray(x, dtype=t)  # noqa: E731
+    args = [c(s_off), c(s_ld), c(s_rs), c(s_cs), c(d_off), c(d_str), c(dl.shapes), c(dl.sizes)]
+    perm = c(perm)
+    rows = np.zeros((n_dst, SEG_W), np.int64)
+    out_src, out_ld, out_coef = np.zeros(nt, np.int64), np.zeros(nt, np.int64), np.zeros(nt)
+    counts = np.zeros(2, np.int64)
+    status = _lib.load().tnb_plan_gather_table(
+        nt, ts.ctypes.data, td.ctypes.data, tc.ctypes.data, len(s_off), args[0].ctypes.data,
+        args[1].ctypes.data, args[2].ctypes.data, args[3].ctypes.data, n_dst,
+        args[4].ctypes.data, args[5].ctypes.data, args[6].ctypes.data, args[7].ctypes.data,
+        keep.ctypes.data, nd, perm.ctypes.data, buf, rows.ctypes.data, out_src.ctypes.data,
+        out_coef.ctypes.data, out_ld.ctypes.data, counts.ctypes.data)
+    if status != 0:
+        raise ValueError(f"a gather plan with a block of rank above the kernel's {MAX_RANK}, "
+                         "or an out-of-range block index")
+    R, T = int(counts[0]), int(counts[1])
+    return rows[:R], out_src[:T], out_coef[:T], out_ld[:T]
+
+
+_ZEROS: dict = {}
+
+
+def _zeros_like_cached(a: np.ndarray) -> np.ndarray:
+    """A read-only zero array of ``a``'s shape, shared per shape."""
+    z = _ZEROS.get(a.shape)
+    if z is None:
+        z = np.zeros(a.shape, np.int64)
+        z.flags.writeable = False
+        _ZEROS[a.shape] = z
+    return z
 
 
 class GatherTable:
@@ -829,11 +838,11 @@ class DotRuns:
         self.n_runs = len(weights)
 
     @property
-    def start(self) -> torch.Tensor:
+    def start(self) -> _DevArray:
         return self._up.ready()[0]
 
     @property
-    def weight(self) -> torch.Tensor:
+    def weight(self) -> _DevArray:
         return self._up.ready()[1]
 
 

@@ -54,6 +54,9 @@ SIGNATURES = {
                                  _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
     "tnb_lanczos_ritz": (_i32, [_vp, _vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                 _i64, _vp, _vp]),
+    "tnb_plan_gather_table": (_i32, [_i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp,
+                                     _vp, _vp, _vp, _vp, _i32, _vp, _i64, _vp, _vp, _vp, _vp,
+                                     _vp]),
     "tnb_plan_gather_rows": (_i32, [_i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
                                     _vp]),
     "tnb_plan_compose": (_i64, [_i64, _vp, _i64, _vp, _vp, _i64]),

@@ -344,27 +344,52 @@ class ArenaLayout:
     coupled: np.ndarray = field(repr=False)  # (n_blocks,) int64 coupled-sector label
 
 
+@dataclass(frozen=True)
+class _LayoutPlan:
+    """The degeneracy-free part of a layout, per pattern: for every axis the distinct space
+    labels its blocks use and each block's index into them (the dual already undone, so
+    the label is the leg space's own), and every block's coupled label."""
+
+    labels: tuple            # per axis, the distinct space labels (sorted)
+    index: np.ndarray        # (n_blocks, ndim) int64 index into labels[axis]
+    coupled: np.ndarray      # (n_blocks,) int64
+
+
+@cache
+def _layout_plan(pat: Pattern) -> _LayoutPlan:
+    p = pat.provider
+    keys = block_keys(pat)
+    n, nd = len(keys), len(pat.legs)
+    oa, ia = pat.out_axes, pat.in_axes
+    lab = np.zeros((n, nd), dtype=np.int64)
+    coupled = np.zeros(n, dtype=np.int64)
+    dual = [bool(leg[2]) for leg in pat.legs]
+    for b, (ot, it) in enumerate(keys):
+        for ax, u in zip(oa, ot[0]):
+            lab[b, ax] = p._dual(u) if dual[ax] else u
+        for ax, u in zip(ia, it[0]):
+            lab[b, ax] = p._dual(u) if dual[ax] else u
+        coupled[b] = ot[2]
+    labels, index = [], np.zeros((n, nd), dtype=np.int64)
+    for ax in range(nd):
+        uniq, inv = np.unique(lab[:, ax], return_inverse=True)
+        labels.append(tuple(int(x) for x in uniq))
+        index[:, ax] = inv.reshape(-1)
+    index.flags.writeable = coupled.flags.writeable = False  # shared by every structure
+    return _LayoutPlan(tuple(labels), index, coupled)
+
+
 @cache
 def layout(s: TensorStructure) -> ArenaLayout:
-    p = s.provider
-    keys = s.keys
-    n, nd = len(keys), s.ndim
-    oa, ia = s.out_axes, s.in_axes
-    # per axis: label -> degeneracy, the dual already applied
-    degs = []
-    for leg in s.legs:
+    """Block shapes, sizes, offsets and C-contiguous strides of ``s``'s arena: the pattern's
+    plan (``_layout_plan``) filled with this structure's degeneracies."""
+    plan = _layout_plan(s.pattern)
+    n, nd = plan.index.shape
+    shapes = np.empty((n, nd), dtype=np.int64)
+    for ax, leg in enumerate(s.legs):
         d = _space_degs(leg.space)
-        degs.append({p._dual(u): m for u, m in d.items()} if leg.dual else d)
-    rows = [[0] * nd for _ in range(n)]
-    coupled = np.zeros(n, dtype=np.int64)
-    for b, (ot, it) in enumerate(keys):
-        row = rows[b]
-        for ax, u in zip(oa, ot[0]):
-            row[ax] = degs[ax][u]
-        for ax, u in zip(ia, it[0]):
-            row[ax] = degs[ax][u]
-        coupled[b] = ot[2]
-    shapes = np.array(rows, dtype=np.int64).reshape(n, nd)
+        vals = np.array([d[u] for u in plan.labels[ax]], dtype=np.int64)
+        shapes[:, ax] = vals[plan.index[:, ax]] if n else 0
     sizes = shapes.prod(axis=1) if n else np.zeros(0, dtype=np.int64)
     offsets = np.zeros(n, dtype=np.int64)
     if n:
@@ -372,7 +397,8 @@ def layout(s: TensorStructure) -> ArenaLayout:
     strides = np.ones((n, nd), dtype=np.int64)
     for ax in range(nd - 2, -1, -1):
         strides[:, ax] = strides[:, ax + 1] * shapes[:, ax + 1]
-    return ArenaLayout(shapes, sizes, offsets, strides, int(sizes.sum()) if n else 0, coupled)
+    return ArenaLayout(shapes, sizes, offsets, strides, int(sizes.sum()) if n else 0,
+                       plan.coupled)
 
 
 # ---------------------------------------------------------------------------------------
@@ -392,44 +418,90 @@ class MatrixLayout:
     cstride: np.ndarray       # (n_blocks, ndim) stride in elements (IN axes)
 
 
+@dataclass(frozen=True)
+class _MatrixPlan:
+    """The degeneracy-free part of a matrix layout, per pattern.  OUT trees (rows) and IN
+    trees (columns) are numbered sector by sector, sectors and trees in sorted order; each
+    block has its sector's and its trees' numbers, each tree its sector's number and a
+    block that carries it (all such blocks share the tree's row or column count)."""
+
+    sectors: tuple           # coupled labels, sorted
+    block_sec: np.ndarray    # (n_blocks,) sector number
+    block_row: np.ndarray    # (n_blocks,) OUT tree number
+    block_col: np.ndarray    # (n_blocks,) IN tree number
+    row_sec: np.ndarray      # (n_rows,) sector number of each OUT tree
+    row_rep: np.ndarray      # (n_rows,) a block with that OUT tree
+    col_sec: np.ndarray
+    col_rep: np.ndarray
+
+
 @cache
-def matrix_layout(s: TensorStructure) -> MatrixLayout:
-    lay = layout(s)
-    keys = s.keys
-    oa, ia = s.out_axes, s.in_axes
-    n, nd = len(keys), s.ndim
-    shapes = lay.shapes
-    rsz = shapes[:, list(oa)].prod(axis=1) if oa else np.ones(n, dtype=np.int64)
-    csz = shapes[:, list(ia)].prod(axis=1) if ia else np.ones(n, dtype=np.int64)
+def _matrix_plan(pat: Pattern) -> _MatrixPlan:
+    keys = block_keys(pat)
     rows: dict = {}
     cols: dict = {}
     for b, (ot, it) in enumerate(keys):
-        rows.setdefault(ot[2], {}).setdefault(ot, int(rsz[b]))
-        cols.setdefault(ot[2], {}).setdefault(it, int(csz[b]))
+        rows.setdefault(ot[2], {}).setdefault(ot, b)
+        cols.setdefault(ot[2], {}).setdefault(it, b)
     sectors = tuple(sorted(rows))
-    shape, base, roff, coff = {}, {}, {}, {}
-    off = 0
-    for c in sectors:
-        r = 0
-        for t in sorted(rows[c]):
-            roff[t] = r
-            r += rows[c][t]
-        q = 0
-        for t in sorted(cols[c]):
-            coff[t] = q
-            q += cols[c][t]
-        shape[c] = (r, q)
-        base[c] = off
-        off += r * q
-    block_sector = np.zeros(n, dtype=np.int64)
-    block_off = np.zeros(n, dtype=np.int64)
-    block_ld = np.zeros(n, dtype=np.int64)
-    for b, (ot, it) in enumerate(keys):
-        c = ot[2]
-        ld = shape[c][1]
-        block_sector[b] = c
-        block_ld[b] = ld
-        block_off[b] = base[c] + roff[ot] * ld + coff[it]
+    sec_no = {c: k for k, c in enumerate(sectors)}
+
+    def number(trees_of):
+        no, sec, rep = {}, [], []
+        for c in sectors:
+            for t in sorted(trees_of[c]):
+                no[(c, t)] = len(sec)
+                sec.append(sec_no[c])
+                rep.append(trees_of[c][t])
+        return no, np.array(sec, dtype=np.int64), np.array(rep, dtype=np.int64)
+
+    row_no, row_sec, row_rep = number(rows)
+    col_no, col_sec, col_rep = number(cols)
+    n = len(keys)
+    block_sec = np.fromiter((sec_no[ot[2]] for ot, _ in keys), dtype=np.int64, count=n)
+    block_row = np.fromiter((row_no[(ot[2], ot)] for ot, _ in keys), dtype=np.int64, count=n)
+    block_col = np.fromiter((col_no[(ot[2], it)] for ot, it in keys), dtype=np.int64, count=n)
+    for a in (block_sec, block_row, block_col, row_sec, row_rep, col_sec, col_rep):
+        a.flags.writeable = False  # shared by every structure of the pattern
+    return _MatrixPlan(sectors, block_sec, block_row, block_col, row_sec, row_rep, col_sec,
+                       col_rep)
+
+
+def _starts(sizes: np.ndarray, group: np.ndarray, n_groups: int) -> tuple:
+    """Per group the total of ``sizes`` and per item its offset inside its group, for
+    items grouped consecutively (``group`` nondecreasing, no group empty); exact integer
+    sums."""
+    if not len(sizes):
+        return np.zeros(n_groups, dtype=np.int64), sizes
+    starts = np.searchsorted(group, np.arange(n_groups))
+    tot = np.add.reduceat(sizes, starts)
+    first = np.zeros(n_groups, dtype=np.int64)
+    first[1:] = np.cumsum(tot)[:-1]
+    return tot, (np.cumsum(sizes) - sizes) - first[group]
+
+
+@cache
+def matrix_layout(s: TensorStructure) -> MatrixLayout:
+    """The coupled-sector matrices of ``s`` (``map_view.py:69-219``): the pattern's plan
+    (``_matrix_plan``) filled with this structure's row and column counts."""
+    lay = layout(s)
+    plan = _matrix_plan(s.pattern)
+    oa, ia = s.out_axes, s.in_axes
+    n, nd = lay.shapes.shape
+    shapes = lay.shapes
+    rsz = shapes[:, list(oa)].prod(axis=1) if oa else np.ones(n, dtype=np.int64)
+    csz = shapes[:, list(ia)].prod(axis=1) if ia else np.ones(n, dtype=np.int64)
+    ns = len(plan.sectors)
+    R, roff = _starts(rsz[plan.row_rep], plan.row_sec, ns)
+    Q, coff = _starts(csz[plan.col_rep], plan.col_sec, ns)
+    area = R * Q
+    base = np.zeros(ns, dtype=np.int64)
+    if ns:
+        base[1:] = np.cumsum(area)[:-1]
+    sec = plan.block_sec
+    block_ld = Q[sec]
+    block_off = base[sec] + roff[plan.block_row] * block_ld + coff[plan.block_col]
+    block_sector = np.array(plan.sectors, dtype=np.int64)[sec] if n else np.zeros(0, np.int64)
     rstride = np.zeros((n, nd), dtype=np.int64)
     cstride = np.zeros((n, nd), dtype=np.int64)
     acc = np.ones(n, dtype=np.int64)
@@ -440,8 +512,10 @@ def matrix_layout(s: TensorStructure) -> MatrixLayout:
     for ax in reversed(ia):
         cstride[:, ax] = acc
         acc = acc * shapes[:, ax]
-    return MatrixLayout(sectors, shape, base, off, block_sector, block_off, block_ld, rstride,
-                        cstride)
+    shape = {c: (int(R[k]), int(Q[k])) for k, c in enumerate(plan.sectors)}
+    bases = {c: int(base[k]) for k, c in enumerate(plan.sectors)}
+    return MatrixLayout(plan.sectors, shape, bases, int(area.sum()), block_sector, block_off,
+                        block_ld, rstride, cstride)
 
 
 def structure_size(s: TensorStructure) -> int:

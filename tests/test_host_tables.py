@@ -242,9 +242,21 @@ def test_native_compose_matches_the_sparse_product_rule():
         assert got.shape == want.shape and np.array_equal(got, want)
 
 
-def test_native_gather_rows_match_the_normalisation_rule():
-    from tenet import _exec
+def _plan_rows(D, DS, RS, CS, d_off, sizes, tb, te, buf):
+    """``tnb_plan_gather_rows`` on host arrays (raises ValueError on a refused row)."""
+    from tenet import _lib
 
+    D = np.asarray(D)
+    R, nd = D.shape
+    rows = np.zeros((R, _exec.SEG_W), np.int64)
+    arrs = [np.ascontiguousarray(x, dtype=np.int64) for x in (D, DS, RS, CS, d_off, sizes, tb, te)]
+    if _lib.load().tnb_plan_gather_rows(R, nd, *(x.ctypes.data for x in arrs), buf,
+                                        rows.ctypes.data) != 0:
+        raise ValueError("refused")
+    return rows
+
+
+def test_native_gather_rows_match_the_normalisation_rule():
     rng = np.random.default_rng(3)
     R, nd = 200, 5
     D = rng.integers(1, 4, size=(R, nd))
@@ -254,7 +266,7 @@ def test_native_gather_rows_match_the_normalisation_rule():
     CS[:, -1], CS[:, -2] = 1, D[:, -1]
     off, size = rng.integers(0, 1000, R), D.prod(axis=1)
     tb = np.arange(R)
-    rows = _exec._plan_rows(D, DS, RS, CS, off, size, tb, tb + 1, 1)
+    rows = _plan_rows(D, DS, RS, CS, off, size, tb, tb + 1, 1)
     for r in range(R):
         segs = _normalise_spec(list(D[r]), list(DS[r]), list(RS[r]), list(CS[r]))
         row = rows[r]
@@ -264,7 +276,73 @@ def test_native_gather_rows_match_the_normalisation_rule():
     with pytest.raises(ValueError):
         big = np.full((1, 9), 2)
         primes = np.array([[29, 23, 19, 17, 13, 11, 7, 5, 3]])  # no two dims merge
-        _exec._plan_rows(big, primes, big * 0, big * 0, [0], [512], [0], [0], 0)
+        _plan_rows(big, primes, big * 0, big * 0, [0], [512], [0], [0], 0)
+
+
+def test_native_gather_table_matches_the_grouping_rule():
+    """``tnb_plan_gather_table``: kept destination blocks' terms grouped by block in block
+    order (given order inside a group), one row each with the first term's source strides
+    permuted, then a zero-writing row per kept block without terms; term outputs in the
+    grouped order."""
+    import ctypes
+
+    from tenet import _lib
+
+    rng = np.random.default_rng(11)
+    for trial in range(30):
+        nd = int(rng.integers(1, 5))
+        n_src, n_dst, nt = int(rng.integers(1, 9)), int(rng.integers(1, 9)), int(rng.integers(0, 25))
+        s_off, s_ld = rng.integers(0, 500, n_src), rng.integers(0, 9, n_src)
+        s_rs, s_cs = rng.integers(0, 5, (n_src, nd)), rng.integers(0, 5, (n_src, nd))
+        d_off, d_str = rng.integers(0, 500, n_dst), rng.integers(0, 7, (n_dst, nd))
+        d_shape = rng.integers(1, 4, (n_dst, nd))
+        d_size = d_shape.prod(axis=1)
+        keep = (rng.random(n_dst) < 0.8).astype(np.uint8)
+        perm = rng.permutation(nd)
+        ts, td = rng.integers(0, n_src, nt), rng.integers(0, n_dst, nt)
+        tc = rng.standard_normal(nt)
+        rows = np.zeros((n_dst, _exec.SEG_W), np.int64)
+        o_src, o_ld, o_cf, counts = (np.zeros(nt, np.int64), np.zeros(nt, np.int64),
+                                     np.zeros(nt), np.zeros(2, np.int64))
+        arrs = [np.ascontiguousarray(x, dtype=np.int64)
+                for x in (ts, td, s_off, s_ld, s_rs, s_cs, d_off, d_str, d_shape, d_size, perm)]
+        st = _lib.load().tnb_plan_gather_table(
+            nt, arrs[0].ctypes.data, arrs[1].ctypes.data, tc.ctypes.data, n_src,
+            *(a.ctypes.data for a in arrs[2:6]), n_dst, *(a.ctypes.data for a in arrs[6:10]),
+            keep.ctypes.data, nd, arrs[10].ctypes.data, 0, rows.ctypes.data, o_src.ctypes.data,
+            o_cf.ctypes.data, o_ld.ctypes.data, counts.ctypes.data)
+        assert st == 0
+        sel = sorted((t for t in range(nt) if keep[td[t]]), key=lambda t: td[t])
+        assert counts[1] == len(sel)
+        assert np.array_equal(o_src[:len(sel)], s_off[ts[sel]])
+        assert np.array_equal(o_ld[:len(sel)], s_ld[ts[sel]])
+        assert np.array_equal(o_cf[:len(sel)], tc[sel])
+        want, q = [], 0
+        while q < len(sel):
+            j, e = td[sel[q]], q
+            while e < len(sel) and td[sel[e]] == j:
+                e += 1
+            i0 = ts[sel[q]]
+            want.append((j, s_rs[i0][perm], s_cs[i0][perm], q, e))
+            q = e
+        covered = set(td.tolist())
+        want += [(j, np.zeros(nd, int), np.zeros(nd, int), len(sel), len(sel))
+                 for j in range(n_dst) if keep[j] and j not in covered]
+        assert counts[0] == len(want)
+        for row, (j, rs, cs, tb, te) in zip(rows, want):
+            segs = _normalise_spec(list(d_shape[j]), list(d_str[j]), list(rs), list(cs))
+            assert tuple(row[:5]) == (d_off[j], d_size[j], len(segs), tb, te)
+            for k, (d, a, b, c) in enumerate(segs):
+                assert (row[8 + k], row[16 + k], row[24 + k], row[32 + k]) == (d, a, b, c)
+        # an out-of-range block index is refused
+        bad = arrs[1].copy()
+        if nt:
+            bad[0] = n_dst
+            assert _lib.load().tnb_plan_gather_table(
+                nt, arrs[0].ctypes.data, bad.ctypes.data, tc.ctypes.data, n_src,
+                *(a.ctypes.data for a in arrs[2:6]), n_dst, *(a.ctypes.data for a in arrs[6:10]),
+                keep.ctypes.data, nd, arrs[10].ctypes.data, 0, rows.ctypes.data,
+                o_src.ctypes.data, o_cf.ctypes.data, o_ld.ctypes.data, counts.ctypes.data) != 0
 
 
 def _seg(dst_off, dims, dstr, rstr, cstr, t0, t1):
