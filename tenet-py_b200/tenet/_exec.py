@@ -165,6 +165,36 @@ class _DevArray:
         return self._n
 
 
+class _UploadSlice:
+    """A table's share of an upload made for several tables at once."""
+
+    __slots__ = ("up", "lo", "hi")
+
+    def __init__(self, up, lo: int, hi: int) -> None:
+        self.up, self.lo, self.hi = up, lo, hi
+
+    def ready(self) -> tuple:
+        return self.up.ready()[self.lo:self.hi]
+
+
+def upload_together(tables) -> None:
+    """One upload (one staging copy, one device buffer, one event) for the arrays of every
+    table in ``tables`` not yet on the device, instead of one each at its first run."""
+    todo, arrays, spans = [], [], []
+    for t in tables:
+        if t is None or getattr(t, "_dev", 1) is not None:
+            continue
+        arrs = t.host_arrays()
+        todo.append(t)
+        spans.append((len(arrays), len(arrays) + len(arrs)))
+        arrays.extend(arrs)
+    if not todo:
+        return
+    up = Uploaded(arrays)
+    for t, (lo, hi) in zip(todo, spans):
+        t._dev = _UploadSlice(up, lo, hi)
+
+
 class Uploaded:
     """Device copies of host arrays, made on the current stream.  A copy from pageable
     host memory may still be in flight when the call returns, so a kernel on another
@@ -351,9 +381,12 @@ class GatherTable:
         destination element written once."""
         return 8 * (self.elems + self.term_elems)
 
+    def host_arrays(self) -> tuple:
+        return (self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map)
+
     def device_arrays(self):
         if self._dev is None:
-            self._dev = Uploaded((self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map))
+            self._dev = Uploaded(self.host_arrays())
         return self._dev.ready()
 
     def run(self, src0, dst0, src1=None, dst1=None) -> None:
@@ -428,10 +461,12 @@ class ProductGather(GatherTable):
         r = self.gemm.table
         return 8 * (self.elems + int((r[:, 0] * r[:, 2] + r[:, 2] * r[:, 1]).sum()))
 
+    def host_arrays(self) -> tuple:
+        return (self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map, self.tprod)
+
     def device_arrays(self):
         if self._dev is None:
-            self._dev = Uploaded((self.seg, self.tsrc, self.tcf, self.tld, self.chunk_map,
-                                  self.tprod))
+            self._dev = Uploaded(self.host_arrays())
         return self._dev.ready()
 
     def run(self, a, b, dst) -> None:
@@ -571,10 +606,13 @@ class GemmTable:
             self._work[key] = buf
         return buf
 
+    def host_arrays(self) -> tuple:
+        return (self.table, self.tile_map)
+
     def device_tables(self):
         """(table, tile_map) on the current device, uploaded on first use."""
         if self._dev is None:
-            self._dev = Uploaded((self.table, self.tile_map))
+            self._dev = Uploaded(self.host_arrays())
         return self._dev.ready()
 
     def run(self, a, b, c) -> None:

@@ -140,6 +140,9 @@ class ContractionExec:
             ap, bp, cp = scratch
         if out is None:
             out = torch.empty(layout(self.out).size, dtype=torch.float64, device=dev)
+        if self.pack._dev is None:  # first run: every table of this contraction at once
+            _exec.upload_together((self.pack, *getattr(self.gemm, "parts", (self.gemm,)),
+                                   self.unpack))
         self.pack.run(a, ap, b, bp)
         self.gemm.run(ap, bp, cp)
         self.unpack.run(cp, out)

@@ -285,6 +285,11 @@ class ChainProgram:
         """Allocate every buffer once and pack the fixed operands (needs the device)."""
         dev = _exec.device()
         f64 = dict(dtype=torch.float64, device=dev)
+        # every table of the chain in one upload, made on the shared template's tables
+        # (programs rebound from one template upload once; private copies share it)
+        _exec.upload_together([t for lk in self.links
+                               for t in (lk.a_gather, lk.b_gather, *lk.gemm.parts)]
+                              + [self.out_gather])
         for lk in self.links:  # split-K scratch of this program's own
             lk.gemm = lk.gemm.private()
         self.a_bufs = [torch.empty(max(1, lk.a_size), **f64) for lk in self.links]
