@@ -38,10 +38,21 @@ IN = Side.IN
 
 @dataclass(frozen=True, slots=True)
 class GradedSpace:
-    """``V = (+)_a C^{m_a} (x) V_a``; sectors sorted, all ``m >= 1`` (``space.py:27-140``)."""
+    """``V = (+)_a C^{m_a} (x) V_a``; sectors sorted, all ``m >= 1`` (``space.py:27-140``).
+    The hash is computed once (spaces key the planner's caches)."""
 
     provider: Provider
     sectors: tuple
+    _hash: int = field(default=0, init=False, repr=False, compare=False)
+
+    def __post_init__(self) -> None:
+        object.__setattr__(self, "_hash", hash((self.provider, self.sectors)))
+
+    def __hash__(self) -> int:
+        return self._hash
+
+    def __reduce__(self):  # rebuilt where it lands: hashes differ between processes
+        return (GradedSpace, (self.provider, self.sectors))
 
     @classmethod
     def new(cls, provider: Provider, sectors: Mapping | Iterable) -> GradedSpace:
@@ -160,10 +171,21 @@ class FusionBlockKey:
 
 @dataclass(frozen=True, slots=True)
 class Pattern:
-    """A structure with degeneracies dropped: provider + per leg (labels, is_out, dual)."""
+    """A structure with degeneracies dropped: provider + per leg (labels, is_out, dual).
+    The hash is computed once (patterns key the planner's caches)."""
 
     provider: Provider
     legs: tuple  # ((labels, is_out, dual), ...)
+    _hash: int = field(default=0, init=False, repr=False, compare=False)
+
+    def __post_init__(self) -> None:
+        object.__setattr__(self, "_hash", hash((self.provider, self.legs)))
+
+    def __hash__(self) -> int:
+        return self._hash
+
+    def __reduce__(self):  # rebuilt where it lands: hashes differ between processes
+        return (Pattern, (self.provider, self.legs))
 
     @property
     def out_axes(self) -> tuple[int, ...]:
