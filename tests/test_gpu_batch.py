@@ -2,7 +2,6 @@
 update on coarsened tensors (``tests/_coarsen.py``), the unbatched device path, and, in
 reduced precision, the FP64 batch."""
 
-import numpy as np
 import pytest
 import torch
 
