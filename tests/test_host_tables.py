@@ -392,3 +392,11 @@ def test_product_gather_plans_windows_and_refuses_the_rest():
     split.table = split.table.copy()
     split.table[0, 12] = 2
     assert _exec.product_gather(g, split) is None
+
+
+def test_graph_matvec_refuses_an_unknown_host_copy_mode():
+    """``GraphMatvec(host_copy=...)`` is checked before anything touches the device."""
+    from tenet.program import GraphMatvec
+
+    with pytest.raises(ValueError, match="host_copy"):
+        GraphMatvec(None, host_io=True, host_copy="zero-copy")
