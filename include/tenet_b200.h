@@ -5,7 +5,7 @@
  * dispatch `ar.do(name, block, ...)` inside a per-block loop.  This library replaces
  * those loops with sm_100a kernels driven by flat descriptor tables that the Python
  * host planner builds once per tensor structure.  A maintainer binds it from Python
- * with ctypes (see INTEGRATION.md); no torch type crosses this boundary.
+ * with ctypes; no torch type crosses this boundary.
  *
  * Conventions for every entry point
  *   - All pointers are DEVICE pointers to caller-owned memory unless stated; the
@@ -195,7 +195,9 @@ int tnb_weighted_dot(const double* x, const double* y, int64_t n,
  * TNB_DOT_NOALLOC_MAX_N = 2,097,152 elements; a larger n is refused with
  * TNB_EINVAL before anything runs.  The first call on a device looks up the array's
  * device address (set-up, once per device, with that device current): make that first
- * call before any stream capture.  Each call zeroes the counter and overwrites the
+ * call before any stream capture.  cudaDeviceReset unloads the module and invalidates
+ * the cached address: a call that then finds its launch refused looks the address up
+ * again and retries once.  Each call zeroes the counter and overwrites the
  * partials; every call shares the one array, so calls that overlap on the GPU (two
  * streams at once) race -- serialise them.  No cudaMalloc, cudaFree or allocating
  * library routine is called.

@@ -9,9 +9,9 @@ namespace tnb {
 __device__ int g_device_error = 0;
 
 static thread_local std::string g_last_error;
-static bool g_pdl = true;
+static std::atomic<bool> g_pdl{true};
 
-bool pdl_enabled() { return g_pdl; }
+bool pdl_enabled() { return g_pdl.load(std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 
@@ -29,8 +29,7 @@ int check_launch(const char* what) {
 extern "C" int tnb_version(void) { return 100; }
 
 extern "C" int tnb_set_pdl(int enabled) {
-  const int prev = tnb::g_pdl ? 1 : 0;
-  tnb::g_pdl = enabled != 0;
+  const int prev = tnb::g_pdl.exchange(enabled != 0) ? 1 : 0;
   return prev;
 }
 

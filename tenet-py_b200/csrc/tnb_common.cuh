@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 
 #include "tenet_b200.h"
@@ -78,6 +80,63 @@ cudaError_t launch_dyn(void (*kernel)(KArgs...), unsigned grid, unsigned block, 
   cfg.numAttrs = pdl_enabled() ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
 }
+
+// Devices a process-wide per-device cache covers.
+constexpr int kMaxDevices = 64;
+
+// A kernel attribute (the dynamic shared-memory opt-in) is set per device, so a
+// process that uses several GPUs must set it once on each.  `once(fn)` runs `fn` the
+// first time it is called with a given device current and caches success; concurrent
+// callers serialise on the mutex, and a failed attempt is retried by the next call.
+class PerDeviceOnce {
+ public:
+  template <class F>
+  cudaError_t once(F&& fn) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (done_[device].load(std::memory_order_acquire)) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(mu_);
+    if (done_[device].load(std::memory_order_relaxed)) return cudaSuccess;
+    e = fn();
+    if (e == cudaSuccess) done_[device].store(true, std::memory_order_release);
+    return e;
+  }
+
+ private:
+  std::mutex mu_;
+  std::atomic<bool> done_[kMaxDevices] = {};
+};
+
+// An integer attribute of the current device, computed once per device by `fn(device,
+// &value)` and cached (0 when it cannot be computed, which is retried next time).
+class PerDeviceInt {
+ public:
+  template <class F>
+  int get(F&& fn) {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) {
+      cudaGetLastError();
+      return 0;
+    }
+    int v = value_[device].load(std::memory_order_acquire);
+    if (v) return v;
+    std::lock_guard<std::mutex> lock(mu_);
+    v = value_[device].load(std::memory_order_relaxed);
+    if (v) return v;
+    if (fn(device, &v) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    value_[device].store(v, std::memory_order_release);
+    return v;
+  }
+
+ private:
+  std::mutex mu_;
+  std::atomic<int> value_[kMaxDevices] = {};
+};
 
 // Tensor-core grouped GEMM launcher (tnb_gemm_tc.cu).
 cudaError_t launch_gemm_tc(int kind, unsigned grid, cudaStream_t s, const int64_t* table,

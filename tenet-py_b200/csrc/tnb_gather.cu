@@ -36,19 +36,10 @@ gather_kernel(const GatherArgs g) {
 
 // SMs of the current device (0 when it cannot be queried), cached per device.
 int device_sms() {
-  static int cached[64] = {0};
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= 64) {
-    cudaGetLastError();
-    return 0;
-  }
-  if (cached[device] == 0 &&
-      cudaDeviceGetAttribute(&cached[device], cudaDevAttrMultiProcessorCount, device) !=
-          cudaSuccess) {
-    cudaGetLastError();
-    cached[device] = 0;
-  }
-  return cached[device];
+  static PerDeviceInt cached;
+  return cached.get([](int device, int* v) {
+    return cudaDeviceGetAttribute(v, cudaDevAttrMultiProcessorCount, device);
+  });
 }
 
 // The product-source form: every source element is an element of C = A x B of a GEMM

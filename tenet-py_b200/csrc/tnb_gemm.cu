@@ -40,13 +40,12 @@ gemm_f64_kernel(const GemmArgs g) {
 template <int TM, int TN>
 cudaError_t launch_gemm_f64(unsigned grid, cudaStream_t s, const GemmArgs& g) {
   constexpr size_t kSmem = sizeof(GemmSmem<TM, TN, kGemmStages<TM>>);
-  static bool opted = false;
-  if (!opted) {
-    const cudaError_t e = cudaFuncSetAttribute(
-        gemm_f64_kernel<TM, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
-    if (e != cudaSuccess) return e;
-    opted = true;
-  }
+  static PerDeviceOnce opted;
+  const cudaError_t e = opted.once([] {
+    return cudaFuncSetAttribute(gemm_f64_kernel<TM, TN>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+  });
+  if (e != cudaSuccess) return e;
   return launch_dyn(gemm_f64_kernel<TM, TN>, grid, (TM / 4) * (TN / 4), kSmem, s, g);
 }
 

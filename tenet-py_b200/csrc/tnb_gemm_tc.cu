@@ -208,7 +208,7 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   __shared__ __align__(8) uint64_t full[kT2Stages], empty[kT2Stages], done;
   __shared__ uint32_t s_tmem;
   __shared__ T2Row s_row;
-  __shared__ int s_ok, s_fail;
+  __shared__ int s_ok, s_fail, s_fills, s_drain_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) {
@@ -227,6 +227,8 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
     s_row = r;
     s_ok = ok;
     s_fail = 0;
+    s_fills = 0;
+    s_drain_fail = 0;
     for (int st = 0; st < kT2Stages; ++st) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&full[st])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&empty[st])) : "memory");
@@ -270,6 +272,7 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
       const uint32_t sa = smem_u32(smem + st * L::kStageBytes);
       bulk_copy(sa, a_src + s * kT2Slab, kT2Slab, fb);
       bulk_copy(sa + kT2Slab, b_src + s * kT2Slab, kT2Slab, fb);
+      s_fills = static_cast<int>(s + 1);
     }
   } else if (tid == 32 && nk > 0) {  // MMA issuer
     uint32_t fphase[kT2Stages] = {0u, 0u, 0u};
@@ -316,10 +319,24 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
                  :: "r"(smem_u32(&done)) : "memory");
   }
   __syncthreads();
-  if (nk > 0 && !s_fail && !mbar_wait(smem_u32(&done), 0u)) {
-    if (lane == 0) {
+  // Drain before the stages are reused and TMEM is freed, on the error path too: the
+  // issuer commits `done` after whatever MMAs it issued, and every stage's last fill has
+  // bulk copies that land whatever happened to the consumer.  A drain that itself gives
+  // up leaves shared memory and TMEM possibly still being written, so the epilogue then
+  // stores nothing.
+  if (tid == 0 && nk > 0) {
+    if (!mbar_wait(smem_u32(&done), 0u)) {
       atomicCAS(&g_device_error, 0, TNB_ETIMEOUT);
       s_fail = 1;
+      s_drain_fail = 1;
+    }
+    if (s_fail) {
+      const int fills = s_fills;
+      for (int st = 0; st < kT2Stages && st < fills; ++st) {
+        const int n_st = (fills - st + kT2Stages - 1) / kT2Stages;  // fills of stage st
+        if (!mbar_wait(smem_u32(&full[st]), static_cast<uint32_t>((n_st - 1) & 1)))
+          s_drain_fail = 1;
+      }
     }
   }
   __syncthreads();
@@ -337,7 +354,7 @@ tc_mma_kernel(const int64_t* __restrict__ table, int64_t n_gemm,
   // conditions are uniform across the warp, as tcgen05.ld requires)
   const int64_t cols = ok ? r.N - n0 : 0;
   const int n_chunks = cols >= kT2N ? kT2N / 16 : static_cast<int>((cols + 15) / 16);
-  const int warp_chunks = ok && row0 < r.M ? n_chunks : 0;
+  const int warp_chunks = ok && row0 < r.M && !s_drain_fail ? n_chunks : 0;
 #pragma unroll 1
   for (int chunk = 0; chunk < warp_chunks; ++chunk) {
     uint32_t v[16];
@@ -382,16 +399,13 @@ cudaError_t launch_tc_mode(unsigned grid, cudaStream_t s, const int64_t* table, 
                            const double* b, int64_t n_b, double* c, int64_t n_c, void* work,
                            int64_t work_bytes, int64_t a_chunks, int64_t b_chunks) {
   using L = T2Layout<MODE>;
-  static bool opted = false;
-  if (!opted) {
-    const cudaError_t e = cudaFuncSetAttribute(tc_mma_kernel<MODE>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               L::kSmemBytes);
-    if (e != cudaSuccess) return e;
-    opted = true;
-  }
+  static PerDeviceOnce opted;
+  cudaError_t e = opted.once([] {
+    return cudaFuncSetAttribute(tc_mma_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                L::kSmemBytes);
+  });
+  if (e != cudaSuccess) return e;
   auto* w = static_cast<uint8_t*>(work);
-  cudaError_t e = cudaSuccess;
   if (a_chunks + b_chunks > 0)
     e = launch(tc_pack_kernel<MODE>, static_cast<unsigned>(a_chunks + b_chunks), kPackThreads, s,
                table, n_gemm, a, n_a, b, n_b, w, work_bytes, a_chunks);

@@ -143,20 +143,23 @@ chain_kernel(const FChain ch, const double* x, double* y, unsigned int* bar) {
 // CTAs of one cooperative chain launch on `device`: as many as can be resident (0 when
 // the kernel cannot be configured).
 int fused_grid(int device) {
-  static int cached[64] = {0};
-  if (device < 0 || device >= 64) return 0;
-  if (cached[device]) return cached[device];
-  const size_t smem = sizeof(FusedSmem);
-  if (cudaFuncSetAttribute(chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(smem)) != cudaSuccess)
+  static PerDeviceInt cached;
+  int current = -1;
+  if (cudaGetDevice(&current) != cudaSuccess || current != device) {
+    cudaGetLastError();
     return 0;
-  int per_sm = 0, sms = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel, kFusedThreads, smem) !=
-          cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
-    return 0;
-  cached[device] = per_sm * sms;
-  return cached[device];
+  }
+  return cached.get([](int dev, int* v) {
+    const size_t smem = sizeof(FusedSmem);
+    cudaError_t e = cudaFuncSetAttribute(chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel, kFusedThreads, smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    *v = per_sm * sms;
+    return e;
+  });
 }
 
 }  // namespace tnb

@@ -304,7 +304,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[256 + 8 * kNoAl
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[128] = {};
 
-static int noalloc_scratch(void** out) {
+// `refresh` drops the cached address first (after cudaDeviceReset the module is loaded
+// again and the array may sit elsewhere).
+static int noalloc_scratch(void** out, bool refresh = false) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= 128) {
@@ -312,6 +314,7 @@ static int noalloc_scratch(void** out) {
     return TNB_ECUDA;
   }
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (refresh) g_noalloc_ptr[dev] = nullptr;
   if (g_noalloc_ptr[dev] == nullptr) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -352,14 +355,20 @@ extern "C" int tnb_weighted_dot_noalloc(const double* x, const double* y, int64_
               "tnb_weighted_dot_noalloc: null input");
   void* base = nullptr;
   if (int st = tnb::noalloc_scratch(&base)) return st;
-  auto* counter = static_cast<unsigned int*>(base);
-  auto* partial = reinterpret_cast<double*>(static_cast<char*>(base) + 256);
   // the counter must start at zero whatever an earlier (possibly failed) call left
-  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), s);
+  cudaError_t e = cudaMemsetAsync(base, 0, sizeof(unsigned int), s);
+  if (e == cudaErrorInvalidValue || e == cudaErrorContextIsDestroyed) {
+    // a stale address from before a device reset: look it up again, once
+    cudaGetLastError();
+    if (int st = tnb::noalloc_scratch(&base, true)) return st;
+    e = cudaMemsetAsync(base, 0, sizeof(unsigned int), s);
+  }
   if (e != cudaSuccess) {
     tnb::set_error(std::string("tnb_weighted_dot_noalloc: ") + cudaGetErrorString(e));
     return TNB_ECUDA;
   }
+  auto* counter = static_cast<unsigned int*>(base);
+  auto* partial = reinterpret_cast<double*>(static_cast<char*>(base) + 256);
   const int64_t grid = (n + tnb::kNoAllocChunk - 1) / tnb::kNoAllocChunk;
   tnb::wdot_kernel<<<static_cast<unsigned>(grid), tnb::kDotThreads, 0, s>>>(
       x, y, n, run_start, run_w, n_runs, tnb::kNoAllocChunk, counter, partial, out);

@@ -30,8 +30,8 @@ import numpy as np
 from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure, layout
 from tenet.symmetry import SU2, U1, Z2, ProductSector, Provider, U1xU1xfZ2, fZ2
 
-__all__ = ["FORMAT_VERSION", "MPS_FORMAT_VERSION", "load", "load_arena", "load_mps", "save",
-           "save_arena", "save_mps"]
+__all__ = ["FORMAT_VERSION", "MPS_FORMAT_VERSION", "accept_su2_gauge", "load", "load_arena",
+           "load_mps", "save", "save_arena", "save_mps"]
 
 FORMAT_VERSION = 1
 MPS_FORMAT_VERSION = 1
@@ -39,7 +39,13 @@ VERSION = "tenet_b200 0.1"
 
 _FZ2_GAUGE = "f=1;r=fermionic;fs=+1;twist=(-1)^p;perm=koszul"
 _SU2_GAUGE = "3j=condon-shortley;cg=condon-shortley;f=tks-su2irrep;r=tks-su2irrep;fs=tks-su2irrep"
-_SU2_READ_PREFIX = "su2=racah;"
+# SU(2) gauges a file may carry besides the one written here, each naming a coefficient
+# source whose F / R / B values are known to equal this build's (to 4.4e-16 on every row
+# of the reference's F fixture): the racah build the reference's on-disk fixtures were
+# written under.  Any other ``su2=racah;<fingerprint>`` is refused, as the reference
+# refuses a racah release that moves coefficient values (``serialize.py:99-103``).
+# ``accept_su2_gauge`` adds one for a racah build a caller has checked against the table.
+_SU2_KNOWN = {"su2=racah;racah-shim-su2-exact-racah-formula"}
 _SIMPLE = {"U1": U1, "Z2": Z2, "fZ2": fZ2, "SU2": SU2}
 
 
@@ -109,11 +115,19 @@ def _gauges(s: TensorStructure) -> dict:
 
 def _check_gauges(path, gauges: dict) -> None:
     for kind, gauge in gauges.items():
-        ok = {"SU2": gauge == _SU2_GAUGE or gauge.startswith(_SU2_READ_PREFIX),
+        ok = {"SU2": gauge == _SU2_GAUGE or gauge in _SU2_KNOWN,
               "fZ2": gauge == _FZ2_GAUGE}.get(kind, True)
         if not ok:
             raise ValueError(f"{path}: {kind} coefficient gauge on disk is {gauge!r}; this build "
                              "runs a different convention and the blocks are not comparable")
+
+
+def accept_su2_gauge(gauge: str) -> None:
+    """Accept files whose SU(2) gauge string is ``gauge`` (e.g. ``"su2=racah;<fingerprint>"``
+    of a racah build whose coefficients the caller has checked equal this build's)."""
+    if not isinstance(gauge, str) or not gauge:
+        raise TypeError("gauge must be a non-empty string")
+    _SU2_KNOWN.add(gauge)
 
 
 def save_arena(s: TensorStructure, host: np.ndarray, path, *, compress: bool = False) -> None:

@@ -323,7 +323,9 @@ def make_f_sample(ref: Path) -> None:
 
 
 def main() -> None:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <path to the TeNeT-py tree>")
+    ref = Path(sys.argv[1])
     _setup(ref)
     store = Store()
     make_cases(store)

@@ -107,4 +107,7 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_serialize_golden.py "
+                         "<path to the TeNeT-py tree>")
+    main(Path(sys.argv[1]))

@@ -69,6 +69,17 @@ def test_loader_refusals(tmp_path):
         serialize.load_arena(write("f.npz", {**header, "format": 2}, blocks))
     with pytest.raises(ValueError, match="gauge"):
         serialize.load_arena(write("g.npz", {**header, "gauges": {"SU2": "other"}}, blocks))
+    # a racah build of unknown coefficients is refused, a known or accepted one loads
+    unknown = write("u.npz", {**header, "gauges": {"SU2": "su2=racah;unknown-build"}}, blocks)
+    with pytest.raises(ValueError, match="gauge"):
+        serialize.load_arena(unknown)
+    serialize.load_arena(write("k.npz", {**header, "gauges": {
+        "SU2": "su2=racah;racah-shim-su2-exact-racah-formula"}}, blocks))
+    serialize.accept_su2_gauge("su2=racah;unknown-build")
+    try:
+        serialize.load_arena(unknown)
+    finally:
+        serialize._SU2_KNOWN.discard("su2=racah;unknown-build")
     with pytest.raises(ValueError, match="blocks"):
         serialize.load_arena(write("n.npz", {**header, "num_blocks": 1}, blocks))
     with pytest.raises(ValueError, match="unexpected"):
