@@ -9,7 +9,7 @@ path; the host only plans.
 
 from tenet import linalg, network, symmetry
 from tenet.serialize import load, save
-from tenet.ops import add, adjoint, compose, contractible, divide, einsum, inner, multiply, \
+from tenet.ops import add, adjoint, block_sqrt, compose, contractible, divide, einsum, inner, multiply, \
     norm, outward_dual, repartition, subtract, tensordot, transpose
 from tenet.structure import IN, OUT, FusionBlockKey, FusionTree, GradedSpace, Leg, Side, \
     TensorStructure
@@ -17,7 +17,7 @@ from tenet.tensor import SymmetricTensor
 
 __all__ = [
     "IN", "OUT", "FusionBlockKey", "FusionTree", "GradedSpace", "Leg", "Side",
-    "SymmetricTensor", "TensorStructure", "add", "adjoint", "compose", "contractible",
+    "SymmetricTensor", "TensorStructure", "add", "adjoint", "block_sqrt", "compose", "contractible",
     "divide", "einsum", "inner", "linalg", "load", "multiply", "network", "norm",
     "outward_dual", "repartition", "save", "subtract", "symmetry", "tensordot", "transpose",
 ]

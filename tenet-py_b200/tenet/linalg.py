@@ -58,8 +58,13 @@ class BondSelection:
     scale: float
 
 
-def decide(spectrum, provider, max_bond, cutoff, cutoff_mode="rsum2", renorm=False):
+def decide(spectrum, provider, max_bond, cutoff, cutoff_mode="rsum2", renorm=False,
+           budget="dense"):
+    """The keep rule (``ops/linalg.py:1274-1324``).  ``budget="reduced"`` counts each
+    kept multiplet as 1 against ``max_bond`` instead of its dimension (a build-side
+    mode; the reference's budget is the dense one)."""
     qdim = provider._qdim
+    cost = qdim if budget == "dense" else (lambda c: 1)
     if not spectrum:
         raise ValueError("svd_truncated: this tensor has no singular values at all")
     adm = _admissible(spectrum, qdim, cutoff, cutoff_mode)
@@ -67,9 +72,11 @@ def decide(spectrum, provider, max_bond, cutoff, cutoff_mode="rsum2", renorm=Fal
     dense = 0.0
     kept_w = 0.0
     n = 0
+    used = 0
     for s, c, _ in spectrum[:adm]:
-        if max_bond is not None and dense + qdim(c) > max_bond:
+        if max_bond is not None and used + cost(c) > max_bond:
             break
+        used += cost(c)
         dense += qdim(c)
         keep[c] = keep.get(c, 0) + 1
         kept_w += qdim(c) * s * s
@@ -97,9 +104,11 @@ def _raise_exec(s: TensorStructure):
 
 
 def svd_truncated(t: SymmetricTensor, axes=None, *, max_bond=None, cutoff=None,
-                  cutoff_mode: str = "rsum2", renorm: bool = False):
+                  cutoff_mode: str = "rsum2", renorm: bool = False, budget: str = "dense"):
     """``U, S, Vh`` on the truncated bond.  Same legs, keep rule and refusals as the
-    reference; returns ``(U, S, Vh)``."""
+    reference; returns ``(U, S, Vh)``.  ``budget`` as in ``decide``."""
+    if budget not in ("dense", "reduced"):
+        raise ValueError(f"unknown budget {budget!r}")
     if max_bond is None and cutoff is None:
         raise ValueError("svd_truncated needs at least one of max_bond or cutoff")
     if max_bond is not None and max_bond <= 0:
@@ -132,7 +141,7 @@ def svd_truncated(t: SymmetricTensor, axes=None, *, max_bond=None, cutoff=None,
     spectrum = [(float(sg), c, i) for c in ml.sectors for i, sg in enumerate(host_s[c])]
     spectrum.sort(key=lambda e: (-e[0], e[1], e[2]))
     p = t.provider
-    sel = decide(spectrum, p, max_bond, cutoff, cutoff_mode, renorm)
+    sel = decide(spectrum, p, max_bond, cutoff, cutoff_mode, renorm, budget)
     bond = GradedSpace.new(p, {p.sector(c): k for c, k in sel.keep.items()})
     su = TensorStructure((*m.codomain, Leg(bond, IN)))
     ss = TensorStructure((Leg(bond, OUT), Leg(bond, IN)))

@@ -12,7 +12,8 @@ pairwise contraction whose bent wires are named (``_composed``, ``network/env.py
 
 from __future__ import annotations
 
-from collections.abc import Callable
+from collections.abc import Callable, Sequence
+from typing import NamedTuple
 
 import numpy as np
 import torch
@@ -21,7 +22,8 @@ from tenet import ops
 from tenet.structure import OUT
 from tenet.tensor import SymmetricTensor
 
-__all__ = ["composed", "env_update_first", "env_update_last", "heff2", "lanczos"]
+__all__ = ["DMRG_out", "Env", "MPO", "MPS", "Sweep", "composed", "ctmrg", "dmrg_",
+           "env_update_first", "env_update_last", "heff2", "lanczos", "spectrum", "sweep_"]
 
 
 def composed(equation: str, a: SymmetricTensor, b: SymmetricTensor, bend: str = "") -> SymmetricTensor:
@@ -52,32 +54,69 @@ def heff2(fl: SymmetricTensor, w1: SymmetricTensor, w2: SymmetricTensor, fr: Sym
     return composed("aPQxs,axB->BPQs", t, fl, bend="a")
 
 
-def env_update_last(f: SymmetricTensor, a: SymmetricTensor, w: SymmetricTensor) -> SymmetricTensor:
-    """``F[(n, n+1)]`` from ``F[(n-1, n)]``, bra = ket (``network/env.py:620-625``)."""
-    bra = ops.adjoint(a)
+def env_update_last(f: SymmetricTensor, a: SymmetricTensor, w: SymmetricTensor,
+                    bra_site: SymmetricTensor | None = None) -> SymmetricTensor:
+    """``F[(n, n+1)]`` from ``F[(n-1, n)]`` (``network/env.py:618-626``); the bra site is
+    ``a`` unless ``bra_site`` is given."""
+    bra = ops.adjoint(a if bra_site is None else bra_site)
     t = ops.einsum("axB,apr->xBpr", f, a)
     t = ops.einsum("xPpm,xBpr->BrPm", w, t)
     return ops.einsum("BPs,BrPm->rms", bra, t)
 
 
-def env_update_first(f: SymmetricTensor, a: SymmetricTensor, w: SymmetricTensor) -> SymmetricTensor:
-    """``F[(n, n-1)]`` from ``F[(n+1, n)]``, bra = ket (``network/env.py:626-629``)."""
-    bra = ops.adjoint(a)
+def env_update_first(f: SymmetricTensor, a: SymmetricTensor, w: SymmetricTensor,
+                     bra_site: SymmetricTensor | None = None) -> SymmetricTensor:
+    """``F[(n, n-1)]`` from ``F[(n+1, n)]`` (``network/env.py:627-633``); the bra site is
+    ``a`` unless ``bra_site`` is given."""
+    bra = ops.adjoint(a if bra_site is None else bra_site)
     t = ops.einsum("apr,rys->apys", a, f)
     t = composed("apys,xPpy->axPs", t, w, bend="p")
     return composed("axPs,BPs->axB", t, bra, bend="P")
 
 
+def _orthonormal(vectors) -> tuple:
+    """Gram-Schmidt of ``vectors`` against each other, null ones dropped
+    (``network/dmrg.py:70-87``): ``(vector, <vector, vector>)`` pairs."""
+    basis: list = []
+    for t in vectors:
+        t = _project_out(t, basis)
+        gram = float(ops.inner(t, t))
+        if abs(gram) > 1e-24 and float(ops.norm(t)) > 1e-12:
+            basis.append((t, gram))
+    return tuple(basis)
+
+
+def _project_out(t: SymmetricTensor, basis) -> SymmetricTensor:
+    """``t - sum_k b_k <b_k, t> / <b_k, b_k>`` (``network/dmrg.py:90-103``)."""
+    for b, gram in basis:
+        t = ops.subtract(t, b * (float(ops.inner(b, t)) / gram))
+    return t
+
+
 def lanczos(matvec: Callable[[SymmetricTensor], SymmetricTensor], v: SymmetricTensor, *,
-            ncv: int = 3, tol: float = 1e-13,
+            ncv: int = 3, tol: float = 1e-13, orthogonal_to: Sequence[SymmetricTensor] = (),
             correct: Callable[[SymmetricTensor], SymmetricTensor] | None = None
             ) -> tuple[float, SymmetricTensor]:
     """Ground Ritz pair of a Hermitian ``matvec`` (``network/dmrg.py:106-227``).
 
-    ``correct`` is the FP64 correction of the precision form: when ``matvec`` runs its
-    products in reduced precision, the returned energy is the Rayleigh quotient
-    ``<v|H v>`` of the Ritz vector under the FP64 operator ``correct`` -- one FP64 matvec
-    per solve -- whose error is quadratic in the Ritz vector's."""
+    ``orthogonal_to`` holds the solve orthogonal to the given vectors by hard projection
+    of the start vector and of every matvec result (the reference's rule; ``ValueError``
+    when the projected start vector vanishes).  ``correct`` is the FP64 correction of the
+    precision form: when ``matvec`` runs its products in reduced precision, the returned
+    energy is the Rayleigh quotient ``<v|H v>`` of the Ritz vector under the FP64
+    operator ``correct`` -- one FP64 matvec per solve -- whose error is quadratic in the
+    Ritz vector's."""
+    basis = _orthonormal(orthogonal_to)
+    if basis:
+        v = _project_out(v, basis)
+        if float(ops.norm(v)) < 1e-12:
+            raise ValueError("the start vector lies in the span of orthogonal_to, so there is "
+                             "no vector left to iterate on at this bond")
+        full = matvec
+
+        def matvec(x: SymmetricTensor) -> SymmetricTensor:
+            return _project_out(full(x), basis)
+
     vecs = [v / ops.norm(v)]
     alphas: list[float] = []
     betas: list[float] = []
@@ -294,6 +333,21 @@ class MPO:
     def __init__(self, sites) -> None:
         self.sites = list(sites)
 
+    @classmethod
+    def identity(cls, n_sites: int, phys) -> "MPO":
+        """The identity operator on ``n_sites`` sites of ``phys`` with a unit MPO bond
+        (``network/mps.py:2745-2777``): the overlap operator of a two-state ``Env``."""
+        from tenet.structure import GradedSpace, Leg
+
+        sym = phys.provider
+        unit = GradedSpace.new(sym, {sym.unit: 1})
+        eye = ops.identity((Leg(unit, OUT), Leg(phys, OUT)))  # (u OUT, p OUT, u IN, p IN)
+        return cls([ops.transpose(eye, (2, 1, 3, 0))] * n_sites)
+
+    def materialize(self) -> "MPO":
+        """The site-tensor form: this MPO already is one."""
+        return self
+
     def __len__(self) -> int:
         return len(self.sites)
 
@@ -409,38 +463,56 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
 
 
 class Env:
-    """``<psi|H|psi>`` environments keyed by directed bond (``network/env.py:435-645``):
+    """``<bra|H|psi>`` environments keyed by directed bond (``network/env.py:435-645``):
     ``F[(n, n+1)] = (ket IN, mpo OUT, bra OUT)`` from sites ``<= n``, ``F[(n, n-1)] =
-    (ket OUT, mpo IN, bra IN)`` from sites ``>= n``.  ``compiled=True`` runs ``heff2`` as a
-    CUDA-graph-captured chain program, rebuilt whenever the bond's tensors change."""
+    (ket OUT, mpo IN, bra IN)`` from sites ``>= n``; ``bra`` defaults to ``psi``.
 
-    def __init__(self, psi: MPS, h: MPO, *, compiled: bool = True,
-                 precision: str = "f64", tc_min_flops: int | None = None) -> None:
+    ``compile`` is the reference's injection seam (``network/env.py:448-453,750-769``): a
+    callable that wraps the bond's two-site matvec once per structure key, and whose result
+    then serves every ``heff2`` call with that key.  Without it the matvec runs as this
+    build's compiled form (``compiled=True``): a recorded, graph-captured chain program
+    rebuilt whenever the bond's structures change, and a device-resident Lanczos."""
+
+    def __init__(self, psi: MPS, h: MPO, *, bra: MPS | None = None, compile=None,
+                 compiled: bool = True, precision: str = "f64",
+                 tc_min_flops: int | None = None) -> None:
         from tenet.structure import IN, Leg
 
         self.psi, self.h, self.compiled, self.precision = psi, h, compiled, precision
+        self.bra = psi if bra is None else bra
+        self.compile = compile
         self.tc_min_flops = tc_min_flops
         n = len(psi)
         kl, kr = psi[0].legs[0], psi[n - 1].legs[2]
+        bl, br = self.bra[0].legs[0], self.bra[len(self.bra) - 1].legs[2]
         wl, wr = h[0].legs[0], h[n - 1].legs[3]
         self.F = {
             (-1, 0): ones((Leg(kl.space, IN, kl.dual), Leg(wl.space, OUT, wl.dual),
-                           Leg(kl.space, OUT, kl.dual))),
+                           Leg(bl.space, OUT, bl.dual))),
             (n, n - 1): ones((Leg(kr.space, OUT, kr.dual), Leg(wr.space, IN, wr.dual),
-                              Leg(kr.space, IN, kr.dual))),
+                              Leg(br.space, IN, br.dual))),
         }
         self._prog: dict = {}
+        self._wrapped: dict = {}
+
+    @property
+    def device_solves(self) -> bool:
+        """Whether a sweep solves this env's bonds by the device-resident Lanczos."""
+        return self.compiled and self.compile is None and self.bra is self.psi
 
     def setup_(self, to: int = 0) -> "Env":
+        if to != 0:
+            raise NotImplementedError("only to=0 is implemented; canonize_ has the same note")
         for n in range(len(self.psi) - 1, 0, -1):
             self.update_(n, to="first")
         return self
 
     def update_(self, n: int, *, to: str) -> None:
+        bra = None if self.bra is self.psi else self.bra[n]
         if to == "last":
-            self.F[n, n + 1] = env_update_last(self.F[n - 1, n], self.psi[n], self.h[n])
+            self.F[n, n + 1] = env_update_last(self.F[n - 1, n], self.psi[n], self.h[n], bra)
         else:
-            self.F[n, n - 1] = env_update_first(self.F[n + 1, n], self.psi[n], self.h[n])
+            self.F[n, n - 1] = env_update_first(self.F[n + 1, n], self.psi[n], self.h[n], bra)
 
     def clear_(self, *sites: int) -> None:
         for n in sites:
@@ -449,9 +521,30 @@ class Env:
 
     def heff2(self, n: int, aa: SymmetricTensor) -> SymmetricTensor:
         fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
+        if self.compile is not None:
+            key = (n, fl.structure, fr.structure, aa.structure)
+            fn = self._wrapped.get(n)
+            if fn is None or fn[0] != key:
+                w1, w2 = self.h[n], self.h[n + 1]
+                fn = (key, self.compile(lambda v: heff2(fl, w1, w2, fr, v)))
+                self._wrapped[n] = fn
+            return fn[1](aa)
         if not self.compiled:
             return heff2(fl, self.h[n], self.h[n + 1], fr, aa)
         return self.matvec(n, aa.structure)(aa)
+
+    def heff2_families(self, n: int, aa: SymmetricTensor) -> tuple:
+        """``heff2``'s term families, unsummed (``network/env.py:772-840``).  A site-tensor
+        MPO carries no term symbols, so -- as in the reference's site-tensor path -- the
+        single family is the operator's own action, ``(heff2(n, aa),)``."""
+        return (self.heff2(n, aa),)
+
+    def project2(self, n: int, aa: SymmetricTensor) -> SymmetricTensor:
+        """``aa`` on the ket's bonds carried to the bra's (``network/env.py:843-920``):
+        ``<bra env| H_n H_{n+1} |aa, ket env>`` by the four site-tensor contractions; with
+        ``h`` the identity MPO it is the ket state's two-site reduced form in the bra's
+        environment gauge."""
+        return heff2(self.F[n - 1, n], self.h[n], self.h[n + 1], self.F[n + 2, n + 1], aa)
 
     def _bond(self, n: int, structure, precision: str) -> dict:
         """The bond's cached programs: one allocated heff2 program per precision (plus what
@@ -533,13 +626,103 @@ def drain(gen):
             return stop.value
 
 
-def sweep_steps(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3):
-    """One left-to-right then right-to-left two-site sweep (``network/dmrg.py:321-542``,
-    noiseless branch) as a generator: it yields right after each bond's Lanczos solve is
-    enqueued on the current stream (so a scheduler can run other work while the device
-    computes) and returns ``(energy, max discarded weight)``."""
+class Sweep(NamedTuple):
+    """One schedule entry (``network/dmrg.py:32-67``): the SVD's ``chi`` cap and
+    ``cutoff``, and the noise mixed in at each split."""
+
+    chi: int = 64
+    cutoff: float = 1e-14
+    noise: float = 0.0
+    noise_type: str = "wavefunction"
+
+
+#: The two spellings of ``noise``; each also decides the decimation (``dmrg.py:229-231``).
+_NOISE_TYPES = ("wavefunction", "perturbative")
+
+
+class DMRG_out(NamedTuple):
+    """The record ``dmrg_`` returns and hands its ``callback`` (``network/dmrg.py:564-617``):
+    ``history`` holds one ``(energy, denergy, dSchmidt, discarded)`` per sweep and
+    ``schedule`` the realised ``Sweep`` entries."""
+
+    sweeps: int
+    energy: float
+    denergy: float
+    max_dSchmidt: float
+    max_discarded_weight: float
+    history: list
+    schedule: list
+    psi: MPS
+
+
+def _schmidt_change(old: dict, new: dict) -> float:
+    """``max_k ||S_k - S_k^old||`` over bonds, zero-padded; infinite before any history
+    (``network/dmrg.py:545-561``)."""
+    if not old:
+        return float("inf")
+    worst = 0.0
+    for n, current in new.items():
+        previous = old.get(n, [])
+        m = max(len(previous), len(current))
+        a = previous + [0.0] * (m - len(previous))
+        b = current + [0.0] * (m - len(current))
+        worst = max(worst, sum((x - y) ** 2 for x, y in zip(a, b, strict=True)) ** 0.5)
+    return worst
+
+
+def _rho(m: SymmetricTensor, forward: bool) -> SymmetricTensor:
+    from tenet import ops
+
+    return ops.compose(m, ops.adjoint(m)) if forward else ops.compose(ops.adjoint(m), m)
+
+
+def _perturbations(env: Env, n: int, aa: SymmetricTensor, noise: float) -> tuple:
+    """The operator's families on ``aa``, each normalised, scaled to total squared norm
+    ``noise`` (``network/dmrg.py:251-272``)."""
+    from tenet import ops
+
+    parts = [(q, float(ops.norm(q))) for q in env.heff2_families(n, aa)]
+    live = [(q, w) for q, w in parts if w > 0.0]
+    if not live:
+        return ()
+    scale = (noise / len(live)) ** 0.5
+    return tuple(q * (scale / w) for q, w in live)
+
+
+def _split_dm(aa, forward, *, chi, cutoff, perturbations=(), budget="dense"):
+    """The density-matrix split of perturbative noise (``network/dmrg.py:275-318``):
+    ``svd_truncated`` of ``rho = tr aa aa^dag`` plus the perturbations' ``rho``, with
+    ``cutoff_mode="rsum1"``; returns ``(left, right, s)``."""
     from tenet import linalg, ops
 
+    m = ops.repartition(aa, (0, 1), (2, 3))
+    rho = _rho(m, forward)
+    for q in perturbations:
+        rho = ops.add(rho, _rho(ops.repartition(q, (0, 1), (2, 3)), forward))
+    v, w, _ = linalg.svd_truncated(rho, max_bond=chi, cutoff=cutoff, cutoff_mode="rsum1",
+                                   budget=budget)
+    s = ops.block_sqrt(w)
+    if forward:
+        return v, ops.compose(ops.adjoint(v), m), s
+    return ops.compose(m, v), ops.transpose(ops.adjoint(v), (2, 0, 1)), s
+
+
+def sweep_steps(psi: MPS, h: MPO, env: Env, schmidt: dict | None = None, *, chi: int,
+                cutoff: float, ncv: int = 3, noise: float = 0.0,
+                noise_type: str = "wavefunction", orthogonal_to=(), seed: int = 0,
+                budget: str = "dense"):
+    """One left-to-right then right-to-left two-site sweep (``network/dmrg.py:321-542``)
+    as a generator: with the device Lanczos it yields right after each bond's solve is
+    enqueued on the current stream (so a scheduler can run other work while the device
+    computes); it returns ``(energy, max discarded weight)``.  ``schmidt`` (bond ->
+    spectrum) is updated in place.  ``budget="reduced"`` caps the number of kept
+    multiplets at ``chi`` instead of the reference's dense dimension (a build-side mode
+    with no reference counterpart)."""
+    from tenet import linalg, ops
+
+    if noise_type not in _NOISE_TYPES:
+        raise ValueError(f"noise_type={noise_type!r} is not one of {_NOISE_TYPES}; it decides "
+                         "the decimation as well as the perturbation")
     n_sites = len(psi)
     energy, max_dw = 0.0, 0.0
     for direction in ("right", "left"):
@@ -547,7 +730,11 @@ def sweep_steps(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int
         bonds = range(n_sites - 1) if forward else range(n_sites - 2, -1, -1)
         for n in bonds:
             aa = _pair(psi[n], psi[n + 1])
-            if env.compiled:
+            if orthogonal_to:
+                proj = [o.project2(n, _pair(o.psi[n], o.psi[n + 1])) for o in orthogonal_to]
+                energy, aa = lanczos(lambda v, n=n: env.heff2(n, v), aa, ncv=ncv,
+                                     orthogonal_to=proj)
+            elif env.device_solves:
                 lz = env.lanczos(n, aa.structure, ncv)
                 if lz.n:
                     lz.launch(aa.arena)
@@ -557,59 +744,129 @@ def sweep_steps(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int
                     energy = 0.0
             else:
                 energy, aa = lanczos(lambda v, n=n: env.heff2(n, v), aa, ncv=ncv)
-            u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff)
-            norm_s = ops.norm(s)
-            max_dw = max(max_dw, 1.0 - float(norm_s / ops.norm(aa)) ** 2)
-            s = s / norm_s
-            psi[n + 1] = vh
-            if forward:
-                psi[n] = u
-                psi[n + 1] = ops.einsum("xy,yqr->xqr", s, psi[n + 1])
+            if noise and noise_type == "perturbative":
+                left, right, s = _split_dm(aa, forward, chi=chi, cutoff=cutoff, budget=budget,
+                                           perturbations=_perturbations(env, n, aa, noise))
+                carrier = right if forward else left
+                norm_c = ops.norm(carrier)
+                max_dw = max(max_dw, 1.0 - float(norm_c / ops.norm(aa)) ** 2)
+                psi[n] = left if forward else left / norm_c
+                psi[n + 1] = right / norm_c if forward else right
+                if schmidt is not None:
+                    schmidt[n] = spectrum(s / ops.norm(s))
             else:
-                psi[n] = ops.einsum("apx,xy->apy", u, s)
+                if noise:
+                    r = SymmetricTensor.random(aa.legs, seed=seed + n)
+                    aa = ops.add(aa, r * float(noise * ops.norm(aa) / ops.norm(r)))
+                    aa = aa / ops.norm(aa)
+                u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi,
+                                                cutoff=cutoff, budget=budget)
+                norm_s = ops.norm(s)
+                max_dw = max(max_dw, 1.0 - float(norm_s / ops.norm(aa)) ** 2)
+                s = s / norm_s
+                psi[n + 1] = vh
+                if forward:
+                    psi[n] = u
+                    psi[n + 1] = ops.einsum("xy,yqr->xqr", s, psi[n + 1])
+                else:
+                    psi[n] = ops.einsum("apx,xy->apy", u, s)
+                if schmidt is not None:
+                    schmidt[n] = spectrum(s)
             psi.center = n + 1 if forward else n
-            env.clear_(n, n + 1)
-            if forward:
-                env.update_(n, to="last")
-            else:
-                env.update_(n + 1, to="first")
+            for e in (env, *orthogonal_to):
+                e.clear_(n, n + 1)
+                if forward:
+                    e.update_(n, to="last")
+                else:
+                    e.update_(n + 1, to="first")
     return energy, max_dw
 
 
-def sweep_(psi: MPS, h: MPO, env: Env, *, chi: int, cutoff: float, ncv: int = 3):
+def sweep_(psi: MPS, h: MPO, env: Env, schmidt: dict | None = None, *, chi: int,
+           cutoff: float, ncv: int = 3, noise: float = 0.0, noise_type: str = "wavefunction",
+           orthogonal_to=(), seed: int = 0, budget: str = "dense"):
     """One two-site sweep; returns ``(energy, max discarded weight)``."""
-    return drain(sweep_steps(psi, h, env, chi=chi, cutoff=cutoff, ncv=ncv))
+    return drain(sweep_steps(psi, h, env, schmidt, chi=chi, cutoff=cutoff, ncv=ncv,
+                             noise=noise, noise_type=noise_type, orthogonal_to=orthogonal_to,
+                             seed=seed, budget=budget))
 
 
-def dmrg_steps(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
-               max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True,
-               precision: str = "f64", tc_min_flops: int | None = None):
-    """``dmrg_`` as a step generator (see ``sweep_steps``)."""
+def dmrg_steps(psi: MPS, h: MPO, *, schedule=None, chi: int | None = None,
+               cutoff: float | None = None, energy_tol: float = 1e-12,
+               schmidt_tol: float = 1e-8, max_sweeps: int = 40, ncv: int = 3,
+               orthogonal_to=None, seed: int = 0, callback=None, compile=None,
+               compiled: bool = True, precision: str = "f64",
+               tc_min_flops: int | None = None, budget: str = "dense"):
+    """``dmrg_`` as a step generator (see ``sweep_steps``); returns the ``DMRG_out``."""
+    if schedule is not None:
+        if chi is not None or cutoff is not None:
+            raise ValueError("pass either schedule=[Sweep(chi=..., cutoff=...), ...] or the "
+                             "flat chi= / cutoff= kwargs, not both")
+        plan = list(schedule)
+        if not plan:
+            raise ValueError("schedule is empty; a run needs at least one Sweep entry")
+    else:
+        plan = [Sweep(64 if chi is None else chi, 1e-14 if cutoff is None else cutoff)]
     psi.canonize_(0)
-    env = Env(psi, h, compiled=compiled, precision=precision,
+    env = Env(psi, h, compile=compile, compiled=compiled, precision=precision,
               tc_min_flops=tc_min_flops).setup_(0)
-    energy, history = float("inf"), []
-    for _ in range(max_sweeps):
-        old = energy
-        energy, _ = yield from sweep_steps(psi, h, env, chi=chi, cutoff=cutoff, ncv=ncv)
-        history.append(energy)
-        if abs(old - energy) < energy_tol:
+    orthos: tuple = ()
+    if orthogonal_to:
+        ident = MPO.identity(len(psi), psi[0].legs[1].space)
+        ends = (psi[0].legs[0], psi[len(psi) - 1].legs[2])
+        orthos = tuple(
+            Env(phi, ident, bra=psi).setup_(0) for phi in orthogonal_to
+            # a state whose boundary legs put it in another sector is orthogonal already
+            if (phi[0].legs[0].space, phi[0].legs[0].dual) == (ends[0].space, ends[0].dual)
+            and (phi[len(phi) - 1].legs[2].space, phi[len(phi) - 1].legs[2].dual)
+            == (ends[1].space, ends[1].dual))
+    schmidt: dict = {}
+    energy = float("inf")
+    history: list = []
+    realized: list = []
+    out = None
+    for it in range(1, max_sweeps + 1):
+        entry = plan[it - 1] if it <= len(plan) else plan[-1]
+        old_energy, old_schmidt = energy, dict(schmidt)
+        energy, max_dw = yield from sweep_steps(
+            psi, h, env, schmidt, chi=entry.chi, cutoff=entry.cutoff, ncv=ncv,
+            noise=entry.noise, noise_type=entry.noise_type, orthogonal_to=orthos,
+            seed=seed + 977 * it, budget=budget)
+        denergy = abs(old_energy - energy)
+        d_schmidt = _schmidt_change(old_schmidt, schmidt)
+        history.append((energy, denergy, d_schmidt, max_dw))
+        realized.append(entry)
+        out = DMRG_out(it, energy, denergy, d_schmidt, max_dw, history, realized, psi)
+        if callback:
+            callback(out)
+        if denergy < energy_tol and d_schmidt < schmidt_tol and it >= len(plan) \
+                and entry.noise == 0.0:
             break
-    return energy, history, psi
+    return out
 
 
-def dmrg_(psi: MPS, h: MPO, *, chi: int = 64, cutoff: float = 1e-14, ncv: int = 3,
-          max_sweeps: int = 40, energy_tol: float = 1e-10, compiled: bool = True,
-          precision: str = "f64", tc_min_flops: int | None = None):
-    """Two-site DMRG to convergence (``network/dmrg.py:620-843``, flat ``chi``/``cutoff``,
-    no noise): returns ``(energy, history, psi)`` with ``history`` the per-sweep energies.
-    Stops on ``|dE| < energy_tol`` or after ``max_sweeps``.  ``precision`` "tf32" or
-    "3xbf16" runs the matvec products big enough for the tensor cores there (see
-    ``tc_min_flops``), with FP64 reorthogonalisation and the FP64 Rayleigh-quotient
-    correction of every such solve; Lanczos, the SVD and the truncation stay FP64."""
-    return drain(dmrg_steps(psi, h, chi=chi, cutoff=cutoff, ncv=ncv, max_sweeps=max_sweeps,
-                            energy_tol=energy_tol, compiled=compiled, precision=precision,
-                            tc_min_flops=tc_min_flops))
+def dmrg_(psi: MPS, h: MPO, *, schedule=None, chi: int | None = None,
+          cutoff: float | None = None, energy_tol: float = 1e-12, schmidt_tol: float = 1e-8,
+          max_sweeps: int = 40, ncv: int = 3, orthogonal_to=None, seed: int = 0,
+          callback=None, compile=None, compiled: bool = True, precision: str = "f64",
+          tc_min_flops: int | None = None, budget: str = "dense") -> DMRG_out:
+    """Sweep ``psi`` to the ground state of ``h`` in place and return a ``DMRG_out``
+    (``network/dmrg.py:620-843``): the same arguments, defaults, refusals, schedule rule
+    (the last entry repeats), noise forms, excited-state projection and the two
+    convergence criteria (``|dE| < energy_tol`` and Schmidt change ``< schmidt_tol`` in one
+    noiseless sweep at the schedule's last entry).
+
+    Beyond the reference's arguments: ``compiled`` (default) solves each bond by the
+    device-resident Lanczos on a graph-captured matvec; ``precision`` "tf32" or "3xbf16"
+    runs the matvec products big enough for the tensor cores there (``tc_min_flops``),
+    with FP64 reorthogonalisation and the FP64 correction of every such solve, while the
+    SVD and truncation stay FP64; ``budget="reduced"`` caps kept multiplets instead of
+    the dense dimension."""
+    return drain(dmrg_steps(psi, h, schedule=schedule, chi=chi, cutoff=cutoff,
+                            energy_tol=energy_tol, schmidt_tol=schmidt_tol,
+                            max_sweeps=max_sweeps, ncv=ncv, orthogonal_to=orthogonal_to,
+                            seed=seed, callback=callback, compile=compile, compiled=compiled,
+                            precision=precision, tc_min_flops=tc_min_flops, budget=budget))
 
 
 # ---------------------------------------------------------------------------------------

@@ -368,6 +368,14 @@ def divide(t: SymmetricTensor, s) -> SymmetricTensor:
     return _axpby(1.0 / float(s), t, 0.0, t)
 
 
+def block_sqrt(t: SymmetricTensor) -> SymmetricTensor:
+    """Entry-by-entry square root of every block (``ops/blocks.py:95-135``): the square
+    root of a singular-value tensor."""
+    out = SymmetricTensor.empty(t.structure)
+    torch.sqrt(t.arena, out=out.arena)
+    return out
+
+
 # ---------------------------------------------------------------------------------------
 # identity and trace
 

@@ -108,6 +108,7 @@ def _solve_steps(req: SolveRequest, *, precision: str, ncv: int, cutoff: float,
     psi = network.MPS.random(_phys(), _start_bonds(req.L), seed=req.seed)
     return (yield from network.dmrg_steps(psi, h, chi=req.chi, cutoff=cutoff, ncv=ncv,
                                           max_sweeps=req.sweeps, energy_tol=0.0,
+                                          schmidt_tol=0.0,
                                           compiled=compiled, precision=precision,
                                           tc_min_flops=tc_min_flops))
 
@@ -115,9 +116,9 @@ def _solve_steps(req: SolveRequest, *, precision: str, ncv: int, cutoff: float,
 def solve_alone(req: SolveRequest, *, precision: str = "f64", ncv: int = 20,
                 cutoff: float = 1e-10, compiled: bool = True, tc_min_flops=None):
     """The same solve outside the server: ``(energy, history)``."""
-    e, hist, _ = network.drain(_solve_steps(req, precision=precision, ncv=ncv, cutoff=cutoff,
+    out = network.drain(_solve_steps(req, precision=precision, ncv=ncv, cutoff=cutoff,
                                             compiled=compiled, tc_min_flops=tc_min_flops))
-    return e, hist
+    return out.energy, [h[0] for h in out.history]
 
 
 @dataclass
@@ -188,7 +189,7 @@ class Server:
                         next(slot.gen)
                         continue
                     except StopIteration as stop:
-                        energy, history, _ = stop.value
+                        energy, history = stop.value.energy, [h[0] for h in stop.value.history]
                     slot.stream.synchronize()
                 active.remove(slot)
                 used -= slot.footprint

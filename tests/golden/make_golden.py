@@ -18,9 +18,12 @@ here is the reference's own output on seeded inputs:
   mid-chain bond (site-tensor path), its Lanczos ground energy at ``ncv=20``, and the
   truncated SVD of the result;
 * ``dmrg.json``: reference DMRG energies and per-bond kept sectors;
+* ``dmrg64.json``: the L = 64, chi = 256 SU(2) Heisenberg DMRG (site-tensor and prepared
+  paths) with its per-sweep history and final bond spaces;
 * ``ctmrg.json``: Z2 Ising CTMRG (beta = 0.44 at chi = 16 and 128 for a fixed number of
   moves; beta = 0.40, chi = 16 to convergence): per-sweep corner-spectrum changes, final
   corner spectrum and bond sectors, the reference's beta f estimate and Onsager's;
+* ``su2_tables.npz``: the reference's full SU(2) F and R fixture tables;
 * ``su2_f_sample.txt``: every 37th row of the reference's F-symbol fixture with the
   value the reference's F-symbol route returns.
 
@@ -278,6 +281,45 @@ def make_dmrg() -> dict:
     return runs
 
 
+def make_dmrg64(ref: Path) -> dict:
+    """The SU(2) Heisenberg chain at L = 64 through the reference's own ``dmrg_``
+    (``network/dmrg.py:620-843``): ``chi = 256`` in the reference's dense sense, cutoff
+    1e-10, ncv = 20, at most 10 sweeps with its default convergence tolerances, from the
+    seeded random start whose bond spins are 2j <= min(i, L - i, 16).  Recorded for the
+    site-tensor path (the MPO materialised: the matvec this build runs) with per-sweep
+    history and every final bond space, and for the prepared path (``MPO.from_terms`` as
+    given) as per-sweep energies; plus the MPSKit N = 64, chi = 256 energy of the
+    reference's fixture ``tests/fixtures/mpskit_heisenberg.json``."""
+    import time
+
+    from tenet import GradedSpace
+    from tenet.models import spin_half
+    from tenet.network import MPO, MPS, dmrg_
+    from tenet.symmetry import SU2, SU2Sector
+
+    site = spin_half(SU2)
+    L, chi = 64, 256
+    h = MPO.from_terms(L, [(1.0, [(site.ops["S.S"], (i, i + 1))]) for i in range(L - 1)])
+    bonds = [GradedSpace.new(SU2, {SU2Sector(j): 1
+                                   for j in range(i % 2, min(i, L - i, 16) + 1, 2)})
+             for i in range(L + 1)]
+    rec = {"L": L, "chi": chi, "ncv": 20, "cutoff": 1e-10, "max_sweeps": 10, "max_2j": 16}
+    for name, op in (("site", h.materialize()), ("prepared", h)):
+        t0 = time.perf_counter()
+        out = dmrg_(MPS.random(site.phys, bonds, seed=0), op, chi=chi, cutoff=1e-10, ncv=20,
+                    max_sweeps=10)
+        run = {"sweeps": out.sweeps, "energy": out.energy,
+               "history": [[float(x) for x in r] for r in out.history],
+               "seconds": time.perf_counter() - t0}
+        if name == "site":
+            run["bonds"] = [[[_sector_int(a), m] for a, m in out.psi[i].legs[0].space.sectors]
+                            for i in range(L)]
+        rec[name] = run
+    fix = json.loads((ref / "tests/fixtures/mpskit_heisenberg.json").read_text())
+    rec["mpskit_N64_chi256"] = fix["N64"]["chi256"]["energy"]
+    return rec
+
+
 def make_ctmrg(ref: Path) -> dict:
     """Z2 CTMRG of the 2D Ising model (``network/ctmrg.py:451-660``): beta = 0.44 near the
     critical point (a fixed number of moves, chi = 16 and 128) and beta = 0.40 run to its
@@ -307,6 +349,17 @@ def make_ctmrg(ref: Path) -> dict:
     return out
 
 
+def make_su2_tables(ref: Path) -> None:
+    """The reference's full SU(2) coefficient fixtures as a compact archive: every row of
+    ``tests/fixtures/su2_f.txt`` (109,900 F-symbols, 2j <= 12) and ``su2_r.txt`` (616
+    R-symbol signs), the tables its ``tests/symmetry/test_su2_recoupling.py`` checks."""
+    f = np.loadtxt(ref / "tests/fixtures/su2_f.txt")
+    r = np.loadtxt(ref / "tests/fixtures/su2_r.txt", dtype=np.int64)
+    np.savez_compressed(HERE / "su2_tables.npz", f_dj=f[:, :6].astype(np.int8),
+                        f_value=f[:, 6], r_dj=r[:, :3].astype(np.int8),
+                        r_value=r[:, 3].astype(np.int8))
+
+
 def make_f_sample(ref: Path) -> None:
     from tenet.symmetry import SU2, SU2Sector
 
@@ -323,10 +376,19 @@ def make_f_sample(ref: Path) -> None:
 
 
 def main() -> None:
-    if len(sys.argv) != 2:
-        raise SystemExit("usage: python tests/golden/make_golden.py <path to the TeNeT-py tree>")
+    if len(sys.argv) not in (2, 3):
+        raise SystemExit("usage: python tests/golden/make_golden.py <path to the TeNeT-py tree>"
+                         " [dmrg64 | su2tables]")
     ref = Path(sys.argv[1])
     _setup(ref)
+    if len(sys.argv) == 3:  # one part alone
+        if sys.argv[2] == "dmrg64":
+            (HERE / "dmrg64.json").write_text(json.dumps(make_dmrg64(ref)))
+        elif sys.argv[2] == "su2tables":
+            make_su2_tables(ref)
+        else:
+            raise SystemExit(f"unknown part {sys.argv[2]!r}")
+        return
     store = Store()
     make_cases(store)
     store.dump("cases")
@@ -336,7 +398,9 @@ def main() -> None:
     hs.dump("heff")
     (HERE / "dmrg.json").write_text(json.dumps(make_dmrg(), indent=1))
     (HERE / "ctmrg.json").write_text(json.dumps(make_ctmrg(ref)))
+    (HERE / "dmrg64.json").write_text(json.dumps(make_dmrg64(ref)))
     make_f_sample(ref)
+    make_su2_tables(ref)
 
 
 if __name__ == "__main__":

@@ -89,10 +89,10 @@ def test_mixed_precision_dmrg_energy(golden_dir, precision):
     phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
     bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
              for i in range(L + 1)]
-    e, hist, _ = network.dmrg_(network.MPS.random(phys, bonds, seed=0),
-                               network.heisenberg_mpo_su2(L), chi=chi, cutoff=1e-10, ncv=20,
-                               max_sweeps=g["sweeps"], energy_tol=0.0, precision=precision,
-                               tc_min_flops=0)  # every product on the tensor cores
+    e = network.dmrg_(network.MPS.random(phys, bonds, seed=0),
+                      network.heisenberg_mpo_su2(L), chi=chi, cutoff=1e-10, ncv=20,
+                      max_sweeps=g["sweeps"], energy_tol=0.0, precision=precision,
+                      tc_min_flops=0).energy  # every product on the tensor cores
     assert abs(e - g["energy"]) / L <= 1e-8, f"|dE/L| = {abs(e - g['energy']) / L:.2e}"
 
 
