@@ -47,6 +47,7 @@ NCU_TRAFFIC = {"block_gather": (480_000 + 1_625_856) // 2,
 BOND = {1: 60, 3: 56, 5: 46, 7: 36, 9: 25, 11: 16, 13: 10, 15: 5, 17: 2}
 MPO = {0: 2, 2: 1}
 PHYS = {1: 1}
+WORKLOAD = "su2-heisenberg-heff2-L64-mid-bond-256-multiplets"
 
 
 def build_workload(seed: int = 0):
@@ -86,16 +87,38 @@ def workload_structures():
 
 
 def oracle_workload(seed: int = 0):
-    """The same tensors for the oracle: same structures, same seeded draws."""
+    """The same tensors for the oracle, built from the oracle's own types (nothing of the
+    tenet package is imported): same structures, same seeded draws."""
     import oracle.tenet_oracle as O
 
-    out = []
-    for k, s in enumerate(workload_structures()):
-        legs = tuple(O.Leg(tuple((a.two_j, m) for a, m in leg.space.sectors),
-                           O.OUT if leg.side.value == "out" else O.IN, bool(leg.dual))
-                     for leg in s.legs)
-        out.append(O.random(O.Structure(O.SU2, legs), seed + (0, 2, 3, 1, 4)[k]))
-    return out
+    def leg(d, side, dual=False):
+        return O.Leg(tuple(sorted(d.items())), side, dual)
+
+    w = (leg(MPO, O.IN, True), leg(PHYS, O.OUT), leg(PHYS, O.IN), leg(MPO, O.OUT, True))
+    legs = {"fl": (leg(BOND, O.IN), leg(MPO, O.OUT, True), leg(BOND, O.OUT)),
+            "w1": w, "w2": w,
+            "fr": (leg(BOND, O.OUT), leg(MPO, O.IN, True), leg(BOND, O.IN)),
+            "aa": (leg(BOND, O.OUT), leg(PHYS, O.OUT), leg(PHYS, O.OUT), leg(BOND, O.IN))}
+    seeds = {"fl": 0, "fr": 1, "w1": 2, "w2": 3, "aa": 4}
+    return [O.random(O.Structure(O.SU2, legs[k]), seed + seeds[k])
+            for k in ("fl", "w1", "w2", "fr", "aa")]
+
+
+def bench_config(world: int = 1) -> dict:
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": WORKLOAD, "bond_multiplets": {str(k): v for k, v in BOND.items()},
+            "mpo_multiplets": {str(k): v for k, v in MPO.items()},
+            "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"replicas{world}"}
+
+
+def host_cores() -> int:
+    try:
+        from threadpoolctl import threadpool_info
+
+        return int(max((i.get("num_threads", 1) for i in threadpool_info()), default=1))
+    except Exception:
+        return os.cpu_count() or 1
 
 
 def heff2_flops() -> int:
@@ -277,7 +300,9 @@ def cpu_baseline(flops: int, budget_s: float = 20.0) -> dict:
     import oracle.tenet_oracle as O
 
     fl, w1, w2, fr, aa = oracle_workload()
+    O.FLOPS[0] = 0
     O.heff2(fl, w1, w2, fr, aa)  # warm the plan caches, as the reference's own bench does
+    assert O.FLOPS[0] == flops, "the oracle's work differs from the planner's"
     times = []
     t_end = time.perf_counter() + budget_s
     while time.perf_counter() < t_end and len(times) < 5:
@@ -285,13 +310,7 @@ def cpu_baseline(flops: int, budget_s: float = 20.0) -> dict:
         O.heff2(fl, w1, w2, fr, aa)
         times.append(time.perf_counter() - t0)
     med = float(np.median(times))
-    try:
-        from threadpoolctl import threadpool_info
-
-        cores = max((i.get("num_threads", 1) for i in threadpool_info()), default=1)
-    except Exception:
-        cores = os.cpu_count() or 1
-    return {"value": flops / med / 1e12, "unit": "TFLOP/s", "cores": int(cores), "kind": "port",
+    return {"value": flops / med / 1e12, "unit": "TFLOP/s", "cores": host_cores(), "kind": "port",
             "sample": f"{len(times)} oracle heff2 matvecs on the same structures (median "
                       f"{med * 1e3:.1f} ms each), plan caches warm",
             "ms_per_matvec": med * 1e3}
@@ -551,6 +570,44 @@ def serving(args) -> dict:
     return out
 
 
+def chain64_start(L: int = 64, max_2j: int = 16, seed: int = 0):
+    """The seeded start of the L = 64 SU(2) Heisenberg runs: bond spins 2j <= min(i, L - i,
+    16), one multiplet each, ``MPS.random`` with ``seed``."""
+    from tenet import network
+    from tenet.structure import GradedSpace
+    from tenet.symmetry import SU2
+
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1
+                                   for j in range(i % 2, min(i, L - i, max_2j) + 1, 2)})
+             for i in range(L + 1)]
+    return network.MPS.random(phys, bonds, seed=seed)
+
+
+def derive_bond(args) -> None:
+    """Grow the L = 64 chain to a cap of ``--derive-chi`` multiplets per bond (cutoff 1e-14,
+    so the cap binds; ncv = 20) and print the converged mid-chain bond's multiplets per
+    spin and the run's per-sweep energies and times: the bond histogram of the large-bond
+    matvec workload."""
+    import torch
+
+    from tenet import network
+
+    L = 64
+    psi = chain64_start(L)
+    t0 = time.perf_counter()
+    rec = []
+    out = network.dmrg_(psi, network.heisenberg_mpo_su2(L), chi=args.derive_chi,
+                        cutoff=1e-14, ncv=20, max_sweeps=args.derive_sweeps, budget="reduced",
+                        callback=lambda o: rec.append((o.energy, time.perf_counter() - t0)))
+    torch.cuda.synchronize()
+    bonds = {n: {int(a.two_j): m for a, m in psi[n].legs[0].space.sectors}
+             for n in (L // 2 - 1, L // 2, L // 2 + 1)}
+    print(json.dumps({"derive_bond": {"L": L, "chi_multiplets": args.derive_chi,
+                                      "sweeps": out.sweeps, "energy": out.energy,
+                                      "per_sweep": rec, "bonds": bonds}}))
+
+
 def max_over_ranks(ms: float, device) -> float:
     """The slowest rank's time: every rank of an initialised process group calls this at
     the same point (one all-reduce); a single process gets its own time back."""
@@ -571,14 +628,20 @@ def job_value(flops: int, steps: int, world: int, ms: float) -> float:
 
 
 def run_reference(args) -> None:
+    """The reference's algorithm for the path on the host cores: the oracle's NumPy
+    restatement of ``Env.heff2`` (the reference is Python and cannot travel to the GPU
+    host; the oracle is pinned to its outputs), all BLAS threads, on the same workload.
+    Only the oracle is imported, never the tenet package.  Rank 0 alone runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    flops = heff2_flops()
     import oracle.tenet_oracle as O
 
     ot = oracle_workload()
-    for _ in range(max(1, min(args.warmup, 1))):
+    O.FLOPS[0] = 0
+    O.heff2(*ot)
+    flops = O.FLOPS[0]
+    for _ in range(max(0, args.warmup - 1)):
         O.heff2(*ot)
     times = []
     for _ in range(args.steps):
@@ -587,21 +650,16 @@ def run_reference(args) -> None:
         times.append(time.perf_counter() - t0)
     total = sum(times)
     value = flops * len(times) / total / 1e12
-    try:
-        from threadpoolctl import threadpool_info
-
-        cores = max((i.get("num_threads", 1) for i in threadpool_info()), default=1)
-    except Exception:
-        cores = os.cpu_count() or 1
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / len(times) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "impl": "reference",
-        "config": {"workload": "su2-heisenberg-heff2-L64-mid-bond-256-multiplets",
-                   "bond_multiplets": BOND, "mpo_multiplets": MPO},
-        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": int(cores), "kind": "port",
-                         "sample": f"{len(times)} oracle heff2 matvecs, one per step"},
+        "data": "synthetic", "impl": "reference", "config": bench_config(args.gpus),
+        "flops_per_matvec": flops,
+        "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": host_cores(),
+                         "kind": "port",
+                         "sample": f"{len(times)} oracle heff2 matvecs, one per step, after "
+                                   f"{max(1, args.warmup)} warm-up calls"},
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
@@ -786,11 +844,8 @@ def run_tenet(args) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "su2-heisenberg-heff2-L64-mid-bond-256-multiplets",
-                       "bond_multiplets": BOND, "mpo_multiplets": MPO,
-                       "flops_per_matvec": flops, "elements_aa": int(aa.arena.numel()),
-                       "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"replicas{world}"},
+            "config": bench_config(world),
+            "flops_per_matvec": flops, "elements_aa": int(aa.arena.numel()),
             "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(aa.arena.numel() * 8),
                     "d2h_bytes_per_step": int(out_size * 8)},
@@ -841,7 +896,15 @@ def main() -> None:
     ap.add_argument("--profile-config3", action="store_true",
                     help="only run the batched environment update a few times (a small, "
                          "fixed launch sequence for profiling its kernels) and exit")
+    ap.add_argument("--derive-bond", action="store_true",
+                    help="grow the L = 64 chain to --derive-chi multiplets and print its "
+                         "mid-chain bond histogram, then exit")
+    ap.add_argument("--derive-chi", type=int, default=256)
+    ap.add_argument("--derive-sweeps", type=int, default=6)
     args = ap.parse_args()
+    if args.derive_bond:
+        derive_bond(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.profile_gemm > 0:

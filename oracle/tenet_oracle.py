@@ -487,13 +487,22 @@ def from_matrices(s: Structure, mats: dict) -> Tensor:
     return Tensor(s, blocks)
 
 
+#: Running total of the sector products' flops (2 M K N each) that ``compose`` performed:
+#: the algorithmic work of a contraction, read by the benchmark's CPU legs.
+FLOPS = [0]
+
+
 def compose(a: Tensor, b: Tensor) -> Tensor:
     """One matmul per shared coupled sector, zero elsewhere (``ops/map.py:155-172``)."""
     s = Structure(a.structure.provider, (*a.structure.codomain, *b.structure.domain))
     ma, mb = to_matrices(a), to_matrices(b)
     mats = {}
     for c, (_, _, nr, nc) in map_layout(s).items():
-        mats[c] = ma[c] @ mb[c] if (c in ma and c in mb) else np.zeros((nr, nc))
+        if c in ma and c in mb:
+            mats[c] = ma[c] @ mb[c]
+            FLOPS[0] += 2 * nr * nc * ma[c].shape[1]
+        else:
+            mats[c] = np.zeros((nr, nc))
     return from_matrices(s, mats)
 
 
