@@ -39,18 +39,30 @@ for _p in (ROOT, ROOT / "tenet-py_b200"):
         sys.path.insert(0, str(_p))
 
 METRIC = "Heff matvec TFLOP/s (SU(2) Heisenberg two-site, FP64)"
-# dram__bytes_read.sum + dram__bytes_write.sum per launch on this workload (ncu captures of
-# two launches each, mean), in bytes
-NCU_TRAFFIC = {"block_gather": (480_000 + 1_625_856) // 2,
-               "grouped_gemm_f64": (786_432 + 1_986_816) // 2}
-# multiplets per bond sector, half-integer bond spins 2j = 1, 3, ..., 17 (sum 256)
-BOND = {1: 60, 3: 56, 5: 46, 7: 36, 9: 25, 11: 16, 13: 10, 15: 5, 17: 2}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch of each kernel class on the
+# headline workload, from one ncu capture of this build (filled in from the capture)
+NCU_TRAFFIC: dict = {}
+# multiplets per spin of the mid-chain bond (sites 31 | 32) of the reference's own
+# converged state of this chain: L = 64, chi = 256 (dense), cutoff 1e-10, ncv = 20, from
+# the seeded start, 6 sweeps (tests/golden/dmrg64.json, bond 32; 85 states dense)
+BOND = {0: 8, 2: 14, 4: 7}
 MPO = {0: 2, 2: 1}
 PHYS = {1: 1}
-WORKLOAD = "su2-heisenberg-heff2-L64-mid-bond-256-multiplets"
+WORKLOAD = "su2-heisenberg-L64-chi256-cutoff1e-10-mid-bond-heff2"
+# further matvec workloads, reported beside the headline: the mid bond of the same chain
+# grown under a cap of 256 multiplets at cutoff 1e-14 (bench.py --derive-bond: the cap never
+# binds; 67 multiplets, 207 states dense), and a synthetic stress bond of 256 multiplets
+# over half-integer spins 2j = 1..17 (no state of this chain needs it)
+WORKLOADS = {
+    "L64_cutoff1e-14_mid_bond": {0: 17, 2: 32, 4: 16, 6: 2},
+    "synthetic_256_multiplets": {1: 60, 3: 56, 5: 46, 7: 36, 9: 25, 11: 16, 13: 10, 15: 5,
+                                 17: 2},
+}
+# the reference's energy for this chain and its sweep count (same run as BOND)
+REF_DMRG = {"energy": -28.175424844464963, "sweeps": 6}
 
 
-def build_workload(seed: int = 0):
+def build_workload(seed: int = 0, bond: dict | None = None):
     """(fl, w1, w2, fr, aa) as tenet tensors with the golden-vector leg conventions of the
     reference's ``Env`` (``network/env.py``): F[(n-1,n)] = (ket IN, mpo OUT*, bra OUT),
     F[(n+2,n+1)] = (ket OUT, mpo IN*, bra IN), W = (x IN*, P OUT, p IN, m OUT*)."""
@@ -61,7 +73,7 @@ def build_workload(seed: int = 0):
     def sp(d):
         return GradedSpace.new(SU2, {SU2.sector(a): m for a, m in d.items()})
 
-    B, M, P = sp(BOND), sp(MPO), sp(PHYS)
+    B, M, P = sp(bond or BOND), sp(MPO), sp(PHYS)
     rnd = tenet.SymmetricTensor.random
     fl = rnd((Leg(B, IN), Leg(M, OUT, True), Leg(B, OUT)), seed=seed)
     fr = rnd((Leg(B, OUT), Leg(M, IN, True), Leg(B, IN)), seed=seed + 1)
@@ -71,7 +83,7 @@ def build_workload(seed: int = 0):
     return fl, w1, w2, fr, aa
 
 
-def workload_structures():
+def workload_structures(bond: dict | None = None):
     """The five structures of ``build_workload`` (host only, no device needed)."""
     from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure
     from tenet.symmetry import SU2
@@ -79,7 +91,7 @@ def workload_structures():
     def sp(d):
         return GradedSpace.new(SU2, {SU2.sector(a): m for a, m in d.items()})
 
-    B, M, P = sp(BOND), sp(MPO), sp(PHYS)
+    B, M, P = sp(bond or BOND), sp(MPO), sp(PHYS)
     w = TensorStructure((Leg(M, IN, True), Leg(P, OUT), Leg(P, IN), Leg(M, OUT, True)))
     return (TensorStructure((Leg(B, IN), Leg(M, OUT, True), Leg(B, OUT))), w, w,
             TensorStructure((Leg(B, OUT), Leg(M, IN, True), Leg(B, IN))),
@@ -121,7 +133,7 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def heff2_flops() -> int:
+def heff2_flops(bond: dict | None = None) -> int:
     """Algorithmic flops of one heff2 from the plans alone (host, no device): the sum of
     2 M K N over every coupled-sector product of the four contractions."""
     from tenet import ops
@@ -150,7 +162,7 @@ def heff2_flops() -> int:
         sb, tb = bent(sb, tb)
         return einsum_s(f"{ta},{tb}->{out}", sa, sb)
 
-    fl, w1, w2, fr, aa = workload_structures()
+    fl, w1, w2, fr, aa = workload_structures(bond)
     t, f0 = einsum_s("apqr,rys->apqys", aa, fr)
     t, f1 = composed_s("apqys,mQqy->apQms", t, w2, "q")
     t, f2 = composed_s("apQms,xPpm->aPQxs", t, w1, "p")
@@ -396,7 +408,7 @@ def batched_matvecs(args, plain_ms: float, graph_ms: float) -> dict:
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in ev) / steps
 
-    out = {"workload": f"{n} SU(2) heff2 matvecs, 256 multiplets per bond (seeds 0, 10, ...), "
+    out = {"workload": f"{n} SU(2) heff2 matvecs on the headline bond (seeds 0, 10, ...), "
                        "shared MPO sites; compiled batched chain (BatchedHeff2) unless named "
                        "eager", "flops_per_batch": flops,
            "l2": "flushed between timed steps (256 MiB write)"}
@@ -665,6 +677,56 @@ def run_reference(args) -> None:
     }))
 
 
+def dmrg_solve(args) -> dict:
+    """Config-2 solves end to end on the GPU: the L = 64 SU(2) Heisenberg chain from the
+    seeded start, chi = 256 (dense), cutoff 1e-10, ncv = 20, the reference's convergence
+    tolerances, at most 10 sweeps -- first from empty plan caches (planning included),
+    then again with the caches warm, and in the 3xBF16 precision form; energies against
+    the reference's own run.  Beside it, the oracle's DMRG (the reference's algorithm in
+    NumPy) on the host cores for its first sweep, a bounded sample of the same solve."""
+    import torch
+
+    from tenet import network
+
+    L = 64
+    out = {"workload": "L=64 SU(2) Heisenberg, chi=256 dense, cutoff 1e-10, ncv=20, max 10 "
+                       "sweeps, seeded start 2j<=16", "reference_energy": REF_DMRG["energy"],
+           "reference_sweeps": REF_DMRG["sweeps"]}
+    for name, kw in (("f64_cold", {}), ("f64_warm", {}), ("3xbf16", {"precision": "3xbf16"})):
+        psi = chain64_start(L)
+        stamps = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        o = network.dmrg_(psi, network.heisenberg_mpo_su2(L), chi=256, cutoff=1e-10, ncv=20,
+                          max_sweeps=10, callback=lambda r: stamps.append(time.perf_counter()),
+                          **kw)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        out[name] = {"seconds": sec, "solves_per_s": 1.0 / sec, "sweeps": o.sweeps,
+                     "energy": o.energy,
+                     "abs_dE_per_site_vs_reference": abs(o.energy - REF_DMRG["energy"]) / L,
+                     "first_sweep_s": stamps[0] - t0 if stamps else None}
+    if not args.no_cpu:
+        import oracle.tenet_oracle as O
+
+        phys = tuple(PHYS.items())
+        bonds = [tuple((j, 1) for j in range(i % 2, min(i, L - i, 16) + 1, 2))
+                 for i in range(L + 1)]
+        psi = [O.random(O.Structure(O.SU2, (O.Leg(bonds[i], O.OUT), O.Leg(phys, O.OUT),
+                                            O.Leg(bonds[i + 1], O.IN))), i) for i in range(L)]
+        t0 = time.perf_counter()
+        stamps = []
+        O.dmrg(psi, O.heisenberg_mpo_su2(L), chi=256, cutoff=1e-10, ncv=20, max_sweeps=1,
+               on_sweep=lambda k, p, e: stamps.append((time.perf_counter() - t0, e)))
+        out["cpu_baseline"] = {
+            "kind": "port", "cores": host_cores(),
+            "sample": "the oracle's DMRG, first sweep of the same solve (canonisation and "
+                      "environment set-up included)",
+            "first_sweep_s": stamps[0][0], "first_sweep_energy": stamps[0][1],
+            "gpu_first_sweep_speedup": stamps[0][0] / out["f64_cold"]["first_sweep_s"]}
+    return out
+
+
 def run_tenet(args) -> None:
     import torch
     import torch.distributed as dist
@@ -679,14 +741,18 @@ def run_tenet(args) -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     from tenet import _exec, _lib, network
-    from tenet.program import GraphMatvec, heff2_program
+    from tenet.program import GraphMatvec, heff2_folded_program, heff2_program
 
     tensors = build_workload(seed=rank)
     fl, w1, w2, fr, aa = tensors
+    # the metric's work: the reference's four-contraction lowering (sum of 2 M K N)
     flops = heff2_flops()
     launches_eager = launches_per_matvec(tensors)
-    prog = heff2_program(fl, w1, w2, fr, aa.structure)
-    assert prog.flops == flops
+    # the timed form: the environments' default, the MPO-folded two-contraction chain
+    lf, rf = network.fold_left(fl, w1), network.fold_right(w2, fr)
+    prog = heff2_folded_program(lf, rf, aa.structure)
+    site = heff2_program(fl, w1, w2, fr, aa.structure)
+    assert site.flops == flops
     gm = GraphMatvec(prog)
     gm.x.copy_(aa.arena)
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
@@ -704,39 +770,37 @@ def run_tenet(args) -> None:
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in ev)
 
-    # the two eager forms, for comparison (the plain FP64 form is the eager op-by-op path)
-    eager_ms = {}
+    # other forms, for comparison: the plain FP64 form (eager, op by op), the reference's
+    # four-contraction order as a graph, the folded chain without a graph, without
+    # programmatic dependent launch, and as one persistent launch
+    gm_site = GraphMatvec(site)
+    gm_site.x.copy_(aa.arena)
+    forms_ms = {}
     for name, fn in (("eager_ops", lambda: network.heff2(fl, w1, w2, fr, aa)),
-                     ("eager_chain", lambda: prog.run(gm.x, gm.y))):
+                     ("eager_chain", lambda: prog.run(gm.x, gm.y)),
+                     ("graph_site_order", gm_site.replay)):
         for _ in range(args.warmup):
             fn()
-        eager_ms[name] = timed(fn, args.steps) / args.steps
-
-    # the same graph-captured chain without programmatic dependent launch, for comparison
+        forms_ms[name] = timed(fn, args.steps) / args.steps
     lib = _lib.load()
     lib.tnb_set_pdl(0)
     gm_plain = GraphMatvec(prog)
     lib.tnb_set_pdl(1)
-    # the persistent one-launch form of the chain (off by default, see _exec.FUSE), and
-    # the six-launch form whose gathers compute the MPO links' products (off by default)
     _exec.FUSE = True
     gm_fused = GraphMatvec(prog)
     _exec.FUSE = False
-    gm_defer = GraphMatvec(heff2_program(fl, w1, w2, fr, aa.structure, defer=True))
-    gm_defer.x.copy_(aa.arena)
-    for name, g in (("graph_chain_without_pdl", gm_plain), ("graph_fused_one_launch", gm_fused),
-                    ("graph_chain_product_gathers", gm_defer)):
+    for name, g in (("graph_without_pdl", gm_plain), ("graph_fused_one_launch", gm_fused)):
         for _ in range(args.warmup):
             g.replay()
-        eager_ms[name] = timed(g.replay, args.steps) / args.steps
+        forms_ms[name] = timed(g.replay, args.steps) / args.steps
 
     # the precision form: the sector products big enough to be dense contractions on the
     # tcgen05 tensor cores (and, for comparison, every non-skinny product there)
     mixed = {}
-    ref_out = prog(aa).numpy_arena()
+    ref_out = site(aa).numpy_arena()
     for precision, tc_min in (("3xbf16", None), ("tf32", None), ("3xbf16", 0), ("tf32", 0)):
-        mprog = heff2_program(fl, w1, w2, fr, aa.structure, precision=precision,
-                              tc_min_flops=tc_min)
+        mprog = heff2_folded_program(lf, rf, aa.structure, precision=precision,
+                                     tc_min_flops=tc_min)
         mg = GraphMatvec(mprog)
         mg.x.copy_(aa.arena)
         for _ in range(args.warmup):
@@ -749,6 +813,25 @@ def run_tenet(args) -> None:
                                         for p in lk.gemm.parts if p.kind in (3, 4)),
             "rel_error_vs_f64": float(np.linalg.norm(got - ref_out) / np.linalg.norm(ref_out))}
 
+    # the other bond histograms: graph matvec, folded and in the reference's order
+    others = {}
+    for wname, bond in WORKLOADS.items():
+        t5 = build_workload(seed=rank, bond=bond)
+        wf = heff2_flops(bond)
+        pf = heff2_folded_program(network.fold_left(t5[0], t5[1]),
+                                  network.fold_right(t5[2], t5[3]), t5[4].structure)
+        ps = heff2_program(*t5[:4], t5[4].structure)
+        row = {"bond_multiplets": {str(k): v for k, v in bond.items()}, "flops_per_matvec": wf}
+        for tag, pp in (("folded", pf), ("site_order", ps)):
+            g = GraphMatvec(pp)
+            g.x.copy_(t5[4].arena)
+            for _ in range(args.warmup):
+                g.replay()
+            wms = timed(g.replay, args.steps) / args.steps
+            row[tag] = {"ms_per_matvec": wms, "tflops": wf / (wms * 1e-3) / 1e12,
+                        "launches": pp.launches}
+        others[wname] = row
+
     for _ in range(args.warmup):
         gm.replay()
     torch.cuda.synchronize()
@@ -756,8 +839,8 @@ def run_tenet(args) -> None:
         dist.barrier()
     with Clocks(local) as clk:
         ms = timed(gm.replay, args.steps)
-        # the timed steps take milliseconds, shorter than the 200 ms sampling period:
-        # keep the same replay loop running for a second so the sampler sees it under load
+        # the timed steps take well under the 200 ms sampling period: keep the same replay
+        # loop running for a second so the sampler sees it under load
         t_end = time.perf_counter() + 1.0
         while time.perf_counter() < t_end:
             for _ in range(50):
@@ -786,6 +869,7 @@ def run_tenet(args) -> None:
     gm_host = GraphMatvec(prog, host_io=True)
     gm_host.host_x.copy_(aa.arena.detach().cpu())
     out_size = aa.arena.numel()
+
     def e2e_step():
         gm_host.replay_host()
 
@@ -808,35 +892,38 @@ def run_tenet(args) -> None:
         gemm_tflops = g["work"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] else 0.0
         gather_gbs = gt["work"] / (gt["ms"] * 1e-3) / 1e9 if gt["ms"] else 0.0
         dominant_is_gemm = g["ms"] >= gt["ms"]
+        key = "grouped_gemm_f64" if dominant_is_gemm else "block_gather"
         roofline = {
             "bound": "tensor" if dominant_is_gemm else "hbm",
-            "kernel": "grouped_gemm_f64" if dominant_is_gemm else "block_gather",
+            "kernel": key,
             "achieved": gemm_tflops if dominant_is_gemm else gather_gbs,
             "peak": dgemm if dominant_is_gemm else pk["hbm_gbs"],
             "unit": "TFLOP/s" if dominant_is_gemm else "GB/s",
             "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in "
                             "MEASURED_PEAKS.json)") if dominant_is_gemm
             else f"MEASURED_PEAKS.json hbm_gbs ({pk['src']})",
-            # DRAM bytes per launch (read + write) of the same kernel from the ncu captures of
-            # this workload, mean of the two captured launches: the operands sit in L2
-            "traffic": NCU_TRAFFIC["grouped_gemm_f64" if dominant_is_gemm else "block_gather"],
-            "traffic_source": "ncu --set full captures, profiles/"
-                              + ("gemm_f64_heff2_su2_256mult.md" if dominant_is_gemm
-                                 else "gather_heff2_su2_256mult.md"),
+            # DRAM bytes per launch (read + write) of the same kernel on this workload, from
+            # one ncu capture of this build (cold cache; in the graph replay the operands
+            # sit in L2), in bytes, mean over the captured launches
+            "traffic": NCU_TRAFFIC.get(key),
             "kernels": {
                 "grouped_gemm_f64": {"launches": g["launches"], "ms": g["ms"],
                                      "share": g["ms"] / total_kernel_ms if total_kernel_ms else 0,
-                                     "tflops": gemm_tflops, "dgemm_peak_tflops": dgemm},
+                                     "tflops_executed": gemm_tflops,
+                                     "dgemm_peak_tflops": dgemm},
                 "block_gather": {"launches": gt["launches"], "ms": gt["ms"],
                                  "share": gt["ms"] / total_kernel_ms if total_kernel_ms else 0,
                                  "gbs": gather_gbs, "hbm_peak_gbs": pk["hbm_gbs"]},
             },
+            "kernel_ms_per_step": total_kernel_ms / args.steps,
+            "graph_ms_per_step": ms / args.steps,
         }
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
+        solve = dmrg_solve(args) if args.dmrg else None
         solves = serving(args) if args.serve_requests > 0 else None
         env3 = batched_env_updates(args) if args.config3_n > 0 else None
-        bmv = (batched_matvecs(args, eager_ms["eager_ops"], ms / args.steps)
+        bmv = (batched_matvecs(args, forms_ms["eager_ops"], ms / args.steps)
                if args.batch_n > 0 else None)
         gprobe = gemm_probe(args.gemm_n, dgemm) if args.gemm_n > 0 else None
         print(json.dumps({
@@ -845,17 +932,21 @@ def run_tenet(args) -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": bench_config(world),
-            "flops_per_matvec": flops, "elements_aa": int(aa.arena.numel()),
+            "flops_per_matvec": flops, "gemm_flops_executed_per_matvec": prog.flops,
+            "elements_aa": int(aa.arena.numel()),
             "e2e": {"value": e2e_value, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(aa.arena.numel() * 8),
                     "d2h_bytes_per_step": int(out_size * 8)},
             "gpu_launches": int(args.steps * launches_per_step),
             "launches_per_step": launches_per_step,
-            "forms_ms_per_matvec": {"graph_chain": ms / args.steps, **eager_ms},
-            "forms_tflops": {"graph_chain": flops / (ms / args.steps * 1e-3) / 1e12,
-                             **{k: flops / (v * 1e-3) / 1e12 for k, v in eager_ms.items()}},
+            "forms_ms_per_matvec": {"graph_folded": ms / args.steps, **forms_ms},
+            "forms_tflops": {"graph_folded": flops / (ms / args.steps * 1e-3) / 1e12,
+                             **{k: flops / (v * 1e-3) / 1e12 for k, v in forms_ms.items()}},
             "launches_per_matvec_eager_ops": launches_eager,
+            "launches_per_matvec_site_order": site.launches,
+            "other_workloads": others,
             "mixed_precision_forms": mixed,
+            "dmrg_solve": solve,
             "serving": solves,
             "batched_env_updates": env3,
             "batched_matvecs": bmv,
@@ -896,6 +987,8 @@ def main() -> None:
     ap.add_argument("--profile-config3", action="store_true",
                     help="only run the batched environment update a few times (a small, "
                          "fixed launch sequence for profiling its kernels) and exit")
+    ap.add_argument("--no-dmrg", dest="dmrg", action="store_false",
+                    help="skip the config-2 DMRG time-to-solution leg")
     ap.add_argument("--derive-bond", action="store_true",
                     help="grow the L = 64 chain to --derive-chi multiplets and print its "
                          "mid-chain bond histogram, then exit")

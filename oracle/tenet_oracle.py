@@ -710,6 +710,159 @@ def lanczos(matvec, v: Tensor, *, ncv: int = 3, tol: float = 1e-13):
 
 
 # ---------------------------------------------------------------------------------------
+# the two-site DMRG driver  (network/mps.py:312-352, network/env.py:506-633,
+# network/dmrg.py:321-843, noiseless flat-chi branch)
+
+
+def heisenberg_mpo_su2(n_sites: int, j: float = 1.0) -> list:
+    """The site tensors of ``MPO.from_terms(L, [(j, [(S.S, (i, i + 1))])]).materialize()``
+    on spin-1/2 SU(2) sites (``network/mps.py:3135-3341``, ``models/sites.py:121-195``): MPO
+    bond channels "start" (2j = 0), "open" (2j = 2, the split ``S.S``'s first factor) and
+    "done" (2j = 0); in the fusion-tree basis the reduced coefficients are 1 on the
+    identity channels, ``sqrt(3/2)`` to open and ``-sqrt(3/8) j`` to close (their
+    product ``-3/4 j`` is the reduced ``S.S``).  Legs ``(x IN*, P OUT, p IN, m OUT*)``."""
+    phys = ((1, 1),)
+
+    def states(b):
+        if b == 0:
+            return [("start", 0)]
+        if b == n_sites:
+            return [("done", 0)]
+        if b == 1:
+            return [("start", 0), ("open", 2)]
+        if b == n_sites - 1:
+            return [("done", 0), ("open", 2)]
+        return [("start", 0), ("done", 0), ("open", 2)]
+
+    def leg(st, side):
+        count: dict = {}
+        for _, a in st:
+            count[a] = count.get(a, 0) + 1
+        return Leg(tuple(sorted(count.items())), side, True)
+
+    def index(st, label):
+        a = dict(st)[label]
+        return a, [x for x, b in st if b == a].index(label)
+
+    rules = [("start", "start", 1.0), ("done", "done", 1.0), ("start", "open", np.sqrt(1.5)),
+             ("open", "done", -np.sqrt(3.0 / 8.0) * j)]
+    out = []
+    for n in range(n_sites):
+        sl, sr = states(n), states(n + 1)
+        s = Structure(SU2, (leg(sl, IN), Leg(phys, OUT), Leg(phys, IN), leg(sr, OUT)))
+        blocks = []
+        for key in block_order(s):
+            (ps, ms), _, c = key[0]
+            (xs, _), _, _ = key[1]
+            blk = np.zeros(block_shape(s, key))
+            if c == 1:
+                for a, b, v in rules:
+                    if a in dict(sl) and b in dict(sr):
+                        (xa, xi), (mb, mi) = index(sl, a), index(sr, b)
+                        if xa == xs and mb == ms:
+                            blk[xi, 0, 0, mi] = v
+            blocks.append(blk)
+        out.append(Tensor(s, blocks))
+    return out
+
+
+def lq(t: Tensor, outputs, inputs):
+    """Reduced LQ per coupled sector (``ops/linalg.py:549-620``): ``(L, Q)`` with the new
+    bond IN on ``L`` and OUT on ``Q``, of degeneracy ``min(rows, cols)``."""
+    m = repartition(t, tuple(outputs), tuple(inputs))
+    p = m.structure.provider
+    mats = to_matrices(m)
+    parts = {}
+    for c, b in mats.items():
+        q, r = np.linalg.qr(b.T)
+        parts[c] = (r.T, q.T)
+    bond = tuple(sorted((c, min(b.shape)) for c, b in mats.items()))
+    sl = Structure(p, (*m.structure.codomain, Leg(bond, IN)))
+    sq = Structure(p, (Leg(bond, OUT), *m.structure.domain))
+    return (from_matrices(sl, {c: v[0] for c, v in parts.items()}),
+            from_matrices(sq, {c: v[1] for c, v in parts.items()}))
+
+
+def _site(t: Tensor) -> Tensor:
+    """The MPS write barrier: a site tensor on ``(l, p | r)`` (``network/mps.py:126-143``)."""
+    return repartition(t, (0, 1), (2,))
+
+
+def canonize(psi: list) -> list:
+    """Right-canonical form by one LQ per site from the right (``network/mps.py:312-352``)."""
+    psi = list(psi)
+    for n in range(len(psi) - 1, 0, -1):
+        left, q = lq(psi[n], (0,), (1, 2))
+        psi[n] = _site(q)
+        psi[n - 1] = _site(einsum("apx,xy->apy", psi[n - 1], left))
+    psi[0] = scale(psi[0], 1.0 / norm(psi[0]))
+    return psi
+
+
+def dmrg(psi: list, h: list, *, chi: int, cutoff: float, ncv: int, max_sweeps: int,
+         energy_tol: float = 1e-12, schmidt_tol: float = 1e-8, on_sweep=None):
+    """Two-site DMRG (``network/dmrg.py:321-843``, no noise, flat ``chi`` / ``cutoff``):
+    canonise, build the environments towards site 0, sweep right then left solving each
+    bond by ``lanczos`` and splitting by ``svd_truncated``, stop when both the energy and
+    the worst Schmidt change fall under their tolerances.  ``psi`` and ``h`` are lists of
+    site tensors; returns ``(energy per sweep, final psi)``.  ``on_sweep(k, psi, energy)``
+    is called after each sweep."""
+    n_sites = len(psi)
+    psi = canonize(psi)
+    kl, kr = psi[0].structure.legs[0], psi[-1].structure.legs[2]
+    wl, wr = h[0].structure.legs[0], h[-1].structure.legs[3]
+    p = psi[0].structure.provider
+    F = {(-1, 0): ones(Structure(p, (Leg(kl.sectors, IN, kl.dual), Leg(wl.sectors, OUT, wl.dual),
+                                     Leg(kl.sectors, OUT, kl.dual)))),
+         (n_sites, n_sites - 1): ones(Structure(p, (Leg(kr.sectors, OUT, kr.dual),
+                                                    Leg(wr.sectors, IN, wr.dual),
+                                                    Leg(kr.sectors, IN, kr.dual))))}
+    for n in range(n_sites - 1, 0, -1):
+        F[n, n - 1] = env_update_first(F[n + 1, n], psi[n], h[n])
+    energies, schmidt, energy = [], {}, float("inf")
+    for it in range(1, max_sweeps + 1):
+        old_e, old_s = energy, dict(schmidt)
+        for forward in (True, False):
+            for n in (range(n_sites - 1) if forward else range(n_sites - 2, -1, -1)):
+                aa = einsum("apx,xqr->apqr", psi[n], psi[n + 1])
+                fl, fr = F[n - 1, n], F[n + 2, n + 1]
+                energy, aa = lanczos(lambda v: heff2(fl, h[n], h[n + 1], fr, v), aa, ncv=ncv)
+                u, s, vh = svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff)
+                s = scale(s, 1.0 / norm(s))
+                if forward:
+                    psi[n], psi[n + 1] = _site(u), _site(einsum("xy,yqr->xqr", s, vh))
+                else:
+                    psi[n], psi[n + 1] = _site(einsum("apx,xy->apy", u, s)), _site(vh)
+                schmidt[n] = corner_spectrum(s)
+                F.pop((n, n - 1), None), F.pop((n, n + 1), None)
+                F.pop((n + 1, n), None), F.pop((n + 1, n + 2), None)
+                if forward:
+                    F[n, n + 1] = env_update_last(F[n - 1, n], psi[n], h[n])
+                else:
+                    F[n + 1, n] = env_update_first(F[n + 2, n + 1], psi[n + 1], h[n + 1])
+        energies.append(energy)
+        if on_sweep is not None:
+            on_sweep(it, psi, energy)
+        if abs(old_e - energy) < energy_tol and _schmidt_change(old_s, schmidt) < schmidt_tol:
+            break
+    return energies, psi
+
+
+def _schmidt_change(old: dict, new: dict) -> float:
+    """Worst bond's zero-padded Schmidt-spectrum distance, infinite before any history
+    (``network/dmrg.py:545-561``)."""
+    if not old:
+        return float("inf")
+    worst = 0.0
+    for n, cur in new.items():
+        prev = old.get(n, [])
+        m = max(len(prev), len(cur))
+        a, b = prev + [0.0] * (m - len(prev)), cur + [0.0] * (m - len(cur))
+        worst = max(worst, sum((x - y) ** 2 for x, y in zip(a, b)) ** 0.5)
+    return worst
+
+
+# ---------------------------------------------------------------------------------------
 # JSON helpers for the golden vectors (tests/golden/make_golden.py writes this format)
 
 

@@ -22,7 +22,7 @@ from tenet import ops
 from tenet.structure import OUT
 from tenet.tensor import SymmetricTensor
 
-__all__ = ["DMRG_out", "Env", "MPO", "MPS", "Sweep", "composed", "ctmrg", "dmrg_",
+__all__ = ["DMRG_out", "Env", "MPO", "MPS", "Sweep", "composed", "ctmrg", "dmrg_", "local_op",
            "env_update_first", "env_update_last", "heff2", "lanczos", "spectrum", "sweep_"]
 
 
@@ -52,6 +52,24 @@ def heff2(fl: SymmetricTensor, w1: SymmetricTensor, w2: SymmetricTensor, fr: Sym
     t = composed("apqys,mQqy->apQms", t, w2, bend="q")
     t = composed("apQms,xPpm->aPQxs", t, w1, bend="p")
     return composed("aPQxs,axB->BPQs", t, fl, bend="a")
+
+
+def fold_left(fl: SymmetricTensor, w1: SymmetricTensor) -> SymmetricTensor:
+    """``F[(n-1, n)] . W[n]`` on ``(a, B, P, p, m)``: the left environment with the left
+    site's MPO tensor folded in (the reference's prepared path folds its environments the
+    same way once per solve, ``network/env.py:234-264``)."""
+    return ops.einsum("axB,xPpm->aBPpm", fl, w1)
+
+
+def fold_right(w2: SymmetricTensor, fr: SymmetricTensor) -> SymmetricTensor:
+    """``W[n+1] . F[(n+2, n+1)]`` on ``(m, Q, q, r, s)``."""
+    return ops.einsum("mQqy,rys->mQqrs", w2, fr)
+
+
+def heff2_folded(lf: SymmetricTensor, rf: SymmetricTensor, aa: SymmetricTensor) -> SymmetricTensor:
+    """``H_eff @ aa`` from the folded environments: ``(aa . rf) . lf``."""
+    t = ops.einsum("apqr,mQqrs->apmQs", aa, rf)
+    return ops.einsum("apmQs,aBPpm->BPQs", t, lf)
 
 
 def env_update_last(f: SymmetricTensor, a: SymmetricTensor, w: SymmetricTensor,
@@ -348,6 +366,32 @@ class MPO:
         """The site-tensor form: this MPO already is one."""
         return self
 
+    @classmethod
+    def from_terms(cls, n_sites: int, terms) -> "MPO":
+        """An MPO from a term list (``network/mps.py:3135-3341``), for the SU(2) spin-1/2
+        chains of this build: every term ``(coef, [(op, (i, j))])`` with ``op`` an
+        invariant two-site operator (``spin_half(SU2).ops["S.S"]`` or any combination of
+        it and the identity) on sites ``i < j`` with ``j - i`` 1 or 2.  The MPO is the
+        finite-state machine of ``su2_chain_mpo``; other term shapes are refused."""
+        j1 = [0.0] * (n_sites - 1)
+        j2 = [0.0] * max(n_sites - 2, 0)
+        onsite = [0.0] * n_sites
+        for term in terms:
+            try:
+                coef, factors = term
+                ((op, where),) = factors
+                i, j = where
+            except (TypeError, ValueError):
+                raise ValueError("from_terms: each term must be (coef, [(op, (i, j))]) with one "
+                                 "invariant two-site operator") from None
+            if not (0 <= i < j < n_sites) or j - i not in (1, 2):
+                raise ValueError(f"from_terms: sites {(i, j)} are not neighbours or next "
+                                 f"neighbours on a chain of {n_sites}")
+            a, b = su2_invariant_coefficients(op.structure, op.numpy_arena())
+            (j1 if j - i == 1 else j2)[i] += float(coef) * a
+            onsite[i] += float(coef) * b
+        return su2_chain_mpo(n_sites, j1, j2, onsite)
+
     def __len__(self) -> int:
         return len(self.sites)
 
@@ -370,7 +414,15 @@ def identity_w(aux, phys) -> SymmetricTensor:
 
 def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
     """``H = J sum_i S_i . S_{i+1} + J2 sum_i S_i . S_{i+2}`` on spin-1/2 SU(2) sites, as
-    site tensors.
+    site tensors (uniform couplings; see ``su2_chain_mpo``)."""
+    if n_sites < 2:
+        raise ValueError("a Heisenberg chain needs at least two sites")
+    return su2_chain_mpo(n_sites, [j] * (n_sites - 1), [j2] * max(n_sites - 2, 0))
+
+
+def su2_chain_mpo(n_sites: int, j1, j2=(), onsite=()) -> MPO:
+    """``H = sum_i j1[i] S_i . S_{i+1} + sum_i j2[i] S_i . S_{i+2} + sum_i onsite[i]`` on
+    spin-1/2 SU(2) sites, as site tensors.
 
     The MPO bond carries the finite-state machine of the invariant terms: a spin-0 "not
     started" channel, a spin-1 channel carrying the first ``S``, and a spin-0 "finished"
@@ -379,10 +431,12 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
     fusion-tree basis of the blocks ``(P, m | x, p)`` the reduced coefficients are 1 for
     the identity channels, ``sqrt(3/2)`` for opening the spin-1 channel and
     ``-sqrt(3/8) J`` for closing it (their product is ``-3/4 J``, the reduced S.S).  With
-    ``j2`` a second spin-1 channel carries the opened ``S`` one site further: the open
-    channel passes a site through the spectator identity (``identity_w``) and closes
-    with ``-sqrt(3/8) J2`` -- the reference's reading of a non-adjacent invariant S.S
-    term in ``from_terms`` (bulk multiplets ``{0: 2, 2: 2}``).
+    any ``j2`` nonzero a second spin-1 channel carries the opened ``S`` one site further:
+    the open channel passes a site through the spectator identity (``identity_w``) and
+    closes with ``-sqrt(3/8) J2`` -- the reference's reading of a non-adjacent invariant
+    S.S term in ``from_terms`` (bulk multiplets ``{0: 2, 2: 2}``).  ``onsite[i]`` is a
+    constant on site ``i`` (the identity part of an invariant two-site term), carried by
+    the start -> finished channel.
     """
     import math
 
@@ -390,7 +444,14 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
     from tenet.symmetry import SU2
 
     if n_sites < 2:
-        raise ValueError("a Heisenberg chain needs at least two sites")
+        raise ValueError("a chain MPO needs at least two sites")
+    j1 = [float(x) for x in j1]
+    j2 = [float(x) for x in j2] + [0.0] * (max(n_sites - 2, 0) - len(j2))
+    onsite = [float(x) for x in onsite] + [0.0] * (n_sites - len(onsite))
+    if len(j1) != n_sites - 1 or len(j2) != max(n_sites - 2, 0) or len(onsite) != n_sites:
+        raise ValueError("su2_chain_mpo: j1 needs n - 1 couplings, j2 at most n - 2, "
+                         "onsite at most n")
+    has_j2 = any(j2)
     phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
 
     # states per bond: list of (label, sector two_j) in degeneracy order within a sector
@@ -405,25 +466,23 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
             st = [("done", 0), ("open", 2)]
         else:
             st = [("start", 0), ("done", 0), ("open", 2)]
-        if j2 and 2 <= b <= n_sites - 1:
+        if has_j2 and 2 <= b <= n_sites - 1:
             st.append(("open2", 2))
         return st
 
     def space(st):
         count: dict = {}
-        for _, s in st:
-            count[s] = count.get(s, 0) + 1
-        return GradedSpace.new(SU2, {SU2.sector(s): m for s, m in count.items()})
+        for _, sec in st:
+            count[sec] = count.get(sec, 0) + 1
+        return GradedSpace.new(SU2, {SU2.sector(sec): m for sec, m in count.items()})
 
     def index(st, label):
         sec = dict(st)[label]
-        return sec, [lab for lab, s in st if s == sec].index(label)
+        return sec, [lab for lab, x in st if x == sec].index(label)
 
     opn, cls = math.sqrt(1.5), -math.sqrt(3.0 / 8.0)
-    rules = [("start", "start", 1.0), ("done", "done", 1.0), ("start", "open", opn),
-             ("open", "done", cls * j), ("open2", "done", cls * j2)]
     spec = None
-    if j2:
+    if has_j2:
         # the spectator's reduced blocks, keyed like the site tensor's own block keys
         v1 = GradedSpace.new(SU2, {SU2.sector(2): 1})
         t = identity_w(Leg(v1, IN, True), phys)
@@ -433,6 +492,11 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
     sites = []
     for n in range(n_sites):
         sl, sr = states(n), states(n + 1)
+        rules = [("start", "start", 1.0), ("done", "done", 1.0), ("start", "open", opn),
+                 ("open", "done", cls * (j1[n - 1] if n >= 1 else 0.0)),
+                 ("open2", "done", cls * (j2[n - 2] if n >= 2 else 0.0))]
+        if onsite[n]:
+            rules.append(("start", "done", onsite[n]))
         legs = (Leg(space(sl), IN, True), Leg(phys, OUT), Leg(phys, IN), Leg(space(sr), OUT, True))
         s = TensorStructure(legs)
         lay = layout(s)
@@ -462,6 +526,51 @@ def heisenberg_mpo_su2(n_sites: int, j: float = 1.0, j2: float = 0.0) -> MPO:
     return MPO(sites)
 
 
+def local_op(matrix, *, phys, charge=None) -> SymmetricTensor:
+    """A dense two-site operator on spin-1/2 SU(2) sites as the invariant rank-4 tensor on
+    ``(p OUT, p OUT, p IN, p IN)`` (``network/mps.py:960-1041``, the ``charge=None`` form).
+    The dense basis is the reference's: magnetic index descending (``m = j - k``).  On two
+    spin-1/2 sites an invariant operator is ``t0`` on the singlet and ``t2`` on the
+    triplet; those are its two blocks.  A matrix that is not invariant is refused."""
+    from tenet.structure import IN, Leg, TensorStructure
+
+    m = np.asarray(matrix, dtype=np.float64)
+    if charge is not None or phys.provider.name != "SU2" \
+            or dict((a.two_j, k) for a, k in phys.sectors) != {1: 1} or m.size != 16:
+        raise ValueError("local_op: this build constructs invariant two-site operators on "
+                         "spin-1/2 SU(2) sites only")
+    m = m.reshape(4, 4)
+    singlet = np.array([0.0, 1.0, -1.0, 0.0]) / np.sqrt(2.0)
+    t0 = float(singlet @ m @ singlet)
+    t2 = float(m[0, 0])
+    want = t2 * np.eye(4) + (t0 - t2) * np.outer(singlet, singlet)
+    if np.abs(m - want).max() > 1e-12 * max(1.0, np.abs(m).max()):
+        raise ValueError("local_op: the matrix is not SU(2)-invariant")
+    s = TensorStructure((Leg(phys, OUT), Leg(phys, OUT), Leg(phys, IN), Leg(phys, IN)))
+    host = np.array([t0 if key[0][2] == 0 else t2 for key in s.keys])
+    return SymmetricTensor.from_numpy_arena(s, host)
+
+
+def su2_invariant_coefficients(structure, host: np.ndarray) -> tuple[float, float]:
+    """``(a, b)`` with ``T = a S.S + b 1`` for an SU(2)-invariant two-site operator ``T``
+    on spin-1/2 legs ``(p OUT, p OUT, p IN, p IN)`` given by its structure and block arena.
+    On two spin-1/2 sites the invariant operators are spanned by the identity and ``S.S``
+    (one reduced value per total spin: ``-3/4`` and ``1/4`` for ``S.S``)."""
+    from tenet.structure import IN
+
+    legs = structure.legs
+    ok = len(legs) == 4 and all(leg.space.provider.name == "SU2" for leg in legs) \
+        and [leg.side is IN for leg in legs] == [False, False, True, True] \
+        and all(dict((a.two_j, m) for a, m in leg.space.sectors) == {1: 1} for leg in legs)
+    if not ok:
+        raise ValueError("from_terms: a two-site SU(2) term must be an invariant operator on "
+                         "spin-1/2 legs (p OUT, p OUT, p IN, p IN), as spin_half(SU2).ops['S.S']")
+    vals = {}
+    for key, v in zip(structure.keys, host):
+        vals[key[0][2]] = float(v)
+    t0, t2 = vals.get(0, 0.0), vals.get(2, 0.0)
+    a = t2 - t0
+    return a, t2 - a / 4.0
 class Env:
     """``<bra|H|psi>`` environments keyed by directed bond (``network/env.py:435-645``):
     ``F[(n, n+1)] = (ket IN, mpo OUT, bra OUT)`` from sites ``<= n``, ``F[(n, n-1)] =
@@ -475,10 +584,11 @@ class Env:
 
     def __init__(self, psi: MPS, h: MPO, *, bra: MPS | None = None, compile=None,
                  compiled: bool = True, precision: str = "f64",
-                 tc_min_flops: int | None = None) -> None:
+                 tc_min_flops: int | None = None, fold: bool = True) -> None:
         from tenet.structure import IN, Leg
 
         self.psi, self.h, self.compiled, self.precision = psi, h, compiled, precision
+        self.fold = fold
         self.bra = psi if bra is None else bra
         self.compile = compile
         self.tc_min_flops = tc_min_flops
@@ -548,23 +658,37 @@ class Env:
 
     def _bond(self, n: int, structure, precision: str) -> dict:
         """The bond's cached programs: one allocated heff2 program per precision (plus what
-        was captured around it), re-packed when only the environment values changed."""
-        from tenet.program import heff2_program
+        was captured around it), re-packed when only the environment values changed.  With
+        ``fold`` (the default) the program is the two-contraction folded form
+        (``heff2_folded_program``), its operands ``fold_left`` / ``fold_right`` of the
+        current environments; otherwise the reference's four-contraction order."""
+        from tenet.program import heff2_folded_program, heff2_program
 
         fl, fr = self.F[n - 1, n], self.F[n + 2, n + 1]
         w1, w2 = self.h[n], self.h[n + 1]
-        skey = (fl.structure, fr.structure, structure)
+        skey = (fl.structure, fr.structure, structure, self.fold)
         hit = self._prog.get((n, precision))
+
+        def operands():
+            if self.fold:
+                return {"lf": fold_left(fl, w1), "rf": fold_right(w2, fr)}
+            return {"fr": fr, "w2": w2, "w1": w1, "fl": fl}
+
         if hit is None or hit["skey"] != skey:
             # one program per bond and precision; a new structure replaces it
-            hit = {"skey": skey, "bound": (fl, fr), "captured": {},
-                   "program": heff2_program(fl, w1, w2, fr, structure, precision=precision,
-                                            tc_min_flops=self.tc_min_flops)}
+            ops_ = operands()
+            if self.fold:
+                prog = heff2_folded_program(ops_["lf"], ops_["rf"], structure,
+                                            precision=precision, tc_min_flops=self.tc_min_flops)
+            else:
+                prog = heff2_program(fl, w1, w2, fr, structure, precision=precision,
+                                     tc_min_flops=self.tc_min_flops)
+            hit = {"skey": skey, "bound": (fl, fr), "captured": {}, "program": prog}
             self._prog[(n, precision)] = hit
         elif hit["bound"][0] is not fl or hit["bound"][1] is not fr:
             # same structures, new environment values: re-pack the fixed operands into the
             # program's buffers; everything captured around them stays valid
-            bound = dict(zip(("fr", "w2", "w1", "fl"), (fr, w2, w1, fl)))
+            bound = operands()
             prog = hit["program"]
             for lk, name in zip(prog.links, prog.operand_names):
                 lk.b_tensor = bound[name]
@@ -796,7 +920,7 @@ def dmrg_steps(psi: MPS, h: MPO, *, schedule=None, chi: int | None = None,
                schmidt_tol: float = 1e-8, max_sweeps: int = 40, ncv: int = 3,
                orthogonal_to=None, seed: int = 0, callback=None, compile=None,
                compiled: bool = True, precision: str = "f64",
-               tc_min_flops: int | None = None, budget: str = "dense"):
+               tc_min_flops: int | None = None, budget: str = "dense", fold: bool = True):
     """``dmrg_`` as a step generator (see ``sweep_steps``); returns the ``DMRG_out``."""
     if schedule is not None:
         if chi is not None or cutoff is not None:
@@ -809,7 +933,7 @@ def dmrg_steps(psi: MPS, h: MPO, *, schedule=None, chi: int | None = None,
         plan = [Sweep(64 if chi is None else chi, 1e-14 if cutoff is None else cutoff)]
     psi.canonize_(0)
     env = Env(psi, h, compile=compile, compiled=compiled, precision=precision,
-              tc_min_flops=tc_min_flops).setup_(0)
+              tc_min_flops=tc_min_flops, fold=fold).setup_(0)
     orthos: tuple = ()
     if orthogonal_to:
         ident = MPO.identity(len(psi), psi[0].legs[1].space)
@@ -849,7 +973,8 @@ def dmrg_(psi: MPS, h: MPO, *, schedule=None, chi: int | None = None,
           cutoff: float | None = None, energy_tol: float = 1e-12, schmidt_tol: float = 1e-8,
           max_sweeps: int = 40, ncv: int = 3, orthogonal_to=None, seed: int = 0,
           callback=None, compile=None, compiled: bool = True, precision: str = "f64",
-          tc_min_flops: int | None = None, budget: str = "dense") -> DMRG_out:
+          tc_min_flops: int | None = None, budget: str = "dense",
+          fold: bool = True) -> DMRG_out:
     """Sweep ``psi`` to the ground state of ``h`` in place and return a ``DMRG_out``
     (``network/dmrg.py:620-843``): the same arguments, defaults, refusals, schedule rule
     (the last entry repeats), noise forms, excited-state projection and the two
@@ -861,12 +986,14 @@ def dmrg_(psi: MPS, h: MPO, *, schedule=None, chi: int | None = None,
     runs the matvec products big enough for the tensor cores there (``tc_min_flops``),
     with FP64 reorthogonalisation and the FP64 correction of every such solve, while the
     SVD and truncation stay FP64; ``budget="reduced"`` caps kept multiplets instead of
-    the dense dimension."""
+    the dense dimension; ``fold`` (default) runs the matvec as two contractions of the
+    MPO-folded environments, ``fold=False`` in the reference's four-contraction order."""
     return drain(dmrg_steps(psi, h, schedule=schedule, chi=chi, cutoff=cutoff,
                             energy_tol=energy_tol, schmidt_tol=schmidt_tol,
                             max_sweeps=max_sweeps, ncv=ncv, orthogonal_to=orthogonal_to,
                             seed=seed, callback=callback, compile=compile, compiled=compiled,
-                            precision=precision, tc_min_flops=tc_min_flops, budget=budget))
+                            precision=precision, tc_min_flops=tc_min_flops, budget=budget,
+                            fold=fold))
 
 
 # ---------------------------------------------------------------------------------------

@@ -306,14 +306,20 @@ def make_dmrg64(ref: Path) -> dict:
     rec = {"L": L, "chi": chi, "ncv": 20, "cutoff": 1e-10, "max_sweeps": 10, "max_2j": 16}
     for name, op in (("site", h.materialize()), ("prepared", h)):
         t0 = time.perf_counter()
+        per_sweep = []
+
+        def record(o, per_sweep=per_sweep):
+            per_sweep.append([[[_sector_int(a), m] for a, m in o.psi[i].legs[0].space.sectors]
+                              for i in range(L)])
+
         out = dmrg_(MPS.random(site.phys, bonds, seed=0), op, chi=chi, cutoff=1e-10, ncv=20,
-                    max_sweeps=10)
+                    max_sweeps=10, callback=record)
         run = {"sweeps": out.sweeps, "energy": out.energy,
                "history": [[float(x) for x in r] for r in out.history],
                "seconds": time.perf_counter() - t0}
         if name == "site":
-            run["bonds"] = [[[_sector_int(a), m] for a, m in out.psi[i].legs[0].space.sectors]
-                            for i in range(L)]
+            run["bonds"] = per_sweep[-1]
+            run["bonds_per_sweep"] = per_sweep
         rec[name] = run
     fix = json.loads((ref / "tests/fixtures/mpskit_heisenberg.json").read_text())
     rec["mpskit_N64_chi256"] = fix["N64"]["chi256"]["energy"]

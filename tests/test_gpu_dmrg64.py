@@ -35,17 +35,29 @@ def golden(golden_dir):
     return json.loads((golden_dir / "dmrg64.json").read_text())
 
 
-def test_dmrg_su2_L64_chi256_matches_reference(golden):
+@pytest.mark.parametrize("fold", [True, False])
+def test_dmrg_su2_L64_chi256_matches_reference(golden, fold):
+    """Same number of sweeps, every bond's kept space identical after every sweep, each
+    sweep's energy within 1e-8 per site (the first sweeps grow the bonds with Lanczos at
+    ncv = 20 without reorthogonalisation, whose Ritz values move at the 1e-7 relative
+    level with the matvec's summation order -- measured alike for a host-driven
+    recurrence with the reference's own operation order), the converged energy within
+    1e-10 relative."""
     g, site = golden, golden["site"]
     L = g["L"]
     psi = _start(g)
+    seen = []
     out = network.dmrg_(psi, network.heisenberg_mpo_su2(L), chi=g["chi"], cutoff=g["cutoff"],
-                        ncv=g["ncv"], max_sweeps=g["max_sweeps"])
+                        ncv=g["ncv"], max_sweeps=g["max_sweeps"], fold=fold,
+                        callback=lambda o: seen.append(
+                            [[[SU2.label(a), k] for a, k in o.psi[i].legs[0].space.sectors]
+                             for i in range(L)]))
     assert out.sweeps == site["sweeps"]
     for got, want in zip(out.history, site["history"]):
-        assert got[0] == pytest.approx(want[0], rel=1e-10)
-    kept = [[[SU2.label(a), k] for a, k in psi[i].legs[0].space.sectors] for i in range(L)]
-    assert kept == site["bonds"], "kept bond sectors differ from the reference's"
+        assert abs(got[0] - want[0]) / L <= 1e-8
+    assert out.energy == pytest.approx(site["energy"], rel=1e-10)
+    for k, (got, want) in enumerate(zip(seen, site["bonds_per_sweep"])):
+        assert got == want, f"kept bond sectors differ from the reference's after sweep {k + 1}"
     assert abs(out.energy - g["prepared"]["energy"]) / L <= 1e-10
     assert abs(out.energy - g["mpskit_N64_chi256"]) / L <= 1e-8
 

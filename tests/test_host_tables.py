@@ -400,3 +400,33 @@ def test_graph_matvec_refuses_an_unknown_host_copy_mode():
 
     with pytest.raises(ValueError, match="host_copy"):
         GraphMatvec(None, host_io=True, host_copy="zero-copy")
+
+
+def test_su2_invariant_two_site_operator_coefficients():
+    """``T = a S.S + b 1`` read off the two reduced values of an invariant two-site operator
+    (what ``MPO.from_terms`` splits); other leg shapes are refused."""
+    from tenet.network import su2_invariant_coefficients
+    from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure
+    from tenet.symmetry import SU2
+
+    phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    s = TensorStructure((Leg(phys, OUT), Leg(phys, OUT), Leg(phys, IN), Leg(phys, IN)))
+    ss = np.array([-0.75 if key[0][2] == 0 else 0.25 for key in s.keys])
+    assert su2_invariant_coefficients(s, ss) == (1.0, 0.0)
+    assert su2_invariant_coefficients(s, 2.0 * ss + 1.0) == (2.0, 1.0)
+    bad = TensorStructure((Leg(phys, OUT), Leg(phys, IN), Leg(phys, OUT), Leg(phys, IN)))
+    with pytest.raises(ValueError, match="invariant"):
+        su2_invariant_coefficients(bad, np.zeros(2))
+
+
+def test_dmrg_record_and_schmidt_change_follow_the_reference():
+    """``DMRG_out`` and ``Sweep`` carry the reference's fields and defaults; the Schmidt
+    change is the zero-padded worst-bond distance (``network/dmrg.py:545-561``)."""
+    from tenet import network
+
+    assert network.DMRG_out._fields == ("sweeps", "energy", "denergy", "max_dSchmidt",
+                                        "max_discarded_weight", "history", "schedule", "psi")
+    assert network.Sweep() == (64, 1e-14, 0.0, "wavefunction")
+    assert network._schmidt_change({}, {0: [1.0]}) == float("inf")
+    got = network._schmidt_change({0: [0.8, 0.6], 1: [1.0]}, {0: [0.8], 1: [1.0], 2: [1.0]})
+    assert got == pytest.approx(1.0)

@@ -147,3 +147,25 @@ def test_onsager_restatement_matches_the_reference_value(golden_dir):
 
     r = json.loads((golden_dir / "ctmrg.json").read_text())["b040_chi16"]
     assert O.onsager_beta_f(r["beta"]) == pytest.approx(r["onsager_beta_f"], rel=1e-12)
+
+
+def test_oracle_dmrg_matches_reference_run(golden_dir):
+    """The oracle's two-site DMRG driver and MPO against the reference's own L = 12 run:
+    per-sweep energies, every kept bond space, and the bulk MPO site tensors."""
+    g = json.loads((golden_dir / "dmrg.json").read_text())["L12_chi32"]
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    L = g["L"]
+    W = O.heisenberg_mpo_su2(L)
+    for key, n in (("w1", 5), ("w2", 6)):
+        want = O.from_arena(O.structure_from_json(m[key]["legs"]), h[m[key]["arena"]])
+        assert W[n].structure == want.structure
+        assert np.abs(W[n].arena() - want.arena()).max() <= 1e-14
+    phys = ((1, 1),)
+    bonds = [tuple((j, 1) for j in range(i % 2, min(i, L - i) + 1, 2)) for i in range(L + 1)]
+    psi = [O.random(O.Structure(O.SU2, (O.Leg(bonds[i], O.OUT), O.Leg(phys, O.OUT),
+                                        O.Leg(bonds[i + 1], O.IN))), i) for i in range(L)]
+    energies, psi = O.dmrg(psi, W, chi=g["chi"], cutoff=1e-10, ncv=20, max_sweeps=g["sweeps"])
+    assert len(energies) == g["sweeps"]
+    np.testing.assert_allclose(energies, g["history"], rtol=1e-12)
+    assert [[list(x) for x in psi[i].structure.legs[0].sectors] for i in range(L)] == g["bonds"]
