@@ -402,6 +402,57 @@ int tnb_plan_gather_table(int64_t n_terms, const int64_t* t_src, const int64_t* 
 int64_t tnb_plan_compose(int64_t n_a, const double* a, int64_t n_b, const double* b, double* out,
                          int64_t cap);
 
+/*
+ * Blockwise SVD of the coupled-sector matrices of a lowered tensor.  Replaces the
+ * reference's per-sector `ar.do("linalg.svd")` loop of svd_truncated
+ * (ops/linalg.py:1593-1612).  One CTA per row of `rows` (8 int64 each):
+ *   [0] m, [1] n         the sector matrix, row-major at a + a_off
+ *   [2] a_off
+ *   [3] u_off            U (m x k, row-major), k = min(m, n)
+ *   [4] s_off            singular values (k), descending
+ *   [5] vt_off           Vh (k x n, row-major)
+ *   [6] w_off            -1: the working copy (max(m,n) k + k^2 + 2k doubles) lives in
+ *                        `smem_doubles` of dynamic shared memory (at most
+ *                        tnb_block_svd_smem_doubles()); else its offset in `work`
+ *   [7] 0
+ * One-sided Jacobi (rotations until every column pair is orthogonal to 1e-15 relative);
+ * columns of exactly zero norm get an orthonormal completion.  info[row] = 0 on
+ * convergence, the sweep count if the 64-sweep limit was reached, -1 on a bad row.
+ */
+int64_t tnb_block_svd_smem_doubles(void);
+int tnb_block_svd(const int64_t* rows, int64_t n_rows, const double* a, int64_t n_a,
+                  double* u, int64_t n_u, double* s, int64_t n_s, double* vt, int64_t n_vt,
+                  double* work, int64_t n_work, int32_t* info, int64_t smem_doubles,
+                  void* stream);
+
+/*
+ * The truncation decision on the device: _spectrum / _admissible / _decide of
+ * ops/linalg.py:1079-1324 in one CTA.  sectors: n_sec rows of 4 int64 [count, s_off,
+ * label, 0] in ascending label order, each a descending list of `count` singular values
+ * at s + s_off; qdim: the sectors' quantum dimensions.  The global order is (-sigma,
+ * sector, index); mode 0..5 = abs, rel, sum2, rsum2, sum1, rsum1 with `cutoff` (< 0: no
+ * cutoff); max_bond (< 0: none) bounds sum qdim (budget 0) or the count (budget 1) of the
+ * kept values, the walk stopping at the first overflow.  The sums run in the reference's
+ * order.  Outputs: keep[sector] counts, the global order (sorted_s, sorted_c: sector
+ * index), stats = {kept, dense dim, discarded weight, total weight, kept weight,
+ * admissible, total count, 0}.
+ */
+int tnb_truncate_decide(const int64_t* sectors, const double* qdim, int64_t n_sec,
+                        const double* s, int64_t n_s, double cutoff, int32_t mode,
+                        double max_bond, int32_t budget, int64_t* keep, double* sorted_s,
+                        int32_t* sorted_c, double* stats, void* stream);
+
+/*
+ * The kept prefixes into the truncated factors' packed coupled-sector matrices
+ * (ops/linalg.py:1599-1612): rows of 12 int64 [m, n, k_full, k, u_off, s_off, vt_off,
+ * pu_off, ps_off, pv_off, 0, 0] -> PU (m x k) = U[:, :k], PS (k x k) = diag(s[:k]) *
+ * scale, PV (k x n) = Vh[:k, :].
+ */
+int tnb_svd_compact(const int64_t* rows, int64_t n_rows, const double* u, int64_t n_u,
+                    const double* s, int64_t n_s, const double* vt, int64_t n_vt,
+                    double scale, double* pu, int64_t n_pu, double* ps, int64_t n_ps,
+                    double* pv, int64_t n_pv, void* stream);
+
 /* Library version (major*10000 + minor*100 + patch). */
 int tnb_version(void);
 

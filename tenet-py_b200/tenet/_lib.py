@@ -60,6 +60,13 @@ SIGNATURES = {
     "tnb_plan_gather_rows": (_i32, [_i64, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64,
                                     _vp]),
     "tnb_plan_compose": (_i64, [_i64, _vp, _i64, _vp, _vp, _i64]),
+    "tnb_block_svd_smem_doubles": (_i64, []),
+    "tnb_block_svd": (_i32, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
+                             _vp, _i64, _vp]),
+    "tnb_truncate_decide": (_i32, [_vp, _vp, _i64, _vp, _i64, _f64, _i32, _f64, _i32, _vp, _vp,
+                                   _vp, _vp, _vp]),
+    "tnb_svd_compact": (_i32, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _f64, _vp, _i64,
+                               _vp, _i64, _vp, _i64, _vp]),
     "tnb_set_pdl": (_i32, [_i32]),
     "tnb_version": (_i32, []),
     "tnb_last_error": (ctypes.c_char_p, []),

@@ -22,7 +22,7 @@ from tenet.plan import repartition_plan, validate_partition
 from tenet.structure import IN, OUT, GradedSpace, Leg, TensorStructure, layout, matrix_layout
 from tenet.tensor import SymmetricTensor
 
-__all__ = ["BondSelection", "lq", "svd_truncated"]
+__all__ = ["BondSelection", "lq", "svd_truncated", "svd_truncated_selected"]
 
 _CUTOFF_MODES = ("abs", "rel", "sum2", "rsum2", "sum1", "rsum1")
 
@@ -103,10 +103,83 @@ def _raise_exec(s: TensorStructure):
                                                terms))
 
 
+class _SvdPlan:
+    """Device tables of one lowered structure's blockwise SVD: per coupled sector (in label
+    order) its shape and the offsets of its full factors, the decision's sector table,
+    and pinned host buffers for the one read-back of a truncation."""
+
+    def __init__(self, m: TensorStructure) -> None:
+        from tenet import _lib
+
+        ml = matrix_layout(m)
+        p = m.provider
+        self.ml = ml
+        self.sectors = tuple(sorted(ml.sectors))
+        smem_max = int(_lib.load().tnb_block_svd_smem_doubles())
+        rows, sec_rows, qd = [], [], []
+        self.kfull = {}
+        uo = so = vo = wo = 0
+        smem = 0
+        for c in self.sectors:
+            r, q = ml.shape[c]
+            k = min(r, q)
+            need = max(r, q) * k + k * k + 2 * k
+            if need <= smem_max:
+                w = -1
+                smem = max(smem, need)
+            else:
+                w = wo
+                wo += need
+            rows.append((r, q, ml.base[c], uo, so, vo, w, 0))
+            sec_rows.append((k, so, c, 0))
+            qd.append(float(p._qdim(c)))
+            self.kfull[c] = (k, uo, so, vo)
+            uo, so, vo = uo + r * k, so + k, vo + k * q
+        self.n_u, self.n_s, self.n_v, self.n_w, self.smem = uo, so, vo, wo, smem
+        self.total = so
+        dev = _exec.device()
+        i64 = dict(dtype=torch.int64, device=dev)
+        self.rows = torch.tensor(rows or [(0,) * 8], **i64)
+        self.sec_rows = torch.tensor(sec_rows or [(0,) * 4], **i64)
+        self.qdim = torch.tensor(qd or [1.0], dtype=torch.float64, device=dev)
+        n = max(1, len(self.sectors))
+        self.keep = torch.zeros(n, **i64)
+        self.info = torch.zeros(n, dtype=torch.int32, device=dev)
+        self.stats = torch.zeros(8, dtype=torch.float64, device=dev)
+        self.h_keep = torch.zeros(n, dtype=torch.int64).pin_memory()
+        self.h_info = torch.zeros(n, dtype=torch.int32).pin_memory()
+        self.h_stats = torch.zeros(8, dtype=torch.float64).pin_memory()
+
+
+@cache
+def _svd_plan(m: TensorStructure) -> _SvdPlan:
+    return _SvdPlan(m)
+
+
+_MODES = {"abs": 0, "rel": 1, "sum2": 2, "rsum2": 3, "sum1": 4, "rsum1": 5}
+
+
 def svd_truncated(t: SymmetricTensor, axes=None, *, max_bond=None, cutoff=None,
                   cutoff_mode: str = "rsum2", renorm: bool = False, budget: str = "dense"):
     """``U, S, Vh`` on the truncated bond.  Same legs, keep rule and refusals as the
-    reference; returns ``(U, S, Vh)``.  ``budget`` as in ``decide``."""
+    reference; returns ``(U, S, Vh)``.  ``budget`` as in ``decide``.
+
+    All on the device: the lowering gather, one blockwise SVD launch (a CTA per coupled
+    sector), the decision launch (global order, cutoff prefix, budget walk), one read-back
+    of the decision, and one launch that packs the kept prefixes before the three raising
+    gathers."""
+    return svd_truncated_selected(t, axes, max_bond=max_bond, cutoff=cutoff,
+                                  cutoff_mode=cutoff_mode, renorm=renorm, budget=budget)[:3]
+
+
+def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cutoff=None,
+                           cutoff_mode: str = "rsum2", renorm: bool = False,
+                           budget: str = "dense"):
+    """``svd_truncated`` plus what its decision read back: ``(U, S, Vh, selection,
+    kept)``, ``selection`` the ``BondSelection`` and ``kept`` the kept singular values in
+    the global order as ``(sigma * scale, sector label)`` pairs."""
+    from tenet import _lib
+
     if budget not in ("dense", "reduced"):
         raise ValueError(f"unknown budget {budget!r}")
     if max_bond is None and cutoff is None:
@@ -121,47 +194,72 @@ def svd_truncated(t: SymmetricTensor, axes=None, *, max_bond=None, cutoff=None,
         axes = (t.structure.out_axes, t.structure.in_axes)
     outputs, inputs = validate_partition(t.ndim, axes[0], axes[1])
     m, lower = _lower_exec(t.structure, outputs, inputs)
-    ml = matrix_layout(m)
-    buf = torch.empty(ml.size, dtype=torch.float64, device=t.arena.device)
+    plan = _svd_plan(m)
+    if plan.total == 0:
+        raise ValueError("svd_truncated: this tensor has no singular values at all")
+    ml = plan.ml
+    dev = t.arena.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    buf = torch.empty(max(1, ml.size), **f64)
     lower.run(t.arena, buf)
-
-    # factorise: batch sectors of equal shape into one cuSOLVER call
-    by_shape: dict = {}
-    for c in ml.sectors:
-        by_shape.setdefault(ml.shape[c], []).append(c)
-    parts = {}
-    for (r, q), cs in by_shape.items():
-        stack = torch.stack([buf[ml.base[c]:ml.base[c] + r * q].view(r, q) for c in cs])
-        u, s, vh = torch.linalg.svd(stack, full_matrices=False)
-        for i, c in enumerate(cs):
-            parts[c] = (u[i], s[i], vh[i])
-
-    # the decision on the host, bit-exact to the reference's keep rule
-    host_s = {c: parts[c][1].cpu().numpy() for c in ml.sectors}
-    spectrum = [(float(sg), c, i) for c in ml.sectors for i, sg in enumerate(host_s[c])]
-    spectrum.sort(key=lambda e: (-e[0], e[1], e[2]))
+    U = torch.empty(max(1, plan.n_u), **f64)
+    Sv = torch.empty(max(1, plan.n_s), **f64)
+    V = torch.empty(max(1, plan.n_v), **f64)
+    W = torch.empty(max(1, plan.n_w), **f64)
+    sorted_s = torch.empty(plan.total, **f64)
+    sorted_c = torch.empty(plan.total, dtype=torch.int32, device=dev)
+    P, st = _exec.ptr, _exec.stream_ptr()
+    ns = len(plan.sectors)
+    _lib.call("tnb_block_svd", P(plan.rows), ns, P(buf), buf.numel(), P(U), U.numel(), P(Sv),
+              Sv.numel(), P(V), V.numel(), P(W), plan.n_w, P(plan.info), plan.smem, st)
+    _lib.call("tnb_truncate_decide", P(plan.sec_rows), P(plan.qdim), ns, P(Sv), Sv.numel(),
+              -1.0 if cutoff is None else float(cutoff), _MODES[cutoff_mode],
+              -1.0 if max_bond is None else float(max_bond), 0 if budget == "dense" else 1,
+              P(plan.keep), P(sorted_s), P(sorted_c), P(plan.stats), st)
+    plan.h_keep.copy_(plan.keep, non_blocking=True)
+    plan.h_info.copy_(plan.info, non_blocking=True)
+    plan.h_stats.copy_(plan.stats, non_blocking=True)
+    h_s = torch.empty(plan.total, dtype=torch.float64, pin_memory=True)
+    h_c = torch.empty(plan.total, dtype=torch.int32, pin_memory=True)
+    h_s.copy_(sorted_s, non_blocking=True)
+    h_c.copy_(sorted_c, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    info = plan.h_info.numpy()[:ns]
+    if np.any(info != 0):
+        raise RuntimeError(f"svd_truncated: the blockwise SVD did not converge (info "
+                           f"{info.tolist()})")
+    keep_h = plan.h_keep.numpy()[:ns]
+    n_kept, dense, disc, total, kept_w = (float(x) for x in plan.h_stats.numpy()[:5])
+    if n_kept == 0:
+        raise ValueError("svd_truncated: the truncation keeps no singular value at all")
+    keep = {c: int(k) for c, k in zip(plan.sectors, keep_h) if k > 0}
+    scale = (total / kept_w) ** 0.5 if renorm else 1.0
     p = t.provider
-    sel = decide(spectrum, p, max_bond, cutoff, cutoff_mode, renorm, budget)
-    bond = GradedSpace.new(p, {p.sector(c): k for c, k in sel.keep.items()})
+    sel = BondSelection(keep, dense, int(n_kept), disc, scale)
+    nk = int(n_kept)
+    kept = [(float(x) * scale, plan.sectors[int(k)])
+            for x, k in zip(h_s.numpy()[:nk], h_c.numpy()[:nk])]
+    bond = GradedSpace.new(p, {p.sector(c): k for c, k in keep.items()})
     su = TensorStructure((*m.codomain, Leg(bond, IN)))
     ss = TensorStructure((Leg(bond, OUT), Leg(bond, IN)))
     sv = TensorStructure((Leg(bond, OUT), *m.domain))
-    dev = t.arena.device
-
-    def assemble(structure, piece):
-        lay = matrix_layout(structure)
-        mbuf = torch.empty(lay.size, dtype=torch.float64, device=dev)
-        for c in lay.sectors:
-            r, q = lay.shape[c]
-            mbuf[lay.base[c]:lay.base[c] + r * q].view(r, q).copy_(piece(c))
-        out = SymmetricTensor.empty(structure)
-        _raise_exec(structure).run(mbuf, out.arena)
-        return out
-
-    U = assemble(su, lambda c: parts[c][0][:, :sel.keep[c]])
-    S = assemble(ss, lambda c: torch.diag(parts[c][1][:sel.keep[c]] * sel.scale))
-    V = assemble(sv, lambda c: parts[c][2][:sel.keep[c], :])
-    return U, S, V
+    lu, ls, lv = matrix_layout(su), matrix_layout(ss), matrix_layout(sv)
+    rows = []
+    for c, k in keep.items():
+        kf, uo, so, vo = plan.kfull[c]
+        r, q = ml.shape[c]
+        rows.append((r, q, kf, k, uo, so, vo, lu.base[c], ls.base[c], lv.base[c], 0, 0))
+    PU, PS, PV = (torch.empty(max(1, x.size), **f64) for x in (lu, ls, lv))
+    crows = torch.tensor(rows, dtype=torch.int64).pin_memory().to(dev, non_blocking=True)
+    _lib.call("tnb_svd_compact", P(crows), len(rows), P(U), U.numel(), P(Sv), Sv.numel(), P(V),
+              V.numel(), float(scale), P(PU), PU.numel(), P(PS), PS.numel(), P(PV), PV.numel(),
+              st)
+    out = []
+    for structure, packed in ((su, PU), (ss, PS), (sv, PV)):
+        o = SymmetricTensor.empty(structure)
+        _raise_exec(structure).run(packed, o.arena)
+        out.append(o)
+    return (*out, sel, kept)
 
 
 def singular_values(s: SymmetricTensor) -> dict:

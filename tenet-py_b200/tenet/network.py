@@ -883,10 +883,15 @@ def sweep_steps(psi: MPS, h: MPO, env: Env, schmidt: dict | None = None, *, chi:
                     r = SymmetricTensor.random(aa.legs, seed=seed + n)
                     aa = ops.add(aa, r * float(noise * ops.norm(aa) / ops.norm(r)))
                     aa = aa / ops.norm(aa)
-                u, s, vh = linalg.svd_truncated(aa, ((0, 1), (2, 3)), max_bond=chi,
-                                                cutoff=cutoff, budget=budget)
-                norm_s = ops.norm(s)
-                max_dw = max(max_dw, 1.0 - float(norm_s / ops.norm(aa)) ** 2)
+                u, s, vh, sel, kept = linalg.svd_truncated_selected(
+                    aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff, budget=budget)
+                # Pythagoras from the decision's read-back: |S|^2 is the kept qdim-weighted
+                # sum of sigma^2 and |aa|^2 the whole one (the reference takes both norms
+                # numerically, network/dmrg.py:514-517)
+                qd = aa.provider._qdim
+                norm_s = sum(qd(c) * x * x for x, c in kept) ** 0.5
+                norm_aa = (sel.discarded_weight + norm_s * norm_s) ** 0.5
+                max_dw = max(max_dw, 1.0 - float(norm_s / norm_aa) ** 2)
                 s = s / norm_s
                 psi[n + 1] = vh
                 if forward:
@@ -895,7 +900,8 @@ def sweep_steps(psi: MPS, h: MPO, env: Env, schmidt: dict | None = None, *, chi:
                 else:
                     psi[n] = ops.einsum("apx,xy->apy", u, s)
                 if schmidt is not None:
-                    schmidt[n] = spectrum(s)
+                    schmidt[n] = sorted((x * qd(c) ** 0.5 / norm_s for x, c in kept),
+                                        reverse=True)
             psi.center = n + 1 if forward else n
             for e in (env, *orthogonal_to):
                 e.clear_(n, n + 1)

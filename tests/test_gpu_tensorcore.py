@@ -59,19 +59,27 @@ def test_tensorcore_gemm_kinds(kind):
 @pytest.mark.parametrize("precision,tol,tc_min", [("3xbf16", 1e-4, None), ("tf32", 1e-2, None),
                                                   ("3xbf16", 1e-4, 0), ("tf32", 1e-2, 0)])
 def test_mixed_precision_heff2_chain(precision, tol, tc_min):
-    """The bench's SU(2) matvec with its big sector products (or, with ``tc_min`` 0, all
-    of them) on the tensor cores."""
+    """The bench's large-bond SU(2) matvec (256 multiplets) with its big sector products
+    (or, with ``tc_min`` 0, all of them) on the tensor cores, in the reference's order and
+    in the folded form."""
     import bench
-    from tenet.program import heff2_program
+    from tenet import network
+    from tenet.program import heff2_folded_program, heff2_program
 
-    tensors = bench.build_workload()
+    tensors = bench.build_workload(bond=bench.WORKLOADS["synthetic_256_multiplets"])
+    fl, w1, w2, fr, aa = tensors
+    lf, rf = network.fold_left(fl, w1), network.fold_right(w2, fr)
+    folded = heff2_folded_program(lf, rf, aa.structure, precision=precision,
+                                  tc_min_flops=tc_min)
+    assert folded.uses_tensor_cores
     exact = heff2_program(*tensors[:4], tensors[4].structure)(tensors[4]).numpy_arena()
     prog = heff2_program(*tensors[:4], tensors[4].structure, precision=precision,
                          tc_min_flops=tc_min)
     assert prog.uses_tensor_cores
-    got = prog(tensors[4]).numpy_arena()
-    err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
-    assert err < tol, f"{precision}: relative error {err:.2e}"
+    for p in (prog, folded):
+        got = p(tensors[4]).numpy_arena()
+        err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
+        assert err < tol, f"{precision}: relative error {err:.2e}"
 
 
 @pytest.mark.parametrize("precision", ["3xbf16"])
