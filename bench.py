@@ -782,6 +782,8 @@ def run_tenet(args) -> None:
         for _ in range(args.warmup):
             fn()
         forms_ms[name] = timed(fn, args.steps) / args.steps
+    from tenet import program as _program
+
     lib = _lib.load()
     lib.tnb_set_pdl(0)
     gm_plain = GraphMatvec(prog)
@@ -789,7 +791,17 @@ def run_tenet(args) -> None:
     _exec.FUSE = True
     gm_fused = GraphMatvec(prog)
     _exec.FUSE = False
-    for name, g in (("graph_without_pdl", gm_plain), ("graph_fused_one_launch", gm_fused)):
+    # the same chain planned for one launch on one thread-block cluster (off by default)
+    _exec.CLUSTER = True
+    _program._HEFF_TABLES.clear()
+    prog_cl = heff2_folded_program(lf, rf, aa.structure)
+    gm_cluster = GraphMatvec(prog_cl) if prog_cl.cluster is not None else None
+    _exec.CLUSTER = False
+    _program._HEFF_TABLES.clear()
+    for name, g in (("graph_without_pdl", gm_plain), ("graph_grid_fused_one_launch", gm_fused),
+                    ("graph_cluster_one_launch", gm_cluster)):
+        if g is None:
+            continue
         for _ in range(args.warmup):
             g.replay()
         forms_ms[name] = timed(g.replay, args.steps) / args.steps
@@ -861,7 +873,27 @@ def run_tenet(args) -> None:
         with log:
             prog.run(gm.x, gm.y)
     kernels = log.summary()
-    log.count = args.steps * launches_per_step
+    # the one-cluster launch alone, timed the same way (head start, events on the stream)
+    cluster_ms = None
+    if prog.cluster is not None:
+        evs = []
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda._sleep(2_000_000)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            prog.run(gm.x, gm.y)
+            b.record()
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        cluster_ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    # algorithmic bytes of one matvec: every gather's source terms and destination, every
+    # product's A, B and C (FP64)
+    gemm_bytes = 8 * sum(int(M) * int(K) + int(K) * int(N) + int(M) * int(N)
+                         for lk in prog.links for part in lk.gemm.parts
+                         for M, N, K in (r[:3] for r in part.table))
+    gather_bytes = kernels.get("block_gather", {"work": 0})["work"] / args.steps
+    matvec_bytes = gemm_bytes + gather_bytes
 
     # end to end through the public API with host buffers: every step copies the input
     # from pinned host memory, runs the chain and copies the result back, all three in
@@ -891,7 +923,7 @@ def run_tenet(args) -> None:
         total_kernel_ms = g["ms"] + gt["ms"]
         gemm_tflops = g["work"] / (g["ms"] * 1e-3) / 1e12 if g["ms"] else 0.0
         gather_gbs = gt["work"] / (gt["ms"] * 1e-3) / 1e9 if gt["ms"] else 0.0
-        dominant_is_gemm = g["ms"] >= gt["ms"]
+        dominant_is_gemm = g["ms"] >= gt["ms"] and cluster_ms is None
         key = "grouped_gemm_f64" if dominant_is_gemm else "block_gather"
         roofline = {
             "bound": "tensor" if dominant_is_gemm else "hbm",
@@ -918,6 +950,17 @@ def run_tenet(args) -> None:
             "kernel_ms_per_step": total_kernel_ms / args.steps,
             "graph_ms_per_step": ms / args.steps,
         }
+        if cluster_ms is not None:
+            # the whole matvec is one kernel: its algorithmic bytes over its duration
+            roofline.update({
+                "bound": "hbm", "kernel": "chain_cluster_kernel",
+                "achieved": matvec_bytes / (cluster_ms * 1e-3) / 1e9, "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({pk['src']})",
+                "traffic": NCU_TRAFFIC.get("chain_cluster_kernel"),
+                "algorithmic_bytes_per_launch": matvec_bytes,
+                "kernel_ms_per_launch": cluster_ms,
+                "cluster_ctas": prog.cluster_ctas,
+                "note": "the kernels entry times the same stages launched one by one"})
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
         solve = dmrg_solve(args) if args.dmrg else None

@@ -333,6 +333,19 @@ int tnb_seq_append(tnb_seq* dst, const tnb_seq* src);
  */
 int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* y_slot, void* barrier,
                  tnb_seq* dst);
+
+/*
+ * The stages of `src` as one launch on a single thread-block cluster of up to `max_ctas`
+ * (1..16) CTAs, the stages separated by the cluster's hardware barrier, appended to `dst`
+ * as one op (*ctas = the cluster size used: the largest power of two <= max_ctas that
+ * the device can make resident).  For chains whose stages each have a few dozen work
+ * items -- a two-site matvec at a small bond -- where a launch per stage or a grid-wide
+ * barrier costs more than the stage.  No counterpart in the reference (its matvec is a
+ * Python loop of per-block calls); the stages are the same tables as the op-by-op
+ * sequence, so the results are bit-identical.
+ */
+int tnb_seq_fuse_cluster(const tnb_seq* src, const void* x_slot, const void* y_slot,
+                         int32_t max_ctas, int32_t* ctas, tnb_seq* dst);
 int tnb_seq_run(const tnb_seq* s, int32_t n_patch, const void* const* from, void* const* to,
                 void* stream);
 

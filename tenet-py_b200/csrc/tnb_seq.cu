@@ -32,6 +32,7 @@ constexpr int32_t kOpGather = 1;
 constexpr int32_t kOpGemm = 2;
 constexpr int32_t kOpFused = 3;
 constexpr int32_t kOpGatherProduct = 4;
+constexpr int32_t kOpCluster = 5;
 
 struct FStage {
   int32_t code;
@@ -96,8 +97,10 @@ __device__ __forceinline__ double* slot(int64_t w, const double* x, double* y) {
                      : w == kSlotY ? y : reinterpret_cast<double*>(static_cast<intptr_t>(w));
 }
 
-__global__ void __launch_bounds__(kFusedThreads, 1)
-chain_kernel(const FChain ch, const double* x, double* y, unsigned int* bar) {
+// Every stage of a chain in order, `sync()` between stages (false: give up).
+template <class Sync>
+__device__ __forceinline__ void run_chain(const FChain& ch, const double* x, double* y,
+                                          Sync sync) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FusedSmem& sm = *reinterpret_cast<FusedSmem*>(smem_raw);
   const int grp = threadIdx.x / kGroupThreads, gtid = threadIdx.x % kGroupThreads;
@@ -136,8 +139,39 @@ chain_kernel(const FChain ch, const double* x, double* y, unsigned int* bar) {
           skinny_tile<kFusedThreads, true>(g, it, sm.skinny, threadIdx.x, CtaSync{});
       }
     }
-    if (s + 1 < ch.n && !grid_barrier(bar)) return;
+    if (s + 1 < ch.n && !sync()) return;
   }
+}
+
+struct GridStageSync {
+  unsigned int* bar;
+  __device__ __forceinline__ bool operator()() const { return grid_barrier(bar); }
+};
+
+struct ClusterStageSync {
+  __device__ __forceinline__ bool operator()() const {
+    __threadfence();
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+                 "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+    return true;
+  }
+};
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+chain_kernel(const __grid_constant__ FChain ch, const double* x, double* y, unsigned int* bar) {
+  run_chain(ch, x, y, GridStageSync{bar});
+}
+
+// The same chain on the CTAs of one thread-block cluster, the stages separated by the
+// cluster's hardware barrier: for chains whose every stage has only a few dozen work
+// items (a matvec at a small bond), where a grid-wide barrier or a launch per stage costs
+// more than the stage.  The fence orders this CTA's global writes before the arrival;
+// the barrier's release / acquire semantics at cluster scope make them visible to the
+// other CTAs, which read them through L2.  Every CTA passes every barrier (no CTA leaves
+// the loop early), so the barrier cannot wait on an exited CTA.
+__global__ void __launch_bounds__(kFusedThreads, 1)
+chain_cluster_kernel(const __grid_constant__ FChain ch, const double* x, double* y) {
+  run_chain(ch, x, y, ClusterStageSync{});
 }
 
 // CTAs of one cooperative chain launch on `device`: as many as can be resident (0 when
@@ -251,6 +285,36 @@ int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* con
           rc = check_launch("tnb_seq_run: fused chain");
         }
       }
+    } else if (op.code == kOpCluster) {
+      // w[0] chain index, w[1] input, w[2] output, w[4] cluster size (the whole grid)
+      w[1] = patched(w[1], n_patch, from, to);
+      w[2] = patched(w[2], n_patch, from, to);
+      if (w[0] < 0 || w[0] >= static_cast<int64_t>(s->chains.size()) || w[4] < 1 || w[4] > 16) {
+        set_error("tnb_seq_run: corrupt cluster op");
+        rc = TNB_EINVAL;
+      } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(static_cast<unsigned>(w[4]));
+        cfg.blockDim = dim3(kFusedThreads);
+        cfg.dynamicSmemBytes = sizeof(FusedSmem);
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = static_cast<unsigned>(w[4]);
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(
+            &cfg, chain_cluster_kernel, s->chains[static_cast<size_t>(w[0])],
+            static_cast<const double*>(as_ptr(w[1])), static_cast<double*>(as_ptr(w[2])));
+        if (e != cudaSuccess) {
+          set_error(std::string("tnb_seq_run: cluster chain launch: ") + cudaGetErrorString(e));
+          rc = TNB_ECUDA;
+        } else {
+          rc = check_launch("tnb_seq_run: cluster chain");
+        }
+      }
     } else {
       set_error("tnb_seq_run: corrupt sequence");
     }
@@ -336,45 +400,98 @@ extern "C" int tnb_seq_append(tnb_seq* dst, const tnb_seq* src) {
   const int64_t base = static_cast<int64_t>(dst->chains.size());
   dst->chains.insert(dst->chains.end(), src->chains.begin(), src->chains.end());
   for (auto op : src->ops) {
-    if (op.code == tnb::kOpFused) op.w[0] += base;  // the copied chain's new index
+    if (op.code == tnb::kOpFused || op.code == tnb::kOpCluster)
+      op.w[0] += base;  // the copied chain's new index
     dst->ops.push_back(op);
   }
   return TNB_OK;
 }
+
+namespace tnb {
+// The stages of `src` as a chain for the one-launch kernels; the slots' words become
+// kSlotX / kSlotY so a replay can patch them.
+static int build_chain(const tnb_seq* src, int64_t xw, int64_t yw, FChain& ch, const char* who) {
+  if (src->ops.empty() || src->ops.size() > static_cast<size_t>(kMaxStages)) {
+    set_error(std::string(who) + ": empty sequence or more stages than one launch holds");
+    return TNB_EINVAL;
+  }
+  ch = FChain{};
+  ch.n = static_cast<int32_t>(src->ops.size());
+  for (size_t i = 0; i < src->ops.size(); ++i) {
+    const auto& op = src->ops[i];
+    FStage& st = ch.st[i];
+    if (op.code != kOpGather && op.code != kOpGemm) {
+      set_error(std::string(who) + ": only gathers and grouped GEMMs fuse (not product-source "
+                "gathers or fused ops)");
+      return TNB_EINVAL;
+    }
+    std::memcpy(st.w, op.w, sizeof(st.w));
+    st.code = op.code;
+    if (op.code == kOpGather) {
+      st.kind = 0;
+      st.items = op.w[3];  // chunks
+      for (int k : kGatherBufs) st.w[k] = st.w[k] == xw ? kSlotX : st.w[k] == yw ? kSlotY : st.w[k];
+    } else {
+      st.kind = static_cast<int32_t>(op.w[4]);
+      if (st.kind != TNB_TILE_64 && st.kind != TNB_TILE_32 && st.kind != TNB_TILE_SKINNY) {
+        set_error(std::string(who) + ": only 64, 32 and skinny GEMM stages fuse");
+        return TNB_EINVAL;
+      }
+      st.items = op.w[3];  // tiles (a 32 x 32 tile goes to one of four groups of a CTA)
+      for (int k : kGemmBufs) st.w[k] = st.w[k] == xw ? kSlotX : st.w[k] == yw ? kSlotY : st.w[k];
+    }
+  }
+  return TNB_OK;
+}
+
+// Largest cluster (16, 8, 4, 2 or 1 CTAs, at most `want`) of the cluster chain kernel
+// that can be resident on the current device (0 if none); computed once per device.
+static int cluster_size_for(int want) {
+  static PerDeviceInt cached;
+  const int best = cached.get([](int, int* v) {
+    cudaError_t e = cudaFuncSetAttribute(chain_cluster_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(sizeof(FusedSmem)));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(chain_cluster_kernel,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    *v = 0;
+    for (int c = 16; c >= 1 && *v == 0; c >>= 1) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(c);
+      cfg.blockDim = dim3(kFusedThreads);
+      cfg.dynamicSmemBytes = sizeof(FusedSmem);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = c;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, chain_cluster_kernel, &cfg) == cudaSuccess &&
+          clusters > 0)
+        *v = c;
+      else
+        cudaGetLastError();
+    }
+    return *v > 0 ? cudaSuccess : cudaErrorInvalidConfiguration;
+  });
+  int c = best;
+  while (c > want) c >>= 1;
+  return c;
+}
+}  // namespace tnb
 
 extern "C" int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* y_slot,
                             void* barrier, tnb_seq* dst) {
   TNB_REQUIRE(src != nullptr && dst != nullptr && src != dst, "tnb_seq_fuse: bad sequences");
   TNB_REQUIRE(x_slot != nullptr && y_slot != nullptr && barrier != nullptr,
               "tnb_seq_fuse: null slot or barrier");
-  TNB_REQUIRE(!src->ops.empty(), "tnb_seq_fuse: empty sequence");
-  TNB_REQUIRE(src->ops.size() <= static_cast<size_t>(tnb::kMaxStages),
-              "tnb_seq_fuse: more stages than one fused launch holds");
-  tnb::FChain ch{};
-  ch.n = static_cast<int32_t>(src->ops.size());
   const int64_t xw = tnb::as_word(x_slot), yw = tnb::as_word(y_slot);
-  for (size_t i = 0; i < src->ops.size(); ++i) {
-    const auto& op = src->ops[i];
-    tnb::FStage& st = ch.st[i];
-    TNB_REQUIRE(op.code == tnb::kOpGather || op.code == tnb::kOpGemm,
-                "tnb_seq_fuse: only gathers and grouped GEMMs fuse (not product-source "
-                "gathers or fused ops)");
-    std::memcpy(st.w, op.w, sizeof(st.w));
-    st.code = op.code;
-    if (op.code == tnb::kOpGather) {
-      st.kind = 0;
-      st.items = op.w[3];  // chunks
-      for (int k : tnb::kGatherBufs)
-        st.w[k] = st.w[k] == xw ? tnb::kSlotX : st.w[k] == yw ? tnb::kSlotY : st.w[k];
-    } else {
-      st.kind = static_cast<int32_t>(op.w[4]);
-      TNB_REQUIRE(st.kind == TNB_TILE_64 || st.kind == TNB_TILE_32 || st.kind == TNB_TILE_SKINNY,
-                  "tnb_seq_fuse: only 64, 32 and skinny GEMM stages fuse");
-      st.items = op.w[3];  // tiles (a 32 x 32 tile goes to one of four groups of a CTA)
-      for (int k : tnb::kGemmBufs)
-        st.w[k] = st.w[k] == xw ? tnb::kSlotX : st.w[k] == yw ? tnb::kSlotY : st.w[k];
-    }
-  }
+  tnb::FChain ch;
+  if (int rc = tnb::build_chain(src, xw, yw, ch, "tnb_seq_fuse")) return rc;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) {
     tnb::set_error("tnb_seq_fuse: no current device");
@@ -389,6 +506,29 @@ extern "C" int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* 
   tnb_seq::Op op{tnb::kOpFused,
                  {static_cast<int64_t>(dst->chains.size() - 1), xw, yw, tnb::as_word(barrier),
                   grid, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+  dst->ops.push_back(op);
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_fuse_cluster(const tnb_seq* src, const void* x_slot, const void* y_slot,
+                                    int32_t max_ctas, int32_t* ctas, tnb_seq* dst) {
+  TNB_REQUIRE(src != nullptr && dst != nullptr && src != dst,
+              "tnb_seq_fuse_cluster: bad sequences");
+  TNB_REQUIRE(x_slot != nullptr && y_slot != nullptr, "tnb_seq_fuse_cluster: null slot");
+  TNB_REQUIRE(max_ctas >= 1 && max_ctas <= 16, "tnb_seq_fuse_cluster: max_ctas must be 1..16");
+  const int64_t xw = tnb::as_word(x_slot), yw = tnb::as_word(y_slot);
+  tnb::FChain ch;
+  if (int rc = tnb::build_chain(src, xw, yw, ch, "tnb_seq_fuse_cluster")) return rc;
+  const int c = tnb::cluster_size_for(max_ctas);
+  if (c <= 0) {
+    tnb::set_error("tnb_seq_fuse_cluster: no cluster of the chain kernel can be resident");
+    return TNB_ECUDA;
+  }
+  if (ctas) *ctas = c;
+  dst->chains.push_back(ch);
+  tnb_seq::Op op{tnb::kOpCluster,
+                 {static_cast<int64_t>(dst->chains.size() - 1), xw, yw, 0, c, 0, 0, 0, 0, 0,
+                  0, 0, 0, 0, 0, 0}};
   dst->ops.push_back(op);
   return TNB_OK;
 }

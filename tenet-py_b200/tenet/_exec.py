@@ -108,6 +108,15 @@ def recording() -> Seq | None:
 #: CTA per SM, which starves its latency-bound gather stages.  The fused launch gives
 #: bit-identical results and stays available for comparison.
 FUSE = False
+#: plan a small chain (every stage at most ``CLUSTER_MAX_ITEMS`` work items) to run as one
+#: launch on a single thread-block cluster (``tnb_seq_fuse_cluster``).  Off by default:
+#: bit-identical, but measured slower than the graph of stage launches on B200 (43 against
+#: 22.5 us for the L = 64 mid-bond matvec: each stage's table loads sit on its critical
+#: path after every barrier, where the stage launches overlap them with the previous
+#: kernel through programmatic dependent launch)
+CLUSTER = False
+CLUSTER_MAX_ITEMS = 48
+CLUSTER_CTAS = 16
 
 
 
@@ -762,7 +771,7 @@ class GemmGroup:
     instead of the size heuristic."""
 
     def __init__(self, products, precision: str = "f64", tc_min_flops: int | None = None,
-                 tuned: bool = False):
+                 tuned: bool = False, split_k: bool = True):
         bulk, cols = thin_rows(products), wide_cols(products)
         skinny = [p for p in products if _is_skinny(p, bulk)]
         wide = [p for p in products if not _is_skinny(p, bulk) and _is_wide(p, cols)]
@@ -779,7 +788,7 @@ class GemmGroup:
                 kind, split = autotune(rest)
                 self.parts.append(make_gemm(rest, kind, split_k=split))
             else:
-                self.parts.append(make_gemm(rest, choose_kind(rest)))
+                self.parts.append(make_gemm(rest, choose_kind(rest), split_k=split_k))
         if skinny:
             self.parts.append(make_gemm(skinny, TILE_SKINNY))
         if wide:

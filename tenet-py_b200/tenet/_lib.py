@@ -49,6 +49,7 @@ SIGNATURES = {
                                 _i64, _vp, _i64, _i64]),
     "tnb_seq_append": (_i32, [_vp, _vp]),
     "tnb_seq_fuse": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "tnb_seq_fuse_cluster": (_i32, [_vp, _vp, _vp, _i32, ctypes.POINTER(_i32), _vp]),
     "tnb_seq_run": (_i32, [_vp, _i32, _vp, _vp, _vp]),
     "tnb_lanczos_solve": (_i32, [_vp, _vp, _vp, _i64, _i32, _f64, _i32, _vp, _vp, _i64, _vp,
                                  _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),

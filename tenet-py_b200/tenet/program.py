@@ -227,9 +227,33 @@ class ChainProgram:
             _exec.gather_rows(self.src[0], self.src[1], dst, "arena", perm, terms))
         if self.defer:
             self._defer_skinny()
+        self.compact = self._compact()
         if allocate:
             self.allocate()
         return self
+
+    def _compact(self) -> bool:
+        """Whether every stage has at most ``_exec.CLUSTER_MAX_ITEMS`` work items (gather
+        chunks, GEMM tiles per CTA-sized item) once split-K is off: such a chain runs as one
+        launch on one thread-block cluster.  Its GEMM tables are then rebuilt without
+        split-K, which only pays across many SMs."""
+        if not _exec.CLUSTER or self.uses_tensor_cores or any(lk.deferred for lk in self.links):
+            return False
+        groups = [_exec.GemmGroup(lk.gemm.products, self.precision, self.tc_min_flops,
+                                  split_k=False) for lk in self.links]
+        items = [self.out_gather.chunks]
+        for lk, gg in zip(self.links, groups):
+            if lk.a_gather is not None:
+                items.append(lk.a_gather.chunks)
+            for part in gg.parts:
+                if part.kind not in (_exec.TILE_64, _exec.TILE_32, _exec.TILE_SKINNY):
+                    return False
+                items.append(-(-part.tiles // 4) if part.kind == _exec.TILE_32 else part.tiles)
+        if max(items) > _exec.CLUSTER_MAX_ITEMS:
+            return False
+        for lk, gg in zip(self.links, groups):
+            lk.gemm = gg
+        return True
 
     def _consumer(self, i: int):
         """The gather that reads link ``i``'s product, or None (a GEMM reads it)."""
@@ -305,6 +329,18 @@ class ChainProgram:
             self._run_tables(self.x_slot, self.y_slot)
         # the same stages as one persistent launch, when they all fuse (no tensor-core
         # stage, no product-source gather, at most the kernel's stage count)
+        self.cluster = None
+        if getattr(self, "compact", False) and _exec.CLUSTER and \
+                0 < len(self.seq) <= FUSED_MAX_STAGES:
+            import ctypes
+
+            from tenet import _lib
+
+            cl, ctas = _exec.Seq(), ctypes.c_int32(0)
+            _lib.call("tnb_seq_fuse_cluster", self.seq.handle, self.x_slot.data_ptr(),
+                      self.y_slot.data_ptr(), _exec.CLUSTER_CTAS, ctypes.byref(ctas),
+                      cl.handle)
+            self.cluster, self.cluster_ctas = cl, ctas.value
         self.fused = None
         if (not self.uses_tensor_cores and not any(lk.deferred for lk in self.links)
                 and 0 < len(self.seq) <= FUSED_MAX_STAGES):
@@ -319,8 +355,11 @@ class ChainProgram:
 
     @property
     def exec_seq(self) -> _exec.Seq:
-        """The sequence a replay runs: the fused launch when there is one (and fusing is
-        on), else the stage-by-stage sequence."""
+        """The sequence a replay runs: the one-cluster launch of a compact chain (when
+        ``_exec.CLUSTER``), the grid-wide fused launch (when ``_exec.FUSE``), else the
+        stage-by-stage sequence."""
+        if self.cluster is not None and _exec.CLUSTER:
+            return self.cluster
         return self.fused if (self.fused is not None and _exec.FUSE) else self.seq
 
     def refresh(self) -> None:
@@ -335,6 +374,8 @@ class ChainProgram:
 
     @property
     def launches(self) -> int:
+        if getattr(self, "cluster", None) is not None and _exec.CLUSTER:
+            return 1
         return sum((0 if lk.deferred else lk.gemm.launches) + (not lk.a_direct)
                    for lk in self.links) + 1
 

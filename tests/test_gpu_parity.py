@@ -335,6 +335,61 @@ def test_folded_heff2_matches_golden_and_site_order(golden_dir):
     close(GraphMatvec(folded)(aa), site)
 
 
+def test_cluster_chain_is_bit_identical_to_stage_by_stage(golden_dir):
+    """A compact chain (every stage a few dozen items) runs as one launch on one
+    thread-block cluster: the same tables and arithmetic as the stage-by-stage replay,
+    identical bits, repeatedly, through a captured graph and in a device Lanczos solve."""
+    import bench
+    from tenet import _exec
+    from tenet.program import GraphMatvec, heff2_folded_program, heff2_program
+
+    from tenet import program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    fl, w1, w2, fr, aa = bench.build_workload()
+    _exec.CLUSTER = True  # planned for the cluster launch (off by default)
+    program._HEFF_TABLES.clear()
+    try:
+        cases = [(heff2_folded_program(network.fold_left(fl, w1), network.fold_right(w2, fr),
+                                       aa.structure), aa),
+                 (heff2_program(fl, w1, w2, fr, aa.structure), aa),
+                 (heff2_folded_program(network.fold_left(T["fl"], T["w1"]),
+                                       network.fold_right(T["w2"], T["fr"]),
+                                       T["aa"].structure), T["aa"])]
+        _check_cluster_cases(cases)
+    finally:
+        _exec.CLUSTER = False
+        program._HEFF_TABLES.clear()
+    close(GraphMatvec(cases[2][0])(T["aa"]), h[m["heff_aa"]["arena"]])
+
+
+def _check_cluster_cases(cases):
+    from tenet import _exec
+    from tenet.program import GraphMatvec
+
+    for prog, x in cases:
+        assert prog.compact and prog.cluster is not None and prog.launches == 1
+        try:
+            _exec.CLUSTER = False
+            want = GraphMatvec(prog)(x).numpy_arena()
+        finally:
+            _exec.CLUSTER = True
+        g = GraphMatvec(prog)
+        for _ in range(3):
+            assert np.array_equal(g(x).numpy_arena(), want)
+        assert np.array_equal(prog(x).numpy_arena(), want)
+        lz = network.DeviceLanczos(prog, 12)
+        e1, v1 = lz.solve(x)
+        try:
+            _exec.CLUSTER = False
+            e0, v0 = network.DeviceLanczos(prog, 12).solve(x)
+        finally:
+            _exec.CLUSTER = True
+        assert e1 == e0 and np.array_equal(v1.numpy_arena(), v0.numpy_arena())
+
+
 def test_bench_workload_program_matches_oracle():
     """The bench's 256-multiplet workload: compiled chain against the oracle, per block."""
     import bench
