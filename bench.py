@@ -40,8 +40,10 @@ for _p in (ROOT, ROOT / "tenet-py_b200"):
 
 METRIC = "Heff matvec TFLOP/s (SU(2) Heisenberg two-site, FP64)"
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of each kernel class on the
-# headline workload, from one ncu capture of this build (filled in from the capture)
-NCU_TRAFFIC: dict = {}
+# headline matvec, mean over the launches of one matvec in one ncu --set full capture of
+# this build (bench.py --profile-heff2 10; cold cache, so the tables and operands count)
+NCU_TRAFFIC: dict = {"block_gather": (65_024 + 98_560 + 65_024) // 3,
+                     "grouped_gemm_f64": (87_808 + 113_152) // 2}
 # multiplets per spin of the mid-chain bond (sites 31 | 32) of the reference's own
 # converged state of this chain: L = 64, chi = 256 (dense), cutoff 1e-10, ncv = 20, from
 # the seeded start, 6 sweeps (tests/golden/dmrg64.json, bond 32; 85 states dense)
@@ -1027,6 +1029,9 @@ def main() -> None:
     ap.add_argument("--profile-gemm", type=int, default=0,
                     help="only run each GEMM tile kind once on this square size (for "
                          "profiling the tensor-core kernels) and exit")
+    ap.add_argument("--profile-heff2", type=int, default=0,
+                    help="only run the headline matvec's stage launches this many times (a "
+                         "small, fixed launch sequence for profiling its kernels) and exit")
     ap.add_argument("--profile-config3", action="store_true",
                     help="only run the batched environment update a few times (a small, "
                          "fixed launch sequence for profiling its kernels) and exit")
@@ -1045,6 +1050,20 @@ def main() -> None:
         args.warmup = 3
     if args.profile_gemm > 0:
         gemm_probe(args.profile_gemm, None, reps=1)
+        return
+    if args.profile_heff2:
+        import torch
+
+        from tenet import network
+        from tenet.program import heff2_folded_program
+
+        fl, w1, w2, fr, aa = build_workload()
+        prog = heff2_folded_program(network.fold_left(fl, w1), network.fold_right(w2, fr),
+                                    aa.structure)
+        y = torch.empty_like(aa.arena)
+        for _ in range(args.profile_heff2):
+            prog.run(aa.arena, y)
+        torch.cuda.synchronize()
         return
     if args.profile_config3:
         import torch
