@@ -168,6 +168,21 @@ int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm, const int32_
                          int64_t work_bytes, int64_t n_counters, void* stream);
 
 /*
+ * A grouped FP64 GEMM whose A operand is a gather evaluated where it is read: the
+ * to_matrices / repartition of the left operand (map_view.py:238-279,
+ * ops/repartition.py:458-476) and compose's per-sector matmul (ops/map.py:155-172) in
+ * one launch.  The table rows are TNB_GEMM_WIDTH rows of TNB_TILE_32 shape without
+ * split-K (columns 12..15 zero), K <= 128, lda == K; a_off indexes the packed A, whose
+ * element e is sum over t in [a_ptr[e], a_ptr[e+1]) of a_cf[t] * src[a_src[t]], summed
+ * from zero in that order (a gather's own arithmetic).  n_ptr = packed A elements + 1.
+ */
+int tnb_grouped_gemm_gather_a(const int64_t* gemm_table, int64_t n_gemm, const int32_t* tile_map,
+                              int64_t total_tiles, const int32_t* a_ptr, int64_t n_ptr,
+                              const int32_t* a_src, const double* a_cf, int64_t n_terms,
+                              const double* src, int64_t n_src, const double* b, int64_t n_b,
+                              double* c, int64_t n_c, void* stream);
+
+/*
  * Weighted inner product  out[0] = sum_r run_w[r] * sum_{i in run r} x[i] * y[i].
  * Runs are contiguous element ranges [run_start[r], run_start[r+1]) of equal weight
  * (consecutive blocks with the same qdim of their coupled sector merged).  Replaces
@@ -331,6 +346,11 @@ int tnb_seq_append(tnb_seq* dst, const tnb_seq* src);
  * (TNB_EINVAL).  Replaces no reference interface (the reference runs each block map and
  * composition as its own Python loop); it is the one-launch form of a compiled chain.
  */
+int tnb_seq_add_gemm_gather_a(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
+                              const int32_t* tile_map, int64_t total_tiles, const int32_t* a_ptr,
+                              int64_t n_ptr, const int32_t* a_src, const double* a_cf,
+                              int64_t n_terms, const double* src, int64_t n_src, const double* b,
+                              int64_t n_b, double* c, int64_t n_c);
 int tnb_seq_fuse(const tnb_seq* src, const void* x_slot, const void* y_slot, void* barrier,
                  tnb_seq* dst);
 

@@ -33,6 +33,7 @@ constexpr int32_t kOpGemm = 2;
 constexpr int32_t kOpFused = 3;
 constexpr int32_t kOpGatherProduct = 4;
 constexpr int32_t kOpCluster = 5;
+constexpr int32_t kOpGemmGatherA = 6;
 
 struct FStage {
   int32_t code;
@@ -215,6 +216,7 @@ namespace {
 constexpr int kGatherBufs[] = {8, 10, 12, 14};  // src0, dst0, src1, dst1
 constexpr int kGemmBufs[] = {5, 7, 9};          // a, b, c
 constexpr int kGatherProductBufs[] = {11, 13, 15};  // a, b, dst
+constexpr int kGemmGatherABufs[] = {9, 11, 13};     // src, b, c
 
 inline void* as_ptr(int64_t w) { return reinterpret_cast<void*>(static_cast<intptr_t>(w)); }
 inline int64_t as_word(const void* p) { return static_cast<int64_t>(reinterpret_cast<intptr_t>(p)); }
@@ -257,6 +259,15 @@ int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* con
           static_cast<const double*>(as_ptr(w[11])), w[12],
           static_cast<const double*>(as_ptr(w[13])), w[14],
           static_cast<double*>(as_ptr(w[15])), w[16], stream);
+    } else if (op.code == kOpGemmGatherA) {
+      for (int k : kGemmGatherABufs) w[k] = patched(w[k], n_patch, from, to);
+      rc = tnb_grouped_gemm_gather_a(
+          static_cast<const int64_t*>(as_ptr(w[0])), w[1], static_cast<const int32_t*>(as_ptr(w[2])),
+          w[3], static_cast<const int32_t*>(as_ptr(w[4])), w[5],
+          static_cast<const int32_t*>(as_ptr(w[6])), static_cast<const double*>(as_ptr(w[7])),
+          w[8], static_cast<const double*>(as_ptr(w[9])), w[10],
+          static_cast<const double*>(as_ptr(w[11])), w[12], static_cast<double*>(as_ptr(w[13])),
+          w[14], stream);
     } else if (op.code == kOpFused) {
       // w[0] chain index, w[1] input, w[2] output, w[3] barrier counters, w[4] grid
       w[1] = patched(w[1], n_patch, from, to);
@@ -369,6 +380,24 @@ extern "C" int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n
                  {as_word(gemm_table), n_gemm, as_word(tile_map), total_tiles, tile_kind,
                   as_word(a), n_a, as_word(b), n_b, as_word(c), n_c, as_word(work), work_bytes,
                   n_counters, 0, 0}};
+  s->ops.push_back(op);
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_add_gemm_gather_a(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
+                                         const int32_t* tile_map, int64_t total_tiles,
+                                         const int32_t* a_ptr, int64_t n_ptr,
+                                         const int32_t* a_src, const double* a_cf,
+                                         int64_t n_terms, const double* src, int64_t n_src,
+                                         const double* b, int64_t n_b, double* c, int64_t n_c) {
+  TNB_REQUIRE(s != nullptr, "tnb_seq_add_gemm_gather_a: null sequence");
+  TNB_REQUIRE(n_gemm >= 0 && total_tiles >= 0 && n_ptr >= 0 && n_terms >= 0,
+              "tnb_seq_add_gemm_gather_a: negative size");
+  using tnb::as_word;
+  tnb_seq::Op op{tnb::kOpGemmGatherA,
+                 {as_word(gemm_table), n_gemm, as_word(tile_map), total_tiles, as_word(a_ptr),
+                  n_ptr, as_word(a_src), as_word(a_cf), n_terms, as_word(src), n_src,
+                  as_word(b), n_b, as_word(c), n_c, 0}};
   s->ops.push_back(op);
   return TNB_OK;
 }

@@ -646,6 +646,117 @@ class GemmTable:
                      else "grouped_gemm_f64", mark, self.flops)
 
 
+#: longest contracted dimension of a product whose A gather runs inside its GEMM
+#: (``GatherAGemm``, ``tnb_grouped_gemm_gather_a``)
+GA_MAX_K = 128
+#: fold an eligible link's A gather into its GEMM launch (``ChainProgram``)
+FUSE_A = True
+
+
+def gather_csr(g: GatherTable, n_dst: int):
+    """The element-level view of a gather into a buffer of ``n_dst`` elements: for every
+    destination element, its terms ``(source offset, coefficient)`` in the gather's own
+    order (``ptr`` of ``n_dst + 1`` entries, int32 ``src``, float64 ``cf``).  Elements no
+    segment covers get no terms (they read as zero).  None when the gather uses its
+    second buffer pair or the sizes exceed int32."""
+    seg = g.seg
+    if g.n_seg and np.any(seg[:, 5] != 0):
+        return None
+    dsts, srcs, cfs = [], [], []
+    for row in seg:
+        size, rank, t0, t1 = int(row[1]), int(row[2]), int(row[3]), int(row[4])
+        if size == 0:
+            continue
+        dims = [int(x) for x in row[8:8 + rank]]
+        idx = np.indices(dims).reshape(rank, -1)  # outermost first, C order = element order
+        dst = int(row[0]) + (row[16:16 + rank, None] * idx).sum(axis=0)
+        R = (row[24:24 + rank, None] * idx).sum(axis=0)
+        C = (row[32:32 + rank, None] * idx).sum(axis=0)
+        if t1 == t0:
+            continue
+        for t in range(t0, t1):
+            dsts.append(dst)
+            srcs.append(int(g.tsrc[t]) + int(g.tld[t]) * R + C)
+            cfs.append(np.full(dst.size, float(g.tcf[t])))
+    if dsts:
+        d = np.concatenate(dsts)
+        sv = np.concatenate(srcs)
+        cv = np.concatenate(cfs)
+        order = np.argsort(d, kind="stable")  # per element, terms stay in table order
+        d, sv, cv = d[order], sv[order], cv[order]
+    else:
+        d = sv = np.zeros(0, np.int64)
+        cv = np.zeros(0)
+    if d.size and (d.min() < 0 or d.max() >= n_dst):
+        raise ValueError("gather_csr: a destination lies outside the buffer")
+    if sv.size and (sv.min() < 0 or sv.max() >= 2 ** 31 - 1) or d.size >= 2 ** 31 - 1:
+        return None
+    ptr = np.zeros(n_dst + 1, np.int64)
+    np.add.at(ptr, d + 1, 1)
+    ptr = np.cumsum(ptr)
+    return ptr.astype(np.int32), sv.astype(np.int32), cv.astype(np.float64)
+
+
+class GatherAGemm:
+    """A link's A gather and grouped FP64 GEMM as one launch (``tnb_grouped_gemm_gather_a``):
+    32 x 32 output tiles without split-K over products with K <= ``GA_MAX_K``, each CTA
+    evaluating its A tile from the gather's element-level terms."""
+
+    def __init__(self, csr, products, n_a: int) -> None:
+        rows, tile, flops = [], 0, 0
+        for M, N, K, ao, lda, bo, ldb, co, ldc in products:
+            if not (M and N):
+                continue
+            out_tiles, tn = _tiles(M, N, TILE_32)
+            rows.append([M, N, K, ao, lda, bo, ldb, co, ldc, tile, tn, out_tiles, 0, 0, 0, 0])
+            tile += out_tiles
+            flops += 2 * M * N * K
+        self.table = np.array(rows, dtype=np.int64).reshape(-1, GEMM_W)
+        self.n_gemm = len(rows)
+        self.tiles = tile
+        self.flops = flops
+        per = self.table[:, 11] if len(rows) else np.zeros(0, np.int64)
+        self.tile_map = np.repeat(np.arange(len(rows), dtype=np.int32), per)
+        self.a_ptr, self.a_src, self.a_cf = csr
+        self.n_a = n_a
+        # algorithmic bytes of one launch: every A term's source element, B and C once
+        self.bytes = 8 * len(self.a_cf) + sum(8 * (K * N + M * N) for M, N, K, *_ in rows)
+        self._dev = None
+
+    launches = 1
+
+    @staticmethod
+    def eligible(products) -> bool:
+        return all(p[2] <= GA_MAX_K and (p[2] == 0 or p[4] == p[2]) for p in products)
+
+    def host_arrays(self) -> tuple:
+        return (self.table, self.tile_map, self.a_ptr, self.a_src, self.a_cf)
+
+    def device_tables(self):
+        if self._dev is None:
+            self._dev = Uploaded(self.host_arrays())
+        return self._dev.ready()
+
+    def private(self):
+        return self
+
+    def run(self, src, b, c) -> None:
+        if self.n_gemm == 0:
+            return
+        table, tile_map, a_ptr, a_src, a_cf = self.device_tables()
+        args = (ptr(table), self.n_gemm, ptr(tile_map), self.tiles, ptr(a_ptr),
+                a_ptr.numel(), ptr(a_src), ptr(a_cf), a_cf.numel(), ptr(src), src.numel(),
+                ptr(b), b.numel(), ptr(c), c.numel())
+        rec = recording()
+        if rec is not None:
+            _lib.call("tnb_seq_add_gemm_gather_a", rec.handle, *args)
+            return
+        mark = _LOG.begin() if _LOG is not None else None
+        _lib.call("tnb_grouped_gemm_gather_a", *args, stream_ptr())
+        if _LOG is not None:
+            _LOG.end("grouped_gemm_gather_a", mark, self.bytes)
+
+
 def _tiles(M, N, kind):
     if kind == TILE_SKINNY:
         return (M + SKINNY_ROWS - 1) // SKINNY_ROWS, 1

@@ -27,6 +27,10 @@ SIGNATURES = {
                                         _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
     "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
                                     _i64, _vp, _i64, _i64, _vp]),
+    "tnb_grouped_gemm_gather_a": (_i32, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _vp,
+                                         _i64, _vp, _i64, _vp, _i64, _vp]),
+    "tnb_seq_add_gemm_gather_a": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64,
+                                         _vp, _i64, _vp, _i64, _vp, _i64]),
     "tnb_dot_work_bytes": (_i64, [_i64]),
     "tnb_weighted_dot": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp]),
     "tnb_weighted_dot_noalloc": (_i32, [_vp, _vp, _i64, _vp, _vp, _i64, _vp, _vp]),

@@ -146,6 +146,7 @@ class _Link:
         if self.a_direct:
             products, self.a_gather, self.a_size = direct, None, 0
         self.gemm = _exec.GemmGroup(products, precision, tc_min_flops)
+        self.ga = None  # the A gather and the GEMM as one launch (ChainProgram._fuse_gathers)
         self.c_struct = sc
         self.b_size, self.c_size = mb.size, mc.size
         self.b_tensor = b_tensor
@@ -228,9 +229,27 @@ class ChainProgram:
         if self.defer:
             self._defer_skinny()
         self.compact = self._compact()
+        if not self.compact:
+            self._fuse_gathers()
         if allocate:
             self.allocate()
         return self
+
+    def _fuse_gathers(self) -> None:
+        """Fold each link's A gather into its GEMM launch (``_exec.GatherAGemm``) when the
+        link's products are FP64 with K <= ``_exec.GA_MAX_K``: the link becomes one launch
+        and its packed A is never written."""
+        if not _exec.FUSE_A or self.precision != "f64":
+            return
+        for lk in self.links:
+            if lk.a_gather is None or lk.a_direct or lk.deferred or lk.gemm.tensor_core:
+                continue
+            if type(lk.a_gather) is not _exec.GatherTable or \
+                    not _exec.GatherAGemm.eligible(lk.gemm.products):
+                continue
+            csr = _exec.gather_csr(lk.a_gather, lk.a_size)
+            if csr is not None:
+                lk.ga = _exec.GatherAGemm(csr, lk.gemm.products, lk.a_size)
 
     def _compact(self) -> bool:
         """Whether every stage has at most ``_exec.CLUSTER_MAX_ITEMS`` work items (gather
@@ -312,11 +331,13 @@ class ChainProgram:
         # every table of the chain in one upload, made on the shared template's tables
         # (programs rebound from one template upload once; private copies share it)
         _exec.upload_together([t for lk in self.links
-                               for t in (lk.a_gather, lk.b_gather, *lk.gemm.parts)]
+                               for t in ((lk.ga, lk.b_gather) if lk.ga is not None else
+                                         (lk.a_gather, lk.b_gather, *lk.gemm.parts))]
                               + [self.out_gather])
         for lk in self.links:  # split-K scratch of this program's own
             lk.gemm = lk.gemm.private()
-        self.a_bufs = [torch.empty(max(1, lk.a_size), **f64) for lk in self.links]
+        self.a_bufs = [torch.empty(max(1, 0 if lk.ga is not None else lk.a_size), **f64)
+                       for lk in self.links]
         self.c_bufs = [torch.empty(max(1, lk.c_size), **f64) for lk in self.links]
         self.b_bufs = [torch.empty(max(1, lk.b_size), **f64) for lk in self.links]
         # placeholder input/output: the recorded sequence reads and writes these, and a
@@ -343,6 +364,7 @@ class ChainProgram:
             self.cluster, self.cluster_ctas = cl, ctas.value
         self.fused = None
         if (not self.uses_tensor_cores and not any(lk.deferred for lk in self.links)
+                and not any(lk.ga is not None for lk in self.links)
                 and 0 < len(self.seq) <= FUSED_MAX_STAGES):
             from tenet import _lib
 
@@ -376,7 +398,8 @@ class ChainProgram:
     def launches(self) -> int:
         if getattr(self, "cluster", None) is not None and _exec.CLUSTER:
             return 1
-        return sum((0 if lk.deferred else lk.gemm.launches) + (not lk.a_direct)
+        return sum(1 if lk.ga is not None else
+                   (0 if lk.deferred else lk.gemm.launches) + (not lk.a_direct)
                    for lk in self.links) + 1
 
     @property
@@ -405,6 +428,10 @@ class ChainProgram:
     def _run_tables(self, x: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
         src, pending = x, None  # pending: the operands of a deferred link's product
         for lk, ab, bb, cb in zip(self.links, self.a_bufs, self.b_bufs, self.c_bufs):
+            if lk.ga is not None:
+                lk.ga.run(src, bb, cb)
+                src = cb
+                continue
             a = src if lk.a_direct else ab
             if isinstance(lk.a_gather, _exec.ProductGather):
                 lk.a_gather.run(*pending, ab)

@@ -390,6 +390,45 @@ def _check_cluster_cases(cases):
         assert e1 == e0 and np.array_equal(v1.numpy_arena(), v0.numpy_arena())
 
 
+def test_gather_fused_gemm_matches_the_two_launch_link(golden_dir):
+    """A link whose A gather runs inside its GEMM (``tnb_grouped_gemm_gather_a``) gives
+    the products of the gather-then-GEMM pair (within 1e-13 per block: the pair splits
+    long K, the fused tile does not) and the reference's heff2 (1e-12 per block); the
+    headline matvec becomes 3 launches, replayed from a graph and in a device Lanczos
+    solve."""
+    import bench
+    from tenet import _exec, program
+    from tenet.program import GraphMatvec, heff2_folded_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    fl, w1, w2, fr, aa = bench.build_workload()
+    cases = [(network.fold_left(fl, w1), network.fold_right(w2, fr), aa),
+             (network.fold_left(T["fl"], T["w1"]), network.fold_right(T["w2"], T["fr"]),
+              T["aa"])]
+    outs = {}
+    for fuse in (True, False):
+        _exec.FUSE_A = fuse
+        program._HEFF_TABLES.clear()
+        try:
+            for k, (lf, rf, x) in enumerate(cases):
+                prog = heff2_folded_program(lf, rf, x.structure)
+                if fuse:
+                    assert any(lk.ga is not None for lk in prog.links)
+                    if k == 0:
+                        assert prog.launches == 3
+                    e, _ = network.DeviceLanczos(prog, 12).solve(x)
+                    outs[("lanczos", k)] = e
+                outs[(fuse, k)] = GraphMatvec(prog)(x)
+        finally:
+            _exec.FUSE_A = True
+            program._HEFF_TABLES.clear()
+    for k in range(len(cases)):
+        close(outs[(True, k)], outs[(False, k)].numpy_arena(), 1e-13)
+    close(outs[(True, 1)], h[m["heff_aa"]["arena"]])
+
+
 def test_bench_workload_program_matches_oracle():
     """The bench's 256-multiplet workload: compiled chain against the oracle, per block."""
     import bench
@@ -600,7 +639,7 @@ def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
           load(h, m["heff_aa"]).numpy_arena(), 1e-12)
     # the product-source gathers give the bits of the GEMM-then-gather chain they replace
     plain = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure, defer=False)
-    assert plain.launches == 8 and not any(lk.deferred for lk in plain.links)
+    assert plain.launches == 5 and not any(lk.deferred for lk in plain.links)
     y_plain = torch.full_like(prog.y_slot, float("nan"))
     plain.run(x, y_plain)
     assert torch.equal(y_plain, y_seq)

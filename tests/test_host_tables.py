@@ -172,7 +172,9 @@ def test_heff2_chain_program_reproduces_reference(golden_dir, defer):
     # the two MPO links' skinny products are computed by the gathers that read them
     assert [lk.a_direct for lk in prog.links] == [True, False, False, False]
     assert [lk.deferred for lk in prog.links] == [False, defer, defer, False]
-    assert prog.launches == (6 if defer else 8)
+    # and, without deferral, every gathered link reads its A inside its GEMM launch
+    assert [lk.ga is not None for lk in prog.links] == [False, not defer, not defer, not defer]
+    assert prog.launches == (6 if defer else 5)
     src, pending = T["aa"][1], None
     for lk in prog.links:
         name = next(k for k in ("fl", "w1", "w2", "fr") if ops_[k] is lk.b_tensor)
@@ -430,3 +432,50 @@ def test_dmrg_record_and_schmidt_change_follow_the_reference():
     assert network._schmidt_change({}, {0: [1.0]}) == float("inf")
     got = network._schmidt_change({0: [0.8, 0.6], 1: [1.0]}, {0: [0.8], 1: [1.0], 2: [1.0]})
     assert got == pytest.approx(1.0)
+
+
+def test_gather_csr_reproduces_the_gather_element_by_element():
+    """The element-level view of a gather (what the gather-fused GEMM reads its A
+    through) gives every destination element the same terms in the same order: summed
+    from zero in that order it equals the table's emulation, on every A gather of the
+    folded heff2 chain of the bench's bonds."""
+    import bench
+    from tenet import network  # noqa: F401  (the folded structures come from its einsums)
+    from tenet.plan import transpose_plan
+    from tenet.program import ChainProgram
+
+    def einsum_s(eq, sa, sb):
+        lhs, out = eq.split("->")
+        ta, tb = lhs.split(",")
+        shared = [x for x in ta if x in tb]
+        axes = (tuple(ta.index(x) for x in shared), tuple(tb.index(x) for x in shared))
+        ex = ops.contraction_exec(sa, sb, axes)
+        free = [x for x in ta if x not in shared] + [x for x in tb if x not in shared]
+        return transpose_plan(ex.out, tuple(free.index(x) for x in out))[0]
+
+    class S:
+        def __init__(self, st):
+            self.structure = st
+
+    for bond in (bench.BOND, bench.WORKLOADS["L64_cutoff1e-14_mid_bond"]):
+        fl, w1, w2, fr, aa = bench.workload_structures(bond)
+        lf, rf = einsum_s("axB,xPpm->aBPpm", fl, w1), einsum_s("mQqy,rys->mQqrs", w2, fr)
+        p = ChainProgram(aa)
+        p.einsum("apqr,mQqrs->apmQs", S(rf))
+        p.einsum("apmQs,aBPpm->BPQs", S(lf))
+        p.finish(False)
+        rng = np.random.default_rng(0)
+        srcs = [rng.standard_normal(layout(aa).size), None]
+        assert p.links[0].ga is not None
+        for lk in p.links:
+            assert (lk.ga is not None) == (max(q[2] for q in lk.gemm.products) <= _exec.GA_MAX_K)
+            src = srcs[0] if srcs[1] is None else srcs[1]
+            want = np.zeros(lk.a_size)
+            _emulate.gather(lk.a_gather, src, want)
+            ptr, s_idx, cf = _exec.gather_csr(lk.a_gather, lk.a_size)
+            got = np.array([sum(cf[t] * src[s_idx[t]] for t in range(ptr[e], ptr[e + 1]))
+                            for e in range(lk.a_size)])
+            assert np.allclose(got, want, rtol=1e-15, atol=1e-15)
+            srcs[1] = rng.standard_normal(lk.c_size)
+        if bond == bench.BOND:
+            assert p.launches == 3
