@@ -12,19 +12,27 @@
 // back, and the link is one launch instead of two.
 //
 // For the small products of a DMRG matvec at small bonds: K <= kGaMaxK, 32 x 32 output
-// tiles, no split-K.  The static CSR row pointers of the tile are staged before the
-// programmatic-dependent-launch wait; the term loads, the source loads and B follow it.
+// tiles, no split-K, at most kGaMaxTerms terms per tile.  The tile's CSR row pointers and
+// terms are static and staged in shared memory before the programmatic-dependent-launch
+// wait; after it, one round of independent loads fetches every term's source value and
+// B, and each A element is summed from shared memory.
 #include <string>
 
 #include "tnb_stages.cuh"
 
 namespace tnb {
 
-constexpr int kGaTM = 32, kGaTN = 32, kGaThreads = 128, kGaMaxK = 128;
+constexpr int kGaTM = 32, kGaTN = 32, kGaThreads = 256, kGaMaxK = 128;
+// terms of one tile's A elements staged in shared memory (the host admits a link only
+// when every tile fits)
+constexpr int kGaMaxTerms = 5120;
 
 struct GaSmem {
   double A[kGaTM][kGaMaxK + 1];
   double B[kGaMaxK][kGaTN];
+  double cf[kGaMaxTerms];
+  double val[kGaMaxTerms];
+  int32_t src[kGaMaxTerms];
   int32_t ptr[kGaTM * kGaMaxK + 1];
   GemmRow row;
   int ok;
@@ -68,60 +76,70 @@ gemm_ga_kernel(const GaArgs ga) {
   const int rows = static_cast<int>(r.M - m0 < kGaTM ? r.M - m0 : kGaTM);
   const int cols = static_cast<int>(r.N - n0 < kGaTN ? r.N - n0 : kGaTN);
   if (rows <= 0 || cols <= 0) return;  // uniform across the CTA
-  // static: the CSR row pointers of the tile's A elements (rows m0.., all of K)
+  const int ne = rows * K;
+  // static, before the wait: the tile's CSR row pointers, then its terms (a contiguous
+  // range of the term arrays: elements and their terms are both in packed-A order)
   const int64_t e0 = r.aoff + m0 * K;
   if (K > 0)
-    for (int i = tid; i <= rows * K; i += kGaThreads) sm.ptr[i] = __ldg(ga.a_ptr + e0 + i);
+    for (int i = tid; i <= ne; i += kGaThreads) sm.ptr[i] = __ldg(ga.a_ptr + e0 + i);
+  __syncthreads();
+  const int32_t tb = K > 0 ? sm.ptr[0] : 0, te = K > 0 ? sm.ptr[ne] : 0;
+  const int nt = te - tb;
+  const bool terms_ok = tb >= 0 && nt >= 0 && nt <= kGaMaxTerms && te <= ga.n_terms;
+  if (terms_ok)
+    for (int i = tid; i < nt; i += kGaThreads) {
+      sm.src[i] = __ldg(ga.a_src + tb + i);
+      sm.cf[i] = __ldg(ga.a_cf + tb + i);
+    }
   pdl_wait();  // the source is the previous kernel's output
   __syncthreads();
-  bool bad = false;
-  for (int i = tid; i < rows * K; i += kGaThreads) {
-    const int32_t t0 = sm.ptr[i], t1 = sm.ptr[i + 1];
-    double acc = 0.0;
-    if (t0 < 0 || t1 < t0 || t1 > ga.n_terms) {
-      bad = true;
-    } else {
-      for (int32_t t = t0; t < t1; ++t) {
-        const int64_t o = __ldg(ga.a_src + t);
-        const double cf = __ldg(ga.a_cf + t);
-        const bool ok = o >= 0 && o < ga.n_src;
-        bad |= !ok;
-        acc = fma(cf, ok ? __ldg(ga.src + o) : 0.0, acc);
-      }
+  bool bad = !terms_ok;
+  // every term's source value in one round of independent loads; then each element
+  // sums its terms in their order, from zero, as the gather does
+  if (terms_ok)
+    for (int i = tid; i < nt; i += kGaThreads) {
+      const int64_t o = sm.src[i];
+      const bool ok = o >= 0 && o < ga.n_src;
+      bad |= !ok;
+      sm.val[i] = ok ? __ldg(ga.src + o) : 0.0;
     }
-    sm.A[i / K][i % K] = acc;
-  }
   for (int i = tid; i < K * kGaTN; i += kGaThreads) {
     const int k = i / kGaTN, n = i % kGaTN;
     sm.B[k][n] = n < cols ? __ldg(g.b + r.boff + static_cast<int64_t>(k) * r.ldb + n0 + n) : 0.0;
   }
+  __syncthreads();
+  for (int i = tid; i < ne; i += kGaThreads) {
+    double acc = 0.0;
+    if (terms_ok) {
+      const int t0 = sm.ptr[i] - tb, t1 = sm.ptr[i + 1] - tb;
+      if (t0 < 0 || t1 < t0 || t1 > nt) {
+        bad = true;
+      } else {
+        for (int t = t0; t < t1; ++t) acc = fma(sm.cf[t], sm.val[t], acc);
+      }
+    }
+    sm.A[i / K][i % K] = acc;
+  }
   if (bad) raise_bounds();
   __syncthreads();
-  // 128 threads x (2 rows x 4 columns): row ty + 16 i, column tx + 8 j
-  const int tx = tid % 8, ty = tid / 8;
-  double acc[2][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  // 256 threads x (2 rows x 2 columns): row ty + 16 i, column tx + 16 j
+  const int tx = tid % 16, ty = tid / 16;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
   for (int k = 0; k < K; ++k) {
-    double av[2], bv[4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) av[i] = (ty + 16 * i) < rows ? sm.A[ty + 16 * i][k] : 0.0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) bv[j] = sm.B[k][tx + 8 * j];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    const double a0 = sm.A[ty][k], a1 = sm.A[ty + 16][k];
+    const double b0 = sm.B[k][tx], b1 = sm.B[k][tx + 16];
+    acc[0][0] = fma(a0, b0, acc[0][0]);
+    acc[0][1] = fma(a0, b1, acc[0][1]);
+    acc[1][0] = fma(a1, b0, acc[1][0]);
+    acc[1][1] = fma(a1, b1, acc[1][1]);
   }
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const int m = ty + 16 * i;
     if (m >= rows) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = tx + 8 * j;
+    for (int j = 0; j < 2; ++j) {
+      const int n = tx + 16 * j;
       if (n < cols) g.c[r.coff + (m0 + m) * r.ldc + n0 + n] = acc[i][j];
     }
   }

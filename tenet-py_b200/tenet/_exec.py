@@ -647,10 +647,17 @@ class GemmTable:
 
 
 #: longest contracted dimension of a product whose A gather runs inside its GEMM
-#: (``GatherAGemm``, ``tnb_grouped_gemm_gather_a``)
+#: (``GatherAGemm``, ``tnb_grouped_gemm_gather_a``), and the most gather terms one of its
+#: 32-row tiles may read (they are staged in shared memory)
 GA_MAX_K = 128
-#: fold an eligible link's A gather into its GEMM launch (``ChainProgram``)
-FUSE_A = True
+GA_MAX_TERMS = 5120
+#: fold an eligible link's A gather into its GEMM launch (``ChainProgram``).  Off by
+#: default: the same results, measured slower on B200 (folded heff2 at the L = 64 mid bond
+#: 20.5 against 16.4 us in 3 against 5 launches; 43.5 against 39.0 us at 256 multiplets):
+#: a tile's A elements, their terms and its K reduction land on the few CTAs of the
+#: product's output tiles, where the separate gather spreads them over 9-32 CTAs and
+#: overlaps its table loads with the previous kernel
+FUSE_A = False
 
 
 def gather_csr(g: GatherTable, n_dst: int):
@@ -728,6 +735,20 @@ class GatherAGemm:
     @staticmethod
     def eligible(products) -> bool:
         return all(p[2] <= GA_MAX_K and (p[2] == 0 or p[4] == p[2]) for p in products)
+
+    @staticmethod
+    def fits(csr, products) -> bool:
+        """Whether every 32-row tile's A elements have at most ``GA_MAX_TERMS`` terms."""
+        a_ptr = csr[0]
+        for M, N, K, ao, *_ in products:
+            if not (M and N and K):
+                continue
+            for m0 in range(0, M, 32):
+                rows = min(32, M - m0)
+                lo, hi = ao + m0 * K, ao + (m0 + rows) * K
+                if hi >= len(a_ptr) or a_ptr[hi] - a_ptr[lo] > GA_MAX_TERMS:
+                    return False
+        return True
 
     def host_arrays(self) -> tuple:
         return (self.table, self.tile_map, self.a_ptr, self.a_src, self.a_cf)

@@ -248,7 +248,7 @@ class ChainProgram:
                     not _exec.GatherAGemm.eligible(lk.gemm.products):
                 continue
             csr = _exec.gather_csr(lk.a_gather, lk.a_size)
-            if csr is not None:
+            if csr is not None and _exec.GatherAGemm.fits(csr, lk.gemm.products):
                 lk.ga = _exec.GatherAGemm(csr, lk.gemm.products, lk.a_size)
 
     def _compact(self) -> bool:

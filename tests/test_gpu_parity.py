@@ -422,7 +422,7 @@ def test_gather_fused_gemm_matches_the_two_launch_link(golden_dir):
                     outs[("lanczos", k)] = e
                 outs[(fuse, k)] = GraphMatvec(prog)(x)
         finally:
-            _exec.FUSE_A = True
+            _exec.FUSE_A = False
             program._HEFF_TABLES.clear()
     for k in range(len(cases)):
         close(outs[(True, k)], outs[(False, k)].numpy_arena(), 1e-13)
@@ -639,7 +639,7 @@ def test_recorded_sequence_replays_the_chain_bit_identically(golden_dir):
           load(h, m["heff_aa"]).numpy_arena(), 1e-12)
     # the product-source gathers give the bits of the GEMM-then-gather chain they replace
     plain = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure, defer=False)
-    assert plain.launches == 5 and not any(lk.deferred for lk in plain.links)
+    assert plain.launches == 8 and not any(lk.deferred for lk in plain.links)
     y_plain = torch.full_like(prog.y_slot, float("nan"))
     plain.run(x, y_plain)
     assert torch.equal(y_plain, y_seq)
@@ -717,13 +717,22 @@ def test_fused_chain_is_bit_identical_to_stage_by_stage(golden_dir):
     and GEMMs only, so its programs are planned without product-source gathers; the
     six-launch chain with them gives the same bits."""
     import bench
-    from tenet import _exec
+    from tenet import _exec, program
     from tenet.program import heff2_program
 
     m = json.loads((golden_dir / "heff.json").read_text())
     h = np.load(golden_dir / "heff.npz")
     T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
     w = bench.build_workload()
+    # the persistent chain runs gathers and plain GEMMs: plan without gather-fused links
+    assert not _exec.FUSE_A
+    _fused_chain_cases(T, w)
+
+
+def _fused_chain_cases(T, w):
+    from tenet import _exec
+    from tenet.program import heff2_program
+
     for ops4, aa in (((T["fl"], T["w1"], T["w2"], T["fr"]), T["aa"]), (w[:4], w[4])):
         prog = heff2_program(*ops4, aa.structure, defer=False)
         assert prog.fused is not None and len(prog.fused) == 1

@@ -172,9 +172,8 @@ def test_heff2_chain_program_reproduces_reference(golden_dir, defer):
     # the two MPO links' skinny products are computed by the gathers that read them
     assert [lk.a_direct for lk in prog.links] == [True, False, False, False]
     assert [lk.deferred for lk in prog.links] == [False, defer, defer, False]
-    # and, without deferral, every gathered link reads its A inside its GEMM launch
-    assert [lk.ga is not None for lk in prog.links] == [False, not defer, not defer, not defer]
-    assert prog.launches == (6 if defer else 5)
+    assert not any(lk.ga is not None for lk in prog.links)  # gather fusion is off by default
+    assert prog.launches == (6 if defer else 8)
     src, pending = T["aa"][1], None
     for lk in prog.links:
         name = next(k for k in ("fl", "w1", "w2", "fr") if ops_[k] is lk.b_tensor)
@@ -463,7 +462,11 @@ def test_gather_csr_reproduces_the_gather_element_by_element():
         p = ChainProgram(aa)
         p.einsum("apqr,mQqrs->apmQs", S(rf))
         p.einsum("apmQs,aBPpm->BPQs", S(lf))
-        p.finish(False)
+        _exec.FUSE_A = True
+        try:
+            p.finish(False)
+        finally:
+            _exec.FUSE_A = False
         rng = np.random.default_rng(0)
         srcs = [rng.standard_normal(layout(aa).size), None]
         assert p.links[0].ga is not None
