@@ -679,6 +679,48 @@ def run_reference(args) -> None:
     }))
 
 
+def precision_lanczos(args) -> dict:
+    """The precision form's Lanczos (ncv = 20) on the 256-multiplet stress bond, whose
+    large products qualify for the tensor cores: the energy against the FP64 form's, and
+    the FP64 relative residual |Hv - <v,Hv> v| / |<v,Hv>| of the Ritz vector with the
+    energy-only correction and with the FP64 residual correction of the vector."""
+    import torch
+
+    from tenet import network, ops
+    from tenet.program import heff2_folded_program
+
+    bond = WORKLOADS["synthetic_256_multiplets"]
+    fl, w1, w2, fr, aa = build_workload(bond=bond)
+    lf, rf = network.fold_left(fl, w1), network.fold_right(w2, fr)
+    p64 = heff2_folded_program(lf, rf, aa.structure)
+
+    def residual(v):
+        hv = p64(v)
+        theta = ops.inner(v, hv)
+        return ops.norm(ops.subtract(hv, v * theta)) / abs(theta)
+
+    e64, v64 = network.DeviceLanczos(p64, 20).solve(aa)
+    out = {"workload": "heff2 Lanczos, ncv = 20, synthetic 256-multiplet bond",
+           "f64": {"energy": e64, "residual": residual(v64)}}
+    for precision in ("3xbf16", "tf32"):
+        ptc = heff2_folded_program(lf, rf, aa.structure, precision=precision)
+        row = {"tensor_core_products": sum(len(q.table) for lk in ptc.links
+                                           for q in lk.gemm.parts if q.kind in (3, 4))}
+        for name, res in (("energy_correction", False), ("residual_correction", True)):
+            lz = network.DeviceLanczos(ptc, 20, correct=p64, residual=res)
+            e, v = lz.solve(aa)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(3):
+                lz.solve(aa)
+            torch.cuda.synchronize()
+            row[name] = {"energy_rel_error_vs_f64": abs(e - e64) / abs(e64),
+                         "residual": residual(v),
+                         "ms_per_solve": (time.perf_counter() - t0) / 3 * 1e3}
+        out[precision] = row
+    return out
+
+
 def dmrg_solve(args) -> dict:
     """Config-2 solves end to end on the GPU: the L = 64 SU(2) Heisenberg chain from the
     seeded start, chi = 256 (dense), cutoff 1e-10, ncv = 20, the reference's convergence
@@ -968,6 +1010,7 @@ def run_tenet(args) -> None:
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
         solve = dmrg_solve(args) if args.dmrg else None
+        plz = precision_lanczos(args) if args.dmrg else None
         solves = serving(args) if args.serve_requests > 0 else None
         env3 = batched_env_updates(args) if args.config3_n > 0 else None
         bmv = (batched_matvecs(args, forms_ms["eager_ops"], ms / args.steps)
@@ -994,6 +1037,7 @@ def run_tenet(args) -> None:
             "other_workloads": others,
             "mixed_precision_forms": mixed,
             "dmrg_solve": solve,
+            "precision_lanczos": plz,
             "serving": solves,
             "batched_env_updates": env3,
             "batched_matvecs": bmv,

@@ -179,7 +179,7 @@ class DeviceLanczos:
     energy)."""
 
     def __init__(self, program, ncv: int, tol: float = 1e-13, correct=None,
-                 reorthogonalize: bool | None = None) -> None:
+                 reorthogonalize: bool | None = None, residual: bool = True) -> None:
         """``reorthogonalize`` (default: on exactly when ``correct`` is given, i.e. in the
         precision form) adds classical Gram-Schmidt, applied twice, of every new Krylov
         vector against all earlier ones in FP64.  A reduced-precision matvec never drives
@@ -190,6 +190,8 @@ class DeviceLanczos:
         from tenet.structure import layout
 
         self.program, self.ncv, self.tol, self.correct = program, ncv, tol, correct
+        # the precision form's FP64 residual correction of the Ritz vector (``finish``)
+        self.residual = residual and correct is not None
         self.reorth = (correct is not None) if reorthogonalize is None else reorthogonalize
         s = program.in_struct
         n = layout(s).size
@@ -213,6 +215,11 @@ class DeviceLanczos:
         self.runs = ops._runs(s)
         self._host_state = torch.zeros(3 * ncv + 2, dtype=torch.float64).pin_memory()
         self._host_coef = torch.zeros(ncv, dtype=torch.float64).pin_memory()
+        if self.residual:
+            self.R = torch.zeros(max(n, 1), **f64)
+            self.W3 = torch.zeros(max(n, 1), **f64)
+            self.dots = torch.zeros(5, **f64)
+            self._host_dots = torch.zeros(5, dtype=torch.float64).pin_memory()
 
     def launch(self, x: torch.Tensor) -> None:
         """Enqueue the recurrence from start vector ``x`` (an arena of ``n`` doubles)."""
@@ -253,13 +260,58 @@ class DeviceLanczos:
                   _exec.stream_ptr())
 
     def finish(self) -> tuple[float, SymmetricTensor]:
-        """After ``launch``: read the tridiagonal, form the Ritz vector, return the pair."""
+        """After ``launch``: read the tridiagonal, form the Ritz vector, return the pair.
+        In the precision form the pair is then corrected in FP64 (``_residual_step``)."""
         values, coef = self.tridiagonal()
         out = SymmetricTensor.empty(self.program.in_struct)
         self.ritz(coef, out.arena)
         if self.correct is not None:
+            if self.residual:
+                return self._residual_step(out)
             return float(self.scal[1].item()), out
         return float(values[0]), out
+
+    def _dot(self, x: torch.Tensor, y: torch.Tensor, k: int) -> None:
+        from tenet import _exec, _lib
+
+        P, r = _exec.ptr, self.runs
+        _lib.call("tnb_weighted_dot", P(x), P(y), self.n, P(r.start), P(r.weight), r.n_runs,
+                  P(self.work), P(self.dots) + 8 * k, _exec.stream_ptr())
+
+    def _residual_step(self, out: SymmetricTensor) -> tuple[float, SymmetricTensor]:
+        """The FP64 residual correction of the reduced-precision Ritz vector: with ``x``
+        the normalised Ritz vector, ``Hx`` its FP64 image (already formed by the Ritz
+        call) and ``r = Hx - <x, Hx> x`` the FP64 residual, the lowest Ritz pair of the
+        FP64 operator on span{x, r} (one more FP64 matvec, a 2 x 2 generalised eigenproblem
+        on the host).  The vector error drops from the reduced-precision solve's first
+        order to second order in it, and the energy with it; a residual already below
+        ``1e-14`` relative leaves the pair as it is."""
+        from tenet import ops
+
+        x, hx = out.arena, self.W2
+        theta = float(self.scal[1].item())
+        ops.axpby_into(1.0, hx, -theta, x, self.R)
+        self.correct.run(self.R, self.W3)
+        for k, (a, b) in enumerate(((hx, self.R), (self.R, self.W3), (x, self.R),
+                                    (self.R, self.R), (x, x))):
+            self._dot(a, b, k)
+        self._host_dots.copy_(self.dots)
+        h12, h22, s12, s22, s11 = (float(v) for v in self._host_dots.numpy())
+        if not s22 > 1e-28 * max(s11, 1e-300):
+            return theta, out
+        h = np.array([[theta * s11, h12], [h12, h22]])
+        sm = np.array([[s11, s12], [s12, s22]])
+        try:
+            import scipy.linalg
+
+            lam, vec = scipy.linalg.eigh(h, sm)
+        except Exception:  # a numerically singular pair: keep the uncorrected one
+            return theta, out
+        c = vec[:, 0]
+        ops.axpby_into(float(c[0]), x, float(c[1]), self.R, x)
+        norm = float(ops.norm(out))
+        ops.axpby_into(1.0 / norm, x, 0.0, x, x)
+        return float(lam[0]), out
 
     def solve(self, v: SymmetricTensor) -> tuple[float, SymmetricTensor]:
         if v.structure != self.program.in_struct:

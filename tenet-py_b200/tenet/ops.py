@@ -348,6 +348,12 @@ def _axpby(alpha, x: SymmetricTensor, beta, y: SymmetricTensor) -> SymmetricTens
     return out
 
 
+def axpby_into(alpha, x: torch.Tensor, beta, y: torch.Tensor, out: torch.Tensor) -> None:
+    """``out = alpha x + beta y`` on raw arenas (``out`` may alias ``x`` or ``y``)."""
+    _lib.call("tnb_axpby", x.numel(), float(alpha), _exec.ptr(x), float(beta), _exec.ptr(y),
+              _exec.ptr(out), _exec.stream_ptr())
+
+
 def add(a: SymmetricTensor, b: SymmetricTensor) -> SymmetricTensor:
     _check_same(a, b, "add")
     return _axpby(1.0, a, 1.0, b)

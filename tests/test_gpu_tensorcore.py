@@ -141,3 +141,32 @@ def test_mixed_precision_ctmrg_chi128_near_criticality():
         assert [m for _, m in bond.sectors] == [64, 64]
     assert abs(out["3xbf16"] - out["f64"]) <= 1e-8 * abs(out["f64"])
     assert abs(out["3xbf16"] - O.onsager_beta_f(0.44)) <= 1e-6 * abs(out["f64"])
+
+
+@pytest.mark.parametrize("precision", ["3xbf16", "tf32"])
+def test_residual_correction_of_the_precision_lanczos_vector(precision):
+    """The precision form's FP64 residual correction (``DeviceLanczos._residual_step``) on
+    the 256-multiplet bond, whose large products run on the tensor cores: the corrected
+    Ritz vector has a smaller FP64 residual than the uncorrected one, and its energy is
+    no higher (the correction is a Rayleigh-Ritz step on span{x, r})."""
+    import bench
+    from tenet import ops
+    from tenet.program import heff2_folded_program
+
+    fl, w1, w2, fr, aa = bench.build_workload(bond=bench.WORKLOADS["synthetic_256_multiplets"])
+    lf, rf = network.fold_left(fl, w1), network.fold_right(w2, fr)
+    p64 = heff2_folded_program(lf, rf, aa.structure)
+    ptc = heff2_folded_program(lf, rf, aa.structure, precision=precision)
+    assert ptc.uses_tensor_cores
+
+    def residual(v):
+        hv = p64(v)
+        theta = ops.inner(v, hv)
+        return ops.norm(ops.subtract(hv, v * theta)) / abs(theta)
+
+    e1, v1 = network.DeviceLanczos(ptc, 20, correct=p64, residual=False).solve(aa)
+    e2, v2 = network.DeviceLanczos(ptc, 20, correct=p64, residual=True).solve(aa)
+    r1, r2 = residual(v1), residual(v2)
+    assert e2 <= e1 + 1e-12 * abs(e1)
+    assert r2 < r1
+    assert abs(ops.norm(v2) - 1.0) < 1e-12
