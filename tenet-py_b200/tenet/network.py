@@ -66,6 +66,25 @@ def fold_right(w2: SymmetricTensor, fr: SymmetricTensor) -> SymmetricTensor:
     return ops.einsum("mQqy,rys->mQqrs", w2, fr)
 
 
+def env_update_last_folded(lf: SymmetricTensor, a: SymmetricTensor,
+                           bra_site: SymmetricTensor | None = None) -> SymmetricTensor:
+    """``F[(n, n+1)]`` from ``lf = fold_left(F[(n-1, n)], W[n])``: the ket contracted into
+    the folded environment, then the bra -- two contractions instead of three, the same
+    operator as ``env_update_last`` (``network/env.py:618-626``)."""
+    bra = ops.adjoint(a if bra_site is None else bra_site)
+    t = ops.einsum("aBPpm,apr->BrPm", lf, a)
+    return ops.einsum("BPs,BrPm->rms", bra, t)
+
+
+def env_update_first_folded(rf: SymmetricTensor, a: SymmetricTensor,
+                            bra_site: SymmetricTensor | None = None) -> SymmetricTensor:
+    """``F[(n, n-1)]`` from ``rf = fold_right(W[n], F[(n+1, n)])``: the counterpart of
+    ``env_update_last_folded`` for ``env_update_first`` (``network/env.py:627-633``)."""
+    bra = ops.adjoint(a if bra_site is None else bra_site)
+    t = composed("apr,xPprs->axPs", a, rf, bend="p")
+    return composed("axPs,BPs->axB", t, bra, bend="P")
+
+
 def heff2_folded(lf: SymmetricTensor, rf: SymmetricTensor, aa: SymmetricTensor) -> SymmetricTensor:
     """``H_eff @ aa`` from the folded environments: ``(aa . rf) . lf``."""
     t = ops.einsum("apqr,mQqrs->apmQs", aa, rf)
@@ -656,6 +675,26 @@ class Env:
         }
         self._prog: dict = {}
         self._wrapped: dict = {}
+        self._lf: dict = {}  # bond n -> (F[(n-1, n)] it was folded from, fold_left)
+        self._rf: dict = {}  # bond n -> (F[(n+2, n+1)] it was folded from, fold_right)
+
+    def fold_l(self, n: int) -> SymmetricTensor:
+        """``fold_left(F[(n-1, n)], W[n])``, kept while that environment is unchanged."""
+        f = self.F[n - 1, n]
+        hit = self._lf.get(n)
+        if hit is None or hit[0] is not f:
+            hit = (f, fold_left(f, self.h[n]))
+            self._lf[n] = hit
+        return hit[1]
+
+    def fold_r(self, n: int) -> SymmetricTensor:
+        """``fold_right(W[n+1], F[(n+2, n+1)])``, kept while that environment is unchanged."""
+        f = self.F[n + 2, n + 1]
+        hit = self._rf.get(n)
+        if hit is None or hit[0] is not f:
+            hit = (f, fold_right(self.h[n + 1], f))
+            self._rf[n] = hit
+        return hit[1]
 
     @property
     def device_solves(self) -> bool:
@@ -670,11 +709,22 @@ class Env:
         return self
 
     def update_(self, n: int, *, to: str) -> None:
+        """With ``fold``, an environment whose MPO site is already folded into the old one
+        (the bond's matvec folded it) grows through that fold: two contractions."""
         bra = None if self.bra is self.psi else self.bra[n]
         if to == "last":
-            self.F[n, n + 1] = env_update_last(self.F[n - 1, n], self.psi[n], self.h[n], bra)
+            hit = self._lf.get(n)
+            if self.fold and hit is not None and hit[0] is self.F.get((n - 1, n)):
+                self.F[n, n + 1] = env_update_last_folded(hit[1], self.psi[n], bra)
+            else:
+                self.F[n, n + 1] = env_update_last(self.F[n - 1, n], self.psi[n], self.h[n], bra)
         else:
-            self.F[n, n - 1] = env_update_first(self.F[n + 1, n], self.psi[n], self.h[n], bra)
+            hit = self._rf.get(n - 1)
+            if self.fold and hit is not None and hit[0] is self.F.get((n + 1, n)):
+                self.F[n, n - 1] = env_update_first_folded(hit[1], self.psi[n], bra)
+            else:
+                self.F[n, n - 1] = env_update_first(self.F[n + 1, n], self.psi[n], self.h[n],
+                                                    bra)
 
     def clear_(self, *sites: int) -> None:
         for n in sites:
@@ -723,7 +773,7 @@ class Env:
 
         def operands():
             if self.fold:
-                return {"lf": fold_left(fl, w1), "rf": fold_right(w2, fr)}
+                return {"lf": self.fold_l(n), "rf": self.fold_r(n)}
             return {"fr": fr, "w2": w2, "w1": w1, "fl": fl}
 
         if hit is None or hit["skey"] != skey:

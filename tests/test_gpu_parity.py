@@ -162,6 +162,25 @@ def test_env_folds_match_oracle(golden_dir):
     close(got, want.arena())
 
 
+def test_folded_env_updates_match_the_three_contraction_ones(golden_dir):
+    """Growing an environment through the folded one (``F . W`` kept from the bond's
+    matvec) gives the same environment as the reference's three contractions."""
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    fl, fr, w1, w2 = (load(h, m[k]) for k in ("fl", "fr", "w1", "w2"))
+    bond, phys = m["aa"]["legs"][0], m["aa"]["legs"][1]
+    site = [dict(bond, side="out"), dict(phys, side="out"), dict(bond, side="in")]
+    a = tenet.SymmetricTensor.random(struct(site).legs, seed=7)
+    want = network.env_update_last(fl, a, w1)
+    got = network.env_update_last_folded(network.fold_left(fl, w1), a)
+    assert got.structure == want.structure
+    close(got, want.numpy_arena(), 1e-13)
+    want = network.env_update_first(fr, a, w2)
+    got = network.env_update_first_folded(network.fold_right(w2, fr), a)
+    assert got.structure == want.structure
+    close(got, want.numpy_arena(), 1e-13)
+
+
 def test_config1_full_size_against_reference_checksums(golden_dir):
     g = json.loads((golden_dir / "config1.json").read_text())
     V = GradedSpace.new(U1, {U1.sector(q): d for q, d in g["degeneracies"]})
