@@ -142,13 +142,23 @@ class _SvdPlan:
         self.rows = torch.tensor(rows or [(0,) * 8], **i64)
         self.sec_rows = torch.tensor(sec_rows or [(0,) * 4], **i64)
         self.qdim = torch.tensor(qd or [1.0], dtype=torch.float64, device=dev)
-        n = max(1, len(self.sectors))
-        self.keep = torch.zeros(n, **i64)
-        self.info = torch.zeros(n, dtype=torch.int32, device=dev)
-        self.stats = torch.zeros(8, dtype=torch.float64, device=dev)
-        self.h_keep = torch.zeros(n, dtype=torch.int64).pin_memory()
-        self.h_info = torch.zeros(n, dtype=torch.int32).pin_memory()
-        self.h_stats = torch.zeros(8, dtype=torch.float64).pin_memory()
+        # everything the decision reads back, in one device buffer and one pinned copy:
+        # stats (8 f64), keep (ns i64), sorted values (T f64), info (ns i32), sorted sectors
+        # (T i32)
+        n, T = max(1, len(self.sectors)), max(1, self.total)
+        self.o_keep = 64
+        self.o_sorted = self.o_keep + 8 * n
+        self.o_info = self.o_sorted + 8 * T
+        self.o_csec = self.o_info + 4 * n
+        nbytes = -(-(self.o_csec + 4 * T) // 8) * 8
+        self.dev = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
+        self.host = torch.zeros(nbytes, dtype=torch.uint8).pin_memory()
+        h = self.host.numpy()
+        self.h_stats = h[:64].view(np.float64)
+        self.h_keep = h[self.o_keep:self.o_sorted].view(np.int64)
+        self.h_sorted = h[self.o_sorted:self.o_info].view(np.float64)
+        self.h_info = h[self.o_info:self.o_csec].view(np.int32)
+        self.h_csec = h[self.o_csec:self.o_csec + 4 * T].view(np.int32)
 
 
 @cache
@@ -206,30 +216,23 @@ def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cuto
     Sv = torch.empty(max(1, plan.n_s), **f64)
     V = torch.empty(max(1, plan.n_v), **f64)
     W = torch.empty(max(1, plan.n_w), **f64)
-    sorted_s = torch.empty(plan.total, **f64)
-    sorted_c = torch.empty(plan.total, dtype=torch.int32, device=dev)
     P, st = _exec.ptr, _exec.stream_ptr()
     ns = len(plan.sectors)
+    base = plan.dev.data_ptr()
     _lib.call("tnb_block_svd", P(plan.rows), ns, P(buf), buf.numel(), P(U), U.numel(), P(Sv),
-              Sv.numel(), P(V), V.numel(), P(W), plan.n_w, P(plan.info), plan.smem, st)
+              Sv.numel(), P(V), V.numel(), P(W), plan.n_w, base + plan.o_info, plan.smem, st)
     _lib.call("tnb_truncate_decide", P(plan.sec_rows), P(plan.qdim), ns, P(Sv), Sv.numel(),
               -1.0 if cutoff is None else float(cutoff), _MODES[cutoff_mode],
               -1.0 if max_bond is None else float(max_bond), 0 if budget == "dense" else 1,
-              P(plan.keep), P(sorted_s), P(sorted_c), P(plan.stats), st)
-    plan.h_keep.copy_(plan.keep, non_blocking=True)
-    plan.h_info.copy_(plan.info, non_blocking=True)
-    plan.h_stats.copy_(plan.stats, non_blocking=True)
-    h_s = torch.empty(plan.total, dtype=torch.float64, pin_memory=True)
-    h_c = torch.empty(plan.total, dtype=torch.int32, pin_memory=True)
-    h_s.copy_(sorted_s, non_blocking=True)
-    h_c.copy_(sorted_c, non_blocking=True)
+              base + plan.o_keep, base + plan.o_sorted, base + plan.o_csec, base, st)
+    plan.host.copy_(plan.dev, non_blocking=True)
     torch.cuda.current_stream().synchronize()
-    info = plan.h_info.numpy()[:ns]
+    info = plan.h_info[:ns]
     if np.any(info != 0):
         raise RuntimeError(f"svd_truncated: the blockwise SVD did not converge (info "
                            f"{info.tolist()})")
-    keep_h = plan.h_keep.numpy()[:ns]
-    n_kept, dense, disc, total, kept_w = (float(x) for x in plan.h_stats.numpy()[:5])
+    keep_h = plan.h_keep[:ns]
+    n_kept, dense, disc, total, kept_w = (float(x) for x in plan.h_stats[:5])
     if n_kept == 0:
         raise ValueError("svd_truncated: the truncation keeps no singular value at all")
     keep = {c: int(k) for c, k in zip(plan.sectors, keep_h) if k > 0}
@@ -238,7 +241,7 @@ def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cuto
     sel = BondSelection(keep, dense, int(n_kept), disc, scale)
     nk = int(n_kept)
     kept = [(float(x) * scale, plan.sectors[int(k)])
-            for x, k in zip(h_s.numpy()[:nk], h_c.numpy()[:nk])]
+            for x, k in zip(plan.h_sorted[:nk], plan.h_csec[:nk])]
     bond = GradedSpace.new(p, {p.sector(c): k for c, k in keep.items()})
     su = TensorStructure((*m.codomain, Leg(bond, IN)))
     ss = TensorStructure((Leg(bond, OUT), Leg(bond, IN)))
