@@ -584,6 +584,57 @@ def serving(args) -> dict:
     return out
 
 
+def serve_stream(args) -> None:
+    """The config-5 stream at full distribution (L in {16, 32, 64, 128}, chi in {32, 64,
+    128, 256}, J2/J1 in [0, 0.4], 8 sweeps, ncv = 20, cutoff 1e-10), ``--serve-requests``
+    requests served by ``--serve-workers`` worker processes in the 3xBF16 precision form:
+    first all at once (the burst throughput), then as Poisson streams at 0.5x and 0.85x
+    that rate; p50 / p99 time-to-solution per arm.  The plain FP64 form (eager matvecs,
+    host-driven Lanczos) solves a seeded sample of the same requests one by one for the
+    baseline solves/s and the per-request |dE/L| of the served energies.  Prints one JSON
+    line and exits."""
+    import torch
+
+    from tenet import serve
+
+    n, w = args.serve_requests, args.serve_workers
+    reqs = serve.request_stream(n, float("inf"), seed=0)
+    out = {"requests": n, "workers": w, "precision": "3xbf16",
+           "distribution": {str(L): sum(r.L == L for r in reqs) for L in (16, 32, 64, 128)}}
+    energies = {}
+    serve.clear_plan_caches()
+    srv = serve.ProcessServer(workers=w, precision="3xbf16")
+    try:
+        t0 = time.perf_counter()
+        res = srv.run(reqs)
+        out["burst"] = serve.summarize(res, time.perf_counter() - t0)
+        energies.update({r.rid: r.energy for r in res})
+        burst = out["burst"]["solves_per_s"]
+        for frac in (0.5, 0.85):
+            stream = serve.request_stream(n, frac * burst, seed=0)
+            t0 = time.perf_counter()
+            res = srv.run(stream)
+            out[f"poisson_{frac}x"] = serve.summarize(res, time.perf_counter() - t0) | {
+                "arrival_rate_per_s": frac * burst}
+    finally:
+        srv.close()
+    k = min(args.serve_plain_sample, n)
+    sample = [reqs[i] for i in np.random.default_rng(1).choice(n, size=k, replace=False)]
+    serve.clear_plan_caches()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = {}
+    for r in sample:
+        plain[r.rid], _ = serve.solve_alone(r, precision="f64", compiled=False)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    out["plain_f64_sample"] = {"requests": k, "wall_s": wall, "solves_per_s": k / wall,
+                               "max_abs_dE_per_site_served_vs_plain": max(
+                                   abs(energies[r.rid] - plain[r.rid]) / r.L for r in sample)}
+    out["burst_solves_per_s_vs_plain_f64"] = burst / (k / wall)
+    print(json.dumps({"serve_stream": out}))
+
+
 def chain64_start(L: int = 64, max_2j: int = 16, seed: int = 0):
     """The seeded start of the L = 64 SU(2) Heisenberg runs: bond spins 2j <= min(i, L - i,
     16), one multiplet each, ``MPS.random`` with ``seed``."""
@@ -1081,6 +1132,11 @@ def main() -> None:
     ap.add_argument("--profile-config3", action="store_true",
                     help="only run the batched environment update a few times (a small, "
                          "fixed launch sequence for profiling its kernels) and exit")
+    ap.add_argument("--serve-stream", action="store_true",
+                    help="only serve the full config-5 stream (--serve-requests requests, "
+                         "--serve-workers workers) at three arrival rates, print and exit")
+    ap.add_argument("--serve-plain-sample", type=int, default=12,
+                    help="requests of the stream the plain FP64 form solves for the baseline")
     ap.add_argument("--no-dmrg", dest="dmrg", action="store_false",
                     help="skip the config-2 DMRG time-to-solution leg")
     ap.add_argument("--derive-bond", action="store_true",
@@ -1091,6 +1147,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.derive_bond:
         derive_bond(args)
+        return
+    if args.serve_stream:
+        serve_stream(args)
         return
     if args.warmup < 3:
         args.warmup = 3

@@ -150,7 +150,7 @@ def test_residual_correction_of_the_precision_lanczos_vector(precision):
     Ritz vector has a smaller FP64 residual than the uncorrected one, and its energy is
     no higher (the correction is a Rayleigh-Ritz step on span{x, r})."""
     import bench
-    from tenet import ops
+    from tenet import network, ops
     from tenet.program import heff2_folded_program
 
     fl, w1, w2, fr, aa = bench.build_workload(bond=bench.WORKLOADS["synthetic_256_multiplets"])
