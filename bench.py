@@ -589,7 +589,9 @@ def serve_stream(args) -> None:
     128, 256}, J2/J1 in [0, 0.4], 8 sweeps, ncv = 20, cutoff 1e-10), ``--serve-requests``
     requests served by ``--serve-workers`` worker processes in the 3xBF16 precision form:
     first all at once (the burst throughput), then as Poisson streams at 0.5x and 0.85x
-    that rate; p50 / p99 time-to-solution per arm.  The plain FP64 form (eager matvecs,
+    that rate (the first ``--serve-rate-requests`` of the same seeded stream); p50 / p99
+    time-to-solution per arm.  The workers keep their plan caches across the arms, as a
+    long-running server does.  The plain FP64 form (eager matvecs,
     host-driven Lanczos) solves a seeded sample of the same requests one by one for the
     baseline solves/s and the per-request |dE/L| of the served energies.  Prints one JSON
     line and exits."""
@@ -610,8 +612,9 @@ def serve_stream(args) -> None:
         out["burst"] = serve.summarize(res, time.perf_counter() - t0)
         energies.update({r.rid: r.energy for r in res})
         burst = out["burst"]["solves_per_s"]
+        nr = min(n, args.serve_rate_requests or n)
         for frac in (0.5, 0.85):
-            stream = serve.request_stream(n, frac * burst, seed=0)
+            stream = serve.request_stream(nr, frac * burst, seed=0)
             t0 = time.perf_counter()
             res = srv.run(stream)
             out[f"poisson_{frac}x"] = serve.summarize(res, time.perf_counter() - t0) | {
@@ -728,48 +731,6 @@ def run_reference(args) -> None:
         "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))
-
-
-def precision_lanczos(args) -> dict:
-    """The precision form's Lanczos (ncv = 20) on the 256-multiplet stress bond, whose
-    large products qualify for the tensor cores: the energy against the FP64 form's, and
-    the FP64 relative residual |Hv - <v,Hv> v| / |<v,Hv>| of the Ritz vector with the
-    energy-only correction and with the FP64 residual correction of the vector."""
-    import torch
-
-    from tenet import network, ops
-    from tenet.program import heff2_folded_program
-
-    bond = WORKLOADS["synthetic_256_multiplets"]
-    fl, w1, w2, fr, aa = build_workload(bond=bond)
-    lf, rf = network.fold_left(fl, w1), network.fold_right(w2, fr)
-    p64 = heff2_folded_program(lf, rf, aa.structure)
-
-    def residual(v):
-        hv = p64(v)
-        theta = ops.inner(v, hv)
-        return ops.norm(ops.subtract(hv, v * theta)) / abs(theta)
-
-    e64, v64 = network.DeviceLanczos(p64, 20).solve(aa)
-    out = {"workload": "heff2 Lanczos, ncv = 20, synthetic 256-multiplet bond",
-           "f64": {"energy": e64, "residual": residual(v64)}}
-    for precision in ("3xbf16", "tf32"):
-        ptc = heff2_folded_program(lf, rf, aa.structure, precision=precision)
-        row = {"tensor_core_products": sum(len(q.table) for lk in ptc.links
-                                           for q in lk.gemm.parts if q.kind in (3, 4))}
-        for name, res in (("energy_correction", False), ("residual_correction", True)):
-            lz = network.DeviceLanczos(ptc, 20, correct=p64, residual=res)
-            e, v = lz.solve(aa)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for _ in range(3):
-                lz.solve(aa)
-            torch.cuda.synchronize()
-            row[name] = {"energy_rel_error_vs_f64": abs(e - e64) / abs(e64),
-                         "residual": residual(v),
-                         "ms_per_solve": (time.perf_counter() - t0) / 3 * 1e3}
-        out[precision] = row
-    return out
 
 
 def dmrg_solve(args) -> dict:
@@ -1061,7 +1022,6 @@ def run_tenet(args) -> None:
         roofline["frac"] = roofline["achieved"] / roofline["peak"] if roofline["peak"] else None
         base = cpu_baseline(flops, budget_s=args.cpu_budget) if not args.no_cpu else None
         solve = dmrg_solve(args) if args.dmrg else None
-        plz = precision_lanczos(args) if args.dmrg else None
         solves = serving(args) if args.serve_requests > 0 else None
         env3 = batched_env_updates(args) if args.config3_n > 0 else None
         bmv = (batched_matvecs(args, forms_ms["eager_ops"], ms / args.steps)
@@ -1088,7 +1048,6 @@ def run_tenet(args) -> None:
             "other_workloads": others,
             "mixed_precision_forms": mixed,
             "dmrg_solve": solve,
-            "precision_lanczos": plz,
             "serving": solves,
             "batched_env_updates": env3,
             "batched_matvecs": bmv,
@@ -1135,6 +1094,8 @@ def main() -> None:
     ap.add_argument("--serve-stream", action="store_true",
                     help="only serve the full config-5 stream (--serve-requests requests, "
                          "--serve-workers workers) at three arrival rates, print and exit")
+    ap.add_argument("--serve-rate-requests", type=int, default=0,
+                    help="requests of each Poisson arm of --serve-stream (0: all)")
     ap.add_argument("--serve-plain-sample", type=int, default=12,
                     help="requests of the stream the plain FP64 form solves for the baseline")
     ap.add_argument("--no-dmrg", dest="dmrg", action="store_false",
