@@ -106,3 +106,24 @@ def test_excited_state_is_orthogonal_to_the_ground_state():
     pair = tenet.einsum("apx,xqr->apqr", g.psi[0], g.psi[1])
     bb = tenet.einsum("apx,xqr->apqr", e.psi[0], e.psi[1])
     assert abs(float(tenet.inner(env.project2(0, pair), bb))) < 1e-8
+
+
+def test_canonize_leaves_right_orthonormal_sites():
+    """``canonize_`` (the device SVD split, every value kept): each site n >= 1 is a
+    right isometry on the bond of min(rows, cols) per sector, and the state is normalised
+    on site 0."""
+    from tenet import ops
+
+    L = 10
+    bonds = [GradedSpace.new(SU2, {SU2.sector(j): 1 + (j % 3)
+                                   for j in range(i % 2, min(i, L - i) + 1, 2)})
+             for i in range(L + 1)]
+    psi = network.MPS.random(SITE.phys, bonds, seed=3)
+    psi.canonize_(0)
+    for n in range(1, L):
+        q = ops.repartition(psi[n], (0,), (1, 2))
+        eye = ops.identity((q.legs[0],))
+        got = ops.compose(q, ops.adjoint(q))
+        assert got.structure == eye.structure
+        np.testing.assert_allclose(got.numpy_arena(), eye.numpy_arena(), atol=1e-13)
+    assert abs(ops.norm(psi[0]) - 1.0) < 1e-12
