@@ -401,20 +401,19 @@ class MPS:
         return serialize.load_mps(path)
 
     def canonize_(self, to: int = 0) -> "MPS":
-        """Right-canonicalise from the right (``network/mps.py:312-352``): each site is
-        split as ``T = L Q`` with ``Q`` row-orthonormal on the bond of ``min(rows, cols)``
-        per coupled sector -- the reference's LQ shape -- and ``L`` moves into the site to
-        the left.  The split is the device blockwise SVD with every value kept (``L = U S``,
-        ``Q = Vh``): an orthonormal ``Q`` in another gauge of the same bond, with no library
-        factorisation and one read-back per site."""
+        """Right-canonicalise by one LQ per site from the right (``network/mps.py:312-352``).
+        The LQ's gauge is the reference's (Householder QR of the transpose, LAPACK's sign
+        convention), which the sweeps that follow depend on at the level of their
+        unreorthogonalised Lanczos: an SVD split in another gauge of the same bonds moved
+        the L = 64 run's first-sweep energy by 3e-6 per site."""
         from tenet import linalg, ops
 
         if to != 0:
             raise NotImplementedError("only to=0 (right-canonical) is implemented")
         for n in range(len(self) - 1, 0, -1):
-            u, s, q = linalg.svd_truncated(self[n], ((0,), (1, 2)), max_bond=1 << 60)
+            left, q = linalg.lq(self[n], ((0,), (1, 2)))
             self[n] = q
-            self[n - 1] = ops.einsum("apx,xy->apy", self[n - 1], ops.einsum("ax,xy->ay", u, s))
+            self[n - 1] = ops.einsum("apx,xy->apy", self[n - 1], left)
         self[0] = self[0] / ops.norm(self[0])
         self.center = to
         return self

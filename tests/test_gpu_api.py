@@ -109,9 +109,8 @@ def test_excited_state_is_orthogonal_to_the_ground_state():
 
 
 def test_canonize_leaves_right_orthonormal_sites():
-    """``canonize_`` (the device SVD split, every value kept): each site n >= 1 is a
-    right isometry on the bond of min(rows, cols) per sector, and the state is normalised
-    on site 0."""
+    """``canonize_``: each site n >= 1 is a right isometry on the bond of min(rows, cols)
+    per sector, and the state is normalised on site 0."""
     from tenet import ops
 
     L = 10

@@ -151,7 +151,7 @@ def test_residual_correction_of_the_precision_lanczos_vector(golden_dir, precisi
     an order of magnitude and the energy moves to the FP64 solve's."""
     import json
 
-    from tenet import ops
+    from tenet import network, ops
     from tenet.program import heff2_folded_program
     from tenet.structure import TensorStructure  # noqa: F401
 
