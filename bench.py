@@ -612,13 +612,17 @@ def serve_stream(args) -> None:
         out["burst"] = serve.summarize(res, time.perf_counter() - t0)
         energies.update({r.rid: r.energy for r in res})
         burst = out["burst"]["solves_per_s"]
+        # each arm's line as soon as it is done (a long stream may outlast its time limit)
+        print(json.dumps({"serve_stream_arm": "burst", **out["burst"]}), flush=True)
         nr = min(n, args.serve_rate_requests or n)
         for frac in (0.5, 0.85):
             stream = serve.request_stream(nr, frac * burst, seed=0)
             t0 = time.perf_counter()
             res = srv.run(stream)
             out[f"poisson_{frac}x"] = serve.summarize(res, time.perf_counter() - t0) | {
-                "arrival_rate_per_s": frac * burst}
+                "arrival_rate_per_s": frac * burst, "requests": nr}
+            print(json.dumps({"serve_stream_arm": f"poisson_{frac}x",
+                              **out[f"poisson_{frac}x"]}), flush=True)
     finally:
         srv.close()
     k = min(args.serve_plain_sample, n)

@@ -486,6 +486,21 @@ int tnb_svd_compact(const int64_t* rows, int64_t n_rows, const double* u, int64_
                     double scale, double* pu, int64_t n_pu, double* ps, int64_t n_ps,
                     double* pv, int64_t n_pv, void* stream);
 
+/*
+ * Blockwise LQ (replaces the per-sector QR loop of `lq`, ops/linalg.py:549-620, which
+ * factors each coupled sector's B^T).  One CTA per sector; `rows` holds n_rows rows of 8
+ * int64 [mb, nb, b_off, l_off, q_off, w_off, 0, 0]: B (mb x nb, row-major) at b + b_off is
+ * factored as B^T = Q R by Householder reflections in LAPACK's convention (dgeqrf/dorgqr:
+ * beta = -sign(alpha) |x|, tau = (beta - alpha) / beta, tau = 0 when nothing lies below
+ * the diagonal), giving L = R^T (mb x k) at l + l_off and Q^T (k x nb) at q + q_off,
+ * k = min(mb, nb), both row-major.  The work area (nb*mb + nb*k + 2k doubles) is dynamic
+ * shared memory when w_off < 0 (smem_doubles <= tnb_block_svd_smem_doubles()), else
+ * work + w_off.  Bounds are checked per row (TNB_EBOUNDS on the device word).
+ */
+int tnb_block_lq(const int64_t* rows, int64_t n_rows, const double* b, int64_t n_b,
+                 double* l, int64_t n_l, double* q, int64_t n_q, double* work, int64_t n_work,
+                 int64_t smem_doubles, void* stream);
+
 /* Library version (major*10000 + minor*100 + patch). */
 int tnb_version(void);
 

@@ -470,3 +470,147 @@ extern "C" int tnb_svd_compact(const int64_t* rows, int64_t n_rows, const double
       rows, n_rows, u, n_u, s, n_s, vt, n_vt, scale, pu, n_pu, ps, n_ps, pv, n_pv);
   return tnb::check_launch("tnb_svd_compact");
 }
+
+// ---------------------------------------------------------------------------------------
+// Blockwise LQ: the reference's `lq` per coupled sector (ops/linalg.py:549-620), which
+// takes the QR of the transpose.  One CTA per sector B (mb x nb, row-major): W = B^T is
+// factorised by Householder reflections in LAPACK's convention (dlarfg: beta =
+// -sign(alpha) |x|, tau = (beta - alpha) / beta, v(0) = 1; a column with nothing below the
+// diagonal gets tau = 0), Q is accumulated backwards from the identity (dorgqr), and the
+// outputs are L = R^T (mb x k) and Q^T (k x nb), k = min(mb, nb), both row-major, so the
+// gauge is the one the reference's LAPACK QR gives.  The reflector's norm is formed as
+// dlapy2 forms it, so a sector whose sub-diagonal part is one element (every sector of a
+// multiplicity-one start state) gets LAPACK's bits exactly.
+
+namespace tnb {
+
+constexpr int kQrRow = 8;  // mb, nb, b_off, l_off, q_off, w_off, 0, 0
+
+__global__ void __launch_bounds__(kSvdThreads)
+block_lq_kernel(const int64_t* __restrict__ rows, int64_t n_rows, const double* __restrict__ b,
+                int64_t n_b, double* __restrict__ lout, int64_t n_l, double* __restrict__ qout,
+                int64_t n_q, double* __restrict__ work, int64_t n_work, int64_t smem_doubles) {
+  extern __shared__ __align__(16) double qr_smem[];
+  __shared__ double red[kSvdWarps];
+  const int64_t blk = blockIdx.x;
+  if (blk >= n_rows) return;
+  const int64_t* row = rows + blk * kQrRow;
+  const int64_t mb = row[0], nb = row[1], b_off = row[2], l_off = row[3], q_off = row[4],
+                w_off = row[5];
+  const int64_t m = nb, n = mb;                 // W = B^T: m x n
+  const int64_t k = m < n ? m : n;
+  const bool ok = mb >= 0 && nb >= 0 && b_off >= 0 && b_off + mb * nb <= n_b && l_off >= 0 &&
+                  l_off + mb * k <= n_l && q_off >= 0 && q_off + k * nb <= n_q &&
+                  (w_off >= 0 ? w_off + m * n + m * k + 2 * k <= n_work
+                              : m * n + m * k + 2 * k <= smem_doubles);
+  if (!ok) {
+    if (threadIdx.x == 0) raise_bounds();
+    return;
+  }
+  if (k == 0) return;
+  double* W = w_off >= 0 ? work + w_off : qr_smem;  // column j at W + j * m
+  double* Q = W + m * n;                             // column j at Q + j * m
+  double* tau = Q + m * k;
+  double* beta = tau + k;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int64_t e = tid; e < m * n; e += kSvdThreads) {
+    const int64_t j = e / m, i = e % m;  // W[i][j] = B[j][i]
+    W[e] = b[b_off + j * nb + i];
+  }
+  __syncthreads();
+  for (int64_t j = 0; j < k; ++j) {
+    double* wj = W + j * m;
+    double x2 = 0.0;
+    for (int64_t i = j + 1 + tid; i < m; i += kSvdThreads) x2 = fma(wj[i], wj[i], x2);
+    x2 = cta_sum(x2, red);
+    const double alpha = wj[j];
+    double t = 0.0, bt = alpha, scale = 0.0;
+    if (x2 > 0.0) {
+      // |(alpha, x)| as LAPACK forms it: xnorm = |x|, then dlapy2(alpha, xnorm) =
+      // w sqrt(1 + (z / w)^2) with w = max, z = min, each operation rounded on its own
+      const double xnorm = sqrt(x2), aa = fabs(alpha);
+      const double w = fmax(aa, xnorm), z = fmin(aa, xnorm);
+      const double q = z / w;
+      const double nrm = z == 0.0 ? w : __dmul_rn(w, sqrt(__dadd_rn(1.0, __dmul_rn(q, q))));
+      bt = alpha >= 0.0 ? -nrm : nrm;
+      t = (bt - alpha) / bt;
+      scale = 1.0 / (alpha - bt);
+    }
+    __syncthreads();  // every thread has read alpha
+    if (x2 > 0.0)
+      for (int64_t i = j + 1 + tid; i < m; i += kSvdThreads) wj[i] *= scale;
+    if (tid == 0) {
+      tau[j] = t;
+      beta[j] = bt;
+    }
+    __syncthreads();
+    if (t != 0.0) {
+      // H = I - tau v v^T (v = [1, wj[j+1..]]) on the trailing columns, a warp per column
+      for (int64_t c = j + 1 + warp; c < n; c += kSvdWarps) {
+        double* wc = W + c * m;
+        double d = lane == 0 ? wc[j] : 0.0;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) d = fma(wj[i], wc[i], d);
+        d = warp_sum(d) * t;
+        if (lane == 0) wc[j] -= d;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) wc[i] = fma(-d, wj[i], wc[i]);
+      }
+    }
+    __syncthreads();
+  }
+  // Q = H_0 ... H_{k-1} [I_k; 0], applied from the last reflection back (dorgqr)
+  for (int64_t e = tid; e < m * k; e += kSvdThreads) Q[e] = (e / m == e % m) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int64_t j = k - 1; j >= 0; --j) {
+    const double t = tau[j];
+    if (t != 0.0) {
+      const double* wj = W + j * m;
+      for (int64_t c = j + warp; c < k; c += kSvdWarps) {
+        double* qc = Q + c * m;
+        double d = lane == 0 ? qc[j] : 0.0;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) d = fma(wj[i], qc[i], d);
+        d = warp_sum(d) * t;
+        if (lane == 0) qc[j] -= d;
+        for (int64_t i = j + 1 + lane; i < m; i += 32) qc[i] = fma(-d, wj[i], qc[i]);
+      }
+    }
+    __syncthreads();
+  }
+  // L = R^T (mb x k): L[i][p] = R[p][i] = W[p][i] for p < i, beta on the diagonal
+  for (int64_t e = tid; e < mb * k; e += kSvdThreads) {
+    const int64_t i = e / k, p = e % k;
+    lout[l_off + e] = p < i ? W[i * m + p] : (p == i ? beta[p] : 0.0);
+  }
+  // Q^T (k x nb): Qt[p][c] = Q[c][p]
+  for (int64_t e = tid; e < k * nb; e += kSvdThreads) {
+    const int64_t p = e / nb, c = e % nb;
+    qout[q_off + e] = Q[p * m + c];
+  }
+}
+
+static PerDeviceOnce g_lq_opt;
+
+}  // namespace tnb
+
+extern "C" int tnb_block_lq(const int64_t* rows, int64_t n_rows, const double* b, int64_t n_b,
+                            double* l, int64_t n_l, double* q, int64_t n_q, double* work,
+                            int64_t n_work, int64_t smem_doubles, void* stream) {
+  TNB_REQUIRE(n_rows >= 0 && n_b >= 0 && n_l >= 0 && n_q >= 0 && n_work >= 0,
+              "tnb_block_lq: negative size");
+  TNB_REQUIRE(smem_doubles >= 0 && smem_doubles <= tnb_block_svd_smem_doubles(),
+              "tnb_block_lq: shared-memory request beyond the limit");
+  if (n_rows == 0) return TNB_OK;
+  TNB_REQUIRE(rows && b && l && q && (n_work == 0 || work), "tnb_block_lq: null pointer");
+  TNB_REQUIRE(n_rows < (1ll << 31), "tnb_block_lq: too many sectors");
+  cudaError_t e = tnb::g_lq_opt.once([] {
+    return cudaFuncSetAttribute(tnb::block_lq_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tnb::kSvdSmemMaxBytes - 1024));
+  });
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_block_lq: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  tnb::block_lq_kernel<<<static_cast<unsigned>(n_rows), tnb::kSvdThreads,
+                         static_cast<size_t>(smem_doubles) * 8, tnb::as_stream(stream)>>>(
+      rows, n_rows, b, n_b, l, n_l, q, n_q, work, n_work, smem_doubles);
+  return tnb::check_launch("tnb_block_lq");
+}

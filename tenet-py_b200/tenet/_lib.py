@@ -72,6 +72,7 @@ SIGNATURES = {
                                    _vp, _vp, _vp]),
     "tnb_svd_compact": (_i32, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _f64, _vp, _i64,
                                _vp, _i64, _vp, _i64, _vp]),
+    "tnb_block_lq": (_i32, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _vp]),
     "tnb_set_pdl": (_i32, [_i32]),
     "tnb_version": (_i32, []),
     "tnb_last_error": (ctypes.c_char_p, []),

@@ -277,36 +277,72 @@ def singular_values(s: SymmetricTensor) -> dict:
     return out
 
 
+class _LqPlan:
+    """Device table of one lowered structure's blockwise LQ: per coupled sector its shape,
+    the sector's offset in the lowered buffer and in the matrix layouts of ``L`` and
+    ``Q`` (which the kernel writes directly), and its work area (shared memory when it
+    fits)."""
+
+    def __init__(self, m: TensorStructure) -> None:
+        from tenet import _lib
+
+        ml = matrix_layout(m)
+        p = m.provider
+        self.ml = ml
+        bond = GradedSpace.new(p, {p.sector(c): min(ml.shape[c]) for c in ml.sectors})
+        self.sl = TensorStructure((*m.codomain, Leg(bond, IN)))
+        self.sq = TensorStructure((Leg(bond, OUT), *m.domain))
+        ll, lq_ = matrix_layout(self.sl), matrix_layout(self.sq)
+        self.n_l, self.n_q = ll.size, lq_.size
+        smem_max = int(_lib.load().tnb_block_svd_smem_doubles())
+        rows, wo, smem = [], 0, 0
+        for c in sorted(ml.sectors):
+            r, q = ml.shape[c]
+            k = min(r, q)
+            assert ll.shape[c] == (r, k) and lq_.shape[c] == (k, q)
+            need = q * r + q * k + 2 * k
+            if need <= smem_max:
+                w = -1
+                smem = max(smem, need)
+            else:
+                w, wo = wo, wo + need
+            rows.append((r, q, ml.base[c], ll.base[c], lq_.base[c], w, 0, 0))
+        self.n_rows, self.n_w, self.smem = len(rows), wo, smem
+        self.rows = torch.tensor(rows or [(0,) * 8], dtype=torch.int64, device=_exec.device())
+
+
+@cache
+def _lq_plan(m: TensorStructure) -> _LqPlan:
+    return _LqPlan(m)
+
+
 def lq(t: SymmetricTensor, axes=None):
     """``T = L o Q``, the reduced LQ per coupled sector (``ops/linalg.py:549-620``): per
-    sector ``B^T = q r`` on the device, ``L = r^T`` with legs ``(*left, bond IN)`` and
-    ``Q = q^T`` with legs ``(bond OUT, *right)``, bond degeneracy ``min(rows, cols)``."""
+    sector ``B^T = q r``, ``L = r^T`` with legs ``(*left, bond IN)`` and ``Q = q^T`` with
+    legs ``(bond OUT, *right)``, bond degeneracy ``min(rows, cols)``.
+
+    One launch factors every sector (a CTA each) by Householder reflections in LAPACK's
+    convention, so ``L`` and ``Q`` carry the gauge of the reference's QR; the lowering and
+    the two raising gathers are the only other launches."""
+    from tenet import _lib
+
     if axes is None:
         axes = (t.structure.out_axes, t.structure.in_axes)
     outputs, inputs = validate_partition(t.ndim, axes[0], axes[1])
     m, lower = _lower_exec(t.structure, outputs, inputs)
-    ml = matrix_layout(m)
-    buf = torch.empty(ml.size, dtype=torch.float64, device=t.arena.device)
-    lower.run(t.arena, buf)
-    p = t.provider
-    parts = {}
-    for c in ml.sectors:
-        r, q = ml.shape[c]
-        qq, rr = torch.linalg.qr(buf[ml.base[c]:ml.base[c] + r * q].view(r, q).T)
-        parts[c] = (rr.T, qq.T)
-    bond = GradedSpace.new(p, {p.sector(c): min(ml.shape[c]) for c in ml.sectors})
-    sl = TensorStructure((*m.codomain, Leg(bond, IN)))
-    sq = TensorStructure((Leg(bond, OUT), *m.domain))
+    plan = _lq_plan(m)
     dev = t.arena.device
-
-    def assemble(structure, piece):
-        lay = matrix_layout(structure)
-        mbuf = torch.empty(lay.size, dtype=torch.float64, device=dev)
-        for c in lay.sectors:
-            r, q = lay.shape[c]
-            mbuf[lay.base[c]:lay.base[c] + r * q].view(r, q).copy_(piece(c))
-        out = SymmetricTensor.empty(structure)
-        _raise_exec(structure).run(mbuf, out.arena)
-        return out
-
-    return assemble(sl, lambda c: parts[c][0]), assemble(sq, lambda c: parts[c][1])
+    f64 = dict(dtype=torch.float64, device=dev)
+    buf = torch.empty(max(1, plan.ml.size), **f64)
+    lower.run(t.arena, buf)
+    lbuf = torch.empty(max(1, plan.n_l), **f64)
+    qbuf = torch.empty(max(1, plan.n_q), **f64)
+    work = torch.empty(max(1, plan.n_w), **f64)
+    P = _exec.ptr
+    _lib.call("tnb_block_lq", P(plan.rows), plan.n_rows, P(buf), buf.numel(), P(lbuf),
+              lbuf.numel(), P(qbuf), qbuf.numel(), P(work), plan.n_w, plan.smem,
+              _exec.stream_ptr())
+    out_l, out_q = SymmetricTensor.empty(plan.sl), SymmetricTensor.empty(plan.sq)
+    _raise_exec(plan.sl).run(lbuf, out_l.arena)
+    _raise_exec(plan.sq).run(qbuf, out_q.arena)
+    return out_l, out_q

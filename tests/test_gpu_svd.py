@@ -5,7 +5,10 @@ both factors isometric and the product reconstructing the matrix to 1e-13; exact
 rank-deficient sectors (zero rows, zero columns, rank one) still give orthonormal
 factors; sectors too large for shared memory take the global work path.  The decision
 kernel is compared with the host restatement of the reference's keep rule (``decide``)
-on seeded spectra with ties across sectors, in every cutoff mode and both budgets."""
+on seeded spectra with ties across sectors, in every cutoff mode and both budgets.  The
+blockwise LQ is compared element by element with NumPy's LAPACK QR of each transpose (the
+reference's gauge), through both work paths, and bit for bit on the one-row sectors of a
+multiplicity-one start state."""
 
 import numpy as np
 import pytest
@@ -98,6 +101,79 @@ def test_block_svd_rank_deficient_and_graded_spectra():
     # high relative accuracy down the spectrum, as far as the input's own rounding allows
     assert np.abs(s - want).max() <= 1e-13
     assert np.all(np.abs(s[:25] - want[:25]) <= 1e-9 * want[:25])
+
+
+def _lq_batch(mats, force_global=False):
+    smax = int(_lib.load().tnb_block_svd_smem_doubles())
+    rows, parts, b_off, lo, qo, wo, smem = [], [], 0, 0, 0, 0, 0
+    for b in mats:
+        mb, nb = b.shape
+        k = min(mb, nb)
+        need = nb * mb + nb * k + 2 * k
+        if need <= smax and not force_global:
+            w, smem = -1, max(smem, need)
+        else:
+            w, wo = wo, wo + need
+        rows.append((mb, nb, b_off, lo, qo, w, 0, 0))
+        parts.append(b.ravel())
+        b_off, lo, qo = b_off + b.size, lo + mb * k, qo + k * nb
+    dev = "cuda"
+    B = torch.tensor(np.concatenate(parts), device=dev)
+    L, Q = (torch.full((max(1, x),), np.nan, dtype=torch.float64, device=dev) for x in (lo, qo))
+    W = torch.zeros(max(1, wo), dtype=torch.float64, device=dev)
+    R = torch.tensor(rows, dtype=torch.int64, device=dev)
+    _lib.call("tnb_block_lq", P(R), len(rows), P(B), B.numel(), P(L), L.numel(), P(Q),
+              Q.numel(), P(W), wo, smem, _exec.stream_ptr())
+    torch.cuda.synchronize()
+    assert _lib.device_error(0) == 0
+    L, Q = L.cpu().numpy(), Q.cpu().numpy()
+    out = []
+    for (mb, nb, _, lo, qo, _, _, _) in rows:
+        k = min(mb, nb)
+        out.append((L[lo:lo + mb * k].reshape(mb, k), Q[qo:qo + k * nb].reshape(k, nb)))
+    return out
+
+
+def test_block_lq_matches_lapack_gauge():
+    rng = np.random.default_rng(5)
+    shapes = [(1, 1), (1, 6), (6, 1), (7, 3), (3, 7), (22, 22), (30, 50), (64, 64), (100, 40),
+              (40, 100), (200, 180)]
+    mats = [rng.standard_normal(sh) for sh in shapes]
+    for force in (False, True):
+        for b, (lf, qf) in zip(mats, _lq_batch(mats, force_global=force)):
+            q, r = np.linalg.qr(b.T)  # LAPACK dgeqrf + dorgqr
+            scale = max(np.abs(b).max(), 1e-300)
+            assert np.abs(lf - r.T).max() <= 1e-12 * scale, b.shape
+            assert np.abs(qf - q.T).max() <= 1e-12, b.shape
+            assert np.abs(lf @ qf - b).max() <= 1e-13 * scale
+
+
+def test_block_lq_one_row_sectors_bit_exact():
+    """A 1 x 2 sector (every sector of a start state with one multiplet per bond spin):
+    one reflection whose norm is formed as LAPACK's dlapy2 forms it, so L and Q equal
+    NumPy's QR of the transpose bit for bit."""
+    rng = np.random.default_rng(7)
+    mats = [rng.standard_normal((1, 2)) * 10.0 ** rng.uniform(-3, 6) for _ in range(400)]
+    for b, (lf, qf) in zip(mats, _lq_batch(mats)):
+        q, r = np.linalg.qr(b.T)
+        assert np.array_equal(lf, r.T) and np.array_equal(qf, q.T), b
+
+
+def test_block_lq_rank_deficient():
+    """Zero rows or columns and rank one: the factors still reconstruct the block and Q
+    stays a right isometry."""
+    rng = np.random.default_rng(6)
+    zero_rows = rng.standard_normal((9, 12))
+    zero_rows[[2, 7], :] = 0.0
+    zero_cols = rng.standard_normal((8, 5))
+    zero_cols[:, [0, 3]] = 0.0
+    rank_one = np.outer(rng.standard_normal(10), rng.standard_normal(7))
+    mats = [zero_rows, zero_cols, rank_one, np.zeros((4, 3))]
+    for b, (lf, qf) in zip(mats, _lq_batch(mats)):
+        k = min(b.shape)
+        assert np.abs(qf @ qf.T - np.eye(k)).max() <= 1e-13
+        assert np.abs(lf @ qf - b).max() <= 1e-13 * max(np.abs(b).max(), 1.0)
+        assert np.all(np.triu(lf, 1) == 0.0)
 
 
 @pytest.mark.parametrize("mode", ["abs", "rel", "sum2", "rsum2", "sum1", "rsum1"])
