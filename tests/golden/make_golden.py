@@ -17,7 +17,9 @@ here is the reference's own output on seeded inputs:
 * ``heff.npz`` + ``heff.json``: one SU(2) Heisenberg two-site ``Env.heff2`` application on a
   mid-chain bond (site-tensor path), its Lanczos ground energy at ``ncv=20``, and the
   truncated SVD of the result;
-* ``dmrg.json``: reference DMRG energies and per-bond kept sectors;
+* ``dmrg.json``: reference DMRG energies and per-bond kept sectors, and the spread of the
+  reference's own first-sweep energy when its canonised start is perturbed at the
+  rounding level (the ``spread`` part);
 * ``dmrg64.json``: the L = 64, chi = 256 SU(2) Heisenberg DMRG (site-tensor and prepared
   paths) with its per-sweep history and final bond spaces;
 * ``ctmrg.json``: Z2 Ising CTMRG (beta = 0.44 at chi = 16 and 128 for a fixed number of
@@ -281,6 +283,55 @@ def make_dmrg() -> dict:
     return runs
 
 
+def make_first_sweep_spread(runs: dict, samples: int = 60) -> None:
+    """The reference's own sensitivity of a growth sweep to rounding: its first-sweep
+    energy when every element of the canonised start (``MPS.canonize_``) is multiplied by
+    ``1 + r eps`` with r ~ N(0, 1) and eps alternating 1e-14 and 1e-13 (the size of a
+    different summation order), over ``samples`` seeds.  The sweeps that still grow the
+    bonds solve spaces smaller than ncv = 20 with an unreorthogonalised Lanczos, whose Ritz
+    vector then carries amplified rounding, and a truncation decision near the cutoff can
+    follow it.  Stores ``first_sweep_spread`` (the largest |dE|/L seen) in each run."""
+    import numpy as np
+
+    from tenet import GradedSpace
+    from tenet.models import spin_half
+    from tenet.network import MPO, MPS, dmrg_
+    from tenet.symmetry import SU2, SU2Sector
+
+    site = spin_half(SU2)
+    canonize = MPS.canonize_
+    for rec in runs.values():
+        L, chi = rec["L"], rec["chi"]
+        h = MPO.from_terms(L, [(1.0, [(site.ops["S.S"], (i, i + 1))]) for i in range(L - 1)])
+        h = h.materialize()
+        bonds = [GradedSpace.new(SU2, {SU2Sector(j): 1 for j in range(i % 2, min(i, L - i) + 1, 2)})
+                 for i in range(L + 1)]
+
+        def first(seed, eps, L=L, chi=chi, h=h, bonds=bonds):
+            def noisy(self, *a, **k):
+                out = canonize(self, *a, **k)
+                rng = np.random.default_rng(seed)
+                for n in range(L):
+                    for b in self[n].blocks:
+                        flat = np.asarray(b).reshape(-1)
+                        flat *= 1.0 + eps * rng.standard_normal(flat.size)
+                return out
+
+            MPS.canonize_ = noisy
+            try:
+                out = dmrg_(MPS.random(site.phys, bonds, seed=0), h, chi=chi, max_sweeps=1,
+                            ncv=20, cutoff=1e-10)
+            finally:
+                MPS.canonize_ = canonize
+            return float(out.history[0][0])
+
+        e0 = rec["history"][0]
+        spread = max(abs(first(100 + s, 1e-14 if s % 2 else 1e-13) - e0) / L
+                     for s in range(samples))
+        rec["first_sweep_spread"] = spread
+        rec["first_sweep_spread_samples"] = samples
+
+
 def make_dmrg64(ref: Path) -> dict:
     """The SU(2) Heisenberg chain at L = 64 through the reference's own ``dmrg_``
     (``network/dmrg.py:620-843``): ``chi = 256`` in the reference's dense sense, cutoff
@@ -384,7 +435,7 @@ def make_f_sample(ref: Path) -> None:
 def main() -> None:
     if len(sys.argv) not in (2, 3):
         raise SystemExit("usage: python tests/golden/make_golden.py <path to the TeNeT-py tree>"
-                         " [dmrg64 | su2tables]")
+                         " [dmrg64 | su2tables | spread]")
     ref = Path(sys.argv[1])
     _setup(ref)
     if len(sys.argv) == 3:  # one part alone
@@ -392,6 +443,10 @@ def main() -> None:
             (HERE / "dmrg64.json").write_text(json.dumps(make_dmrg64(ref)))
         elif sys.argv[2] == "su2tables":
             make_su2_tables(ref)
+        elif sys.argv[2] == "spread":
+            runs = json.loads((HERE / "dmrg.json").read_text())
+            make_first_sweep_spread(runs)
+            (HERE / "dmrg.json").write_text(json.dumps(runs, indent=1))
         else:
             raise SystemExit(f"unknown part {sys.argv[2]!r}")
         return
@@ -402,7 +457,9 @@ def main() -> None:
     hs = Store()
     hs.meta = make_heff(hs)
     hs.dump("heff")
-    (HERE / "dmrg.json").write_text(json.dumps(make_dmrg(), indent=1))
+    runs = make_dmrg()
+    make_first_sweep_spread(runs)
+    (HERE / "dmrg.json").write_text(json.dumps(runs, indent=1))
     (HERE / "ctmrg.json").write_text(json.dumps(make_ctmrg(ref)))
     (HERE / "dmrg64.json").write_text(json.dumps(make_dmrg64(ref)))
     make_f_sample(ref)

@@ -518,12 +518,15 @@ def test_heisenberg_mpo_matches_reference_site_tensors(golden_dir):
 def test_dmrg_su2_matches_reference(golden_dir, run, fold):
     """Full two-site DMRG on the GPU against the reference's own run (``dmrg_`` at
     ncv = 20, cutoff 1e-10, same seeded start): the same number of sweeps, every kept
-    bond space identical, every sweep's energy within 1e-8 per site and the last one
-    within 1e-10 relative.  (The sweeps that still grow the bonds solve each bond by
-    Lanczos at ncv = 20 without reorthogonalisation, whose Ritz value moves at the 1e-9
-    level with the summation order of the matvec; the converged sweeps do not.)  Both
-    matvec forms: the folded two-contraction one (default) and the reference's
-    four-contraction order."""
+    bond space identical, every sweep after the first within 1e-8 per site and the last
+    one within 1e-10 relative.  The first sweep grows the bonds from one multiplet per
+    spin: it solves spaces smaller than ncv = 20 with an unreorthogonalised Lanczos, whose
+    Ritz vector then carries amplified rounding, and a truncation near the cutoff can
+    follow it.  The reference itself moves that sweep's energy by up to
+    ``first_sweep_spread`` per site (2.1e-7 at L = 12) when its canonised start changes at
+    the rounding level (``make_golden.py ... spread``, 60 seeds); the first sweep is held
+    to five times that.  Both matvec forms: the folded two-contraction one (default) and
+    the reference's four-contraction order."""
     g = json.loads((golden_dir / "dmrg.json").read_text())[run]
     L, chi = g["L"], g["chi"]
     phys = GradedSpace.new(SU2, {SU2.sector(1): 1})
@@ -533,8 +536,9 @@ def test_dmrg_su2_matches_reference(golden_dir, run, fold):
     out = network.dmrg_(psi, network.heisenberg_mpo_su2(L), chi=chi, cutoff=1e-10,
                         ncv=20, max_sweeps=g["sweeps"], fold=fold)
     assert out.sweeps == g["sweeps"] and out.psi is psi
-    for got, want in zip(out.history, g["history"]):
-        assert abs(got[0] - want) / L <= 1e-8
+    first_tol = max(1e-8, 5.0 * g["first_sweep_spread"])
+    for k, (got, want) in enumerate(zip(out.history, g["history"])):
+        assert abs(got[0] - want) / L <= (first_tol if k == 0 else 1e-8), k
     assert out.energy == pytest.approx(g["history"][-1], rel=1e-10)
     kept = [[[SU2.label(a), k] for a, k in psi[i].legs[0].space.sectors] for i in range(L)]
     assert kept == g["bonds"], "kept bond sectors differ from the reference's"
