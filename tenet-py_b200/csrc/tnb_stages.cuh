@@ -66,30 +66,7 @@ struct GatherSmem {
   int64_t row[TNB_SEG_WIDTH];
   int64_t t_src[kStagedTerms], t_ld[kStagedTerms], t_prod[kStagedTerms];
   double t_cf[kStagedTerms];
-  uint32_t dmul[TNB_MAX_RANK], dshr[TNB_MAX_RANK];  // the row's dims as fast divisors
 };
-
-// Division by a divisor fixed for a whole row, as a multiply and a shift (Granlund and
-// Montgomery, "Division by invariant integers using multiplication", 1994): for d >= 2
-// with l = ceil(log2 d) and p = 31 + l, m = ceil(2^p / d) is below 2^32 and m d - 2^p <=
-// d - 1 < 2^l = 2^(p - 31), so floor(n m / 2^p) = floor(n / d) for every n < 2^31.  d <= 1
-// is marked by m = 0 (the quotient is n).
-__device__ __forceinline__ void make_divisor(uint32_t d, uint32_t& mul, uint32_t& shr) {
-  if (d <= 1) {
-    mul = 0;
-    shr = 0;
-    return;
-  }
-  const int l = 32 - __clz(d - 1);
-  const int p = 31 + l;
-  mul = static_cast<uint32_t>(((1ull << p) + d - 1) / d);
-  shr = static_cast<uint32_t>(l - 1);
-}
-
-// floor(n / d) for n < 2^31 from make_divisor's (mul, shr).
-__device__ __forceinline__ uint32_t fast_div(uint32_t n, uint32_t mul, uint32_t shr) {
-  return mul ? __umulhi(n, mul) >> shr : n;
-}
 
 // C[m, n] of a product-source gather, computed as the FP64 GEMM kernels compute it: one
 // FMA chain over k from zero, so the value is bit-identical to the materialised product.
@@ -147,9 +124,6 @@ __device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSm
   int64_t roff[KE], coff[KE], doff[KE];
   bool live[KE];
   double acc[KE];
-  // element indices of a row below 2^31 (every row a table builder makes) take the
-  // multiply-shift division; larger ones the hardware sequence
-  const bool fast = ge.lim <= (int64_t(1) << 31);
 #pragma unroll
   for (int k = 0; k < KE; ++k) {
     const int64_t e = ge.base + tid + k * NT;
@@ -159,9 +133,8 @@ __device__ __forceinline__ void gather_elems(const GatherArgs& g, const GatherSm
 #pragma unroll
     for (int d = TNB_MAX_RANK - 1; d >= 0; --d) {
       if (d < rank) {
-        const uint32_t q = fast ? fast_div(rem, sm.dmul[d], sm.dshr[d]) : rem / dims[d];
-        const uint32_t j = rem - q * dims[d];
-        rem = q;
+        const uint32_t j = rem % dims[d];
+        rem /= dims[d];
         dd += static_cast<int64_t>(j) * dstr[d];
         rr += static_cast<int64_t>(j) * rstr[d];
         cc += static_cast<int64_t>(j) * cstr[d];
@@ -314,8 +287,7 @@ template <int NT, bool kFused, class Sync, bool kProd = false, bool kRelease = t
 __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm, int tid,
                              Sync sync) {
   static_assert(!(kFused && kProd), "product-source gathers run standalone only");
-  static_assert(NT >= TNB_SEG_WIDTH && NT >= kStagedTerms + TNB_MAX_RANK,
-                "a group stages a row, its terms and its divisors");
+  static_assert(NT >= TNB_SEG_WIDTH && NT >= kStagedTerms, "a group stages a row and its terms");
   if constexpr (kFused) sync();  // the previous item's readers are done with sm
   const int64_t seg = g.chunk_map[chunk];
   if (seg < 0 || seg >= g.n_seg) {
@@ -325,10 +297,6 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   if (tid < TNB_SEG_WIDTH) sm.row[tid] = g.segs[seg * TNB_SEG_WIDTH + tid];
   sync();
   const bool ok = stage_terms<kProd>(g, sm, tid);
-  if (tid >= kStagedTerms && tid < kStagedTerms + TNB_MAX_RANK) {
-    const int d = tid - kStagedTerms;
-    make_divisor(static_cast<uint32_t>(sm.row[8 + d]), sm.dmul[d], sm.dshr[d]);
-  }
   sync();
   if (!ok) {
     if (tid == 0) raise_bounds();

@@ -235,10 +235,11 @@ class DeviceLanczos:
         self._host_state = torch.zeros(3 * ncv + 2, dtype=torch.float64).pin_memory()
         self._host_coef = torch.zeros(ncv, dtype=torch.float64).pin_memory()
         if self.residual:
-            self.R = torch.zeros(max(n, 1), **f64)
-            self.W3 = torch.zeros(max(n, 1), **f64)
-            self.dots = torch.zeros(5, **f64)
-            self._host_dots = torch.zeros(5, dtype=torch.float64).pin_memory()
+            # residual r, its image Hr, the previous direction p and Hp, and a scratch
+            self.R, self.W3, self.Pd, self.HP, self.T = (
+                torch.zeros(max(n, 1), **f64) for _ in range(5))
+            self.dots = torch.zeros(12, **f64)
+            self._host_dots = torch.zeros(12, dtype=torch.float64).pin_memory()
 
     def launch(self, x: torch.Tensor) -> None:
         """Enqueue the recurrence from start vector ``x`` (an arena of ``n`` doubles)."""
@@ -297,40 +298,77 @@ class DeviceLanczos:
         _lib.call("tnb_weighted_dot", P(x), P(y), self.n, P(r.start), P(r.weight), r.n_runs,
                   P(self.work), P(self.dots) + 8 * k, _exec.stream_ptr())
 
+    #: FP64 refinement steps after a reduced-precision solve, and the relative residual
+    #: ``|Hx - theta x| / |theta|`` at which they stop early
+    REFINE_STEPS = 4
+    REFINE_TOL = 1e-12
+
     def _residual_step(self, out: SymmetricTensor) -> tuple[float, SymmetricTensor]:
-        """The FP64 residual correction of the reduced-precision Ritz vector: with ``x``
-        the normalised Ritz vector, ``Hx`` its FP64 image (already formed by the Ritz
-        call) and ``r = Hx - <x, Hx> x`` the FP64 residual, the lowest Ritz pair of the
-        FP64 operator on span{x, r} (one more FP64 matvec, a 2 x 2 generalised eigenproblem
-        on the host).  The vector error drops from the reduced-precision solve's first
-        order to second order in it, and the energy with it; a residual already below
-        ``1e-14`` relative leaves the pair as it is."""
+        """The FP64 residual correction of the reduced-precision Ritz vector: locally
+        optimal block-free steps (Knyazev's LOBPCG with one vector) in FP64.  With ``x`` the
+        normalised Ritz vector, ``Hx`` its FP64 image (formed by the Ritz call) and ``r =
+        Hx - theta x`` the FP64 residual, each step takes the lowest Ritz pair of the FP64
+        operator on span{x, r, p} (``p`` the previous step's direction; span{x, r} on the
+        first step): one FP64 matvec (``H r``; ``H x`` and ``H p`` follow by linearity) and
+        a 3 x 3 generalised eigenproblem on the host.  Up to ``REFINE_STEPS`` steps, ending
+        once the relative residual is below ``REFINE_TOL``; a basis that has become
+        numerically dependent drops ``p``, then stops."""
         from tenet import ops
 
-        x, hx = out.arena, self.W2
+        x, hx, r, hr, p, hp, t = out.arena, self.W2, self.R, self.W3, self.Pd, self.HP, self.T
         theta = float(self.scal[1].item())
-        ops.axpby_into(1.0, hx, -theta, x, self.R)
-        self.correct.run(self.R, self.W3)
-        for k, (a, b) in enumerate(((hx, self.R), (self.R, self.W3), (x, self.R),
-                                    (self.R, self.R), (x, x))):
-            self._dot(a, b, k)
-        self._host_dots.copy_(self.dots)
-        h12, h22, s12, s22, s11 = (float(v) for v in self._host_dots.numpy())
-        if not s22 > 1e-28 * max(s11, 1e-300):
-            return theta, out
-        h = np.array([[theta * s11, h12], [h12, h22]])
-        sm = np.array([[s11, s12], [s12, s22]])
-        try:
-            import scipy.linalg
+        have_p = False
+        for _ in range(self.REFINE_STEPS):
+            ops.axpby_into(1.0, hx, -theta, x, r)
+            self.correct.run(r, hr)
+            pairs = [(x, x), (x, hx), (x, r), (r, r), (r, hx), (r, hr)]
+            if have_p:
+                pairs += [(x, p), (r, p), (p, p), (x, hp), (r, hp), (p, hp)]
+            for k, (a, b) in enumerate(pairs):
+                self._dot(a, b, k)
+            self._host_dots.copy_(self.dots)
+            d = self._host_dots.numpy()
+            sxx, hxx, sxr, srr, hrx, hrr = (float(v) for v in d[:6])
+            if not srr > 0.0 or srr ** 0.5 <= self.REFINE_TOL * abs(theta) * sxx ** 0.5:
+                break
+            A = [[hxx, hrx], [hrx, hrr]]
+            B = [[sxx, sxr], [sxr, srr]]
+            if have_p:
+                sxp, srp, spp, hxp, hrp, hpp = (float(v) for v in d[6:12])
+                A = [[hxx, hrx, hxp], [hrx, hrr, hrp], [hxp, hrp, hpp]]
+                B = [[sxx, sxr, sxp], [sxr, srr, srp], [sxp, srp, spp]]
+            lam = c = None
+            try:
+                import scipy.linalg
 
-            lam, vec = scipy.linalg.eigh(h, sm)
-        except Exception:  # a numerically singular pair: keep the uncorrected one
-            return theta, out
-        c = vec[:, 0]
-        ops.axpby_into(float(c[0]), x, float(c[1]), self.R, x)
-        norm = float(ops.norm(out))
-        ops.axpby_into(1.0 / norm, x, 0.0, x, x)
-        return float(lam[0]), out
+                lam, vec = scipy.linalg.eigh(np.array(A), np.array(B))
+                c = vec[:, 0]
+            except Exception:  # numerically dependent: retry without p, else stop
+                if not have_p:
+                    break
+                have_p = False
+                continue
+            if not np.isfinite(lam[0]) or lam[0] > theta + 1e-14 * abs(theta):
+                break  # the span holds x, so a larger value is rounding: keep the pair
+            c1, c2 = float(c[1]), float(c[2]) if have_p else 0.0
+            # p <- c1 r + c2 p and Hp likewise; x <- c0 x + p and Hx likewise
+            if have_p:
+                ops.axpby_into(c1, r, c2, p, t)
+                ops.axpby_into(c1, hr, c2, hp, hp)
+                p, t = t, p
+            else:
+                ops.axpby_into(c1, r, 0.0, r, p)
+                ops.axpby_into(c1, hr, 0.0, hr, hp)
+            self.Pd, self.T = p, t
+            c0 = float(c[0])
+            ops.axpby_into(c0, x, 1.0, p, x)
+            ops.axpby_into(c0, hx, 1.0, hp, hx)
+            nrm = float(ops.norm(out))
+            ops.axpby_into(1.0 / nrm, x, 0.0, x, x)
+            ops.axpby_into(1.0 / nrm, hx, 0.0, hx, hx)
+            theta = float(lam[0])
+            have_p = True
+        return theta, out
 
     def solve(self, v: SymmetricTensor) -> tuple[float, SymmetricTensor]:
         if v.structure != self.program.in_struct:
