@@ -234,6 +234,7 @@ class DeviceLanczos:
         self.runs = ops._runs(s)
         self._host_state = torch.zeros(3 * ncv + 2, dtype=torch.float64).pin_memory()
         self._host_coef = torch.zeros(ncv, dtype=torch.float64).pin_memory()
+        self._uses, self._graph, self._x0 = 0, None, None
         if self.residual:
             # residual r, its image Hr, the previous direction p and Hp, and a scratch
             self.R, self.W3, self.Pd, self.HP, self.T = (
@@ -241,8 +242,11 @@ class DeviceLanczos:
             self.dots = torch.zeros(12, **f64)
             self._host_dots = torch.zeros(12, dtype=torch.float64).pin_memory()
 
-    def launch(self, x: torch.Tensor) -> None:
-        """Enqueue the recurrence from start vector ``x`` (an arena of ``n`` doubles)."""
+    #: replay a solve from a CUDA graph once the same solver runs a second time (a bond
+    #: whose structure came back in the next sweep); a solver used once runs eagerly
+    GRAPH = True
+
+    def _solve_call(self, x: torch.Tensor) -> None:
         from tenet import _exec, _lib
 
         P, p, r = _exec.ptr, self.program, self.runs
@@ -251,6 +255,34 @@ class DeviceLanczos:
                   self.V.stride(0), P(self.W), P(self.state), P(self.scal),
                   P(self.ptrs), P(self.gs), P(r.start), P(r.weight), r.n_runs, P(self.work),
                   P(self.mwork), _exec.stream_ptr())
+
+    def launch(self, x: torch.Tensor) -> None:
+        """Enqueue the recurrence from start vector ``x`` (an arena of ``n`` doubles).  The
+        first call launches its ~9 ncv kernels one by one; from the second on, the whole
+        solve -- every buffer it touches is this solver's own and fixed -- is one graph
+        launch after a copy of ``x`` into the solver's start buffer."""
+        if not (self.GRAPH and self._uses) or self._graph is False:
+            self._uses += 1
+            self._solve_call(x)
+            return
+        if self._graph is None:
+            self._x0 = torch.empty_like(self.W)
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream()
+            try:
+                with torch.cuda.stream(side):
+                    g.capture_begin(capture_error_mode="thread_local")
+                    try:
+                        self._solve_call(self._x0)
+                    finally:
+                        g.capture_end()
+            except RuntimeError:  # a stream that cannot be captured: stay eager
+                self._graph = False
+                return self.launch(x)
+            self._graph = g
+        self._x0[:self.n].copy_(x.reshape(-1)[:self.n])
+        self._graph.replay()
+        self._uses += 1
 
     def tridiagonal(self) -> tuple[np.ndarray, np.ndarray]:
         """Ground eigenpair of the recorded tridiagonal (one synchronising read)."""

@@ -612,6 +612,31 @@ def test_device_lanczos_matches_reference(golden_dir):
     assert e60 == pytest.approx(network.lanczos(prog, T["aa"], ncv=60)[0], rel=1e-10)
 
 
+def test_device_lanczos_graph_replay_is_bit_identical(golden_dir):
+    """From its second solve on, a solver replays the whole recurrence from a CUDA graph:
+    the same energy and Ritz vector bits as its first (eager) solve, from another start
+    vector too, and as a solver that never captures."""
+    from tenet.program import heff2_program
+
+    m = json.loads((golden_dir / "heff.json").read_text())
+    h = np.load(golden_dir / "heff.npz")
+    T = {k: load(h, m[k]) for k in ("aa", "fl", "fr", "w1", "w2")}
+    prog = heff2_program(T["fl"], T["w1"], T["w2"], T["fr"], T["aa"].structure)
+    from tenet import ops
+
+    other = ops.add(T["aa"] * 0.5, tenet.SymmetricTensor.random(T["aa"].legs, seed=11) * 0.1)
+    lg = network.DeviceLanczos(prog, 20)
+    runs = [lg.solve(v) for v in (T["aa"], T["aa"], other, T["aa"])]
+    assert lg._graph not in (None, False)
+    eager = network.DeviceLanczos(prog, 20)
+    eager.GRAPH = False
+    want = {0: eager.solve(T["aa"]), 2: eager.solve(other)}
+    for k, (e, v) in enumerate(runs):
+        we, wv = want[2 if k == 2 else 0]
+        assert e == we
+        assert np.array_equal(v.numpy_arena(), wv.numpy_arena())
+
+
 def test_multi_dot_and_reorth_kernels():
     """The reorthogonalisation primitives through the C ABI against NumPy."""
     import ctypes
