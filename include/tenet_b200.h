@@ -268,6 +268,20 @@ int tnb_lanczos_next(int64_t n, const double* w, double* vnext, double* state, i
 int tnb_scale_rsqrt(int64_t n, const double* s2, const double* x, double* out, void* stream);
 
 /*
+ * The whole of step j after the matvec for a vector of n <= tnb_lanczos_step_max_n()
+ * doubles, in one launch of one CTA: alpha_j = <v_j, w> into state + j, the update,
+ * ||w||^2 into state + 2 ncv + j and the stop decision with v_{j+1} (vnext) -- what
+ * tnb_weighted_dot, tnb_lanczos_update, tnb_weighted_dot and tnb_lanczos_next do in five
+ * launches, with their arithmetic (for n <= 2048 the same bits).  Once `state` says the
+ * recurrence stopped it only zeroes vnext.  tnb_lanczos_solve takes it for such vectors
+ * when it does not reorthogonalise.
+ */
+int64_t tnb_lanczos_step_max_n(void);
+int tnb_lanczos_step(int64_t n, double* w, const double* v, const double* vprev, double* vnext,
+                     double* state, int32_t j, int32_t ncv, double tol, const int64_t* run_start,
+                     const double* run_w, int64_t n_runs, void* stream);
+
+/*
  * FP64 reorthogonalisation for the precision form (no counterpart in the reference,
  * whose Lanczos is not reorthogonalised): tnb_multi_dot writes out[j] = <vecs[j], x>
  * (qdim-weighted, runs as tnb_weighted_dot) for j < k in one pass with caller scratch of

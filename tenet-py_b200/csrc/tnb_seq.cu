@@ -597,10 +597,17 @@ extern "C" int tnb_lanczos_solve(const tnb_seq* matvec, const void* x_slot, cons
   TNB_TRY(tnb_weighted_dot(x0, x0, n, run_start, run_w, n_runs, dot_work, scal, stream));
   TNB_TRY(tnb_scale_rsqrt(n, scal, x0, v, stream));
   const void* from[2] = {x_slot, y_slot};
+  // a vector one CTA can carry takes each step's five vector launches as one
+  const bool one_cta = !reorth && n <= tnb_lanczos_step_max_n();
   for (int32_t j = 0; j < ncv; ++j) {
     double* vj = v + static_cast<int64_t>(j) * ldv;
     void* to[2] = {vj, w};
     TNB_TRY(tnb::replay(matvec, 2, from, to, s));
+    if (one_cta) {
+      TNB_TRY(tnb_lanczos_step(n, w, vj, j ? vj - ldv : nullptr, vj + ldv, state, j, ncv, tol,
+                               run_start, run_w, n_runs, stream));
+      continue;
+    }
     TNB_TRY(tnb_weighted_dot(vj, w, n, run_start, run_w, n_runs, dot_work, state + j, stream));
     TNB_TRY(tnb_lanczos_update(n, w, vj, j ? vj - ldv : nullptr, state, j, ncv, stream));
     if (reorth) {

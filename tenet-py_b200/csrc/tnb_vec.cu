@@ -16,6 +16,8 @@ namespace tnb {
 constexpr int kDotThreads = 256;
 constexpr int64_t kDotMaxCtas = 4 * 148;
 constexpr int64_t kDotMinChunk = 2048;
+// longest vector whose Lanczos step runs as one CTA (tnb_lanczos_step)
+constexpr int64_t kLanczosStepMaxN = 4 * kDotMinChunk;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -168,6 +170,70 @@ __global__ void lanczos_record_kernel(double* state, int j, int ncv, double tol)
   } else if (stop_now) {
     state[3 * ncv] = static_cast<double>(j + 1);
     state[3 * ncv + 1] = 1.0;
+  }
+}
+
+// Sum of w_r * sum_i x_i y_i over the runs of [0, n), by one CTA of kDotThreads, in the
+// order wdot_kernel takes over one chunk covering the whole vector (so for n up to
+// kDotMinChunk -- one chunk -- the value is the standalone dot's, bit for bit).  Valid in
+// every thread.
+__device__ double cta_weighted_dot(const double* x, const double* y, int64_t n,
+                                   const int64_t* __restrict__ run_start,
+                                   const double* __restrict__ run_w, int64_t n_runs,
+                                   double* bcast) {
+  double acc = 0.0;
+  for (int64_t r = 0; r < n_runs && run_start[r] < n; ++r) {
+    const int64_t a = run_start[r];
+    const int64_t b = min(n, run_start[r + 1]);
+    double s = 0.0;
+    for (int64_t i = a + threadIdx.x; i < b; i += kDotThreads) s = fma(x[i], y[i], s);
+    acc = fma(run_w[r], s, acc);
+  }
+  const double total = block_sum(acc);
+  if (threadIdx.x == 0) *bcast = total + 0.0;  // as the standalone dot's final reduction
+  __syncthreads();
+  const double v = *bcast;
+  __syncthreads();
+  return v;
+}
+
+// One whole step j of the recurrence after the matvec (w = H v_j) for a vector small
+// enough for one CTA: alpha_j = <v_j, w>, the update, ||w||^2 and the next vector with
+// the stop decision -- the work of five launches (tnb_weighted_dot, tnb_lanczos_update,
+// tnb_weighted_dot, tnb_lanczos_next) in one, with the same arithmetic and state words.
+__global__ void __launch_bounds__(kDotThreads)
+lanczos_step_kernel(int64_t n, double* w, const double* v, const double* vprev, double* vnext,
+                    double* state, int j, int ncv, double tol,
+                    const int64_t* __restrict__ run_start, const double* __restrict__ run_w,
+                    int64_t n_runs) {
+  __shared__ double bcast;
+  if (state[3 * ncv + 1] != 0.0) {  // the recurrence already stopped
+    for (int64_t i = threadIdx.x; i < n; i += kDotThreads) vnext[i] = 0.0;
+    return;
+  }
+  const double a = cta_weighted_dot(v, w, n, run_start, run_w, n_runs, &bcast);
+  const double b = j > 0 ? state[ncv + j - 1] : 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += kDotThreads) {
+    double x = __dsub_rn(w[i], __dmul_rn(v[i], a));
+    if (j > 0) x = __dsub_rn(x, __dmul_rn(vprev[i], b));
+    w[i] = x;
+  }
+  __syncthreads();
+  const double nrm2 = cta_weighted_dot(w, w, n, run_start, run_w, n_runs, &bcast);
+  const double beta = sqrt(fmax(nrm2, 0.0));
+  const bool stop_now = j + 1 == ncv || beta < tol;
+  for (int64_t i = threadIdx.x; i < n; i += kDotThreads)
+    vnext[i] = stop_now ? 0.0 : __ddiv_rn(w[i], beta);
+  if (threadIdx.x == 0) {
+    state[j] = a;
+    state[2 * ncv + j] = nrm2;
+    if (stop_now) {
+      state[3 * ncv] = static_cast<double>(j + 1);
+      state[3 * ncv + 1] = 1.0;
+    } else {
+      state[ncv + j] = beta;
+      state[3 * ncv] = static_cast<double>(j + 2);
+    }
   }
 }
 
@@ -515,4 +581,20 @@ extern "C" int tnb_lincomb(int64_t n, int64_t k, const double* coeffs,
   tnb::lincomb_kernel<<<tnb::elementwise_grid(n), 256, 0, tnb::as_stream(stream)>>>(n, k, coeffs,
                                                                                     vecs, out);
   return tnb::check_launch("tnb_lincomb");
+}
+
+extern "C" int64_t tnb_lanczos_step_max_n(void) { return tnb::kLanczosStepMaxN; }
+
+extern "C" int tnb_lanczos_step(int64_t n, double* w, const double* v, const double* vprev,
+                                double* vnext, double* state, int32_t j, int32_t ncv,
+                                double tol, const int64_t* run_start, const double* run_w,
+                                int64_t n_runs, void* stream) {
+  TNB_REQUIRE(n > 0 && n <= tnb::kLanczosStepMaxN && j >= 0 && ncv > 0 && j < ncv &&
+                  n_runs > 0,
+              "tnb_lanczos_step: bad size or step");
+  TNB_REQUIRE(w && v && vnext && state && run_start && run_w && (j == 0 || vprev),
+              "tnb_lanczos_step: null pointer");
+  tnb::lanczos_step_kernel<<<1, tnb::kDotThreads, 0, tnb::as_stream(stream)>>>(
+      n, w, v, vprev, vnext, state, j, ncv, tol, run_start, run_w, n_runs);
+  return tnb::check_launch("tnb_lanczos_step");
 }

@@ -39,6 +39,9 @@ SIGNATURES = {
     "tnb_lanczos_update": (_i32, [_i64, _vp, _vp, _vp, _vp, _i32, _i32, _vp]),
     "tnb_lanczos_next": (_i32, [_i64, _vp, _vp, _vp, _i32, _i32, _f64, _vp]),
     "tnb_scale_rsqrt": (_i32, [_i64, _vp, _vp, _vp, _vp]),
+    "tnb_lanczos_step_max_n": (_i64, []),
+    "tnb_lanczos_step": (_i32, [_i64, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _f64, _vp, _vp, _i64,
+                                _vp]),
     "tnb_multi_dot_work_bytes": (_i64, [_i64, _i64]),
     "tnb_multi_dot": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp]),
     "tnb_lanczos_reorth": (_i32, [_i64, _i64, _vp, _vp, _vp, _vp, _i32, _vp]),

@@ -243,8 +243,11 @@ class DeviceLanczos:
             self._host_dots = torch.zeros(12, dtype=torch.float64).pin_memory()
 
     #: replay a solve from a CUDA graph once the same solver runs a second time (a bond
-    #: whose structure came back in the next sweep); a solver used once runs eagerly
-    GRAPH = True
+    #: whose structure came back in the next sweep); a solver used once runs eagerly.
+    #: Off by default: capturing and instantiating a solve's graph took ~6 ms on B200
+    #: against ~0.6 ms of launches saved per replay, and a DMRG solve reuses a bond's
+    #: solver about six times (L = 64 warm solve 1.65 s with it, 1.53 s without)
+    GRAPH = False
 
     def _solve_call(self, x: torch.Tensor) -> None:
         from tenet import _exec, _lib

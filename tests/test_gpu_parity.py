@@ -613,9 +613,10 @@ def test_device_lanczos_matches_reference(golden_dir):
 
 
 def test_device_lanczos_graph_replay_is_bit_identical(golden_dir):
-    """From its second solve on, a solver replays the whole recurrence from a CUDA graph:
-    the same energy and Ritz vector bits as its first (eager) solve, from another start
-    vector too, and as a solver that never captures."""
+    """With ``GRAPH`` on, from its second solve on a solver replays the whole recurrence
+    from a CUDA graph: the same energy and Ritz vector bits as its first (eager) solve,
+    from another start vector too, and as a solver that never captures.  The step kernel that carries the
+    recurrence for small vectors (``tnb_lanczos_step``) runs in both."""
     from tenet.program import heff2_program
 
     m = json.loads((golden_dir / "heff.json").read_text())
@@ -626,6 +627,7 @@ def test_device_lanczos_graph_replay_is_bit_identical(golden_dir):
 
     other = ops.add(T["aa"] * 0.5, tenet.SymmetricTensor.random(T["aa"].legs, seed=11) * 0.1)
     lg = network.DeviceLanczos(prog, 20)
+    lg.GRAPH = True
     runs = [lg.solve(v) for v in (T["aa"], T["aa"], other, T["aa"])]
     assert lg._graph not in (None, False)
     eager = network.DeviceLanczos(prog, 20)
@@ -635,6 +637,58 @@ def test_device_lanczos_graph_replay_is_bit_identical(golden_dir):
         we, wv = want[2 if k == 2 else 0]
         assert e == we
         assert np.array_equal(v.numpy_arena(), wv.numpy_arena())
+
+
+@pytest.mark.parametrize("n", [1500, 6000])
+def test_lanczos_step_kernel_against_the_five_launches(n):
+    """``tnb_lanczos_step`` (one CTA) against tnb_weighted_dot + tnb_lanczos_update +
+    tnb_weighted_dot + tnb_lanczos_next on the same state: bit-identical while the dots
+    are one chunk (n <= 2048), within rounding beyond; also the stop at j + 1 == ncv and
+    the zero vector once stopped."""
+    lib = _lib.load()
+    P = lambda t: t.data_ptr()  # noqa: E731
+    g = torch.Generator(device="cuda").manual_seed(5)
+    v, vp, w0 = (torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+                 for _ in range(3))
+    starts = torch.tensor([0, n // 3, n // 2, n], dtype=torch.int64, device="cuda")
+    weights = torch.tensor([1.0, 3.0, 2.0], dtype=torch.float64, device="cuda")
+    ncv, j = 8, 3
+    st0 = torch.zeros(3 * ncv + 2, dtype=torch.float64, device="cuda")
+    st0[ncv + j - 1] = 0.7
+    work = torch.zeros(int(lib.tnb_dot_work_bytes(n)), dtype=torch.uint8, device="cuda")
+    outs = []
+    for fused in (False, True):
+        st, w = st0.clone(), w0.clone()
+        nxt = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+        if fused:
+            _lib.call("tnb_lanczos_step", n, P(w), P(v), P(vp), P(nxt), P(st), j, ncv, 1e-13,
+                      P(starts), P(weights), 3, None)
+        else:
+            _lib.call("tnb_weighted_dot", P(v), P(w), n, P(starts), P(weights), 3, P(work),
+                      P(st) + 8 * j, None)
+            _lib.call("tnb_lanczos_update", n, P(w), P(v), P(vp), P(st), j, ncv, None)
+            _lib.call("tnb_weighted_dot", P(w), P(w), n, P(starts), P(weights), 3, P(work),
+                      P(st) + 8 * (2 * ncv + j), None)
+            _lib.call("tnb_lanczos_next", n, P(w), P(nxt), P(st), j, ncv, 1e-13, None)
+        torch.cuda.synchronize()
+        outs.append((st.cpu().numpy(), w.cpu().numpy(), nxt.cpu().numpy()))
+    (s1, w1, x1), (s2, w2, x2) = outs
+    if n <= 2048:
+        assert np.array_equal(s1, s2) and np.array_equal(w1, w2) and np.array_equal(x1, x2)
+    else:
+        assert np.allclose(s1, s2, rtol=1e-13, atol=0) and np.abs(x1 - x2).max() < 1e-13
+    assert s2[3 * ncv] == j + 2 and s2[3 * ncv + 1] == 0.0
+    # the last step stops; a stopped recurrence only zeroes the next vector
+    st, w = st0.clone(), w0.clone()
+    nxt = torch.ones(n, dtype=torch.float64, device="cuda")
+    _lib.call("tnb_lanczos_step", n, P(w), P(v), P(vp), P(nxt), P(st), ncv - 1, ncv, 1e-13,
+              P(starts), P(weights), 3, None)
+    _lib.call("tnb_lanczos_step", n, P(w), P(v), P(vp), P(nxt), P(st), ncv - 1, ncv, 1e-13,
+              P(starts), P(weights), 3, None)
+    torch.cuda.synchronize()
+    assert st[3 * ncv].item() == ncv and st[3 * ncv + 1].item() == 1.0
+    assert (nxt == 0).all()
+    assert lib.tnb_lanczos_step_max_n() >= 6000
 
 
 def test_multi_dot_and_reorth_kernels():
