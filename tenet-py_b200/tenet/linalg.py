@@ -159,6 +159,7 @@ class _SvdPlan:
         self.h_sorted = h[self.o_sorted:self.o_info].view(np.float64)
         self.h_info = h[self.o_info:self.o_csec].view(np.int32)
         self.h_csec = h[self.o_csec:self.o_csec + 4 * T].view(np.int32)
+        self.post: dict = {}  # kept counts -> truncated structures and compaction table
 
 
 @cache
@@ -242,19 +243,28 @@ def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cuto
     nk = int(n_kept)
     kept = [(float(x) * scale, plan.sectors[int(k)])
             for x, k in zip(plan.h_sorted[:nk], plan.h_csec[:nk])]
-    bond = GradedSpace.new(p, {p.sector(c): k for c, k in keep.items()})
-    su = TensorStructure((*m.codomain, Leg(bond, IN)))
-    ss = TensorStructure((Leg(bond, OUT), Leg(bond, IN)))
-    sv = TensorStructure((Leg(bond, OUT), *m.domain))
-    lu, ls, lv = matrix_layout(su), matrix_layout(ss), matrix_layout(sv)
-    rows = []
-    for c, k in keep.items():
-        kf, uo, so, vo = plan.kfull[c]
-        r, q = ml.shape[c]
-        rows.append((r, q, kf, k, uo, so, vo, lu.base[c], ls.base[c], lv.base[c], 0, 0))
-    PU, PS, PV = (torch.empty(max(1, x.size), **f64) for x in (lu, ls, lv))
-    crows = torch.tensor(rows, dtype=torch.int64).pin_memory().to(dev, non_blocking=True)
-    _lib.call("tnb_svd_compact", P(crows), len(rows), P(U), U.numel(), P(Sv), Sv.numel(), P(V),
+    # the truncated structures and the compaction table depend on the kept counts only:
+    # a bond that keeps what it kept before (every converged sweep) reuses them
+    post = plan.post.get(tuple(keep.items()))
+    if post is None:
+        bond = GradedSpace.new(p, {p.sector(c): k for c, k in keep.items()})
+        su = TensorStructure((*m.codomain, Leg(bond, IN)))
+        ss = TensorStructure((Leg(bond, OUT), Leg(bond, IN)))
+        sv = TensorStructure((Leg(bond, OUT), *m.domain))
+        lu, ls, lv = matrix_layout(su), matrix_layout(ss), matrix_layout(sv)
+        rows = []
+        for c, k in keep.items():
+            kf, uo, so, vo = plan.kfull[c]
+            r, q = ml.shape[c]
+            rows.append((r, q, kf, k, uo, so, vo, lu.base[c], ls.base[c], lv.base[c], 0, 0))
+        crows = torch.tensor(rows, dtype=torch.int64, device=dev)
+        post = (su, ss, sv, lu.size, ls.size, lv.size, crows, len(rows))
+        if len(plan.post) >= 64:
+            plan.post.pop(next(iter(plan.post)))
+        plan.post[tuple(keep.items())] = post
+    su, ss, sv, nu, nsz, nv, crows, n_rows = post
+    PU, PS, PV = (torch.empty(max(1, x), **f64) for x in (nu, nsz, nv))
+    _lib.call("tnb_svd_compact", P(crows), n_rows, P(U), U.numel(), P(Sv), Sv.numel(), P(V),
               V.numel(), float(scale), P(PU), PU.numel(), P(PS), PS.numel(), P(PV), PV.numel(),
               st)
     out = []
