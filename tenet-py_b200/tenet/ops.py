@@ -275,34 +275,50 @@ def _parse(equation: str, n: int):
     return terms, out
 
 
+@cache
+def _pair_plan(equation: str, na: int, nb: int):
+    """``(axes, perm)`` of a two-operand equation on operands of ``na`` and ``nb`` axes,
+    validated once (a sweep repeats a handful of equations thousands of times)."""
+    terms, out = _parse(equation, 2)
+    for term, n in zip(terms, (na, nb)):
+        if len(term) != n:
+            raise ValueError(f"einsum: term {term!r} labels {len(term)} axes of a {n}-axis tensor")
+    shared = [x for x in terms[0] if x in terms[1]]
+    axes = (tuple(terms[0].index(x) for x in shared), tuple(terms[1].index(x) for x in shared))
+    free = [x for x in terms[0] if x not in shared] + [x for x in terms[1] if x not in shared]
+    return axes, tuple(free.index(x) for x in out)
+
+
 def einsum(equation: str, *operands: SymmetricTensor, optimize=None) -> SymmetricTensor:
     """Label-equation contraction (``ops/contraction.py:695-794``).  Three or more operands
     are contracted left to right in the caller's order."""
+    if len(operands) == 2:
+        a, b = operands
+        axes, perm = _pair_plan(equation, a.ndim, b.ndim)
+        prec = current_precision()
+        if a.provider.abelian:
+            # one +-1 term per block: the transpose folds into the unpack exactly
+            ex = contraction_exec(a.structure, b.structure, axes, *prec, perm)
+            return SymmetricTensor(ex.out, arena=ex.run(a.arena, b.arena))
+        # SU(2): the unpack and the transpose stay two passes, the reference's order of
+        # roundings (composing their multi-term maps would round the sums differently)
+        ex = contraction_exec(a.structure, b.structure, axes, *prec, None)
+        return transpose(SymmetricTensor(ex.out, arena=ex.run(a.arena, b.arena)), perm)
     terms, out = _parse(equation, len(operands))
     for term, t in zip(terms, operands):
         if len(term) != t.ndim:
             raise ValueError(f"einsum: term {term!r} labels {len(term)} axes of a {t.ndim}-axis tensor")
     if len(operands) == 1:
         return transpose(operands[0], tuple(terms[0].index(x) for x in out))
-    if len(operands) > 2:
-        keep = set(out)
-        acc, at = operands[0], terms[0]
-        for k in range(1, len(operands)):
-            later = keep.union(*map(set, terms[k + 1:]))
-            mid = "".join([x for x in at if x in later] + [x for x in terms[k] if x in later])
-            acc = einsum(f"{at},{terms[k]}->{mid}", acc, operands[k])
-            at = mid
-        return transpose(acc, tuple(at.index(x) for x in out))
-    shared = [x for x in terms[0] if x in terms[1]]
-    axes = (tuple(terms[0].index(x) for x in shared), tuple(terms[1].index(x) for x in shared))
-    free = [x for x in terms[0] if x not in shared] + [x for x in terms[1] if x not in shared]
-    perm = tuple(free.index(x) for x in out)
-    if operands[0].provider.abelian:
-        # one +-1 term per block: the transpose folds into the unpack exactly
-        return tensordot(operands[0], operands[1], axes, perm)
-    # SU(2): the unpack and the transpose stay two passes, the reference's order of
-    # roundings (composing their multi-term maps would round the sums differently)
-    return transpose(tensordot(operands[0], operands[1], axes), perm)
+    # three or more operands
+    keep = set(out)
+    acc, at = operands[0], terms[0]
+    for k in range(1, len(operands)):
+        later = keep.union(*map(set, terms[k + 1:]))
+        mid = "".join([x for x in at if x in later] + [x for x in terms[k] if x in later])
+        acc = einsum(f"{at},{terms[k]}->{mid}", acc, operands[k])
+        at = mid
+    return transpose(acc, tuple(at.index(x) for x in out))
 
 
 # ---------------------------------------------------------------------------------------
