@@ -482,3 +482,20 @@ def test_gather_csr_reproduces_the_gather_element_by_element():
             srcs[1] = rng.standard_normal(lk.c_size)
         if bond == bench.BOND:
             assert p.launches == 3
+
+
+def test_two_operand_einsum_plan_and_its_refusals():
+    """The cached two-operand plan: shared labels contracted in the first operand's order,
+    the output order of the free labels; every malformed equation still refused, and
+    refused again on a repeat (a refusal is never cached)."""
+    from tenet import ops
+
+    axes, perm = ops._pair_plan("apx,xy->apy", 3, 2)
+    assert axes == ((2,), (0,)) and perm == (0, 1, 2)
+    axes, perm = ops._pair_plan("apmQs,aBPpm->BPQs", 5, 5)
+    assert axes == ((0, 1, 2), (0, 3, 4)) and perm == (2, 3, 0, 1)
+    for eq, na, nb in (("ab,bc->ac", 3, 2), ("a.b,bc->ac", 2, 2), ("ab,bb->a", 2, 2),
+                       ("ab,bc->a", 2, 2), ("ab,bc,cd->ad", 2, 2)):
+        for _ in range(2):
+            with pytest.raises(ValueError):
+                ops._pair_plan(eq, na, nb)
