@@ -90,6 +90,25 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
                      void* stream);
 
 /*
+ * The same gather with its table as one row per chunk instead of rows + chunk map: row k
+ * (TNB_CHUNK_ROW_WIDTH int64) is the segment row that chunk k belongs to (all 40 words,
+ * word [6] still that segment's first chunk), then the segment's first term inline --
+ * [40] term_src, [41] the bits of term_coeff, [42] term_ld -- and pad.  A chunk of a
+ * one-term segment (every segment of a U(1) / Z2 / fZ2 map) then reads its whole table in
+ * one round of loads instead of three dependent ones (chunk map, row, terms), which is
+ * what bounds many-wave gathers; segments with more terms read them from the term arrays
+ * as tnb_block_gather does.  Same arithmetic and results, bit for bit.  No counterpart
+ * in the reference (a table layout).
+ */
+#define TNB_CHUNK_ROW_WIDTH 48
+int tnb_block_gather_direct(const int64_t* chunk_rows, int64_t total_chunks,
+                            const int64_t* term_src, const double* term_coeff,
+                            const int64_t* term_ld, int64_t n_term,
+                            const double* src0, int64_t n_src0, double* dst0, int64_t n_dst0,
+                            const double* src1, int64_t n_src1, double* dst1, int64_t n_dst1,
+                            void* stream);
+
+/*
  * Block gather whose source is a product with a short K, never materialised: the source
  * is C = A * B over the grouped-GEMM table prod_table (n_prod rows in the TNB_GEMM_WIDTH
  * layout below, K at most 4).  The segment rows are those of tnb_block_gather, with one

@@ -34,6 +34,15 @@ gather_kernel(const GatherArgs g) {
                                                                          threadIdx.x, CtaSync{});
 }
 
+// The per-chunk-row form (tnb_block_gather_direct), the same two builds.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kGatherThreads, kMinBlocks)
+gather_direct_kernel(const GatherArgs g, const int64_t* __restrict__ chunk_rows) {
+  __shared__ GatherSmem sm;
+  gather_chunk_direct<kGatherThreads, (kMinBlocks == 3)>(g, chunk_rows, blockIdx.x, sm,
+                                                         threadIdx.x);
+}
+
 // SMs of the current device (0 when it cannot be queried), cached per device.
 int device_sms() {
   static PerDeviceInt cached;
@@ -119,4 +128,33 @@ extern "C" int tnb_block_gather_product(const int64_t* seg_table, int64_t n_seg,
     return TNB_ECUDA;
   }
   return tnb::check_launch("tnb_block_gather_product");
+}
+
+extern "C" int tnb_block_gather_direct(const int64_t* chunk_rows, int64_t total_chunks,
+                                       const int64_t* term_src, const double* term_coeff,
+                                       const int64_t* term_ld, int64_t n_term,
+                                       const double* src0, int64_t n_src0, double* dst0,
+                                       int64_t n_dst0, const double* src1, int64_t n_src1,
+                                       double* dst1, int64_t n_dst1, void* stream) {
+  TNB_REQUIRE(total_chunks >= 0 && n_term >= 0, "tnb_block_gather_direct: negative size");
+  if (total_chunks == 0) return TNB_OK;
+  TNB_REQUIRE(chunk_rows != nullptr, "tnb_block_gather_direct: chunk_rows is null");
+  TNB_REQUIRE(n_term == 0 || (term_src != nullptr && term_coeff != nullptr && term_ld != nullptr),
+              "tnb_block_gather_direct: term arrays are null");
+  TNB_REQUIRE(dst0 != nullptr || dst1 != nullptr, "tnb_block_gather_direct: no destination buffer");
+  TNB_REQUIRE(total_chunks < (int64_t(1) << 31),
+              "tnb_block_gather_direct: too many chunks for one launch");
+  const tnb::GatherArgs g{nullptr, 0, nullptr, term_src, term_coeff, term_ld, n_term,
+                          src0, n_src0, dst0, n_dst0, src1, n_src1, dst1, n_dst1};
+  const bool large = total_chunks > 2 * 3 * static_cast<int64_t>(tnb::device_sms());
+  cudaError_t e =
+      large ? tnb::launch(tnb::gather_direct_kernel<4>, static_cast<unsigned>(total_chunks),
+                          tnb::kGatherThreads, tnb::as_stream(stream), g, chunk_rows)
+            : tnb::launch(tnb::gather_direct_kernel<3>, static_cast<unsigned>(total_chunks),
+                          tnb::kGatherThreads, tnb::as_stream(stream), g, chunk_rows);
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_block_gather_direct: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  return tnb::check_launch("tnb_block_gather_direct");
 }

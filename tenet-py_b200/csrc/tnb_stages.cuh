@@ -66,6 +66,7 @@ struct GatherSmem {
   int64_t row[TNB_SEG_WIDTH];
   int64_t t_src[kStagedTerms], t_ld[kStagedTerms], t_prod[kStagedTerms];
   double t_cf[kStagedTerms];
+  int64_t inl[3];  // a per-chunk row's inline first term (tnb_block_gather_direct)
 };
 
 // C[m, n] of a product-source gather, computed as the FP64 GEMM kernels compute it: one
@@ -304,6 +305,45 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   }
   if constexpr (!kFused) pdl_wait<kRelease>();  // tables are static; the source may be the previous kernel's output
   gather_staged<NT, kFused, kProd>(g, chunk, sm, tid);
+}
+
+// One chunk of a gather whose table is a row per chunk (TNB_CHUNK_ROW_WIDTH words: the
+// segment row, then its first term inline): the row and, for a one-term row, its term
+// arrive in one round of independent loads -- no chunk map to read first, no term array
+// to read after.  Rows with more terms stage them as gather_chunk does.  The loads of the
+// static table come before the dependent-launch wait.
+template <int NT, bool kRelease = true>
+__device__ void gather_chunk_direct(const GatherArgs& g, const int64_t* __restrict__ crows,
+                                    int64_t chunk, GatherSmem& sm, int tid) {
+  static_assert(NT >= TNB_CHUNK_ROW_WIDTH && NT >= kStagedTerms,
+                "a CTA stages a chunk row and its terms");
+  const int64_t* cr = crows + chunk * TNB_CHUNK_ROW_WIDTH;
+  if (tid < TNB_SEG_WIDTH) {
+    sm.row[tid] = __ldg(cr + tid);
+  } else if (tid < TNB_SEG_WIDTH + 3) {
+    sm.inl[tid - TNB_SEG_WIDTH] = __ldg(cr + tid);
+  }
+  __syncthreads();
+  const int64_t t0 = sm.row[3], t1 = sm.row[4];
+  const bool ok = t0 >= 0 && t1 <= g.n_term && t0 <= t1;
+  if (ok && t1 - t0 == 1) {
+    if (tid == 0) {
+      sm.t_src[0] = sm.inl[0];
+      sm.t_cf[0] = __longlong_as_double(static_cast<long long>(sm.inl[1]));
+      sm.t_ld[0] = sm.inl[2];
+    }
+  } else if (ok && t1 - t0 <= kStagedTerms && tid < t1 - t0) {
+    sm.t_src[tid] = __ldg(g.term_src + t0 + tid);
+    sm.t_ld[tid] = __ldg(g.term_ld + t0 + tid);
+    sm.t_cf[tid] = __ldg(g.term_coeff + t0 + tid);
+  }
+  __syncthreads();
+  if (!ok) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  pdl_wait<kRelease>();  // the source may be the previous kernel's output
+  gather_staged<NT, false, false>(g, chunk, sm, tid);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -27,6 +27,9 @@ from tenet.structure import TensorStructure, layout, matrix_layout
 
 SEG_W = 40
 GEMM_W = 16
+#: words of a per-chunk gather row (``tnb_block_gather_direct``): the segment row, then
+#: its first term inline
+CHUNK_ROW_W = 48
 CHUNK = 1024
 MAX_RANK = 8
 TILE_64, TILE_32, TILE_SKINNY, TILE_TC_TF32, TILE_TC_3XBF16, TILE_WIDE = 0, 1, 2, 3, 4, 5
@@ -383,6 +386,7 @@ class GatherTable:
         self.term_elems = int((seg[:, 1] * (seg[:, 4] - seg[:, 3])).sum()) if len(seg) else 0
         self.chunk_map = np.repeat(np.arange(len(seg), dtype=np.int32), per)
         self._dev = None
+        self._ddev = None
 
     @property
     def bytes_moved(self) -> int:
@@ -398,11 +402,40 @@ class GatherTable:
             self._dev = Uploaded(self.host_arrays())
         return self._dev.ready()
 
+    def chunk_rows(self) -> np.ndarray:
+        """The table as one ``CHUNK_ROW_W`` row per chunk: the chunk's segment row, then the
+        segment's first term (source, coefficient bits, leading dimension) inline."""
+        rows = np.zeros((self.chunks, CHUNK_ROW_W), dtype=np.int64)
+        if self.chunks:
+            own = self.seg[self.chunk_map]
+            rows[:, :SEG_W] = own
+            has = own[:, 4] > own[:, 3]
+            t0 = own[has, 3]
+            rows[has, SEG_W] = self.tsrc[t0]
+            rows[has, SEG_W + 1] = self.tcf[t0].view(np.int64)
+            rows[has, SEG_W + 2] = self.tld[t0]
+        return rows
+
+    def direct_arrays(self):
+        if self._ddev is None:
+            self._ddev = Uploaded((self.chunk_rows(), self.tsrc, self.tcf, self.tld))
+        return self._ddev.ready()
+
     def run(self, src0, dst0, src1=None, dst1=None) -> None:
         if self.n_seg == 0:
             return
-        seg, tsrc, tcf, tld, cmap = self.device_arrays()
         rec = recording()
+        if rec is None and DIRECT_GATHER and self.chunks >= DIRECT_MIN_CHUNKS:
+            crows, tsrc, tcf, tld = self.direct_arrays()
+            mark = _LOG.begin() if _LOG is not None else None
+            _lib.call("tnb_block_gather_direct", ptr(crows), self.chunks, ptr(tsrc), ptr(tcf),
+                      ptr(tld), self.n_term, ptr(src0), src0.numel(), ptr(dst0), dst0.numel(),
+                      ptr(src1), 0 if src1 is None else src1.numel(),
+                      ptr(dst1), 0 if dst1 is None else dst1.numel(), stream_ptr())
+            if _LOG is not None:
+                _LOG.end("block_gather", mark, self.bytes_moved)
+            return
+        seg, tsrc, tcf, tld, cmap = self.device_arrays()
         if rec is not None:
             _lib.call("tnb_seq_add_gather", rec.handle, ptr(seg), self.n_seg, ptr(cmap),
                       self.chunks, ptr(tsrc), ptr(tcf), ptr(tld), self.n_term,
@@ -419,6 +452,12 @@ class GatherTable:
         if _LOG is not None:
             _LOG.end("block_gather", mark, self.bytes_moved)
 
+
+#: run gathers of at least DIRECT_MIN_CHUNKS chunks (more than two waves of resident
+#: CTAs, where each CTA's table loads are not hidden behind another kernel) from their
+#: per-chunk rows (``tnb_block_gather_direct``): one round of table loads per CTA
+DIRECT_GATHER = True
+DIRECT_MIN_CHUNKS = 2 * 3 * N_SM + 1
 
 #: resident gather CTAs per SM (the kernels' launch bounds): plain, product-source
 GATHER_CTAS_PER_SM = 3

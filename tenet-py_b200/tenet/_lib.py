@@ -21,6 +21,8 @@ _i64, _i32, _f64, _vp = ctypes.c_int64, ctypes.c_int, ctypes.c_double, ctypes.c_
 SIGNATURES = {
     "tnb_block_gather": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
                                 _i64, _vp, _i64, _vp, _i64, _vp]),
+    "tnb_block_gather_direct": (_i32, [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp, _i64,
+                                       _vp, _i64, _vp, _i64, _vp]),
     "tnb_copy_f64": (_i32, [_i64, _vp, _vp, _vp]),
     "tnb_mapped_address": (_i32, [_vp, ctypes.POINTER(_vp)]),
     "tnb_block_gather_product": (_i32, [_vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp,

@@ -71,3 +71,28 @@ def gemm(table, a, b, c):
         out = A @ B
         for m in range(M):
             c[co + m * ldc: co + m * ldc + N] = out[m]
+
+
+def gather_direct(rows, tsrc, tcf, tld, src0, dst0, src1=None, dst1=None, chunk=1024):
+    """``tnb_block_gather_direct`` from its per-chunk rows: each chunk its own slice of its
+    segment, a one-term segment's term taken from the row's inline words."""
+    srcs, dsts = (src0, src1), (dst0, dst1)
+    for k, row in enumerate(rows):
+        dst_off, size, rank, t0, t1, buf, first, ce = (int(x) for x in row[:8])
+        ce = ce or chunk
+        lo, hi = (k - first) * ce, min(size, (k - first + 1) * ce)
+        dims = [int(x) for x in row[8:8 + rank]]
+        dstr, rstr, cstr = (np.array(row[o:o + rank], dtype=np.int64) for o in (16, 24, 32))
+        J = np.indices(dims).reshape(rank, -1)[:, lo:hi]
+        doff = dst_off + (J * dstr[:, None]).sum(0)
+        R = (J * rstr[:, None]).sum(0)
+        C = (J * cstr[:, None]).sum(0)
+        if t1 - t0 == 1:
+            terms = [(int(row[40]), float(np.int64(row[41]).view(np.float64)), int(row[42]))]
+        else:
+            terms = [(int(tsrc[t]), float(tcf[t]), int(tld[t])) for t in range(t0, t1)]
+        acc = np.zeros(J.shape[1])
+        for s, cf, ld in terms:
+            o = s + ld * R + C
+            acc = acc + cf * srcs[buf][o]
+        dsts[buf][doff] = acc

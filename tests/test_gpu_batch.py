@@ -2,6 +2,7 @@
 update on coarsened tensors (``tests/_coarsen.py``), the unbatched device path, and, in
 reduced precision, the FP64 batch."""
 
+import numpy as np
 import pytest
 import torch
 
@@ -91,3 +92,46 @@ def test_batched_heff2_matches_each_member():
         assert out.structure == want.structure == compiled.structure
         assert rel(out[k].numpy_arena(), want.numpy_arena()) <= 1e-13
         assert rel(compiled[k].numpy_arena(), want.numpy_arena()) <= 1e-13
+
+
+def test_per_chunk_row_gathers_are_bit_identical():
+    """``tnb_block_gather_direct`` (a row per chunk, one-term segments' terms inline)
+    against ``tnb_block_gather`` on the same tables: the 64-member U(1) x U(1) x fZ2
+    environment update (its many-wave gathers take the direct form by default) and an
+    SU(2) contraction's multi-term tables forced onto it -- the same bits, and no bounds
+    error."""
+    import bench
+    from tenet import _exec
+    from tenet.structure import layout
+
+    F, A, W = bench.config3_batch(8)
+    outs = []
+    for min_chunks in (10 ** 9, 0):  # never, then every gather from its chunk rows
+        _exec.DIRECT_MIN_CHUNKS, old = min_chunks, _exec.DIRECT_MIN_CHUNKS
+        try:
+            outs.append(batch.env_update_last(F, A, W).arena.cpu().numpy())
+        finally:
+            _exec.DIRECT_MIN_CHUNKS = old
+    assert np.array_equal(outs[0], outs[1])
+
+    fl, w1, w2, fr, aa = bench.build_workload(seed=3, bond=bench.WORKLOADS["L64_cutoff1e-14_mid_bond"])
+    ex = ops.contraction_exec(aa.structure, fr.structure, ((3,), (0,)))
+    assert np.any(ex.pack.seg[:, 4] - ex.pack.seg[:, 3] > 1)  # multi-term segments
+    res = []
+    for min_chunks in (10 ** 9, 0):
+        _exec.DIRECT_MIN_CHUNKS, old = min_chunks, _exec.DIRECT_MIN_CHUNKS
+        try:
+            ap = torch.full((ex.a_mat,), np.nan, dtype=torch.float64, device="cuda")
+            bp = torch.full((ex.b_mat,), np.nan, dtype=torch.float64, device="cuda")
+            ex.pack.run(aa.arena, ap, fr.arena, bp)
+            out = torch.full((layout(ex.out).size,), np.nan, dtype=torch.float64, device="cuda")
+            cp = torch.randn(ex.c_mat, dtype=torch.float64, device="cuda",
+                             generator=torch.Generator(device="cuda").manual_seed(4))
+            ex.unpack.run(cp, out)
+            res.append([t.cpu().numpy() for t in (ap, bp, out)])
+        finally:
+            _exec.DIRECT_MIN_CHUNKS = old
+    torch.cuda.synchronize()
+    assert _lib.device_error(0) == 0
+    for a, b in zip(*res):
+        assert np.array_equal(a, b, equal_nan=True)

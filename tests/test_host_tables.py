@@ -499,3 +499,37 @@ def test_two_operand_einsum_plan_and_its_refusals():
         for _ in range(2):
             with pytest.raises(ValueError):
                 ops._pair_plan(eq, na, nb)
+
+
+def test_per_chunk_gather_rows_reproduce_the_gather():
+    """``GatherTable.chunk_rows`` (the table of ``tnb_block_gather_direct``): executed chunk
+    by chunk from those rows alone -- inline first terms for one-term segments -- the pack
+    and unpack tables of a U(1) x U(1) x fZ2 environment-update contraction and of an SU(2)
+    two-site contraction give the standard gather's result bit for bit, and every chunk
+    row carries its segment's words."""
+    import bench
+    from tenet.structure import IN, OUT, Leg, TensorStructure, layout
+
+    V, M, Pp = bench.config3_spaces(1000, 24.0, 256)
+    sf = TensorStructure((Leg(V, IN), Leg(M, OUT, True), Leg(V, OUT)))
+    sa = TensorStructure((Leg(V, OUT), Leg(Pp, OUT), Leg(V, IN)))
+    fl, w1, w2, fr, aa = bench.workload_structures(bench.WORKLOADS["L64_cutoff1e-14_mid_bond"])
+    rng = np.random.default_rng(9)
+    cases = []
+    for x, y, axes in ((sf, sa, ((0,), (0,))), (aa, fr, ((3,), (0,)))):
+        ex = ops.contraction_exec(x, y, axes)
+        cases.append((ex.pack, (layout(x).size, layout(y).size), (ex.a_mat, ex.b_mat)))
+        cases.append((ex.unpack, (ex.c_mat, 0), (layout(ex.out).size, 0)))
+    for t, (n0, n1), (d0, d1) in cases:
+        rows = t.chunk_rows()
+        assert rows.shape == (t.chunks, _exec.CHUNK_ROW_W)
+        assert np.array_equal(rows[:, :_exec.SEG_W], t.seg[t.chunk_map])
+        srcs = [rng.standard_normal(max(n0, 1)), rng.standard_normal(max(n1, 1))]
+        want = [np.full(max(d0, 1), np.nan), np.full(max(d1, 1), np.nan)]
+        got = [np.full(max(d0, 1), np.nan), np.full(max(d1, 1), np.nan)]
+        two = n1 > 0
+        _emulate.gather(t, srcs[0], want[0], srcs[1] if two else None, want[1] if two else None)
+        _emulate.gather_direct(rows, t.tsrc, t.tcf, t.tld, srcs[0], got[0],
+                               srcs[1] if two else None, got[1] if two else None)
+        for w, g in zip(want, got):
+            assert np.array_equal(w, g, equal_nan=True)
