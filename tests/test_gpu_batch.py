@@ -115,20 +115,16 @@ def test_per_chunk_row_gathers_are_bit_identical():
     assert np.array_equal(outs[0], outs[1])
 
     fl, w1, w2, fr, aa = bench.build_workload(seed=3, bond=bench.WORKLOADS["L64_cutoff1e-14_mid_bond"])
-    ex = ops.contraction_exec(aa.structure, fr.structure, ((3,), (0,)))
-    assert np.any(ex.pack.seg[:, 4] - ex.pack.seg[:, 3] > 1)  # multi-term segments
+    # swapping the two physical legs is an F R F move: segments of several terms
+    dst, table = ops._map_exec(aa.structure, "t", (0, 2, 1, 3), None)
+    assert np.any(table.seg[:, 4] - table.seg[:, 3] > 1)
     res = []
     for min_chunks in (10 ** 9, 0):
         _exec.DIRECT_MIN_CHUNKS, old = min_chunks, _exec.DIRECT_MIN_CHUNKS
         try:
-            ap = torch.full((ex.a_mat,), np.nan, dtype=torch.float64, device="cuda")
-            bp = torch.full((ex.b_mat,), np.nan, dtype=torch.float64, device="cuda")
-            ex.pack.run(aa.arena, ap, fr.arena, bp)
-            out = torch.full((layout(ex.out).size,), np.nan, dtype=torch.float64, device="cuda")
-            cp = torch.randn(ex.c_mat, dtype=torch.float64, device="cuda",
-                             generator=torch.Generator(device="cuda").manual_seed(4))
-            ex.unpack.run(cp, out)
-            res.append([t.cpu().numpy() for t in (ap, bp, out)])
+            out = torch.full((layout(dst).size,), np.nan, dtype=torch.float64, device="cuda")
+            table.run(aa.arena, out)
+            res.append([out.cpu().numpy()])
         finally:
             _exec.DIRECT_MIN_CHUNKS = old
     torch.cuda.synchronize()
