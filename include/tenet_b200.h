@@ -93,14 +93,18 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
  * The same gather with its table as one row per chunk instead of rows + chunk map: row k
  * (TNB_CHUNK_ROW_WIDTH int64) is the segment row that chunk k belongs to (all 40 words,
  * word [6] still that segment's first chunk), then the segment's first term inline --
- * [40] term_src, [41] the bits of term_coeff, [42] term_ld -- and pad.  A chunk of a
+ * [40] term_src, [41] the bits of term_coeff, [42] term_ld -- a pad word, and [48 + d]
+ * the division constant of extent d (mul = ceil(2^(31 + l) / dims[d]) with l =
+ * ceil(log2 dims[d]) in the low 32 bits, l - 1 above them; 0 for an extent of 1), with
+ * which rows of rank <= 4 split element indices by a multiply and a shift (a constant
+ * without the needed property falls back to division).  A chunk of a
  * one-term segment (every segment of a U(1) / Z2 / fZ2 map) then reads its whole table in
  * one round of loads instead of three dependent ones (chunk map, row, terms), which is
  * what bounds many-wave gathers; segments with more terms read them from the term arrays
  * as tnb_block_gather does.  Same arithmetic and results, bit for bit.  No counterpart
  * in the reference (a table layout).
  */
-#define TNB_CHUNK_ROW_WIDTH 48
+#define TNB_CHUNK_ROW_WIDTH 56
 int tnb_block_gather_direct(const int64_t* chunk_rows, int64_t total_chunks,
                             const int64_t* term_src, const double* term_coeff,
                             const int64_t* term_ld, int64_t n_term,

@@ -9,6 +9,8 @@
 // change during a launch and are read through the read-only path in both.
 #pragma once
 
+#include <type_traits>
+
 #include "tnb_common.cuh"
 
 namespace tnb {
@@ -67,6 +69,7 @@ struct GatherSmem {
   int64_t t_src[kStagedTerms], t_ld[kStagedTerms], t_prod[kStagedTerms];
   double t_cf[kStagedTerms];
   int64_t inl[3];  // a per-chunk row's inline first term (tnb_block_gather_direct)
+  int64_t dmag[TNB_MAX_RANK];  // and its extents' division constants
 };
 
 // C[m, n] of a product-source gather, computed as the FP64 GEMM kernels compute it: one
@@ -307,6 +310,172 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   gather_staged<NT, kFused, kProd>(g, chunk, sm, tid);
 }
 
+// floor(n / d) for n < 2^31 from a division constant of a per-chunk row: mul in the low
+// 32 bits, the shift above them, as the host computes them (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", 1994: with l = ceil(log2 d) and
+// p = 31 + l, mul = ceil(2^p / d) < 2^32 and mul d - 2^p < 2^(p - 31), so floor(n mul /
+// 2^p) = floor(n / d) for every n < 2^31); mul = 0 stands for d = 1.
+__device__ __forceinline__ uint32_t magic_div(uint32_t n, int64_t mag) {
+  const uint32_t mul = static_cast<uint32_t>(mag);
+  return mul ? __umulhi(n, mul) >> static_cast<uint32_t>(mag >> 32) : n;
+}
+
+// gather_elems for a row of compile-time rank R with the row's extents, strides and
+// division constants in registers: the same offsets, terms and FMA order.
+template <int R, int KE, int NT>
+__device__ __forceinline__ void gather_elems_rank(const GatherArgs& g, const GatherSmem& sm,
+                                                  const GatherElems& ge, int tid) {
+  uint32_t dims[R];
+  int64_t dstr[R], rstr[R], cstr[R], mag[R];
+#pragma unroll
+  for (int d = 0; d < R; ++d) {
+    dims[d] = static_cast<uint32_t>(sm.row[8 + d]);
+    dstr[d] = sm.row[16 + d];
+    rstr[d] = sm.row[24 + d];
+    cstr[d] = sm.row[32 + d];
+    mag[d] = sm.dmag[d];
+  }
+  // a constant is taken only if it has the property the identity needs (2^p <= mul d <
+  // 2^p + 2^l with l = ceil(log2 d)); otherwise, or past 2^31 elements, hardware division
+  bool mok = true;
+#pragma unroll
+  for (int d = 0; d < R; ++d) {
+    const uint64_t m = static_cast<uint32_t>(mag[d]);
+    const int l = static_cast<int>((mag[d] >> 32) & 63) + 1;
+    if (dims[d] <= 1) {
+      mok = mok && m == 0;
+    } else {
+      const bool lok = l <= 31 && l == 32 - __clz(dims[d] - 1);
+      const uint64_t prod = m * dims[d], two_p = 1ull << (lok ? 31 + l : 0);
+      mok = mok && lok && prod >= two_p && prod - two_p < (1ull << l);
+    }
+  }
+  const bool fast = mok && ge.lim <= (int64_t(1) << 31);
+  int64_t roff[KE], coff[KE], doff[KE];
+  bool live[KE];
+  double acc[KE];
+#pragma unroll
+  for (int k = 0; k < KE; ++k) {
+    const int64_t e = ge.base + tid + k * NT;
+    live[k] = e < ge.lim;
+    uint32_t rem = live[k] ? static_cast<uint32_t>(e) : 0u;
+    int64_t dd = 0, rr = 0, cc = 0;
+#pragma unroll
+    for (int d = R - 1; d >= 0; --d) {
+      const uint32_t q = fast ? magic_div(rem, mag[d]) : rem / dims[d];
+      const uint32_t j = rem - q * dims[d];
+      rem = q;
+      dd += static_cast<int64_t>(j) * dstr[d];
+      rr += static_cast<int64_t>(j) * rstr[d];
+      cc += static_cast<int64_t>(j) * cstr[d];
+    }
+    roff[k] = rr;
+    coff[k] = cc;
+    doff[k] = ge.dst_off + dd;
+    acc[k] = 0.0;
+  }
+  bool bad = false;
+  auto fetch = [&](int64_t ts, int64_t tl, int k) -> double {
+    const int64_t o = ts + tl * roff[k] + coff[k];
+    const bool ok = live[k] && o >= 0 && o < ge.n_src;
+    bad |= live[k] && !ok;
+    return ok ? __ldg(ge.src + o) : 0.0;
+  };
+  auto term = [&](int64_t t, int64_t& ts, int64_t& tl, double& cf) {
+    if (ge.staged) {
+      ts = sm.t_src[t - ge.t0];
+      tl = sm.t_ld[t - ge.t0];
+      cf = sm.t_cf[t - ge.t0];
+    } else {
+      ts = __ldg(g.term_src + t);
+      tl = __ldg(g.term_ld + t);
+      cf = __ldg(g.term_coeff + t);
+    }
+  };
+  // four loads in flight per thread, as gather_elems
+  constexpr int kU = KE >= 4 ? 1 : 4 / KE;
+  int64_t t = ge.t0;
+  for (; t + kU <= ge.t1; t += kU) {
+    int64_t ts[kU], tl[kU];
+    double cf[kU], v[kU][KE];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) term(t + u, ts[u], tl[u], cf[u]);
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+#pragma unroll
+      for (int k = 0; k < KE; ++k) v[u][k] = fetch(ts[u], tl[u], k);
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+#pragma unroll
+      for (int k = 0; k < KE; ++k) acc[k] = fma(cf[u], v[u][k], acc[k]);
+  }
+  for (; t < ge.t1; ++t) {
+    int64_t ts, tl;
+    double cf, v[KE];
+    term(t, ts, tl, cf);
+#pragma unroll
+    for (int k = 0; k < KE; ++k) v[k] = fetch(ts, tl, k);
+#pragma unroll
+    for (int k = 0; k < KE; ++k) acc[k] = fma(cf, v[k], acc[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < KE; ++k) {
+    if (!live[k]) continue;
+    if (doff[k] < 0 || doff[k] >= ge.n_dst) {
+      bad = true;
+      continue;
+    }
+    ge.dst[doff[k]] = acc[k];
+  }
+  if (bad) raise_bounds();
+}
+
+// The chunk of a per-chunk row staged in `sm` (row, terms, division constants): the checks
+// of gather_staged, then rows of rank 1 to 4 through gather_elems_rank, higher ranks
+// through gather_staged itself.
+template <int NT>
+__device__ void gather_direct_staged(const GatherArgs& g, int64_t chunk, const GatherSmem& sm,
+                                     int tid) {
+  constexpr int kEpt = TNB_GATHER_CHUNK / NT;
+  const int64_t* row = sm.row;
+  const int rank = static_cast<int>(row[2]);
+  if (rank > 4) {
+    gather_staged<NT, false, false>(g, chunk, sm, tid);
+    return;
+  }
+  const int64_t size = row[1], t0 = row[3], t1 = row[4];
+  const bool second = row[5] != 0;
+  const int64_t ce = row[7] ? row[7] : TNB_GATHER_CHUNK;
+  if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || ce <= 0 || ce > TNB_GATHER_CHUNK ||
+      ce % kGatherThreads || chunk < row[6] || (chunk - row[6]) * ce >= size) {
+    if (tid == 0) raise_bounds();
+    return;
+  }
+  const int64_t base = (chunk - row[6]) * ce;
+  const GatherElems ge{second ? g.src1 : g.src0, second ? g.dst1 : g.dst0,
+                       second ? g.n_src1 : g.n_src0, second ? g.n_dst1 : g.n_dst0, row[0],
+                       base, min(size, base + ce), t0, t1, t1 - t0 <= kStagedTerms};
+  auto run = [&](auto rank_tag) {
+    constexpr int R = decltype(rank_tag)::value;
+    if (ce <= NT) {
+      gather_elems_rank<R, 1, NT>(g, sm, ge, tid);
+    } else if (ce <= 2 * NT) {
+      gather_elems_rank<R, (2 <= kEpt ? 2 : kEpt), NT>(g, sm, ge, tid);
+    } else {
+      gather_elems_rank<R, kEpt, NT>(g, sm, ge, tid);
+    }
+  };
+  switch (rank) {
+    case 1: run(std::integral_constant<int, 1>{}); break;
+    case 2: run(std::integral_constant<int, 2>{}); break;
+    case 3: run(std::integral_constant<int, 3>{}); break;
+    default: run(std::integral_constant<int, 4>{}); break;
+  }
+}
+
+// word of a per-chunk row where its extents' division constants begin
+constexpr int kChunkRowMagic = 48;
+
 // One chunk of a gather whose table is a row per chunk (TNB_CHUNK_ROW_WIDTH words: the
 // segment row, then its first term inline): the row and, for a one-term row, its term
 // arrive in one round of independent loads -- no chunk map to read first, no term array
@@ -322,6 +491,8 @@ __device__ void gather_chunk_direct(const GatherArgs& g, const int64_t* __restri
     sm.row[tid] = __ldg(cr + tid);
   } else if (tid < TNB_SEG_WIDTH + 3) {
     sm.inl[tid - TNB_SEG_WIDTH] = __ldg(cr + tid);
+  } else if (tid >= kChunkRowMagic && tid < kChunkRowMagic + TNB_MAX_RANK) {
+    sm.dmag[tid - kChunkRowMagic] = __ldg(cr + tid);
   }
   __syncthreads();
   const int64_t t0 = sm.row[3], t1 = sm.row[4];
@@ -343,7 +514,7 @@ __device__ void gather_chunk_direct(const GatherArgs& g, const int64_t* __restri
     return;
   }
   pdl_wait<kRelease>();  // the source may be the previous kernel's output
-  gather_staged<NT, false, false>(g, chunk, sm, tid);
+  gather_direct_staged<NT>(g, chunk, sm, tid);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -27,9 +27,23 @@ from tenet.structure import TensorStructure, layout, matrix_layout
 
 SEG_W = 40
 GEMM_W = 16
-#: words of a per-chunk gather row (``tnb_block_gather_direct``): the segment row, then
-#: its first term inline
-CHUNK_ROW_W = 48
+#: words of a per-chunk gather row (``tnb_block_gather_direct``): the segment row, its
+#: first term inline, a pad word, then its extents' division constants
+CHUNK_ROW_W = 56
+CHUNK_ROW_MAGIC = 48
+
+
+def division_constants(dims: np.ndarray) -> np.ndarray:
+    """Per extent d >= 2: mul = ceil(2^(31 + l) / d), l = ceil(log2 d), packed as mul | (l
+    - 1) << 32 (0 for d <= 1), so that floor(n / d) = (n mul) >> (31 + l) for n < 2^31
+    (Granlund and Montgomery, 1994)."""
+    out = np.zeros(dims.shape, dtype=np.int64)
+    flat, res = dims.reshape(-1), out.reshape(-1)
+    for i, d in enumerate(flat.tolist()):
+        if d >= 2:
+            l = (d - 1).bit_length()
+            res[i] = ((1 << (31 + l)) + d - 1) // d | (l - 1) << 32
+    return out
 CHUNK = 1024
 MAX_RANK = 8
 TILE_64, TILE_32, TILE_SKINNY, TILE_TC_TF32, TILE_TC_3XBF16, TILE_WIDE = 0, 1, 2, 3, 4, 5
@@ -403,8 +417,9 @@ class GatherTable:
         return self._dev.ready()
 
     def chunk_rows(self) -> np.ndarray:
-        """The table as one ``CHUNK_ROW_W`` row per chunk: the chunk's segment row, then the
-        segment's first term (source, coefficient bits, leading dimension) inline."""
+        """The table as one ``CHUNK_ROW_W`` row per chunk: the chunk's segment row, the
+        segment's first term (source, coefficient bits, leading dimension) inline, and the
+        division constants of its extents."""
         rows = np.zeros((self.chunks, CHUNK_ROW_W), dtype=np.int64)
         if self.chunks:
             own = self.seg[self.chunk_map]
@@ -414,6 +429,8 @@ class GatherTable:
             rows[has, SEG_W] = self.tsrc[t0]
             rows[has, SEG_W + 1] = self.tcf[t0].view(np.int64)
             rows[has, SEG_W + 2] = self.tld[t0]
+            mags = division_constants(self.seg[:, 8:8 + 8])
+            rows[:, CHUNK_ROW_MAGIC:CHUNK_ROW_MAGIC + 8] = mags[self.chunk_map]
         return rows
 
     def direct_arrays(self):

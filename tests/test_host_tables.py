@@ -533,3 +533,12 @@ def test_per_chunk_gather_rows_reproduce_the_gather():
                                srcs[1] if two else None, got[1] if two else None)
         for w, g in zip(want, got):
             assert np.array_equal(w, g, equal_nan=True)
+        # the division constants: floor(n / d) by multiply and shift for every n < 2^31
+        mags = rows[:, _exec.CHUNK_ROW_MAGIC:_exec.CHUNK_ROW_MAGIC + 8]
+        for d, mag in zip(rows[:, 8:16].reshape(-1).tolist(), mags.reshape(-1).tolist()):
+            if d <= 1:
+                assert mag == 0
+                continue
+            mul, shr = mag & 0xFFFFFFFF, mag >> 32
+            for n in (0, 1, d - 1, d, 2 ** 31 - 1, *rng.integers(0, 2 ** 31, 8).tolist()):
+                assert ((n * mul) >> 32) >> shr == n // d
