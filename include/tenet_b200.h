@@ -191,6 +191,18 @@ int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm, const int32_
                          int64_t work_bytes, int64_t n_counters, void* stream);
 
 /*
+ * The FP64 tile kinds (TNB_TILE_64 / 32 / SKINNY / WIDE) of tnb_grouped_gemm_f64 with the
+ * table as one TNB_GEMM_WIDTH row per tile -- row t is the row that tile t belongs to,
+ * word [9] still that row's first tile -- instead of rows + tile map: a tile reads its row
+ * in one load instead of two dependent ones.  Same arithmetic, split-K and work buffer, bit
+ * for bit.  No counterpart in the reference (a table layout).
+ */
+int tnb_grouped_gemm_f64_rows(const int64_t* tile_rows, int64_t total_tiles, int32_t tile_kind,
+                              const double* a, int64_t n_a, const double* b, int64_t n_b,
+                              double* c, int64_t n_c, void* work, int64_t work_bytes,
+                              int64_t n_counters, void* stream);
+
+/*
  * A grouped FP64 GEMM whose A operand is a gather evaluated where it is read: the
  * to_matrices / repartition of the left operand (map_view.py:238-279,
  * ops/repartition.py:458-476) and compose's per-sector matmul (ops/map.py:155-172) in

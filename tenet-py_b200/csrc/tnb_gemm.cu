@@ -119,3 +119,49 @@ extern "C" int tnb_grouped_gemm_f64(const int64_t* gemm_table, int64_t n_gemm,
   }
   return tnb::check_launch("tnb_grouped_gemm_f64");
 }
+
+extern "C" int tnb_grouped_gemm_f64_rows(const int64_t* tile_rows, int64_t total_tiles,
+                                         int32_t tile_kind, const double* a, int64_t n_a,
+                                         const double* b, int64_t n_b, double* c, int64_t n_c,
+                                         void* work, int64_t work_bytes, int64_t n_counters,
+                                         void* stream) {
+  TNB_REQUIRE(total_tiles >= 0, "tnb_grouped_gemm_f64_rows: negative size");
+  if (total_tiles == 0) return TNB_OK;
+  TNB_REQUIRE(tile_rows != nullptr && c != nullptr, "tnb_grouped_gemm_f64_rows: null rows or C");
+  TNB_REQUIRE(total_tiles < (int64_t(1) << 31), "tnb_grouped_gemm_f64_rows: too many tiles");
+  TNB_REQUIRE(tile_kind == TNB_TILE_64 || tile_kind == TNB_TILE_32 ||
+                  tile_kind == TNB_TILE_SKINNY || tile_kind == TNB_TILE_WIDE,
+              "tnb_grouped_gemm_f64_rows: FP64 tile kinds only");
+  TNB_REQUIRE(work_bytes >= 0 && n_counters >= 0 && (work_bytes == 0 || work != nullptr) &&
+                  tnb::gemm_work_parts_offset(n_counters) <= work_bytes,
+              "tnb_grouped_gemm_f64_rows: bad work buffer");
+  auto* counters = static_cast<unsigned int*>(work);
+  const int64_t poff = tnb::gemm_work_parts_offset(n_counters);
+  double* parts = work_bytes > poff
+                      ? reinterpret_cast<double*>(static_cast<char*>(work) + poff) : nullptr;
+  const int64_t n_parts = work_bytes > poff ? (work_bytes - poff) / 8 : 0;
+  const unsigned grid = static_cast<unsigned>(total_tiles);
+  cudaStream_t s = tnb::as_stream(stream);
+  const tnb::GemmArgs g{nullptr, total_tiles, nullptr, a, n_a, b, n_b, c, n_c, counters,
+                        n_counters, parts, n_parts, tile_rows};
+  cudaError_t e = cudaSuccess;
+  switch (tile_kind) {
+    case TNB_TILE_64:
+      e = tnb::launch_gemm_f64<64, 64>(grid, s, g);
+      break;
+    case TNB_TILE_32:
+      e = tnb::launch_gemm_f64<32, 32>(grid, s, g);
+      break;
+    case TNB_TILE_SKINNY:
+      e = tnb::launch(tnb::gemm_f64_skinny_kernel, grid, tnb::kSkinnyThreads, s, g);
+      break;
+    default:
+      e = tnb::launch(tnb::gemm_f64_wide_kernel, grid, tnb::kSkinnyThreads, s, g);
+      break;
+  }
+  if (e != cudaSuccess) {
+    tnb::set_error(std::string("tnb_grouped_gemm_f64_rows: ") + cudaGetErrorString(e));
+    return TNB_ECUDA;
+  }
+  return tnb::check_launch("tnb_grouped_gemm_f64_rows");
+}

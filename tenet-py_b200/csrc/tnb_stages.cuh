@@ -544,6 +544,9 @@ struct GemmArgs {
   int64_t n_cnt;
   double* parts;
   int64_t n_parts;
+  // when set, the table as one row per tile (tnb_grouped_gemm_f64_rows): tile t's row at
+  // tile_rows + t * TNB_GEMM_WIDTH, no tile map to read first
+  const int64_t* tile_rows;
 };
 
 struct GemmRow {
@@ -557,6 +560,16 @@ __device__ __forceinline__ bool load_row(const int64_t* __restrict__ table, int6
   const int64_t g = tile_map[tile];
   if (g < 0 || g >= n_gemm) return false;
   const int64_t* t = table + g * TNB_GEMM_WIDTH;
+  r.M = t[0]; r.N = t[1]; r.K = t[2]; r.aoff = t[3]; r.lda = t[4]; r.boff = t[5];
+  r.ldb = t[6]; r.coff = t[7]; r.ldc = t[8]; r.tile_begin = t[9]; r.tiles_n = t[10];
+  r.splits = t[12] > 1 ? t[12] : 1; r.ksplit = t[13]; r.part_off = t[14]; r.cnt_off = t[15];
+  return true;
+}
+
+__device__ __forceinline__ bool load_row(const GemmArgs& g, int64_t tile, GemmRow& r) {
+  if (g.tile_rows == nullptr) return load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+  if (tile < 0 || tile >= g.n_gemm) return false;  // n_gemm holds the tile count here
+  const int64_t* t = g.tile_rows + tile * TNB_GEMM_WIDTH;
   r.M = t[0]; r.N = t[1]; r.K = t[2]; r.aoff = t[3]; r.lda = t[4]; r.boff = t[5];
   r.ldb = t[6]; r.coff = t[7]; r.ldc = t[8]; r.tile_begin = t[9]; r.tiles_n = t[10];
   r.splits = t[12] > 1 ? t[12] : 1; r.ksplit = t[13]; r.part_off = t[14]; r.cnt_off = t[15];
@@ -610,7 +623,7 @@ __device__ void gemm_tile(const GemmArgs& g, int64_t tile, GemmSmem<TM, TN, S>& 
   if constexpr (kFused) sync();  // the previous item's readers are done with sm
   if (tid == 0) {
     GemmRow r;
-    bool ok = load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+    bool ok = load_row(g, tile, r);
     ok = ok && footprint_ok(r, g.n_a, g.n_b, g.n_c);
     if (ok && r.splits > 1) {
       const int64_t nt = ((r.M + TM - 1) / TM) * r.tiles_n;
@@ -805,7 +818,7 @@ __device__ void skinny_tile(const GemmArgs& g, int64_t tile, SkinnySmem& sm, int
   if constexpr (kFused) sync();
   if (tid == 0) {
     GemmRow r;
-    bool ok = load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+    bool ok = load_row(g, tile, r);
     ok = ok && footprint_ok(r, g.n_a, g.n_b, g.n_c) && r.N <= kSkinnyMax && r.K <= kSkinnyMax;
     if (!ok) raise_bounds();
     sm.row = r;
@@ -855,7 +868,7 @@ __device__ inline void wide_tile(const GemmArgs& g, int64_t tile, SkinnySmem& sm
   const int tid = threadIdx.x;
   if (tid == 0) {
     GemmRow r;
-    bool ok = load_row(g.table, g.n_gemm, g.tile_map, tile, r);
+    bool ok = load_row(g, tile, r);
     ok = ok && footprint_ok(r, g.n_a, g.n_b, g.n_c) && r.M <= kSkinnyMax && r.K <= kSkinnyMax;
     if (!ok) raise_bounds();
     sm.row = r;

@@ -475,6 +475,10 @@ class GatherTable:
 #: per-chunk rows (``tnb_block_gather_direct``): one round of table loads per CTA
 DIRECT_GATHER = True
 DIRECT_MIN_CHUNKS = 2 * 3 * N_SM + 1
+#: likewise FP64 grouped GEMMs of at least DIRECT_MIN_TILES tiles from one row per tile
+#: (``tnb_grouped_gemm_f64_rows``): one table load per tile instead of two dependent ones
+DIRECT_GEMM = True
+DIRECT_MIN_TILES = 4 * N_SM
 
 #: resident gather CTAs per SM (the kernels' launch bounds): plain, product-source
 GATHER_CTAS_PER_SM = 3
@@ -638,6 +642,7 @@ class GemmTable:
         per = table[:, 11] if len(table) else np.zeros(0, np.int64)
         self.tile_map = np.repeat(np.arange(len(table), dtype=np.int32), per)
         self._dev = None
+        self._rows_dev = None
         self._work: dict = {}
         self._private = False
 
@@ -680,14 +685,30 @@ class GemmTable:
             self._dev = Uploaded(self.host_arrays())
         return self._dev.ready()
 
+    def tile_rows(self) -> np.ndarray:
+        """The table as one row per tile (``tnb_grouped_gemm_f64_rows``)."""
+        return np.ascontiguousarray(self.table[self.tile_map])
+
     def run(self, a, b, c) -> None:
         """Launch on the current stream.  The split-K counters of a private table belong
         to it, so one private table must not run on two streams at once."""
         if self.n_gemm == 0:
             return
-        table, tile_map = self.device_tables()
         work = self.work()
         rec = recording()
+        if (rec is None and DIRECT_GEMM and self.tiles >= DIRECT_MIN_TILES
+                and self.kind in (TILE_64, TILE_32, TILE_SKINNY, TILE_WIDE)):
+            if self._rows_dev is None:
+                self._rows_dev = Uploaded((self.tile_rows(),))
+            (rows,) = self._rows_dev.ready()
+            mark = _LOG.begin() if _LOG is not None else None
+            _lib.call("tnb_grouped_gemm_f64_rows", ptr(rows), self.tiles, self.kind, ptr(a),
+                      a.numel(), ptr(b), b.numel(), ptr(c), c.numel(), ptr(work),
+                      self.work_bytes, self.n_counters, stream_ptr())
+            if _LOG is not None:
+                _LOG.end("grouped_gemm_f64", mark, self.flops)
+            return
+        table, tile_map = self.device_tables()
         if rec is not None:
             _lib.call("tnb_seq_add_gemm", rec.handle, ptr(table), self.n_gemm, ptr(tile_map),
                       self.tiles, self.kind, ptr(a), a.numel(), ptr(b), b.numel(), ptr(c),

@@ -29,6 +29,8 @@ SIGNATURES = {
                                         _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp]),
     "tnb_grouped_gemm_f64": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
                                     _i64, _vp, _i64, _i64, _vp]),
+    "tnb_grouped_gemm_f64_rows": (_i32, [_vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp, _i64, _vp,
+                                         _i64, _i64, _vp]),
     "tnb_grouped_gemm_gather_a": (_i32, [_vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64, _vp,
                                          _i64, _vp, _i64, _vp, _i64, _vp]),
     "tnb_seq_add_gemm_gather_a": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64,

@@ -95,10 +95,11 @@ def test_batched_heff2_matches_each_member():
 
 
 def test_per_chunk_row_gathers_are_bit_identical():
-    """``tnb_block_gather_direct`` (a row per chunk, one-term segments' terms inline)
-    against ``tnb_block_gather`` on the same tables: the 64-member U(1) x U(1) x fZ2
-    environment update (its many-wave gathers take the direct form by default) and an
-    SU(2) contraction's multi-term tables forced onto it -- the same bits, and no bounds
+    """``tnb_block_gather_direct`` (a row per chunk, one-term segments' terms inline) and
+    ``tnb_grouped_gemm_f64_rows`` (a row per tile) against ``tnb_block_gather`` and
+    ``tnb_grouped_gemm_f64`` on the same tables: a U(1) x U(1) x fZ2 environment-update
+    batch with every table forced onto the row forms (size-rule and autotuned tile kinds,
+    split-K included) and an SU(2) braid's multi-term table -- the same bits, and no bounds
     error."""
     import bench
     from tenet import _exec
@@ -106,13 +107,18 @@ def test_per_chunk_row_gathers_are_bit_identical():
 
     F, A, W = bench.config3_batch(8)
     outs = []
-    for min_chunks in (10 ** 9, 0):  # never, then every gather from its chunk rows
-        _exec.DIRECT_MIN_CHUNKS, old = min_chunks, _exec.DIRECT_MIN_CHUNKS
+    # never, then every gather from its chunk rows and every FP64 GEMM from its tile rows
+    for least in (10 ** 9, 0):
+        old = (_exec.DIRECT_MIN_CHUNKS, _exec.DIRECT_MIN_TILES)
+        _exec.DIRECT_MIN_CHUNKS = _exec.DIRECT_MIN_TILES = least
         try:
-            outs.append(batch.env_update_last(F, A, W).arena.cpu().numpy())
+            for autotune in (False, True):  # the size rule's kinds, then the tuned ones
+                batch.AUTOTUNE = autotune
+                outs.append(batch.env_update_last(F, A, W).arena.cpu().numpy())
         finally:
-            _exec.DIRECT_MIN_CHUNKS = old
-    assert np.array_equal(outs[0], outs[1])
+            _exec.DIRECT_MIN_CHUNKS, _exec.DIRECT_MIN_TILES = old
+            batch.AUTOTUNE = True
+    assert np.array_equal(outs[0], outs[2]) and np.array_equal(outs[1], outs[3])
 
     fl, w1, w2, fr, aa = bench.build_workload(seed=3, bond=bench.WORKLOADS["L64_cutoff1e-14_mid_bond"])
     # swapping the two physical legs is an F R F move: segments of several terms
