@@ -96,8 +96,9 @@ int tnb_block_gather(const int64_t* seg_table, int64_t n_seg, const int32_t* chu
  * [40] term_src, [41] the bits of term_coeff, [42] term_ld -- a pad word, and [48 + d]
  * the division constant of extent d (mul = ceil(2^(31 + l) / dims[d]) with l =
  * ceil(log2 dims[d]) in the low 32 bits, l - 1 above them; 0 for an extent of 1), with
- * which rows of rank <= 4 split element indices by a multiply and a shift (a constant
- * without the needed property falls back to division).  A chunk of a
+ * which element indices are split by a multiply and a shift (a constant without the
+ * needed property falls back to division).  Every segment must have rank <= 4 (a
+ * higher rank raises the bounds error; tnb_block_gather takes any).  A chunk of a
  * one-term segment (every segment of a U(1) / Z2 / fZ2 map) then reads its whole table in
  * one round of loads instead of three dependent ones (chunk map, row, terms), which is
  * what bounds many-wave gathers; segments with more terms read them from the term arrays

@@ -310,43 +310,38 @@ __device__ void gather_chunk(const GatherArgs& g, int64_t chunk, GatherSmem& sm,
   gather_staged<NT, kFused, kProd>(g, chunk, sm, tid);
 }
 
-// floor(n / d) for n < 2^31 from a division constant of a per-chunk row: mul in the low
-// 32 bits, the shift above them, as the host computes them (Granlund and Montgomery,
-// "Division by invariant integers using multiplication", 1994: with l = ceil(log2 d) and
-// p = 31 + l, mul = ceil(2^p / d) < 2^32 and mul d - 2^p < 2^(p - 31), so floor(n mul /
-// 2^p) = floor(n / d) for every n < 2^31); mul = 0 stands for d = 1.
-__device__ __forceinline__ uint32_t magic_div(uint32_t n, int64_t mag) {
-  const uint32_t mul = static_cast<uint32_t>(mag);
-  return mul ? __umulhi(n, mul) >> static_cast<uint32_t>(mag >> 32) : n;
-}
+// Division constants of a per-chunk row (tnb_block_gather_direct): mul in the low 32 bits
+// and l - 1 above them, as the host computes them (Granlund and Montgomery, "Division by
+// invariant integers using multiplication", 1994: with l = ceil(log2 d) and p = 31 + l,
+// mul = ceil(2^p / d) < 2^32 and mul d - 2^p < 2^(p - 31), so floor(n mul / 2^p) =
+// floor(n / d) for every n < 2^31); mul = 0 stands for d = 1.
 
 // gather_elems for a row of compile-time rank R with the row's extents, strides and
 // division constants in registers: the same offsets, terms and FMA order.
 template <int R, int KE, int NT>
 __device__ __forceinline__ void gather_elems_rank(const GatherArgs& g, const GatherSmem& sm,
                                                   const GatherElems& ge, int tid) {
-  uint32_t dims[R];
-  int64_t dstr[R], rstr[R], cstr[R], mag[R];
+  uint32_t dims[R], mul[R], shr[R];
+  int64_t dstr[R], rstr[R], cstr[R];
+  // a constant is taken only if it has the property the identity needs (2^p <= mul d <
+  // 2^p + 2^l with l = ceil(log2 d)); otherwise, or past 2^31 elements, hardware division
+  bool mok = true;
 #pragma unroll
   for (int d = 0; d < R; ++d) {
     dims[d] = static_cast<uint32_t>(sm.row[8 + d]);
     dstr[d] = sm.row[16 + d];
     rstr[d] = sm.row[24 + d];
     cstr[d] = sm.row[32 + d];
-    mag[d] = sm.dmag[d];
-  }
-  // a constant is taken only if it has the property the identity needs (2^p <= mul d <
-  // 2^p + 2^l with l = ceil(log2 d)); otherwise, or past 2^31 elements, hardware division
-  bool mok = true;
-#pragma unroll
-  for (int d = 0; d < R; ++d) {
-    const uint64_t m = static_cast<uint32_t>(mag[d]);
-    const int l = static_cast<int>((mag[d] >> 32) & 63) + 1;
+    const int64_t mag = sm.dmag[d];
+    mul[d] = static_cast<uint32_t>(mag);
+    const int l = static_cast<int>((mag >> 32) & 63) + 1;
+    shr[d] = static_cast<uint32_t>(l - 1);
     if (dims[d] <= 1) {
-      mok = mok && m == 0;
+      mok = mok && mul[d] == 0;
     } else {
       const bool lok = l <= 31 && l == 32 - __clz(dims[d] - 1);
-      const uint64_t prod = m * dims[d], two_p = 1ull << (lok ? 31 + l : 0);
+      const uint64_t prod = static_cast<uint64_t>(mul[d]) * dims[d];
+      const uint64_t two_p = 1ull << (lok ? 31 + l : 0);
       mok = mok && lok && prod >= two_p && prod - two_p < (1ull << l);
     }
   }
@@ -362,7 +357,8 @@ __device__ __forceinline__ void gather_elems_rank(const GatherArgs& g, const Gat
     int64_t dd = 0, rr = 0, cc = 0;
 #pragma unroll
     for (int d = R - 1; d >= 0; --d) {
-      const uint32_t q = fast ? magic_div(rem, mag[d]) : rem / dims[d];
+      const uint32_t q = fast ? (mul[d] ? __umulhi(rem, mul[d]) >> shr[d] : rem)
+                              : rem / dims[d];
       const uint32_t j = rem - q * dims[d];
       rem = q;
       dd += static_cast<int64_t>(j) * dstr[d];
@@ -381,8 +377,13 @@ __device__ __forceinline__ void gather_elems_rank(const GatherArgs& g, const Gat
     bad |= live[k] && !ok;
     return ok ? __ldg(ge.src + o) : 0.0;
   };
+  const bool one = ge.t1 - ge.t0 == 1;
   auto term = [&](int64_t t, int64_t& ts, int64_t& tl, double& cf) {
-    if (ge.staged) {
+    if (one) {
+      ts = sm.inl[0];
+      cf = __longlong_as_double(static_cast<long long>(sm.inl[1]));
+      tl = sm.inl[2];
+    } else if (ge.staged) {
       ts = sm.t_src[t - ge.t0];
       tl = sm.t_ld[t - ge.t0];
       cf = sm.t_cf[t - ge.t0];
@@ -431,22 +432,21 @@ __device__ __forceinline__ void gather_elems_rank(const GatherArgs& g, const Gat
 }
 
 // The chunk of a per-chunk row staged in `sm` (row, terms, division constants): the checks
-// of gather_staged, then rows of rank 1 to 4 through gather_elems_rank, higher ranks
-// through gather_staged itself.
+// of gather_staged, then gather_elems_rank for the row's rank (1 to kDirectMaxRank; the
+// host sends tables with higher ranks to tnb_block_gather).
+constexpr int kDirectMaxRank = 4;
+
 template <int NT>
 __device__ void gather_direct_staged(const GatherArgs& g, int64_t chunk, const GatherSmem& sm,
                                      int tid) {
   constexpr int kEpt = TNB_GATHER_CHUNK / NT;
   const int64_t* row = sm.row;
   const int rank = static_cast<int>(row[2]);
-  if (rank > 4) {
-    gather_staged<NT, false, false>(g, chunk, sm, tid);
-    return;
-  }
   const int64_t size = row[1], t0 = row[3], t1 = row[4];
   const bool second = row[5] != 0;
   const int64_t ce = row[7] ? row[7] : TNB_GATHER_CHUNK;
-  if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || ce <= 0 || ce > TNB_GATHER_CHUNK ||
+  if (t0 < 0 || t1 > g.n_term || t0 > t1 || rank < 1 || rank > kDirectMaxRank || ce <= 0 ||
+      ce > TNB_GATHER_CHUNK ||
       ce % kGatherThreads || chunk < row[6] || (chunk - row[6]) * ce >= size) {
     if (tid == 0) raise_bounds();
     return;
@@ -497,18 +497,16 @@ __device__ void gather_chunk_direct(const GatherArgs& g, const int64_t* __restri
   __syncthreads();
   const int64_t t0 = sm.row[3], t1 = sm.row[4];
   const bool ok = t0 >= 0 && t1 <= g.n_term && t0 <= t1;
-  if (ok && t1 - t0 == 1) {
-    if (tid == 0) {
-      sm.t_src[0] = sm.inl[0];
-      sm.t_cf[0] = __longlong_as_double(static_cast<long long>(sm.inl[1]));
-      sm.t_ld[0] = sm.inl[2];
+  // a one-term row's term is read from the inline words where it is used; more terms are
+  // staged (the condition is uniform across the CTA, so is the barrier)
+  if (ok && t1 - t0 > 1) {
+    if (t1 - t0 <= kStagedTerms && tid < t1 - t0) {
+      sm.t_src[tid] = __ldg(g.term_src + t0 + tid);
+      sm.t_ld[tid] = __ldg(g.term_ld + t0 + tid);
+      sm.t_cf[tid] = __ldg(g.term_coeff + t0 + tid);
     }
-  } else if (ok && t1 - t0 <= kStagedTerms && tid < t1 - t0) {
-    sm.t_src[tid] = __ldg(g.term_src + t0 + tid);
-    sm.t_ld[tid] = __ldg(g.term_ld + t0 + tid);
-    sm.t_cf[tid] = __ldg(g.term_coeff + t0 + tid);
+    __syncthreads();
   }
-  __syncthreads();
   if (!ok) {
     if (tid == 0) raise_bounds();
     return;

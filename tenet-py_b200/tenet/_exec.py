@@ -416,6 +416,12 @@ class GatherTable:
             self._dev = Uploaded(self.host_arrays())
         return self._dev.ready()
 
+    @property
+    def direct_ok(self) -> bool:
+        """Whether ``tnb_block_gather_direct`` takes this table (every segment of rank <=
+        4)."""
+        return bool(self.n_seg) and int(self.seg[:, 2].max()) <= DIRECT_MAX_RANK
+
     def chunk_rows(self) -> np.ndarray:
         """The table as one ``CHUNK_ROW_W`` row per chunk: the chunk's segment row, the
         segment's first term (source, coefficient bits, leading dimension) inline, and the
@@ -442,7 +448,7 @@ class GatherTable:
         if self.n_seg == 0:
             return
         rec = recording()
-        if rec is None and DIRECT_GATHER and self.chunks >= DIRECT_MIN_CHUNKS:
+        if rec is None and DIRECT_GATHER and self.chunks >= DIRECT_MIN_CHUNKS and self.direct_ok:
             crows, tsrc, tcf, tld = self.direct_arrays()
             mark = _LOG.begin() if _LOG is not None else None
             _lib.call("tnb_block_gather_direct", ptr(crows), self.chunks, ptr(tsrc), ptr(tcf),
@@ -475,6 +481,7 @@ class GatherTable:
 #: per-chunk rows (``tnb_block_gather_direct``): one round of table loads per CTA
 DIRECT_GATHER = True
 DIRECT_MIN_CHUNKS = 2 * 3 * N_SM + 1
+DIRECT_MAX_RANK = 4
 #: likewise FP64 grouped GEMMs of at least DIRECT_MIN_TILES tiles from one row per tile
 #: (``tnb_grouped_gemm_f64_rows``): one table load per tile instead of two dependent ones
 DIRECT_GEMM = True
