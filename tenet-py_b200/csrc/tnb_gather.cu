@@ -35,12 +35,15 @@ gather_kernel(const GatherArgs g) {
 }
 
 // The per-chunk-row form (tnb_block_gather_direct), the same two builds.
-template <int kMinBlocks>
+// (The many-wave build takes kDirectChunksPerCta chunks per CTA: one table wait for both.)
+constexpr int kDirectChunksPerCta = 2;
+
+template <int kMinBlocks, int CP>
 __global__ void __launch_bounds__(kGatherThreads, kMinBlocks)
-gather_direct_kernel(const GatherArgs g, const int64_t* __restrict__ chunk_rows) {
-  __shared__ GatherSmem sm;
-  gather_chunk_direct<kGatherThreads, (kMinBlocks == 3)>(g, chunk_rows, blockIdx.x, sm,
-                                                         threadIdx.x);
+gather_direct_kernel(const GatherArgs g, const int64_t* __restrict__ chunk_rows, int64_t total) {
+  __shared__ GatherSmem sm[CP];
+  gather_chunks_direct<kGatherThreads, CP, (kMinBlocks == 3)>(
+      g, chunk_rows, static_cast<int64_t>(blockIdx.x) * CP, total, sm, threadIdx.x);
 }
 
 // SMs of the current device (0 when it cannot be queried), cached per device.
@@ -147,11 +150,14 @@ extern "C" int tnb_block_gather_direct(const int64_t* chunk_rows, int64_t total_
   const tnb::GatherArgs g{nullptr, 0, nullptr, term_src, term_coeff, term_ld, n_term,
                           src0, n_src0, dst0, n_dst0, src1, n_src1, dst1, n_dst1};
   const bool large = total_chunks > 2 * 3 * static_cast<int64_t>(tnb::device_sms());
+  constexpr int CP = tnb::kDirectChunksPerCta;
   cudaError_t e =
-      large ? tnb::launch(tnb::gather_direct_kernel<4>, static_cast<unsigned>(total_chunks),
-                          tnb::kGatherThreads, tnb::as_stream(stream), g, chunk_rows)
-            : tnb::launch(tnb::gather_direct_kernel<3>, static_cast<unsigned>(total_chunks),
-                          tnb::kGatherThreads, tnb::as_stream(stream), g, chunk_rows);
+      large ? tnb::launch(tnb::gather_direct_kernel<4, CP>,
+                          static_cast<unsigned>((total_chunks + CP - 1) / CP), tnb::kGatherThreads,
+                          tnb::as_stream(stream), g, chunk_rows, total_chunks)
+            : tnb::launch(tnb::gather_direct_kernel<3, 1>, static_cast<unsigned>(total_chunks),
+                          tnb::kGatherThreads, tnb::as_stream(stream), g, chunk_rows,
+                          total_chunks);
   if (e != cudaSuccess) {
     tnb::set_error(std::string("tnb_block_gather_direct: ") + cudaGetErrorString(e));
     return TNB_ECUDA;

@@ -476,43 +476,59 @@ __device__ void gather_direct_staged(const GatherArgs& g, int64_t chunk, const G
 // word of a per-chunk row where its extents' division constants begin
 constexpr int kChunkRowMagic = 48;
 
-// One chunk of a gather whose table is a row per chunk (TNB_CHUNK_ROW_WIDTH words: the
-// segment row, then its first term inline): the row and, for a one-term row, its term
-// arrive in one round of independent loads -- no chunk map to read first, no term array
-// to read after.  Rows with more terms stage them as gather_chunk does.  The loads of the
-// static table come before the dependent-launch wait.
-template <int NT, bool kRelease = true>
-__device__ void gather_chunk_direct(const GatherArgs& g, const int64_t* __restrict__ crows,
-                                    int64_t chunk, GatherSmem& sm, int tid) {
-  static_assert(NT >= TNB_CHUNK_ROW_WIDTH && NT >= kStagedTerms,
-                "a CTA stages a chunk row and its terms");
-  const int64_t* cr = crows + chunk * TNB_CHUNK_ROW_WIDTH;
-  if (tid < TNB_SEG_WIDTH) {
-    sm.row[tid] = __ldg(cr + tid);
-  } else if (tid < TNB_SEG_WIDTH + 3) {
-    sm.inl[tid - TNB_SEG_WIDTH] = __ldg(cr + tid);
-  } else if (tid >= kChunkRowMagic && tid < kChunkRowMagic + TNB_MAX_RANK) {
-    sm.dmag[tid - kChunkRowMagic] = __ldg(cr + tid);
+// CP consecutive chunks first, first + 1, ... (those below `total`) of a gather whose table
+// is a row per chunk (TNB_CHUNK_ROW_WIDTH words: the segment row, its first term inline,
+// its extents' division constants), by one CTA: every chunk's row -- and, for a one-term
+// row, its term -- arrives in the same round of independent loads (a 64-thread group
+// per chunk), so the CTA waits on its table once for CP chunks; rows with more terms
+// stage them in a second round.  The chunks then run one after the other.  The loads of
+// the static table come before the dependent-launch wait.
+template <int NT, int CP, bool kRelease = true>
+__device__ void gather_chunks_direct(const GatherArgs& g, const int64_t* __restrict__ crows,
+                                     int64_t first, int64_t total, GatherSmem* sm, int tid) {
+  static_assert(TNB_CHUNK_ROW_WIDTH <= 64 && CP * 64 <= NT && NT >= kStagedTerms,
+                "a 64-thread group stages each chunk row");
+  {
+    const int i = tid / 64, w = tid % 64;
+    if (i < CP && first + i < total) {
+      const int64_t* cr = crows + (first + i) * TNB_CHUNK_ROW_WIDTH;
+      GatherSmem& c = sm[i];
+      if (w < TNB_SEG_WIDTH) {
+        c.row[w] = __ldg(cr + w);
+      } else if (w < TNB_SEG_WIDTH + 3) {
+        c.inl[w - TNB_SEG_WIDTH] = __ldg(cr + w);
+      } else if (w >= kChunkRowMagic && w < kChunkRowMagic + TNB_MAX_RANK) {
+        c.dmag[w - kChunkRowMagic] = __ldg(cr + w);
+      }
+    }
   }
   __syncthreads();
-  const int64_t t0 = sm.row[3], t1 = sm.row[4];
-  const bool ok = t0 >= 0 && t1 <= g.n_term && t0 <= t1;
-  // a one-term row's term is read from the inline words where it is used; more terms are
-  // staged (the condition is uniform across the CTA, so is the barrier)
-  if (ok && t1 - t0 > 1) {
-    if (t1 - t0 <= kStagedTerms && tid < t1 - t0) {
-      sm.t_src[tid] = __ldg(g.term_src + t0 + tid);
-      sm.t_ld[tid] = __ldg(g.term_ld + t0 + tid);
-      sm.t_cf[tid] = __ldg(g.term_coeff + t0 + tid);
+  // a one-term row's term is read from the inline words where it is used; rows with more
+  // terms stage them (every condition here is uniform across the CTA, so is the barrier)
+  bool ok[CP], staged = false;
+#pragma unroll
+  for (int i = 0; i < CP; ++i) {
+    ok[i] = false;
+    if (first + i >= total) continue;
+    GatherSmem& c = sm[i];
+    const int64_t t0 = c.row[3], t1 = c.row[4];
+    ok[i] = t0 >= 0 && t1 <= g.n_term && t0 <= t1;
+    if (!ok[i]) {
+      if (tid == 0) raise_bounds();
+    } else if (t1 - t0 > 1) {
+      if (t1 - t0 <= kStagedTerms && tid < t1 - t0) {
+        c.t_src[tid] = __ldg(g.term_src + t0 + tid);
+        c.t_ld[tid] = __ldg(g.term_ld + t0 + tid);
+        c.t_cf[tid] = __ldg(g.term_coeff + t0 + tid);
+      }
+      staged = true;
     }
-    __syncthreads();
   }
-  if (!ok) {
-    if (tid == 0) raise_bounds();
-    return;
-  }
+  if (staged) __syncthreads();
   pdl_wait<kRelease>();  // the source may be the previous kernel's output
-  gather_direct_staged<NT>(g, chunk, sm, tid);
+#pragma unroll
+  for (int i = 0; i < CP; ++i)
+    if (ok[i]) gather_direct_staged<NT>(g, first + i, sm[i], tid);
 }
 
 // ---------------------------------------------------------------------------------------
