@@ -369,6 +369,12 @@ int tnb_seq_add_gather(tnb_seq* s, const int64_t* seg_table, int64_t n_seg,
                        const double* term_coeff, const int64_t* term_ld, int64_t n_term,
                        const double* src0, int64_t n_src0, double* dst0, int64_t n_dst0,
                        const double* src1, int64_t n_src1, double* dst1, int64_t n_dst1);
+/* Records a tnb_block_gather_direct launch (the per-chunk-row table form). */
+int tnb_seq_add_gather_direct(tnb_seq* s, const int64_t* chunk_rows, int64_t total_chunks,
+                              const int64_t* term_src, const double* term_coeff,
+                              const int64_t* term_ld, int64_t n_term, const double* src0,
+                              int64_t n_src0, double* dst0, int64_t n_dst0, const double* src1,
+                              int64_t n_src1, double* dst1, int64_t n_dst1);
 int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n_gemm,
                      const int32_t* tile_map, int64_t total_tiles, int32_t tile_kind,
                      const double* a, int64_t n_a, const double* b, int64_t n_b, double* c,

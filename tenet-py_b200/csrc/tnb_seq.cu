@@ -34,6 +34,7 @@ constexpr int32_t kOpFused = 3;
 constexpr int32_t kOpGatherProduct = 4;
 constexpr int32_t kOpCluster = 5;
 constexpr int32_t kOpGemmGatherA = 6;
+constexpr int32_t kOpGatherDirect = 7;
 
 struct FStage {
   int32_t code;
@@ -217,6 +218,7 @@ constexpr int kGatherBufs[] = {8, 10, 12, 14};  // src0, dst0, src1, dst1
 constexpr int kGemmBufs[] = {5, 7, 9};          // a, b, c
 constexpr int kGatherProductBufs[] = {11, 13, 15};  // a, b, dst
 constexpr int kGemmGatherABufs[] = {9, 11, 13};     // src, b, c
+constexpr int kGatherDirectBufs[] = {6, 8, 10, 12};  // src0, dst0, src1, dst1
 
 inline void* as_ptr(int64_t w) { return reinterpret_cast<void*>(static_cast<intptr_t>(w)); }
 inline int64_t as_word(const void* p) { return static_cast<int64_t>(reinterpret_cast<intptr_t>(p)); }
@@ -259,6 +261,15 @@ int replay(const tnb_seq* s, int32_t n_patch, const void* const* from, void* con
           static_cast<const double*>(as_ptr(w[11])), w[12],
           static_cast<const double*>(as_ptr(w[13])), w[14],
           static_cast<double*>(as_ptr(w[15])), w[16], stream);
+    } else if (op.code == kOpGatherDirect) {
+      for (int k : kGatherDirectBufs) w[k] = patched(w[k], n_patch, from, to);
+      rc = tnb_block_gather_direct(
+          static_cast<const int64_t*>(as_ptr(w[0])), w[1],
+          static_cast<const int64_t*>(as_ptr(w[2])), static_cast<const double*>(as_ptr(w[3])),
+          static_cast<const int64_t*>(as_ptr(w[4])), w[5],
+          static_cast<const double*>(as_ptr(w[6])), w[7], static_cast<double*>(as_ptr(w[8])),
+          w[9], static_cast<const double*>(as_ptr(w[10])), w[11],
+          static_cast<double*>(as_ptr(w[12])), w[13], stream);
     } else if (op.code == kOpGemmGatherA) {
       for (int k : kGemmGatherABufs) w[k] = patched(w[k], n_patch, from, to);
       rc = tnb_grouped_gemm_gather_a(
@@ -380,6 +391,23 @@ extern "C" int tnb_seq_add_gemm(tnb_seq* s, const int64_t* gemm_table, int64_t n
                  {as_word(gemm_table), n_gemm, as_word(tile_map), total_tiles, tile_kind,
                   as_word(a), n_a, as_word(b), n_b, as_word(c), n_c, as_word(work), work_bytes,
                   n_counters, 0, 0}};
+  s->ops.push_back(op);
+  return TNB_OK;
+}
+
+extern "C" int tnb_seq_add_gather_direct(tnb_seq* s, const int64_t* chunk_rows,
+                                         int64_t total_chunks, const int64_t* term_src,
+                                         const double* term_coeff, const int64_t* term_ld,
+                                         int64_t n_term, const double* src0, int64_t n_src0,
+                                         double* dst0, int64_t n_dst0, const double* src1,
+                                         int64_t n_src1, double* dst1, int64_t n_dst1) {
+  TNB_REQUIRE(s != nullptr, "tnb_seq_add_gather_direct: null sequence");
+  TNB_REQUIRE(total_chunks >= 0 && n_term >= 0, "tnb_seq_add_gather_direct: negative size");
+  using tnb::as_word;
+  tnb_seq::Op op{tnb::kOpGatherDirect,
+                 {as_word(chunk_rows), total_chunks, as_word(term_src), as_word(term_coeff),
+                  as_word(term_ld), n_term, as_word(src0), n_src0, as_word(dst0), n_dst0,
+                  as_word(src1), n_src1, as_word(dst1), n_dst1}};
   s->ops.push_back(op);
   return TNB_OK;
 }

@@ -19,6 +19,8 @@ import ctypes
 import threading
 from dataclasses import dataclass
 
+from contextlib import contextmanager
+
 import numpy as np
 import torch
 
@@ -448,6 +450,13 @@ class GatherTable:
         if self.n_seg == 0:
             return
         rec = recording()
+        if rec is not None and CHAIN_DIRECT_GATHER and not _STANDARD[0] and self.direct_ok:
+            crows, tsrc, tcf, tld = self.direct_arrays()
+            _lib.call("tnb_seq_add_gather_direct", rec.handle, ptr(crows), self.chunks,
+                      ptr(tsrc), ptr(tcf), ptr(tld), self.n_term, ptr(src0), src0.numel(),
+                      ptr(dst0), dst0.numel(), ptr(src1), 0 if src1 is None else src1.numel(),
+                      ptr(dst1), 0 if dst1 is None else dst1.numel())
+            return
         if rec is None and DIRECT_GATHER and self.chunks >= DIRECT_MIN_CHUNKS and self.direct_ok:
             crows, tsrc, tcf, tld = self.direct_arrays()
             mark = _LOG.begin() if _LOG is not None else None
@@ -482,6 +491,21 @@ class GatherTable:
 DIRECT_GATHER = True
 DIRECT_MIN_CHUNKS = 2 * 3 * N_SM + 1
 DIRECT_MAX_RANK = 4
+#: record the gathers of compiled chains (a matvec's recorded sequence) in the per-chunk-row
+#: form whatever their size: a one-wave gather there waits on its table once, not three
+#: times, ahead of the data the previous launch produces
+CHAIN_DIRECT_GATHER = True
+_STANDARD = [0]  # > 0 inside standard_gathers()
+
+
+@contextmanager
+def standard_gathers():
+    """Record chunk-map gathers only (the one-launch chain kernels take no other form)."""
+    _STANDARD[0] += 1
+    try:
+        yield
+    finally:
+        _STANDARD[0] -= 1
 #: likewise FP64 grouped GEMMs of at least DIRECT_MIN_TILES tiles from one row per tile
 #: (``tnb_grouped_gemm_f64_rows``): one table load per tile instead of two dependent ones
 DIRECT_GEMM = True

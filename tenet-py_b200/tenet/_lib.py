@@ -56,6 +56,8 @@ SIGNATURES = {
                                           _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64]),
     "tnb_seq_add_gather": (_i32, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64,
                                   _vp, _i64, _vp, _i64, _vp, _i64]),
+    "tnb_seq_add_gather_direct": (_i32, [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _i64, _vp,
+                                         _i64, _vp, _i64, _vp, _i64]),
     "tnb_seq_add_gemm": (_i32, [_vp, _vp, _i64, _vp, _i64, _i32, _vp, _i64, _vp, _i64, _vp,
                                 _i64, _vp, _i64, _i64]),
     "tnb_seq_append": (_i32, [_vp, _vp]),

@@ -348,29 +348,36 @@ class ChainProgram:
         self.seq = _exec.Seq()
         with self.seq:
             self._run_tables(self.x_slot, self.y_slot)
+        # the one-launch forms fuse a chunk-map recording of the same stages
+        std = self.seq
+        if _exec.CHAIN_DIRECT_GATHER:
+            std = _exec.Seq()
+            with _exec.standard_gathers(), std:
+                self._run_tables(self.x_slot, self.y_slot)
+        self._std_seq = std
         # the same stages as one persistent launch, when they all fuse (no tensor-core
         # stage, no product-source gather, at most the kernel's stage count)
         self.cluster = None
         if getattr(self, "compact", False) and _exec.CLUSTER and \
-                0 < len(self.seq) <= FUSED_MAX_STAGES:
+                0 < len(std) <= FUSED_MAX_STAGES:
             import ctypes
 
             from tenet import _lib
 
             cl, ctas = _exec.Seq(), ctypes.c_int32(0)
-            _lib.call("tnb_seq_fuse_cluster", self.seq.handle, self.x_slot.data_ptr(),
+            _lib.call("tnb_seq_fuse_cluster", std.handle, self.x_slot.data_ptr(),
                       self.y_slot.data_ptr(), _exec.CLUSTER_CTAS, ctypes.byref(ctas),
                       cl.handle)
             self.cluster, self.cluster_ctas = cl, ctas.value
         self.fused = None
         if (not self.uses_tensor_cores and not any(lk.deferred for lk in self.links)
                 and not any(lk.ga is not None for lk in self.links)
-                and 0 < len(self.seq) <= FUSED_MAX_STAGES):
+                and 0 < len(std) <= FUSED_MAX_STAGES):
             from tenet import _lib
 
             self.barrier = torch.zeros(2, dtype=torch.int32, device=dev)
             fused = _exec.Seq()
-            _lib.call("tnb_seq_fuse", self.seq.handle, self.x_slot.data_ptr(),
+            _lib.call("tnb_seq_fuse", std.handle, self.x_slot.data_ptr(),
                       self.y_slot.data_ptr(), self.barrier.data_ptr(), fused.handle)
             self.fused = fused
         self._built = True

@@ -907,3 +907,35 @@ def test_host_copies_refuse_pageable_memory():
     assert torch.equal(back[:n - 1], pinned[1:])
     assert lib.tnb_mapped_address(dev.data_ptr(), ctypes.byref(out)) == 0
     assert out.value == dev.data_ptr()
+
+
+def test_chain_direct_gathers_are_bit_identical():
+    """A compiled matvec records its gathers in the per-chunk-row form
+    (``tnb_seq_add_gather_direct``) when every segment has rank <= 4: the same bits as the
+    chunk-map recording, through the graph and the device Lanczos, on the bench's three
+    bonds; the one-launch chain still builds from a chunk-map recording."""
+    import bench
+    from tenet import _exec
+    from tenet import program as _program
+    from tenet.program import GraphMatvec, heff2_folded_program
+
+    for bond in (bench.BOND, *bench.WORKLOADS.values()):
+        fl, w1, w2, fr, aa = bench.build_workload(seed=5, bond=bond)
+        lf, rf = network.fold_left(fl, w1), network.fold_right(w2, fr)
+        outs = []
+        for direct in (False, True):
+            _exec.CHAIN_DIRECT_GATHER = direct
+            _program._HEFF_TABLES.clear()
+            try:
+                prog = heff2_folded_program(lf, rf, aa.structure)
+                y = GraphMatvec(prog)(aa).numpy_arena()
+                e, v = network.DeviceLanczos(prog, 12).solve(aa)
+                outs.append((y, e, v.numpy_arena(), prog.fused is not None))
+            finally:
+                _exec.CHAIN_DIRECT_GATHER = True
+                _program._HEFF_TABLES.clear()
+        (y0, e0, v0, f0), (y1, e1, v1, f1) = outs
+        assert np.array_equal(y0, y1) and e0 == e1 and np.array_equal(v0, v1)
+        assert f0 == f1
+    torch.cuda.synchronize()
+    assert _lib.device_error(0) == 0
