@@ -492,9 +492,11 @@ DIRECT_GATHER = True
 DIRECT_MIN_CHUNKS = 2 * 3 * N_SM + 1
 DIRECT_MAX_RANK = 4
 #: record the gathers of compiled chains (a matvec's recorded sequence) in the per-chunk-row
-#: form whatever their size: a one-wave gather there waits on its table once, not three
-#: times, ahead of the data the previous launch produces
-CHAIN_DIRECT_GATHER = True
+#: form whatever their size.  Off by default: the same bits, but a one-wave gather's table
+#: wait already overlaps the previous launch (programmatic dependent launch), and with a
+#: cold L2 the larger rows cost more than the saved round trips (headline matvec 22.6-25.4
+#: against 21.7-22.6 us, L2 flushed; equal with a warm L2)
+CHAIN_DIRECT_GATHER = False
 _STANDARD = [0]  # > 0 inside standard_gathers()
 
 

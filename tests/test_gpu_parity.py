@@ -910,8 +910,9 @@ def test_host_copies_refuse_pageable_memory():
 
 
 def test_chain_direct_gathers_are_bit_identical():
-    """A compiled matvec records its gathers in the per-chunk-row form
-    (``tnb_seq_add_gather_direct``) when every segment has rank <= 4: the same bits as the
+    """With ``CHAIN_DIRECT_GATHER`` on, a compiled matvec records its gathers in the
+    per-chunk-row form (``tnb_seq_add_gather_direct``) when every segment has rank <= 4:
+    the same bits as the
     chunk-map recording, through the graph and the device Lanczos, on the bench's three
     bonds; the one-launch chain still builds from a chunk-map recording."""
     import bench
@@ -932,7 +933,7 @@ def test_chain_direct_gathers_are_bit_identical():
                 e, v = network.DeviceLanczos(prog, 12).solve(aa)
                 outs.append((y, e, v.numpy_arena(), prog.fused is not None))
             finally:
-                _exec.CHAIN_DIRECT_GATHER = True
+                _exec.CHAIN_DIRECT_GATHER = False
                 _program._HEFF_TABLES.clear()
         (y0, e0, v0, f0), (y1, e1, v1, f1) = outs
         assert np.array_equal(y0, y1) and e0 == e1 and np.array_equal(v0, v1)
