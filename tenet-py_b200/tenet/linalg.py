@@ -150,16 +150,35 @@ class _SvdPlan:
         self.o_sorted = self.o_keep + 8 * n
         self.o_info = self.o_sorted + 8 * T
         self.o_csec = self.o_info + 4 * n
-        nbytes = -(-(self.o_csec + 4 * T) // 8) * 8
-        self.dev = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
-        self.host = torch.zeros(nbytes, dtype=torch.uint8).pin_memory()
+        self.nbytes = -(-(self.o_csec + 4 * T) // 8) * 8
+        self.T = T
+        self._readbacks: dict = {}  # stream -> _Readback
+        self.post: dict = {}  # kept counts -> truncated structures and compaction table
+
+    def readback(self, stream: int) -> "_Readback":
+        """This stream's read-back buffers: a decision in flight on one stream (between
+        ``svd_truncated_launch`` and ``svd_truncated_finish``) never shares them with a
+        decision of the same structure on another."""
+        rb = self._readbacks.get(stream)
+        if rb is None:
+            rb = self._readbacks[stream] = _Readback(self)
+        return rb
+
+
+class _Readback:
+    """One device buffer and its pinned copy holding what a decision reads back: stats (8
+    f64), keep (ns i64), sorted values (T f64), info (ns i32), sorted sectors (T i32)."""
+
+    def __init__(self, plan: _SvdPlan) -> None:
+        self.dev = torch.zeros(plan.nbytes, dtype=torch.uint8, device=_exec.device())
+        self.host = torch.zeros(plan.nbytes, dtype=torch.uint8).pin_memory()
         h = self.host.numpy()
         self.h_stats = h[:64].view(np.float64)
-        self.h_keep = h[self.o_keep:self.o_sorted].view(np.int64)
-        self.h_sorted = h[self.o_sorted:self.o_info].view(np.float64)
-        self.h_info = h[self.o_info:self.o_csec].view(np.int32)
-        self.h_csec = h[self.o_csec:self.o_csec + 4 * T].view(np.int32)
-        self.post: dict = {}  # kept counts -> truncated structures and compaction table
+        self.h_keep = h[plan.o_keep:plan.o_sorted].view(np.int64)
+        self.h_sorted = h[plan.o_sorted:plan.o_info].view(np.float64)
+        self.h_info = h[plan.o_info:plan.o_csec].view(np.int32)
+        self.h_csec = h[plan.o_csec:plan.o_csec + 4 * plan.T].view(np.int32)
+        self.event = torch.cuda.Event()
 
 
 @cache
@@ -189,6 +208,24 @@ def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cuto
     """``svd_truncated`` plus what its decision read back: ``(U, S, Vh, selection,
     kept)``, ``selection`` the ``BondSelection`` and ``kept`` the kept singular values in
     the global order as ``(sigma * scale, sector label)`` pairs."""
+    return svd_truncated_finish(svd_truncated_launch(
+        t, axes, max_bond=max_bond, cutoff=cutoff, cutoff_mode=cutoff_mode, renorm=renorm,
+        budget=budget))
+
+
+class _SvdPending:
+    """A truncation between its launch and its read-back."""
+
+    __slots__ = ("plan", "m", "rb", "U", "Sv", "V", "keep_alive", "renorm", "dev", "ns")
+
+
+def svd_truncated_launch(t: SymmetricTensor, axes=None, *, max_bond=None, cutoff=None,
+                         cutoff_mode: str = "rsum2", renorm: bool = False,
+                         budget: str = "dense") -> _SvdPending:
+    """The first half of ``svd_truncated_selected``: the argument checks (the reference's
+    refusals), the lowering, the blockwise SVD, the decision and the copy of the decision to
+    pinned host memory, all enqueued on the current stream; nothing waits.  A caller with
+    other work (a serving loop) does it before ``svd_truncated_finish``."""
     from tenet import _lib
 
     if budget not in ("dense", "reduced"):
@@ -219,35 +256,52 @@ def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cuto
     W = torch.empty(max(1, plan.n_w), **f64)
     P, st = _exec.ptr, _exec.stream_ptr()
     ns = len(plan.sectors)
-    base = plan.dev.data_ptr()
+    rb = plan.readback(st)
+    base = rb.dev.data_ptr()
     _lib.call("tnb_block_svd", P(plan.rows), ns, P(buf), buf.numel(), P(U), U.numel(), P(Sv),
               Sv.numel(), P(V), V.numel(), P(W), plan.n_w, base + plan.o_info, plan.smem, st)
     _lib.call("tnb_truncate_decide", P(plan.sec_rows), P(plan.qdim), ns, P(Sv), Sv.numel(),
               -1.0 if cutoff is None else float(cutoff), _MODES[cutoff_mode],
               -1.0 if max_bond is None else float(max_bond), 0 if budget == "dense" else 1,
               base + plan.o_keep, base + plan.o_sorted, base + plan.o_csec, base, st)
-    plan.host.copy_(plan.dev, non_blocking=True)
-    torch.cuda.current_stream().synchronize()
-    info = plan.h_info[:ns]
+    rb.host.copy_(rb.dev, non_blocking=True)
+    rb.event.record()
+    p = _SvdPending()
+    p.plan, p.m, p.rb, p.U, p.Sv, p.V = plan, m, rb, U, Sv, V
+    p.keep_alive, p.renorm, p.dev, p.ns = (buf, W), renorm, dev, ns
+    return p
+
+
+def svd_truncated_finish(p: _SvdPending):
+    """The second half: wait for the decision's read-back, build the truncated structures
+    and pack the kept factors (on the current stream, which must be the launch's)."""
+    from tenet import _lib
+
+    plan, m, rb, ns = p.plan, p.m, p.rb, p.ns
+    ml = plan.ml
+    f64 = dict(dtype=torch.float64, device=p.dev)
+    P, st = _exec.ptr, _exec.stream_ptr()
+    rb.event.synchronize()
+    info = rb.h_info[:ns]
     if np.any(info != 0):
         raise RuntimeError(f"svd_truncated: the blockwise SVD did not converge (info "
                            f"{info.tolist()})")
-    keep_h = plan.h_keep[:ns]
-    n_kept, dense, disc, total, kept_w = (float(x) for x in plan.h_stats[:5])
+    keep_h = rb.h_keep[:ns]
+    n_kept, dense, disc, total, kept_w = (float(x) for x in rb.h_stats[:5])
     if n_kept == 0:
         raise ValueError("svd_truncated: the truncation keeps no singular value at all")
     keep = {c: int(k) for c, k in zip(plan.sectors, keep_h) if k > 0}
-    scale = (total / kept_w) ** 0.5 if renorm else 1.0
-    p = t.provider
+    scale = (total / kept_w) ** 0.5 if p.renorm else 1.0
+    prov = m.provider
     sel = BondSelection(keep, dense, int(n_kept), disc, scale)
     nk = int(n_kept)
     kept = [(float(x) * scale, plan.sectors[int(k)])
-            for x, k in zip(plan.h_sorted[:nk], plan.h_csec[:nk])]
+            for x, k in zip(rb.h_sorted[:nk], rb.h_csec[:nk])]
     # the truncated structures and the compaction table depend on the kept counts only:
     # a bond that keeps what it kept before (every converged sweep) reuses them
     post = plan.post.get(tuple(keep.items()))
     if post is None:
-        bond = GradedSpace.new(p, {p.sector(c): k for c, k in keep.items()})
+        bond = GradedSpace.new(prov, {prov.sector(c): k for c, k in keep.items()})
         su = TensorStructure((*m.codomain, Leg(bond, IN)))
         ss = TensorStructure((Leg(bond, OUT), Leg(bond, IN)))
         sv = TensorStructure((Leg(bond, OUT), *m.domain))
@@ -257,13 +311,14 @@ def svd_truncated_selected(t: SymmetricTensor, axes=None, *, max_bond=None, cuto
             kf, uo, so, vo = plan.kfull[c]
             r, q = ml.shape[c]
             rows.append((r, q, kf, k, uo, so, vo, lu.base[c], ls.base[c], lv.base[c], 0, 0))
-        crows = torch.tensor(rows, dtype=torch.int64, device=dev)
+        crows = torch.tensor(rows, dtype=torch.int64, device=p.dev)
         post = (su, ss, sv, lu.size, ls.size, lv.size, crows, len(rows))
         if len(plan.post) >= 64:
             plan.post.pop(next(iter(plan.post)))
         plan.post[tuple(keep.items())] = post
     su, ss, sv, nu, nsz, nv, crows, n_rows = post
     PU, PS, PV = (torch.empty(max(1, x), **f64) for x in (nu, nsz, nv))
+    U, Sv, V = p.U, p.Sv, p.V
     _lib.call("tnb_svd_compact", P(crows), n_rows, P(U), U.numel(), P(Sv), Sv.numel(), P(V),
               V.numel(), float(scale), P(PU), PU.numel(), P(PS), PS.numel(), P(PV), PV.numel(),
               st)

@@ -1016,8 +1016,9 @@ def sweep_steps(psi: MPS, h: MPO, env: Env, schmidt: dict | None = None, *, chi:
                 budget: str = "dense"):
     """One left-to-right then right-to-left two-site sweep (``network/dmrg.py:321-542``)
     as a generator: with the device Lanczos it yields right after each bond's solve is
-    enqueued on the current stream (so a scheduler can run other work while the device
-    computes); it returns ``(energy, max discarded weight)``.  ``schmidt`` (bond ->
+    enqueued on the current stream and again after its truncation is (so a scheduler can
+    run other work while the device computes); it returns ``(energy, max discarded
+    weight)``.  ``schmidt`` (bond ->
     spectrum) is updated in place.  ``budget="reduced"`` caps the number of kept
     multiplets at ``chi`` instead of the reference's dense dimension (a build-side mode
     with no reference counterpart)."""
@@ -1062,8 +1063,11 @@ def sweep_steps(psi: MPS, h: MPO, env: Env, schmidt: dict | None = None, *, chi:
                     r = SymmetricTensor.random(aa.legs, seed=seed + n)
                     aa = ops.add(aa, r * float(noise * ops.norm(aa) / ops.norm(r)))
                     aa = aa / ops.norm(aa)
-                u, s, vh, sel, kept = linalg.svd_truncated_selected(
+                pending = linalg.svd_truncated_launch(
                     aa, ((0, 1), (2, 3)), max_bond=chi, cutoff=cutoff, budget=budget)
+                if env.device_solves:
+                    yield n  # the decision is on its way back: a scheduler runs others
+                u, s, vh, sel, kept = linalg.svd_truncated_finish(pending)
                 # Pythagoras from the decision's read-back: |S|^2 is the kept qdim-weighted
                 # sum of sigma^2 and |aa|^2 the whole one (the reference takes both norms
                 # numerically, network/dmrg.py:514-517)

@@ -221,3 +221,33 @@ def test_device_decision_matches_the_keep_rule(mode, budget):
             assert stats[2] == pytest.approx(want.discarded_weight, rel=1e-15, abs=1e-300)
             order = [(float(x), labels[k]) for x, k in zip(ss.cpu().numpy(), sc.cpu().numpy())]
             assert order == [(x, c) for x, c, _ in spectrum]
+
+
+def test_truncations_in_flight_on_two_streams():
+    """Two truncations of the same structure launched on two streams before either reads
+    its decision back (what the serving loop does across requests): each gets its own
+    result, equal to the same truncation run alone."""
+    import tenet
+    from tenet.structure import IN, OUT, GradedSpace, Leg
+
+    V = GradedSpace.new(SU2, {SU2.sector(0): 6, SU2.sector(2): 5, SU2.sector(4): 3})
+    P = GradedSpace.new(SU2, {SU2.sector(1): 1})
+    legs = (Leg(V, OUT), Leg(P, OUT), Leg(P, OUT), Leg(V, IN))
+    a, b = (tenet.SymmetricTensor.random(legs, seed=s) for s in (21, 22))
+    kw = dict(max_bond=20, cutoff=1e-12)
+    alone = [linalg.svd_truncated_selected(t, ((0, 1), (2, 3)), **kw) for t in (a, b)]
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s1):
+        pa = linalg.svd_truncated_launch(a, ((0, 1), (2, 3)), **kw)
+    with torch.cuda.stream(s2):
+        pb = linalg.svd_truncated_launch(b, ((0, 1), (2, 3)), **kw)
+    with torch.cuda.stream(s1):
+        ra = linalg.svd_truncated_finish(pa)
+    with torch.cuda.stream(s2):
+        rb = linalg.svd_truncated_finish(pb)
+    torch.cuda.synchronize()
+    for got, want in zip((ra, rb), alone):
+        assert got[3].keep == want[3].keep and got[4] == want[4]
+        for x, y in zip(got[:3], want[:3]):
+            assert np.array_equal(x.numpy_arena(), y.numpy_arena())
