@@ -516,7 +516,9 @@ def serving(args) -> dict:
     compiled FP64 form one solve at a time, the single-process serving loop in FP64 and
     in the precision form, the same with host-parallel worker processes (started and
     warmed before the timed run), every request arriving at once, and the worker form
-    again at a Poisson arrival rate of 0.7 x its burst throughput for the latency point."""
+    again at a Poisson arrival rate of 0.7 x its burst throughput for the latency point;
+    then the single-process loop and the compiled sequential solves again with the plan
+    caches warm, as in a long-running server."""
     import torch
 
     from tenet import serve
@@ -529,11 +531,13 @@ def serving(args) -> dict:
            "requests": [{"rid": r.rid, "L": r.L, "chi": r.chi, "j2": round(r.j2, 4)}
                         for r in reqs],
            "timing": "wall clock from the first arrival to the last result; every arm starts "
-                     "with empty host plan caches"}
+                     "with empty host plan caches except the two *_warm_caches arms, which "
+                     "run after the arms before them have planned every structure"}
     energies = {}
 
-    def sequential(name, **kw):
-        serve.clear_plan_caches()
+    def sequential(name, warm=False, **kw):
+        if not warm:
+            serve.clear_plan_caches()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         done, en = [], {}
@@ -547,8 +551,9 @@ def serving(args) -> dict:
         out[name] = {"solves_per_s": len(reqs) / wall, "wall_s": wall,
                      "p50_s": float(np.percentile(done, 50)), "p99_s": float(np.percentile(done, 99))}
 
-    def served(name, requests, workers=0, **kw):
-        serve.clear_plan_caches()
+    def served(name, requests, workers=0, warm=False, **kw):
+        if not warm:
+            serve.clear_plan_caches()
         if workers:  # worker processes, started and warmed before the timed run
             srv = serve.ProcessServer(workers=workers, **kw)
         else:
@@ -564,6 +569,9 @@ def serving(args) -> dict:
     sequential("plain_f64_sequential", precision="f64", compiled=False)
     sequential("compiled_f64_sequential", precision="f64")
     served("served_f64", reqs, precision="f64")
+    # a long-running server keeps its host plan caches: the same two arms again, warm
+    served("served_f64_warm_caches", reqs, warm=True, precision="f64")
+    sequential("compiled_f64_sequential_warm_caches", warm=True, precision="f64")
     served("served_3xbf16", reqs, precision="3xbf16")
     w = args.serve_workers
     served(f"served_f64_{w}workers", reqs, workers=w, precision="f64")
@@ -580,7 +588,8 @@ def serving(args) -> dict:
     out["solves_per_s_vs_plain_f64"] = {
         k: out[k]["solves_per_s"] / base for k in
         ("compiled_f64_sequential", "served_f64", "served_3xbf16", f"served_f64_{w}workers",
-         f"served_3xbf16_{w}workers")}
+         f"served_3xbf16_{w}workers", "served_f64_warm_caches",
+         "compiled_f64_sequential_warm_caches")}
     return out
 
 
