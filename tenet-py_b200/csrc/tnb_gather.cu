@@ -37,7 +37,8 @@ gather_kernel(const GatherArgs g) {
 // The per-chunk-row form (tnb_block_gather_direct), the same two builds.
 // (The many-wave build takes kDirectChunksPerCta chunks per CTA: one table wait for both.
 // Measured on the config-3 batch: 1.66 ms of gathers with one chunk per CTA, 1.51 with
-// two, 1.60 with three, 1.68 with four -- fewer resident CTAs per chunk in flight.)
+// two, 1.60 with three, 1.68 with four -- fewer resident CTAs per chunk in flight; two
+// per CTA in the three-CTA-per-SM build (80 registers, no spills) took 1.71.)
 constexpr int kDirectChunksPerCta = 2;
 
 template <int kMinBlocks, int CP>
