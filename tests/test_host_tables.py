@@ -542,3 +542,22 @@ def test_per_chunk_gather_rows_reproduce_the_gather():
             mul, shr = mag & 0xFFFFFFFF, mag >> 32
             for n in (0, 1, d - 1, d, 2 ** 31 - 1, *rng.integers(0, 2 ** 31, 8).tolist()):
                 assert ((n * mul) >> 32) >> shr == n // d
+
+
+def test_division_constants_at_the_extremes():
+    """``_exec.division_constants`` (the per-chunk rows' multiply-shift constants): for
+    extents 2 .. 2^31 - 1, powers of two and their neighbours, floor(n / d) = (n mul) >>
+    (32 + shift) for n from 0 to 2^31 - 1, and 0 for extents of 0 or 1."""
+    rng = np.random.default_rng(12)
+    ds = [2, 3, 5, 7, 25, 1000, 2 ** 31 - 1]
+    ds += [2 ** k + o for k in range(2, 31) for o in (-1, 0, 1)]
+    mags = _exec.division_constants(np.array([0, 1, *ds], dtype=np.int64))
+    assert mags[0] == 0 and mags[1] == 0
+    for d, mag in zip(ds, mags[2:].tolist()):
+        mul, shr = mag & 0xFFFFFFFF, mag >> 32
+        assert 0 < mul < 2 ** 32 and shr == (d - 1).bit_length() - 1
+        ns = [0, 1, d - 1, d, d + 1, 2 ** 31 - 1, (2 ** 31 - 1) // d * d - 1,
+              *rng.integers(0, 2 ** 31, 16).tolist()]
+        for n in ns:
+            if 0 <= n < 2 ** 31:
+                assert ((n * mul) >> 32) >> shr == n // d, (d, n)
